@@ -1,0 +1,325 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 multigrid Poisson solve.
+
+Workload: the 256^3 channel (periodic x and z, tanh-clustered walls in y,
+gamma = 2; seeded divergence RHS plus a sin(2 pi x) cos(pi y) mode), solved
+to 1e-8 relative residual, V(2,2), red-black Gauss-Seidel, coarsest 4^3
+direct.  One step = one complete solve from a zero initial guess.
+
+value      ms per solve of the headline method (FP32 cycles inside FP64
+           iterative refinement), device-resident inputs, CUDA events.
+e2e        the same through the reference-facing plugin call
+           (GPUMG.solve on pinned host arrays: host->device copy of b and
+           device->host copy of x inside the timed region).
+roofline   the level-0 red-black pass of the headline path, achieved
+           algorithmic GB/s against the measured HBM copy bandwidth.
+cpu_baseline / --impl reference
+           the CPU restatement of the reference multigrid (oracle/, "port"),
+           one full solve of the same workload on the host cores.
+
+Multi-GPU: the solve does not shard (one brick on one GPU); with --gpus N
+each rank runs an independent replica and value is the job's time per
+solve (max over ranks of the timed region / (N * steps)).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ms/solve to 1e-8 rel residual @256^3: learned+mixed vs plain GPU MG; HBM GB/s"
+SOLVER_KEYS = {"relTol": 1e-8, "tolerance": 0, "cycleType": "V", "nSweepsPre": 2, "nSweepsPost": 2,
+               "coarseLevel": 1, "smoother": "rbgs"}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi clock and throttle samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx = float(parts[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference(N: int, steps: int | None = None, warmup: int = 0):
+    """Time the oracle (CPU restatement of the reference MG, all host threads)
+    on the benchmark workload: full solves from a zero guess."""
+    from briscola_b200 import workloads
+    from oracle.pyoracle import Oracle
+
+    mesh, b, _ = workloads.channel(N)
+    br = mesh.bricks[0]
+    threads = os.cpu_count() or 1
+    o = Oracle(br.points, periodic=br.periodic, nthreads=threads)
+    bb = b.reshape(br.N)
+    kw = dict(rel_tol=1e-8, abs_tol=0.0, n_pre=2, n_post=2, cycle_type="V", coarse_level=1)
+    times, cycles = [], 0
+    for s in range(warmup + (steps or 1)):
+        t = time.perf_counter()
+        x, rep, hist, rc = o.solve(bb, **kw)
+        dt = (time.perf_counter() - t) * 1e3
+        cycles = rep.iterations
+        if s >= warmup:
+            times.append(dt)
+    return times, cycles, threads
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    times, cycles, threads = cpu_reference(args.size, steps=args.steps, warmup=args.warmup)
+    v = sum(times) / len(times)
+    sample = f"{args.steps} full solves of the {args.size}^3 channel, {cycles} V(2,2) cycles each"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "ms/solve",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v, 3),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": workload_config(args),
+        "cpu_baseline": {"value": round(v, 3), "unit": "ms/solve", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": round(v, 3), "unit": "ms/solve", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(args):
+    return {"workload": f"channel {args.size}^3 (periodic x,z; tanh gamma=2 walls in y), seeded "
+                        "div(N(0,1) velocity) + sin(2 pi x)cos(pi y) RHS, zero mean",
+            "grid": [args.size] * 3, "solver": "V(2,2) RBGS, linear transfers, coarsest 4^3 direct",
+            "stop": "1e-8 relative residual (FP64-checked)", "precision": "fp32 cycles + fp64 refinement",
+            "l2_flush": "inputs and hierarchy larger than L2 (x, b 134 MB each at 256^3)",
+            "parallelism": "replicas" if args.gpus > 1 else "single GPU"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    import briscola_b200 as bb
+    from briscola_b200 import workloads
+
+    mesh, b, _ = workloads.channel(args.size)
+    n = b.size
+    stream = torch.cuda.current_stream()
+    ctx = {}
+    for prec in ("mixed", "fp64"):
+        ctx[prec] = bb.Context(mesh, bb.make_options(dict(SOLVER_KEYS, precision=prec, device=local)))
+        ctx[prec].set_stream(stream.cuda_stream)
+    b_d = torch.from_numpy(b).to(f"cuda:{local}")
+    x_d = torch.zeros_like(b_d)
+
+    def solve(prec):
+        rep = ctx[prec].solve(b_d, x_d, zero_guess=True)
+        if rep.status != 0:
+            raise RuntimeError(f"solve failed: status {rep.status}")
+        return rep
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(prec, steps):
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        launches, cycles = 0, []
+        e0.record(stream)
+        for _ in range(steps):
+            rep = solve(prec)
+            launches += rep.kernel_launches
+            cycles.append(rep.cycles)
+        e1.record(stream)
+        barrier()
+        ms = e0.elapsed_time(e1)
+        if dist is not None:
+            t = torch.tensor([ms], device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, launches, cycles
+
+    for _ in range(args.warmup):
+        solve("mixed")
+        solve("fp64")
+    clk = Clocks(local)
+    clk.start()
+    ms_mixed, launches, cyc_mixed = timed("mixed", args.steps)
+    clocks = clk.stop()
+    ms_fp64, _, cyc_fp64 = timed("fp64", args.steps)
+    rep_mixed = solve("mixed")
+    per_solve = ms_mixed / (args.steps * world)
+
+    # ---- roofline of the dominant kernel: level-0 red-black pass (FP32) ----
+    c = ctx["mixed"]
+    reps = 50
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    pass_ms = []
+    for r in range(reps):
+        e0.record(stream)
+        c.colour_pass(0, r & 1, precision=1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        pass_ms.append(e0.elapsed_time(e1))
+    t_pass = statistics.median(pass_ms) * 1e-3
+    cells = n
+    alg_bytes = 6.0 * cells  # half of a full FP32 sweep: read x, read b, write x = 12 B/cell
+    hbm, peak_kind = peaks()
+    achieved = alg_bytes / t_pass / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get("colour_pass_fp32_256", None)
+
+    # ---- end to end through the plugin call with host buffers ----
+    d = bb.Dictionary(dict(SOLVER_KEYS, type="GPUMG", precision="mixed", device=local))
+    s = bb.solver.New(d, mesh)
+    s.context.set_stream(stream.cuda_stream)
+    bh = torch.from_numpy(b).pin_memory()
+    xh = torch.zeros(n, dtype=torch.float64).pin_memory()
+    sys_ = bb.LinearSystem(mesh, xh.numpy(), bh.numpy())
+    import contextlib
+    import io
+
+    with contextlib.redirect_stdout(io.StringIO()):
+        for _ in range(2):
+            s.solve(sys_)
+        barrier()
+        e0.record(stream)
+        for _ in range(args.steps):
+            s.solve(sys_)
+        e1.record(stream)
+        barrier()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item()) / world
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        times, cycles, threads = cpu_reference(args.size, steps=1)
+        cpu = {"value": round(times[0], 1), "unit": "ms/solve", "cores": threads, "kind": "port",
+               "sample": f"one full solve of the same {args.size}^3 workload by the CPU restatement "
+                         f"of the reference MG ({cycles} V(2,2) cycles, {threads} threads)"}
+
+    # algorithmic bytes of one FP64 V(2,2) cycle: 164.6 B per finest cell
+    hbm_gbs_fp64 = 164.6 * cells * statistics.mean(cyc_fp64) / (ms_fp64 / args.steps * 1e-3) / 1e9
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(per_solve, 4), "unit": "ms/solve", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_mixed / args.steps, 4),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic", "config": workload_config(args),
+            "method": "mixed (FP32 V-cycles inside FP64 refinement); learned guess not yet in this line",
+            "plain_fp64_ms_per_solve": round(ms_fp64 / (args.steps * world), 4),
+            "speedup_vs_plain_fp64": round(ms_fp64 / ms_mixed, 3),
+            "cycles_mixed": cyc_mixed[0], "cycles_fp64": cyc_fp64[0],
+            "rel_residual": rep_mixed.rel_residual,
+            "hbm_gbs_fp64_cycle_algorithmic": round(hbm_gbs_fp64, 1),
+            "roofline": {"bound": "hbm", "kernel": "k_colour_pass<float> level 0",
+                         "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                         "frac": round(achieved / hbm, 4), "peak_kind": peak_kind,
+                         "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,
+                         "launch_us": round(t_pass * 1e6, 2)},
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(e2e_ms, 4), "unit": "ms/solve", "h2d_bytes_per_step": 8 * n,
+                    "d2h_bytes_per_step": 8 * n},
+            "gpu_launches": launches, "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    for cc in ctx.values():
+        cc.close()
+    s.context.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

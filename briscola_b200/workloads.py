@@ -1,0 +1,113 @@
+"""Seeded synthetic workloads of the benchmark configurations.
+
+No dataset is involved: every right-hand side is generated from a seed.
+
+* ``cavity(N)``  -- single brick N^3 on the unit cube, all walls (closed
+  cavity), uniform spacing; RHS = discrete divergence of an N(0,1) face
+  velocity field (wall-normal faces zero), volume-weighted zero mean.
+* ``channel(N)`` -- N^3 on the unit cube, periodic x and z, walls in y with
+  tanh clustering (gamma = 2); RHS = divergence of N(0,1) face velocities
+  plus sin(2 pi x) cos(pi y) at the cell centres, zero mean.
+* ``sphere(N)``  -- all walls, density 1 outside / 1000 inside a sphere of
+  radius 0.2 at a seeded centre in [0.3,0.7]^3, VOF fraction from the signed
+  distance ramped over 2 cells, face coefficient lambda = mean of 1/rho of the
+  two cells; N(0,1) zero-mean RHS.
+
+Each returns (mesh, b, lam) with b the system right-hand side
+b_sys = -V f of the reference (linearSystem.C:547-556) as a flat float64
+array and lam None or the three face arrays.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .mesh import NEUMANN, PERIODIC, Brick, Mesh, tanh_points, uniform_points
+
+
+def face_divergence(brick: Brick, ux, uy, uz) -> np.ndarray:
+    """Net outward flux of face velocities per cell (= V * div u)."""
+    hx, hy, hz = (brick.cell_sizes(d) for d in range(3))
+    ax = hy[:, None] * hz[None, :]
+    ay = hx[:, None] * hz[None, :]
+    az = hx[:, None] * hy[None, :]
+    return ((ux[1:] - ux[:-1]) * ax[None] + (uy[:, 1:] - uy[:, :-1]) * ay[:, None, :]
+            + (uz[:, :, 1:] - uz[:, :, :-1]) * az[:, :, None])
+
+
+def random_face_velocity(brick: Brick, rng: np.random.Generator):
+    n0, n1, n2 = brick.N
+    per = brick.periodic
+    u = []
+    for d, shape in enumerate([(n0 + 1, n1, n2), (n0, n1 + 1, n2), (n0, n1, n2 + 1)]):
+        a = rng.standard_normal(shape)
+        sl_lo = [slice(None)] * 3
+        sl_hi = [slice(None)] * 3
+        sl_lo[d] = 0
+        sl_hi[d] = -1
+        if per[d]:
+            a[tuple(sl_hi)] = a[tuple(sl_lo)]  # the periodic face is one face
+        else:
+            a[tuple(sl_lo)] = 0.0
+            a[tuple(sl_hi)] = 0.0
+        u.append(a)
+    return u
+
+
+def zero_mean(f: np.ndarray, V: np.ndarray) -> np.ndarray:
+    return f - (V * f).sum() / V.sum()
+
+
+def cavity(N: int = 64, seed: int = 1000):
+    br = Brick([uniform_points(N)] * 3, (NEUMANN,) * 6)
+    rng = np.random.default_rng(seed)
+    V = br.cell_volumes()
+    flux = face_divergence(br, *random_face_velocity(br, rng))
+    f = zero_mean(flux / V, V)
+    return Mesh([br]), np.ascontiguousarray((-V * f).ravel()), None
+
+
+def channel(N: int = 256, gamma: float = 2.0, seed: int = 2000):
+    pts = [uniform_points(N), tanh_points(N, gamma), uniform_points(N)]
+    br = Brick(pts, (PERIODIC, PERIODIC, NEUMANN, NEUMANN, PERIODIC, PERIODIC))
+    rng = np.random.default_rng(seed)
+    V = br.cell_volumes()
+    flux = face_divergence(br, *random_face_velocity(br, rng))
+    xc = br.cell_centres(0)[:, None, None]
+    yc = br.cell_centres(1)[None, :, None]
+    f = flux / V + np.sin(2 * np.pi * xc) * np.cos(np.pi * yc) * np.ones((1, 1, N))
+    f = zero_mean(f, V)
+    return Mesh([br]), np.ascontiguousarray((-V * f).ravel()), None
+
+
+def sphere_lambda(brick: Brick, centre, radius=0.2, rho_in=1000.0, rho_out=1.0, ramp_cells=2.0):
+    xc, yc, zc = (brick.cell_centres(d) for d in range(3))
+    h = min(float(np.min(brick.cell_sizes(d))) for d in range(3))
+    dist = np.sqrt((xc[:, None, None] - centre[0]) ** 2 + (yc[None, :, None] - centre[1]) ** 2
+                   + (zc[None, None, :] - centre[2]) ** 2) - radius
+    alpha = np.clip(0.5 - dist / (ramp_cells * h), 0.0, 1.0)
+    rho = alpha * rho_in + (1.0 - alpha) * rho_out
+    inv = 1.0 / rho
+    n0, n1, n2 = brick.N
+    lx = np.empty((n0 + 1, n1, n2))
+    ly = np.empty((n0, n1 + 1, n2))
+    lz = np.empty((n0, n1, n2 + 1))
+    lx[1:-1] = 0.5 * (inv[1:] + inv[:-1])
+    lx[0], lx[-1] = inv[0], inv[-1]
+    ly[:, 1:-1] = 0.5 * (inv[:, 1:] + inv[:, :-1])
+    ly[:, 0], ly[:, -1] = inv[:, 0], inv[:, -1]
+    lz[:, :, 1:-1] = 0.5 * (inv[:, :, 1:] + inv[:, :, :-1])
+    lz[:, :, 0], lz[:, :, -1] = inv[:, :, 0], inv[:, :, -1]
+    return [np.ascontiguousarray(a) for a in (lx, ly, lz)]
+
+
+def sphere(N: int = 256, seed: int = 4000):
+    br = Brick([uniform_points(N)] * 3, (NEUMANN,) * 6)
+    rng = np.random.default_rng(seed)
+    centre = rng.uniform(0.3, 0.7, size=3)
+    lam = sphere_lambda(br, centre)
+    V = br.cell_volumes()
+    f = zero_mean(rng.standard_normal(br.N), V)
+    return Mesh([br]), np.ascontiguousarray((-V * f).ravel()), lam
+
+
+CONFIGS = {"cavity": cavity, "channel": channel, "sphere": sphere}

@@ -1,0 +1,162 @@
+/*
+ * bmg.h -- C ABI of the B200 geometric-multigrid Poisson solver.
+ *
+ * This is the boundary a Briscola linear-solver plugin (type "GPUMG") binds.
+ * It replaces the reference's multigrid solve behind
+ *   solver<SType,Type,MeshType>::solve(linearSystem&, bool constMatrix)
+ *       src/briscolaFiniteVolume/solvers/solver/solver.H:280-284
+ * selected by name through the runtime table
+ *   src/briscolaFiniteVolume/solvers/solver/solver.H:240-251,
+ *   src/briscolaFiniteVolume/solvers/solver/solver.C:130-157,
+ *   registered as in src/briscolaFiniteVolume/solvers/MG/MGSolvers.C:13-21.
+ *
+ * Plain pointers and sizes only.  Every function returns a bmg_status code
+ * and never throws.  One context owns its device memory and serves one
+ * stream; a context is not thread-safe, distinct contexts are independent.
+ *
+ * Arrays: per brick, interior cells only, k fastest:
+ *   lin(i,j,k) = (i*Ny + j)*Nz + k     (src/briscolaCore/include/utils.H:569)
+ * and bricks concatenated in brick order.  The system follows the
+ * reference's sign convention: A is negative semi-definite (off-diagonal
+ * +area*delta*lambda, centre minus their sum; linearGaussLaplacianScheme.C
+ * :59-94), and b is the system right-hand side (b_sys = -V f for the
+ * Poisson source f, linearSystem.C:547-556).
+ */
+#ifndef BMG_H
+#define BMG_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum bmg_status {
+    BMG_OK = 0,
+    BMG_NOT_CONVERGED = 1, /* maxIter reached (the reference prints stats and returns, MG.C:246-253) */
+    BMG_NAN_DETECTED = 2,  /* a residual norm became NaN or Inf                                     */
+    BMG_BAD_ARG = 3,       /* invalid argument (the reference aborts with FatalError)                */
+    BMG_CUDA_ERROR = 4,    /* a CUDA runtime call failed; see bmg_last_error()                       */
+    BMG_TIMEOUT = 5,       /* the solve exceeded its wall-clock budget (bmg_options.timeout_ms)      */
+    BMG_NO_DEVICE = 6,     /* no usable sm_100 device                                                */
+    BMG_UNSUPPORTED = 7    /* a valid option this build does not implement                           */
+} bmg_status;
+
+/* Boundary condition of one outer brick face. */
+enum { BMG_BC_NEUMANN = 0, BMG_BC_PERIODIC = 1 };
+
+/* Cycle types (MG.H:106-124) and smoothers (MG.C:313-373). */
+enum { BMG_CYCLE_V = 0, BMG_CYCLE_W = 1, BMG_CYCLE_F = 2 };
+enum { BMG_SMOOTHER_RBGS = 0, BMG_SMOOTHER_JACOBI = 1 };
+/* Arithmetic of the cycles: plain FP64, or FP32 cycles inside FP64
+ * iterative refinement (FP64 residual, update, coarse solve, mean). */
+enum { BMG_PRECISION_FP64 = 0, BMG_PRECISION_MIXED = 1 };
+
+/* bmg_solve flags */
+enum {
+    BMG_DEVICE_PTRS = 1, /* b and x are device pointers on the context's device */
+    BMG_ZERO_GUESS = 2   /* ignore the incoming x and start from zero           */
+};
+
+typedef struct bmg_brick {
+    int n[3];                 /* cells along x, y, z                                   */
+    const double* points[3];  /* n[d]+1 vertex coordinates along axis d (host memory)  */
+    int bc[6];                /* x-lo, x-hi, y-lo, y-hi, z-lo, z-hi: BMG_BC_*          */
+    int origin[3];            /* cell offset in the global lattice (multi-brick)       */
+} bmg_brick;
+
+typedef struct bmg_mesh_desc {
+    int n_bricks;
+    const bmg_brick* bricks;
+} bmg_mesh_desc;
+
+/* Dictionary keys of the reference MG (MG.C:257-305, solver.C:115-123) plus
+ * the B200-specific ones. */
+typedef struct bmg_options {
+    double rel_tol;     /* relTol                                              */
+    double abs_tol;     /* tolerance                                           */
+    int min_iter;       /* minIter      (0)                                    */
+    int max_iter;       /* maxIter      (999)                                  */
+    int n_pre;          /* nSweepsPre   (0)                                    */
+    int n_post;         /* nSweepsPost  (2)                                    */
+    int cycle_type;     /* cycleType    (F)                                    */
+    int coarse_level;   /* coarseLevel  (0), counted from the coarsest level   */
+    int smoother;       /* smoother     (rbgs)                                 */
+    int precision;      /* precision    (fp64)                                 */
+    int use_graph;      /* graph        (1): whole solve as one CUDA graph     */
+    int remove_mean;    /* subtract the volume-weighted mean of x (singular)   */
+    int device;         /* CUDA device ordinal                                 */
+    double timeout_ms;  /* wall-clock budget per solve, <= 0: none             */
+} bmg_options;
+
+typedef struct bmg_report {
+    int status;
+    int cycles;               /* V/W/F cycles performed (inner cycles when mixed) */
+    int outer_iterations;     /* FP64 refinement steps (mixed), else = cycles     */
+    double initial_residual;  /* Briscola-normalised (solver.C:13-61)             */
+    double final_residual;    /* Briscola-normalised                              */
+    double rel_residual;      /* ||b - A x||_2 / ||b - A x0||_2                    */
+    double final_l2;          /* ||b - A x||_2                                    */
+    double norm_factor;       /* normFactor of solver.C:13-61                     */
+    float ms;                 /* device time of the solve (CUDA events)           */
+    long kernel_launches;     /* kernels this solve launched (graph nodes count)  */
+} bmg_report;
+
+int bmg_default_options(bmg_options* opts);
+
+/* Build the level hierarchy and device buffers for a mesh.  Replaces the MG
+ * constructor (MG.C:257-399) and the per-solve setup of MG.C:431-459. */
+int bmg_create(struct bmg_ctx** ctx, const bmg_mesh_desc* mesh, const bmg_options* opts);
+void bmg_destroy(struct bmg_ctx* ctx);
+
+/* Variable coefficient lambda on the level-0 faces (host arrays), one per
+ * face direction with shapes (Nx+1,Ny,Nz), (Nx,Ny+1,Nz), (Nx,Ny,Nz+1) per
+ * brick, concatenated.  Restricted to coarse levels area-weighted
+ * (areaWeightedFaceRestrictionScheme.C:19-57).  NULLs: constant coefficient. */
+int bmg_set_coefficients(struct bmg_ctx* ctx, const double* lambda_x, const double* lambda_y,
+                         const double* lambda_z);
+
+int bmg_set_stream(struct bmg_ctx* ctx, void* cuda_stream);
+int bmg_set_options(struct bmg_ctx* ctx, const bmg_options* opts);
+
+/* Solve A x = b.  Replaces MG::solve (MG.C:402-483).  x holds the initial
+ * guess on entry unless BMG_ZERO_GUESS, and the solution on return. */
+int bmg_solve(struct bmg_ctx* ctx, const double* b, double* x, int flags, bmg_report* report);
+
+/* Number of cells of all bricks on level 0 (length of b and x). */
+long bmg_num_cells(const struct bmg_ctx* ctx);
+int bmg_num_levels(const struct bmg_ctx* ctx);
+int bmg_level_shape(const struct bmg_ctx* ctx, int level, int brick, int n[3]);
+
+const char* bmg_status_string(int status);
+const char* bmg_last_error(const struct bmg_ctx* ctx);
+
+/* ---- Building blocks, for per-kernel parity tests --------------------------
+ * They act on the context's level buffers.  Fields: 0 = x, 1 = b (both as
+ * the reference's unscaled values), interior cells of every brick in brick
+ * order.  The precision argument selects the FP64 (0) or FP32 (1) buffers. */
+int bmg_level_upload(struct bmg_ctx* ctx, int level, int field, int precision, const double* host);
+int bmg_level_download(struct bmg_ctx* ctx, int level, int field, int precision, double* host);
+/* one red-black colour pass (colour 0: (i+j+k) even) on level l:
+ * replaces one pass of rbgsSmoother.C:65-183 */
+int bmg_op_colour_pass(struct bmg_ctx* ctx, int level, int colour, int precision);
+/* n_sweeps sweeps of the configured smoother on level l */
+int bmg_op_smooth(struct bmg_ctx* ctx, int level, int n_sweeps, int precision);
+/* r = b - A x on level l, written into host r (unscaled); replaces
+ * linearSystemResidual.C:280-332 */
+int bmg_op_residual(struct bmg_ctx* ctx, int level, int precision, double* host_r);
+/* b(l+1) = restriction of b(l) - A x(l) (fused residual + restriction,
+ * linearRestrictionScheme.C:103-159 with scale); x(l+1) = 0 */
+int bmg_op_residual_restrict(struct bmg_ctx* ctx, int level, int precision);
+/* x(l) += prolongation of x(l+1) (linearProlongationScheme.C:112-147) */
+int bmg_op_prolong_correct(struct bmg_ctx* ctx, int level, int precision);
+/* direct solve on the coarse solve level (APLU.C:91-128) */
+int bmg_op_coarse_solve(struct bmg_ctx* ctx, int precision);
+/* the configured coarse solve level index */
+int bmg_coarse_level_index(const struct bmg_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BMG_H */
