@@ -71,26 +71,37 @@ class Clocks:
         except OSError:
             self.proc = None
 
+    def _lines(self):
+        with open(self.path) as f:
+            return f.readlines()
+
+    def mark(self) -> None:
+        """Start of the timed region: later samples count."""
+        if self.proc is not None:
+            time.sleep(1.0)  # nvidia-smi takes a moment to begin sampling
+            self.first = len(self._lines())
+
     def stop(self) -> dict:
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
         self.proc.terminate()
         self.proc.wait()
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        with open(self.path) as f:
-            for line in f:
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) < 9:
-                    continue
-                try:
-                    sm.append(float(parts[1]))
-                    mx = float(parts[2])
-                except ValueError:
-                    continue
-                for n, v in zip(names, parts[5:9]):
-                    if v.lower().startswith("active"):
-                        reasons.add(n)
+        lines = self._lines()[getattr(self, "first", 0):]
+        for line in lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
         os.unlink(self.path)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
                 "reasons": sorted(reasons), "samples": len(sm)}
@@ -221,11 +232,12 @@ def main():
             ms = float(t.item())
         return ms, launches, cycles
 
+    clk = Clocks(local)
+    clk.start()
     for _ in range(args.warmup):
         solve("mixed")
         solve("fp64")
-    clk = Clocks(local)
-    clk.start()
+    clk.mark()
     ms_mixed, launches, cyc_mixed = timed("mixed", args.steps)
     clocks = clk.stop()
     ms_fp64, _, cyc_fp64 = timed("fp64", args.steps)
@@ -262,7 +274,7 @@ def main():
     s.context.set_stream(stream.cuda_stream)
     bh = torch.from_numpy(b).pin_memory()
     xh = torch.zeros(n, dtype=torch.float64).pin_memory()
-    sys_ = bb.LinearSystem(mesh, xh.numpy(), bh.numpy())
+    sys_ = bb.LinearSystem(mesh, xh.numpy(), bh.numpy(), zero_guess=True)
     import contextlib
     import io
 

@@ -53,29 +53,35 @@ __device__ __forceinline__ void stencil(const T* x, long c, long si, long sj, co
 // Store an interior value and its periodic ghost images (faces, edges and
 // corners), replacing the reference's per-sweep periodic ghost copy
 // (periodicBoundaryCondition.C:53-92).
+// Per axis a cell has up to two images: in the upper ghost layer (cell 0)
+// and in the lower one (cell n-1); both when n == 1.  All 26 combinations
+// are unrolled into predicated stores, so nothing lives in local memory.
 template <typename T>
 __device__ __forceinline__ void store_x(const LevelView<T>& L, long c, int i, int j, int k, T v) {
     L.x[c] = v;
-    if (!(L.per0 | L.per1 | L.per2)) return;
-    long o0[3] = {0, 0, 0}, o1[3] = {0, 0, 0}, o2[3] = {0, 0, 0};
-    int m0 = 1, m1 = 1, m2 = 1;
-    if (L.per0) {
-        if (i == 0) o0[m0++] = (long)L.n0 * L.si;
-        if (i == L.n0 - 1) o0[m0++] = -(long)L.n0 * L.si;
+    const long up0 = (L.per0 && i == 0) ? (long)L.n0 * L.si : 0;
+    const long dn0 = (L.per0 && i == L.n0 - 1) ? -(long)L.n0 * L.si : 0;
+    const long up1 = (L.per1 && j == 0) ? (long)L.n1 * L.sj : 0;
+    const long dn1 = (L.per1 && j == L.n1 - 1) ? -(long)L.n1 * L.sj : 0;
+    const long up2 = (L.per2 && k == 0) ? (long)L.n2 : 0;
+    const long dn2 = (L.per2 && k == L.n2 - 1) ? -(long)L.n2 : 0;
+    if (!(up0 | dn0 | up1 | dn1 | up2 | dn2)) return;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const long o0 = a == 0 ? 0 : a == 1 ? up0 : dn0;
+        if (a && !o0) continue;
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+            const long o1 = e == 0 ? 0 : e == 1 ? up1 : dn1;
+            if (e && !o1) continue;
+#pragma unroll
+            for (int f = 0; f < 3; ++f) {
+                const long o2 = f == 0 ? 0 : f == 1 ? up2 : dn2;
+                if (f && !o2) continue;
+                if (a | e | f) L.x[c + o0 + o1 + o2] = v;
+            }
+        }
     }
-    if (L.per1) {
-        if (j == 0) o1[m1++] = (long)L.n1 * L.sj;
-        if (j == L.n1 - 1) o1[m1++] = -(long)L.n1 * L.sj;
-    }
-    if (L.per2) {
-        if (k == 0) o2[m2++] = (long)L.n2;
-        if (k == L.n2 - 1) o2[m2++] = -(long)L.n2;
-    }
-    if (m0 == 1 && m1 == 1 && m2 == 1) return;
-    for (int a = 0; a < m0; ++a)
-        for (int b = 0; b < m1; ++b)
-            for (int e = 0; e < m2; ++e)
-                if (a | b | e) L.x[c + o0[a] + o1[b] + o2[e]] = v;
 }
 
 // ---------------------------------------------------------------------------

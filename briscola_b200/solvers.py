@@ -117,11 +117,13 @@ class LinearSystem:
     x and b are float64 arrays of the mesh's cell count (numpy on the host, or
     torch CUDA tensors for device-resident solves)."""
 
-    def __init__(self, mesh: Mesh, x, b, lam=None):
+    def __init__(self, mesh: Mesh, x, b, lam=None, zero_guess: bool = False):
         self.mesh = mesh
         self.x = x
         self.b = b
         self.lam = lam
+        # start from x = 0 instead of the incoming x (no host->device copy of x)
+        self.zero_guess = zero_guess
 
     @classmethod
     def poisson(cls, mesh: Mesh, x, source: np.ndarray, lam=None) -> "LinearSystem":
@@ -362,7 +364,7 @@ class GPUMG(solver):
             if sys.lam is not None or self._lam_id is not None:
                 self.context.set_coefficients(sys.lam)
             self._lam_id = lam_key
-        rep = self.context.solve(sys.b, sys.x)
+        rep = self.context.solve(sys.b, sys.x, zero_guess=sys.zero_guess)
         self.last_report = rep
         print(f"{self.typeName}: Solving for colocated x, initial residual = {rep.initial_residual:g}, "
               f"final residual = {rep.final_residual:g}, nIter = {rep.cycles}")

@@ -35,7 +35,7 @@ def oracle_for(br: Brick, lam=None):
 
 
 MESHES = {
-    "uniform_walls": lambda: Brick([uniform_points(16), uniform_points(12), uniform_points(10)]),
+    "uniform_walls": lambda: Brick([uniform_points(16), uniform_points(12), uniform_points(24)]),
     "graded_walls": lambda: Brick([geometric_points(16, 2.0), uniform_points(8), geometric_points(12, 0.5)]),
     "channel": lambda: Brick([uniform_points(16), tanh_points(16, 2.0), uniform_points(8)],
                              (PERIODIC, PERIODIC, NEUMANN, NEUMANN, PERIODIC, PERIODIC)),
@@ -133,7 +133,9 @@ def test_kernel_parity_fp32(native, name):
     o = oracle_for(br)
     o.assemble(**V22)
     rng = np.random.default_rng(11)
-    for l in range(c.num_levels - 1):
+    # the coarse-solve level carries the singularity pin in the oracle's
+    # matrix (solver.C:201-231); smoothers never run there
+    for l in range(c.coarse_level_index):
         x = rng.standard_normal(c.shape(l))
         b = rng.standard_normal(c.shape(l))
         c.upload(l, "x", x, precision=1)
@@ -263,13 +265,20 @@ def test_status_codes(native):
 
 
 def test_initial_guess_is_used(native):
+    """A warm start is judged like the reference judges it: the relative
+    criterion is relative to the initial residual (solver.C:64-95), so a
+    converged guess only stops at once through the absolute tolerance."""
     mesh, b, _ = workloads.cavity(32, seed=4)
-    c = ctx_for(mesh, relTol=1e-12)
+    c = ctx_for(mesh, relTol=1e-12, tolerance=1e-11)
     x = np.zeros_like(b)
     rep0 = c.solve(b, x, zero_guess=True)
-    rep1 = c.solve(b, x)  # warm start from the converged solution
-    assert rep1.cycles <= 1
-    assert rep0.cycles > 3
+    rep1 = c.solve(b, x)
+    assert rep0.cycles > 3 and rep0.status == 0
+    assert rep1.cycles == 0 and rep1.status == 0
+    # relative criterion only: a converged guess cannot improve by relTol
+    c2 = ctx_for(mesh, relTol=1e-8, maxIter=5)
+    rep2 = c2.solve(b, x)
+    assert rep2.status == NA.NOT_CONVERGED and rep2.cycles == 5
 
 
 def test_semicoarsening_shapes(native):
