@@ -27,6 +27,7 @@ EXPORTED = (
     "bmg_status_string", "bmg_last_error", "bmg_level_upload", "bmg_level_download",
     "bmg_op_colour_pass", "bmg_op_smooth", "bmg_op_residual", "bmg_op_residual_restrict",
     "bmg_op_prolong_correct", "bmg_op_coarse_solve", "bmg_coarse_level_index",
+    "bmg_residual_norm_noalloc",
 )
 
 
@@ -120,6 +121,7 @@ def load(path: str = LIB_PATH):
     L.bmg_op_prolong_correct.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     L.bmg_op_coarse_solve.argtypes = [vp, ctypes.c_int]
     L.bmg_coarse_level_index.argtypes = [vp]
+    L.bmg_residual_norm_noalloc.argtypes = [vp, vp, ip, vp, vp, vp, ip, vp, vp]
     _lib = L
     return L
 

@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_lib", "libbmg.so")
-SOURCES = ["bmg_host.cu", "bmg_kernels.cu"]
+SOURCES = ["bmg_host.cu", "bmg_kernels.cu", "bmg_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -155,6 +155,35 @@ int bmg_op_coarse_solve(struct bmg_ctx* ctx, int precision);
 /* the configured coarse solve level index */
 int bmg_coarse_level_index(const struct bmg_ctx* ctx);
 
+/* ---- Residual norm without any device allocation ---------------------------
+ * No counterpart in the reference: an addition for callers that must not
+ * call cudaMalloc when they want a residual -- an application whose device
+ * memory belongs to its own pool, a loop that cannot take the device-wide
+ * synchronisation an allocation may bring, or a failure path running after
+ * device memory ran out.
+ *
+ * *norm_out = ||b - A x||_2 for one brick with the solver's level-0 operator
+ * (constant coefficient).  x, b: device arrays of interior cells, k fastest;
+ * points_*: device arrays of n[d]+1 vertex coordinates; bc: host array of
+ * BMG_BC_* per face; norm_out: one device double.  Work is queued on
+ * `stream` (a cudaStream_t, NULL for the default stream); the result is
+ * ready once the stream has reached that point.
+ *
+ * Scratch: a file-scope static device array of BMG_NOALLOC_MAX_ROWS doubles
+ * (512 KB on every GPU that loads the library, until exit), one partial sum
+ * per (i, j) row: n[0]*n[1] above the limit is rejected with BMG_BAD_ARG and
+ * a message on stderr.  Every call overwrites the partials it reads, so no
+ * state carries over, but all calls on a device share the array: calls that
+ * overlap on the GPU (different streams, or threads without ordering) race.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture. */
+#define BMG_NOALLOC_MAX_ROWS 65536
+int bmg_residual_norm_noalloc(const double* x, const double* b, const int n[3],
+                              const double* points_x, const double* points_y,
+                              const double* points_z, const int bc[6], double* norm_out,
+                              void* stream);
+
 #ifdef __cplusplus
 }
 #endif
