@@ -244,29 +244,37 @@ def main():
     rep_mixed = solve("mixed")
     per_solve = ms_mixed / (args.steps * world)
 
-    # ---- roofline of the dominant kernel: level-0 red-black pass (FP32) ----
+    # ---- roofline of the dominant kernel: the level-0 fused smoothing step
+    # (FP32, V(2,2): two sweeps = 5 colour stages in one launch) ----
     c = ctx["mixed"]
-    reps = 50
+    reps = 30
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     pass_ms = []
     for r in range(reps):
         e0.record(stream)
-        c.colour_pass(0, r & 1, precision=1)
+        c.smooth(0, SOLVER_KEYS["nSweepsPost"], precision=1)
         e1.record(stream)
         torch.cuda.synchronize()
         pass_ms.append(e0.elapsed_time(e1))
-    t_pass = statistics.median(pass_ms) * 1e-3
+    # the step's colour stages (5 for two sweeps) go in launches of S stages
+    stages_per_launch, chunk = c.tuning(0, 1)
+    n_stages = 5 if SOLVER_KEYS["nSweepsPost"] == 2 else 3 * SOLVER_KEYS["nSweepsPost"]
+    launches_per_step = -(-n_stages // max(stages_per_launch, 1))
+    t_pass = statistics.median(pass_ms) * 1e-3 / launches_per_step
     cells = n
-    alg_bytes = 6.0 * cells  # half of a full FP32 sweep: read x, read b, write x = 12 B/cell
+    # FP32 algorithmic bytes per launch: a single colour pass needs half a
+    # sweep's read x, read b, write x (6 B/cell); a fused launch of two or
+    # more stages needs a whole one (12 B/cell)
+    alg_bytes = (12.0 if stages_per_launch >= 2 else 6.0) * cells
     hbm, peak_kind = peaks()
     achieved = alg_bytes / t_pass / 1e9
     traffic = None
     tp = os.path.join(ROOT, "profiles", "roofline_traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
-            traffic = json.load(f).get("colour_pass_fp32_256", None)
+            traffic = json.load(f).get("smooth_fused_fp32_s5_256", None)
 
     # ---- end to end through the plugin call with host buffers ----
     d = bb.Dictionary(dict(SOLVER_KEYS, type="GPUMG", precision="mixed", device=local))
@@ -315,7 +323,12 @@ def main():
             "cycles_mixed": cyc_mixed[0], "cycles_fp64": cyc_fp64[0],
             "rel_residual": rep_mixed.rel_residual,
             "hbm_gbs_fp64_cycle_algorithmic": round(hbm_gbs_fp64, 1),
-            "roofline": {"bound": "hbm", "kernel": "k_colour_pass<float> level 0",
+            "roofline": {"bound": "hbm",
+                         "kernel": (f"k_smooth_fused<float,S={stages_per_launch}> level 0 "
+                                    f"({launches_per_step} launches per 2-sweep step, {chunk}-plane chunks)"
+                                    if stages_per_launch else
+                                    f"k_colour_pass<float> level 0 ({launches_per_step} passes per "
+                                    "2-sweep step; autotuner's choice)"),
                          "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                          "frac": round(achieved / hbm, 4), "peak_kind": peak_kind,
                          "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,

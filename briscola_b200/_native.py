@@ -27,7 +27,7 @@ EXPORTED = (
     "bmg_status_string", "bmg_last_error", "bmg_level_upload", "bmg_level_download",
     "bmg_op_colour_pass", "bmg_op_smooth", "bmg_op_residual", "bmg_op_residual_restrict",
     "bmg_op_prolong_correct", "bmg_op_coarse_solve", "bmg_coarse_level_index",
-    "bmg_residual_norm_noalloc",
+    "bmg_residual_norm_noalloc", "bmg_level_tuning",
 )
 
 
@@ -58,6 +58,8 @@ class Options(ctypes.Structure):
         ("precision", ctypes.c_int),
         ("use_graph", ctypes.c_int),
         ("remove_mean", ctypes.c_int),
+        ("fused", ctypes.c_int),
+        ("autotune", ctypes.c_int),
         ("device", ctypes.c_int),
         ("timeout_ms", ctypes.c_double),
     ]
@@ -122,6 +124,7 @@ def load(path: str = LIB_PATH):
     L.bmg_op_coarse_solve.argtypes = [vp, ctypes.c_int]
     L.bmg_coarse_level_index.argtypes = [vp]
     L.bmg_residual_norm_noalloc.argtypes = [vp, vp, ip, vp, vp, vp, ip, vp, vp]
+    L.bmg_level_tuning.argtypes = [vp, ctypes.c_int, ctypes.c_int, ip, ip]
     _lib = L
     return L
 

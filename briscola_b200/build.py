@@ -13,7 +13,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_lib", "libbmg.so")
-SOURCES = ["bmg_host.cu", "bmg_kernels.cu", "bmg_noalloc.cu"]
+SOURCES = ["bmg_host.cu", "bmg_kernels.cu", "bmg_smooth_fused.cu", "bmg_noalloc.cu"]
+HEADERS = ["bmg_internal.h", "bmg_stencil.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -26,7 +27,7 @@ def nvcc() -> str:
 
 def build_native(force: bool = False, verbose: bool = False) -> str:
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
-    deps = srcs + [os.path.join(CSRC, "bmg_internal.h"), os.path.join(HERE, "..", "include", "bmg.h")]
+    deps = srcs + [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(HERE, "..", "include", "bmg.h")]
     if not force and os.path.exists(OUT):
         t = os.path.getmtime(OUT)
         if all(os.path.getmtime(d) <= t for d in deps if os.path.exists(d)):

@@ -53,6 +53,12 @@ struct HostLevel {
     std::vector<double> lam_host[3];  // ghost-framed face lambda (variable coefficient)
     double* jtmp64 = nullptr;
     float* jtmp32 = nullptr;
+    double* x64b = nullptr;  // second x buffers: fused smoothing writes here, then swaps
+    float* x32b = nullptr;
+    bool fusedOK = false;    // level large enough for the fused smoother
+    // per precision (0: FP64, 1: FP32), picked by autotune():
+    int fusedS[2] = {kFusedMaxStages, kFusedMaxStages};  // colour stages per fused launch
+    int fusedTi[2] = {64, 64};                             // planes per CTA chunk
     long ncell() const { return (long)n[0] * n[1] * n[2]; }
     long at(int i, int j, int k) const { return base + (long)i * si + (long)j * sj + k; }
 };
@@ -102,9 +108,15 @@ struct bmg_ctx {
     double* stage_x = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::string err;
-    int cycles_done = 0;
     long launches = 0;  // kernels launched by the current solve
     std::vector<int> visits;
+    // whole-solve CUDA graph (captured on the first solve, reused)
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    cudaGraphConditionalHandle cond = 0;
+    cudaStream_t capStream = nullptr;  // private stream used only for capture
+    bool graphZero = false;
+    long launchesInitPost = 0, launchesBody = 0;
 };
 
 namespace {
@@ -131,11 +143,15 @@ void finishAxis(Axis& a, int n, bool periodic) {
     }
 }
 
+// Rows of pitch p2 = round_up(n2 + 5, 4) with interior k = 0 at offset 4:
+// rows and interiors start on 16-byte (FP32) / 32-byte (FP64) boundaries so
+// pairs and quads of k-neighbours load as one vector; the k ghosts sit at
+// offsets 3 and n2 + 4.
 void layout(HostLevel& L) {
-    const long p2 = L.n[2] + 2, p1 = L.n[1] + 2, p0 = L.n[0] + 2;
+    const long p2 = ((L.n[2] + 5) + 3) / 4 * 4, p1 = L.n[1] + 2, p0 = L.n[0] + 2;
     L.sj = p2;
     L.si = p1 * p2;
-    L.base = L.si + L.sj + 1;
+    L.base = L.si + L.sj + 4;
     L.cells = p0 * p1 * p2;
 }
 
@@ -317,7 +333,7 @@ void buildCoarseInverse(bmg_ctx* c) {
 void freeAll(bmg_ctx* c) {
     for (auto& L : c->lv) {
         for (void* p : {(void*)L.x64, (void*)L.b64, (void*)L.x32, (void*)L.b32, (void*)L.tab64,
-                        (void*)L.tab32, (void*)L.jtmp64, (void*)L.jtmp32})
+                        (void*)L.tab32, (void*)L.jtmp64, (void*)L.jtmp32, (void*)L.x64b, (void*)L.x32b})
             if (p) cudaFree(p);
         for (int d = 0; d < 3; ++d) {
             if (L.lam64[d]) cudaFree(L.lam64[d]);
@@ -332,6 +348,9 @@ void freeAll(bmg_ctx* c) {
     if (c->st_host) cudaFreeHost(c->st_host);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    if (c->capStream) cudaStreamDestroy(c->capStream);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -343,6 +362,7 @@ void validateOptions(const bmg_options* o) {
     if (o->smoother < 0 || o->smoother > 1) throw BadArg{BMG_BAD_ARG, "unsupported smoother type"};
     if (o->precision < 0 || o->precision > 1) throw BadArg{BMG_BAD_ARG, "unknown precision"};
     if (o->coarse_level < 0) throw BadArg{BMG_BAD_ARG, "negative coarseLevel"};
+    if (o->fused < 0) throw BadArg{BMG_BAD_ARG, "negative fused stage count"};
 }
 
 void build(bmg_ctx* c, const bmg_mesh_desc* mesh) {
@@ -407,6 +427,13 @@ void build(bmg_ctx* c, const bmg_mesh_desc* mesh) {
         L.b32 = dalloc<float>(L.cells);
         L.tab64 = dalloc<double>(L.tab.size());
         L.tab32 = dalloc<float>(L.tab.size());
+        // the fused smoother marches along axis 0 in chunks and wraps at most
+        // one period there (extent >= 2 * stages)
+        L.fusedOK = L.n[0] >= 16 && L.n[1] >= 16 && L.n[2] >= 16;
+        if (L.fusedOK) {
+            L.x64b = dalloc<double>(L.cells);
+            L.x32b = dalloc<float>(L.cells);
+        }
         upload(L.tab64, L.tab);
         upload(L.tab32, to_f32(L.tab));
     }
@@ -461,7 +488,7 @@ void build(bmg_ctx* c, const bmg_mesh_desc* mesh) {
         upload(t.pw64, pw);
         upload(t.pw32, to_f32(pw));
     }
-    c->partials = dalloc<double>(2 * kReduceBlocks);
+    c->partials = dalloc<double>(2 * reduce_blocks(view<double>(c, 0)));
     c->st = dalloc<SolveState>(1);
     BMG_CUDA(cudaMallocHost(&c->st_host, sizeof(SolveState)));
     c->stage_b = dalloc<double>(c->lv[0].ncell());
@@ -505,10 +532,63 @@ std::vector<int> colourSequence(const HostLevel& L, int sweeps) {
     return seq;
 }
 
+FusedGeom fusedGeom(const bmg_ctx* c, const HostLevel& L, int prec) {
+    FusedGeom g{};
+    g.m_axis = 0;
+    g.nm = L.n[0];
+    g.na = L.n[1];
+    g.nk = L.n[2];
+    g.sm = L.si;
+    g.sa = L.sj;
+    g.perm = c->periodic[0];
+    g.pera = c->periodic[1];
+    g.perk = c->periodic[2];
+    g.ti = std::min(L.fusedTi[prec], L.n[0]);
+    g.wl_m = L.to.wl[0];
+    g.wh_m = L.to.wh[0];
+    g.wl_a = L.to.wl[1];
+    g.wh_a = L.to.wh[1];
+    return g;
+}
+
+template <typename T>
+void swapX(HostLevel& L) {
+    if constexpr (sizeof(T) == 8)
+        std::swap(L.x64, L.x64b);
+    else
+        std::swap(L.x32, L.x32b);
+}
+
 template <typename T>
 void smooth(bmg_ctx* c, int l, int sweeps) {
     const LevelView<T> L = view<T>(c, l);
     cudaStream_t s = c->stream;
+    HostLevel& H = c->lv[l];
+    const int precIdx = sizeof(T) == 8 ? 0 : 1;
+    if (c->opt.smoother == BMG_SMOOTHER_RBGS && c->opt.fused > 0 && H.fusedOK && H.fusedS[precIdx] > 0) {
+        // the colour sequence alternates; run it in launches of up to
+        // maxS stages, each writing the other x buffer
+        const std::vector<int> seq = colourSequence(H, sweeps);
+        const int prec = sizeof(T) == 8 ? 0 : 1;
+        const FusedGeom g = fusedGeom(c, H, prec);
+        const size_t maxS = (size_t)std::min({c->opt.fused, H.fusedS[prec], kFusedMaxStages});
+        for (size_t p = 0; p < seq.size(); p += maxS) {
+            const int stages = (int)std::min<size_t>(maxS, seq.size() - p);
+            const LevelView<T> in = view<T>(c, l);
+            T* out;
+            if constexpr (sizeof(T) == 8)
+                out = reinterpret_cast<T*>(H.x64b);
+            else
+                out = reinterpret_cast<T*>(H.x32b);
+            c->launches += 1;
+            if (c->variable)
+                launch_smooth_fused<T, true>(in, out, g, seq[p], stages, s);
+            else
+                launch_smooth_fused<T, false>(in, out, g, seq[p], stages, s);
+            swapX<T>(H);
+        }
+        return;
+    }
     if (c->opt.smoother == BMG_SMOOTHER_JACOBI) {
         T* tmp;
         if constexpr (sizeof(T) == 8)
@@ -557,6 +637,64 @@ void coarseSolve(bmg_ctx* c) {
     launch_coarse_solve<T>(view<T>(c, c->lc), c->ainv, c->ncoarse, c->stream);
 }
 
+// Launch-shape autotuner: for every level the fused smoother handles, time
+// one smoothing step (the configured sweep count) for each number of colour
+// stages per launch and each plane-chunk length, and keep the fastest.  The
+// tile (16 x 64 cells) is fixed by the kernel's register window; stages and
+// chunk length trade halo recomputation against memory passes and CTA count.
+template <typename T>
+void autotuneLevel(bmg_ctx* c, int l, int sweeps, cudaEvent_t e0, cudaEvent_t e1) {
+    HostLevel& H = c->lv[l];
+    const int prec = sizeof(T) == 8 ? 0 : 1;
+    float best = 1e30f;
+    int bestS = H.fusedS[prec], bestTi = H.fusedTi[prec];
+    // S = 0: one launch per colour pass (no temporal blocking)
+    for (int S = 0; S <= kFusedMaxStages; ++S)
+        for (int ti : {32, 64, 128}) {
+            if (ti > 2 * H.n[0] && ti != 32) continue;
+            if (S == 0 && ti != 32) continue;
+            H.fusedS[prec] = S;
+            H.fusedTi[prec] = ti;
+            smooth<T>(c, l, sweeps);  // warm-up
+            BMG_CUDA(cudaEventRecord(e0, c->stream));
+            for (int r = 0; r < 3; ++r) smooth<T>(c, l, sweeps);
+            BMG_CUDA(cudaEventRecord(e1, c->stream));
+            BMG_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            BMG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best) {
+                best = ms;
+                bestS = S;
+                bestTi = ti;
+            }
+        }
+    H.fusedS[prec] = bestS;
+    H.fusedTi[prec] = bestTi;
+}
+
+void autotune(bmg_ctx* c) {
+    if (c->opt.smoother != BMG_SMOOTHER_RBGS || c->opt.fused <= 0) return;
+    const int sweeps = std::max({c->opt.n_pre, c->opt.n_post, 1});
+    cudaEvent_t e0, e1;
+    BMG_CUDA(cudaEventCreate(&e0));
+    BMG_CUDA(cudaEventCreate(&e1));
+    for (int l = 0; l < (int)c->lv.size(); ++l) {
+        if (!c->lv[l].fusedOK) continue;
+        autotuneLevel<double>(c, l, sweeps, e0, e1);
+        autotuneLevel<float>(c, l, sweeps, e0, e1);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // the timing runs smoothed whatever the buffers held: start clean
+    for (auto& L : c->lv) {
+        BMG_CUDA(cudaMemsetAsync(L.x64, 0, L.cells * sizeof(double), c->stream));
+        BMG_CUDA(cudaMemsetAsync(L.x32, 0, L.cells * sizeof(float), c->stream));
+        if (L.x64b) BMG_CUDA(cudaMemsetAsync(L.x64b, 0, L.cells * sizeof(double), c->stream));
+        if (L.x32b) BMG_CUDA(cudaMemsetAsync(L.x32b, 0, L.cells * sizeof(float), c->stream));
+    }
+    BMG_CUDA(cudaStreamSynchronize(c->stream));
+}
+
 int levelReps(const bmg_ctx* c, int l) {  // MG.H:106-124
     if (c->opt.cycle_type == BMG_CYCLE_V) return 1;
     if (c->opt.cycle_type == BMG_CYCLE_W) return 1 + (l > 0);
@@ -588,7 +726,9 @@ void checkLaunch() {
     if (e != cudaSuccess) throw CudaError{std::string("kernel launch: ") + cudaGetErrorString(e)};
 }
 
-void residualNorm(bmg_ctx* c, int mode) {
+// level-0 FP64 residual norm and the convergence decision; inside a graph
+// the decision also sets the WHILE node's condition
+void residualNorm(bmg_ctx* c, int mode, bool setCondition) {
     const LevelView<double> L = view<double>(c, 0);
     float* b32 = c->opt.precision == BMG_PRECISION_MIXED ? c->lv[0].b32 : nullptr;
     c->launches += 2;
@@ -596,32 +736,30 @@ void residualNorm(bmg_ctx* c, int mode) {
         launch_residual_norm<true>(L, mode, c->partials, b32, nullptr, c->stream);
     else
         launch_residual_norm<false>(L, mode, c->partials, b32, nullptr, c->stream);
-    launch_finalize(c->partials, c->st, mode, c->stream);
+    launch_finalize(L, c->partials, c->st, mode, c->cond, setCondition ? 1 : 0, c->stream);
 }
 
-int solveImpl(bmg_ctx* c, const double* b, double* x, int flags, bmg_report* rep) {
-    BMG_CUDA(cudaSetDevice(c->opt.device));
+SolveState initialState(const bmg_ctx* c) {
+    const HostLevel& L0 = c->lv[0];
+    SolveState init{};
+    init.rel_tol = c->opt.rel_tol;
+    init.abs_tol = c->opt.abs_tol;
+    init.min_iter = c->opt.min_iter;
+    init.max_iter = c->opt.max_iter;
+    init.ncells = (double)L0.ncell();
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int d = 0; d < 3; ++d)
+        for (int i = 0; i < L0.n[d]; ++i) v[d] += L0.ax[d].h[i + 1];
+    init.vol_total = v[0] * v[1] * v[2];
+    return init;
+}
+
+// MG.C:144-190: load b (scaled) and x, initial residual, normFactor and the
+// first convergence test.  The state is copied from the pinned host copy,
+// which the caller fills before every solve (also when replayed as a graph).
+void segInit(bmg_ctx* c, const double* bsrc, const double* xsrc, bool zero, bool setCondition) {
     cudaStream_t s = c->stream;
     HostLevel& L0 = c->lv[0];
-    const long n = L0.ncell();
-    const bool dev = flags & BMG_DEVICE_PTRS;
-    const bool zero = flags & BMG_ZERO_GUESS;
-    const bool mixed = c->opt.precision == BMG_PRECISION_MIXED;
-    if (c->opt.smoother == BMG_SMOOTHER_JACOBI) ensureJacobiBuffers(c);
-    const auto t0 = std::chrono::steady_clock::now();
-    c->launches = 0;
-
-    BMG_CUDA(cudaEventRecord(c->ev0, s));
-    const double* bsrc = b;
-    const double* xsrc = x;
-    if (!dev) {
-        BMG_CUDA(cudaMemcpyAsync(c->stage_b, b, n * sizeof(double), cudaMemcpyHostToDevice, s));
-        bsrc = c->stage_b;
-        if (!zero) {
-            BMG_CUDA(cudaMemcpyAsync(c->stage_x, x, n * sizeof(double), cudaMemcpyHostToDevice, s));
-            xsrc = c->stage_x;
-        }
-    }
     const LevelView<double> V0 = view<double>(c, 0);
     launch_load_b(V0, bsrc, s);
     BMG_CUDA(cudaMemsetAsync(L0.x64, 0, L0.cells * sizeof(double), s));
@@ -630,59 +768,165 @@ int solveImpl(bmg_ctx* c, const double* b, double* x, int flags, bmg_report* rep
         launch_load_x(V0, xsrc, s);
         c->launches += 1;
     }
-
-    SolveState init{};
-    init.rel_tol = c->opt.rel_tol;
-    init.abs_tol = c->opt.abs_tol;
-    init.min_iter = c->opt.min_iter;
-    init.max_iter = c->opt.max_iter;
-    init.ncells = (double)n;
-    double vol = 0.0;
-    for (int i = 0; i < L0.n[0]; ++i) vol += L0.ax[0].h[i + 1];
-    double vy = 0.0, vz = 0.0;
-    for (int j = 0; j < L0.n[1]; ++j) vy += L0.ax[1].h[j + 1];
-    for (int k = 0; k < L0.n[2]; ++k) vz += L0.ax[2].h[k + 1];
-    init.vol_total = vol * vy * vz;
-    *c->st_host = init;
     BMG_CUDA(cudaMemcpyAsync(c->st, c->st_host, sizeof(SolveState), cudaMemcpyHostToDevice, s));
-    residualNorm(c, 0);
-    checkLaunch();
+    residualNorm(c, 0, setCondition);
+}
 
-    int status = BMG_OK;
-    c->cycles_done = 0;
-    for (;;) {
-        BMG_CUDA(cudaMemcpyAsync(c->st_host, c->st, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
-        BMG_CUDA(cudaStreamSynchronize(s));
-        if (!c->st_host->keep_going) break;
-        if (c->opt.timeout_ms > 0) {
-            const double ms =
-                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-            if (ms > c->opt.timeout_ms) {
-                status = BMG_TIMEOUT;
-                break;
-            }
-        }
-        std::fill(c->visits.begin(), c->visits.end(), 0);
-        if (mixed) {
-            BMG_CUDA(cudaMemsetAsync(L0.x32, 0, L0.cells * sizeof(float), s));
-            cycle<float>(c, 0);
-            launch_add_correction(V0, view<float>(c, 0), s);
-            c->launches += 1;
-        } else {
-            cycle<double>(c, 0);
-        }
-        residualNorm(c, 1);
-        checkLaunch();
-        c->cycles_done++;
+// MG.C:191-242: one cycle and the new residual.  Mixed precision: the FP32
+// cycle solves for the correction of the FP64 residual (written in FP32 by
+// the residual kernel), which is then added in FP64.
+void segBody(bmg_ctx* c, bool setCondition) {
+    cudaStream_t s = c->stream;
+    HostLevel& L0 = c->lv[0];
+    std::fill(c->visits.begin(), c->visits.end(), 0);
+    if (c->opt.precision == BMG_PRECISION_MIXED) {
+        BMG_CUDA(cudaMemsetAsync(L0.x32, 0, L0.cells * sizeof(float), s));
+        cycle<float>(c, 0);
+        launch_add_correction(view<double>(c, 0), view<float>(c, 0), s);
+        c->launches += 1;
+    } else {
+        cycle<double>(c, 0);
     }
+    residualNorm(c, 1, setCondition);
+}
+
+void segPost(bmg_ctx* c, double* xdst) {
+    const LevelView<double> V0 = view<double>(c, 0);
     if (c->opt.remove_mean) {
-        launch_mean(V0, c->partials, c->st, s);
+        launch_mean(V0, c->partials, c->st, c->stream);
         c->launches += 3;
     }
-    double* xdst = dev ? x : c->stage_x;
-    launch_store_x(V0, xdst, s);
+    launch_store_x(V0, xdst, c->stream);
     c->launches += 1;
-    if (!dev) BMG_CUDA(cudaMemcpyAsync(x, c->stage_x, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+}
+
+void destroyGraph(bmg_ctx* c) {
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    c->gexec = nullptr;
+    c->graph = nullptr;
+}
+
+// Whole solve as one graph: init -> WHILE(keep_going){ cycle, residual,
+// decision } -> mean removal and store.  Reads b from stage_b (and x from
+// stage_x), writes x to stage_x.
+void captureGraph(bmg_ctx* c, bool zero) {
+    destroyGraph(c);
+    // capture on the context's private stream (capturing the legacy default
+    // stream is not allowed); the instantiated graph runs on any stream
+    const cudaStream_t user = c->stream;
+    c->stream = c->capStream;
+    struct Restore {
+        bmg_ctx* c;
+        cudaStream_t s;
+        ~Restore() {
+            // a capture left open by an error is ended and dropped
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+            if (cudaStreamIsCapturing(c->capStream, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+                cudaGraph_t g = nullptr;
+                cudaStreamEndCapture(c->capStream, &g);
+                if (g && g != c->graph) cudaGraphDestroy(g);
+            }
+            c->stream = s;
+        }
+    } restore{c, user};
+    cudaStream_t s = c->stream;
+    BMG_CUDA(cudaGraphCreate(&c->graph, 0));
+    BMG_CUDA(cudaGraphConditionalHandleCreate(&c->cond, c->graph, 0, 0));
+    const long l0 = c->launches;
+    BMG_CUDA(cudaStreamBeginCaptureToGraph(s, c->graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    segInit(c, c->stage_b, c->stage_x, zero, true);
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaGraph_t capg = nullptr;
+    BMG_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &capg, &deps, &ndeps));
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = c->cond;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t loop;
+    BMG_CUDA(cudaGraphAddNode(&loop, c->graph, deps, ndeps, &p));
+    cudaGraph_t body = p.conditional.phGraph_out[0];
+    BMG_CUDA(cudaStreamUpdateCaptureDependencies(s, &loop, 1, cudaStreamSetCaptureDependencies));
+    segPost(c, c->stage_x);
+    BMG_CUDA(cudaStreamEndCapture(s, &capg));
+    const long l1 = c->launches;
+
+    double* x0 = c->lv[0].x64;
+    BMG_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    segBody(c, true);
+    // the fused smoother swaps x buffers; level-0 x must come back to the
+    // buffer the next iteration (and the post segment) reads
+    if (c->lv[0].x64 != x0) {
+        BMG_CUDA(cudaMemcpyAsync(x0, c->lv[0].x64, c->lv[0].cells * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        std::swap(c->lv[0].x64, c->lv[0].x64b);
+    }
+    BMG_CUDA(cudaStreamEndCapture(s, &body));
+    c->launchesInitPost = l1 - l0;
+    c->launchesBody = c->launches - l1;
+    BMG_CUDA(cudaGraphInstantiate(&c->gexec, c->graph, 0));
+    c->graphZero = zero;
+}
+
+int solveImpl(bmg_ctx* c, const double* b, double* x, int flags, bmg_report* rep) {
+    BMG_CUDA(cudaSetDevice(c->opt.device));
+    cudaStream_t s = c->stream;
+    const long n = c->lv[0].ncell();
+    const bool dev = flags & BMG_DEVICE_PTRS;
+    const bool zero = flags & BMG_ZERO_GUESS;
+    if (c->opt.smoother == BMG_SMOOTHER_JACOBI) ensureJacobiBuffers(c);
+    const auto t0 = std::chrono::steady_clock::now();
+    *c->st_host = initialState(c);
+    int status = BMG_OK;
+    // the graph runs the loop on the device; a wall-clock budget needs the
+    // host between cycles
+    const bool useGraph = c->opt.use_graph && !(c->opt.timeout_ms > 0);
+
+    if (useGraph) {
+        if (!c->gexec || c->graphZero != zero) captureGraph(c, zero);
+        const cudaMemcpyKind kin = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        BMG_CUDA(cudaEventRecord(c->ev0, s));
+        BMG_CUDA(cudaMemcpyAsync(c->stage_b, b, n * sizeof(double), kin, s));
+        if (!zero) BMG_CUDA(cudaMemcpyAsync(c->stage_x, x, n * sizeof(double), kin, s));
+        BMG_CUDA(cudaGraphLaunch(c->gexec, s));
+        BMG_CUDA(cudaMemcpyAsync(x, c->stage_x, n * sizeof(double),
+                                 dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+    } else {
+        c->launches = 0;
+        BMG_CUDA(cudaEventRecord(c->ev0, s));
+        const double* bsrc = b;
+        const double* xsrc = x;
+        if (!dev) {
+            BMG_CUDA(cudaMemcpyAsync(c->stage_b, b, n * sizeof(double), cudaMemcpyHostToDevice, s));
+            bsrc = c->stage_b;
+            if (!zero) {
+                BMG_CUDA(cudaMemcpyAsync(c->stage_x, x, n * sizeof(double), cudaMemcpyHostToDevice, s));
+                xsrc = c->stage_x;
+            }
+        }
+        segInit(c, bsrc, xsrc, zero, false);
+        checkLaunch();
+        for (;;) {
+            BMG_CUDA(cudaMemcpyAsync(c->st_host, c->st, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+            BMG_CUDA(cudaStreamSynchronize(s));
+            if (!c->st_host->keep_going) break;
+            if (c->opt.timeout_ms > 0) {
+                const double ms =
+                    std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+                if (ms > c->opt.timeout_ms) {
+                    status = BMG_TIMEOUT;
+                    break;
+                }
+            }
+            segBody(c, false);
+            checkLaunch();
+        }
+        double* xdst = dev ? x : c->stage_x;
+        segPost(c, xdst);
+        if (!dev) BMG_CUDA(cudaMemcpyAsync(x, c->stage_x, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
     BMG_CUDA(cudaEventRecord(c->ev1, s));
     BMG_CUDA(cudaMemcpyAsync(c->st_host, c->st, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
     BMG_CUDA(cudaStreamSynchronize(s));
@@ -706,7 +950,7 @@ int solveImpl(bmg_ctx* c, const double* b, double* x, int flags, bmg_report* rep
         rep->final_l2 = st.l2;
         rep->norm_factor = st.nf;
         rep->ms = ms;
-        rep->kernel_launches = c->launches;
+        rep->kernel_launches = useGraph ? c->launchesInitPost + c->launchesBody * st.iter : c->launches;
     }
     return status;
 }
@@ -796,6 +1040,8 @@ int bmg_default_options(bmg_options* o) {
     o->precision = BMG_PRECISION_FP64;
     o->use_graph = 1;
     o->remove_mean = 1;
+    o->fused = kFusedMaxStages;
+    o->autotune = 1;
     o->device = 0;
     o->timeout_ms = 0.0;
     return BMG_OK;
@@ -820,8 +1066,11 @@ int bmg_create(bmg_ctx** out, const bmg_mesh_desc* mesh, const bmg_options* opts
         BMG_CUDA(cudaSetDevice(c->opt.device));
         BMG_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
         c->own_stream = true;
+        BMG_CUDA(cudaStreamCreateWithFlags(&c->capStream, cudaStreamNonBlocking));
+        configure_fused_kernels();
         build(c, mesh);
         configureCoarse(c);
+        if (c->opt.autotune) autotune(c);
         return BMG_OK;
     });
     if (rc != BMG_OK) {
@@ -848,9 +1097,13 @@ int bmg_set_options(bmg_ctx* c, const bmg_options* o) {
         validateOptions(o);
         if (o->device != c->opt.device) throw BadArg{BMG_BAD_ARG, "the device of a context is fixed"};
         const bool coarseChanged = o->coarse_level != c->opt.coarse_level;
+        const bool retune = o->autotune && (!c->opt.autotune || o->fused != c->opt.fused ||
+                                            o->n_pre != c->opt.n_pre || o->n_post != c->opt.n_post);
         c->opt = *o;
+        destroyGraph(c);
         BMG_CUDA(cudaSetDevice(c->opt.device));
         if (coarseChanged) configureCoarse(c);
+        if (retune) autotune(c);
         return BMG_OK;
     });
 }
@@ -876,6 +1129,7 @@ int bmg_set_coefficients(bmg_ctx* c, const double* lx, const double* ly, const d
             c->variable = true;
         }
         buildCoarseInverse(c);
+        destroyGraph(c);  // kernels differ between constant and variable coefficients
         return BMG_OK;
     });
 }
@@ -902,6 +1156,15 @@ int bmg_solve(bmg_ctx* c, const double* b, double* x, int flags, bmg_report* rep
 long bmg_num_cells(const bmg_ctx* c) { return c ? c->lv[0].ncell() : 0; }
 int bmg_num_levels(const bmg_ctx* c) { return c ? (int)c->lv.size() : 0; }
 int bmg_coarse_level_index(const bmg_ctx* c) { return c ? c->lc : -1; }
+
+int bmg_level_tuning(const bmg_ctx* c, int l, int prec, int* stages, int* chunk) {
+    if (!validLevel(c, l) || prec < 0 || prec > 1 || !stages || !chunk) return BMG_BAD_ARG;
+    const HostLevel& L = c->lv[l];
+    const bool fused = c->opt.smoother == BMG_SMOOTHER_RBGS && c->opt.fused > 0 && L.fusedOK && L.fusedS[prec] > 0;
+    *stages = fused ? std::min({c->opt.fused, L.fusedS[prec], kFusedMaxStages}) : 0;
+    *chunk = fused ? std::min(L.fusedTi[prec], L.n[0]) : 0;
+    return BMG_OK;
+}
 
 int bmg_level_shape(const bmg_ctx* c, int l, int brick, int n[3]) {
     if (!validLevel(c, l) || brick != 0 || !n) return BMG_BAD_ARG;

@@ -83,7 +83,25 @@ struct SolveState {
     int pad[2];
 };
 
-constexpr int kReduceBlocks = 592;   // 4 x 148 SMs: fixed so sums are deterministic
+// Geometry of a fused smoothing launch: march axis m (0 or 1), the other
+// non-contiguous axis a, and k (axis 2); see bmg_smooth_fused.cu.
+struct FusedGeom {
+    int m_axis;
+    int nm, na, nk;
+    long sm, sa;        // strides of m and a (k contiguous)
+    int perm, pera, perk;
+    int ti;             // planes per CTA chunk along m
+    int wl_m, wh_m;     // coupling-table offsets of the m axis
+    int wl_a, wh_a;     // ... of the a axis
+};
+
+// all `stages` colour passes (colours c1, 1-c1, c1, ...) of one smoothing
+// step in one launch, reading L.x and writing xout
+template <typename T, bool VAR>
+void launch_smooth_fused(const LevelView<T>& L, T* xout, const FusedGeom& g, int c1, int stages,
+                         cudaStream_t s);
+constexpr int kFusedMaxStages = 3;
+
 constexpr int kReduceThreads = 256;
 
 // ---- launchers (bmg_kernels.cu) -------------------------------------------
@@ -108,7 +126,12 @@ void launch_residual_out(const LevelView<T>& L, double* r_unscaled_compact, cuda
 template <bool VAR>
 void launch_residual_norm(const LevelView<double>& L, int mode, double* partials, float* b32,
                           const LevelView<float>* L32, cudaStream_t s);
-void launch_finalize(const double* partials, SolveState* st, int mode, cudaStream_t s);
+void launch_finalize(const LevelView<double>& L, const double* partials, SolveState* st, int mode,
+                     cudaGraphConditionalHandle cond, int setCondition, cudaStream_t s);
+// number of per-block partial sums the level-0 reductions write
+long reduce_blocks(const LevelView<double>& L);
+// sets the dynamic shared memory limits of the fused smoother instances
+void configure_fused_kernels();
 void launch_mean(const LevelView<double>& L, double* partials, SolveState* st, cudaStream_t s);
 
 // compact interior <-> ghost-framed conversions (level 0, FP64)

@@ -5,7 +5,7 @@
 // FP32 arithmetic chosen by the template parameter.  Layout and coefficient
 // conventions are described in bmg_internal.h.
 
-#include "bmg_internal.h"
+#include "bmg_stencil.cuh"
 
 #include <cmath>
 
@@ -13,96 +13,52 @@ namespace bmg {
 
 namespace {
 
-template <typename T>
-__device__ __forceinline__ T ldg(const T* p) {
-    return __ldg(p);
-}
-
-// Row-scaled couplings of cell (i,j,k) to its six neighbours, in the order
-// of the reference's row product: l, r, b, t, a, f (linearSystemFunctions.H
-// :96-102).
-template <typename T, bool VAR>
-__device__ __forceinline__ void couplings(const LevelView<T>& L, int i, int j, int k, long c,
-                                          T w[6]) {
-    w[0] = ldg(L.tab + L.to.wl[0] + i);
-    w[1] = ldg(L.tab + L.to.wh[0] + i);
-    w[2] = ldg(L.tab + L.to.wl[1] + j);
-    w[3] = ldg(L.tab + L.to.wh[1] + j);
-    w[4] = ldg(L.tab + L.to.wl[2] + k);
-    w[5] = ldg(L.tab + L.to.wh[2] + k);
-    if (VAR) {
-        w[0] *= ldg(L.lam0 + c);
-        w[1] *= ldg(L.lam0 + c + L.si);
-        w[2] *= ldg(L.lam1 + c);
-        w[3] *= ldg(L.lam1 + c + L.sj);
-        w[4] *= ldg(L.lam2 + c);
-        w[5] *= ldg(L.lam2 + c + 1);
-    }
-}
-
-// sum of couplings times neighbour values, and the sum of couplings
-// (= minus the centre coefficient)
-template <typename T>
-__device__ __forceinline__ void stencil(const T* x, long c, long si, long sj, const T w[6], T& s,
-                                        T& d) {
-    s = w[0] * x[c - si] + w[1] * x[c + si] + w[2] * x[c - sj] + w[3] * x[c + sj] +
-        w[4] * x[c - 1] + w[5] * x[c + 1];
-    d = w[0] + w[1] + w[2] + w[3] + w[4] + w[5];
-}
-
-// Store an interior value and its periodic ghost images (faces, edges and
-// corners), replacing the reference's per-sweep periodic ghost copy
-// (periodicBoundaryCondition.C:53-92).
-// Per axis a cell has up to two images: in the upper ghost layer (cell 0)
-// and in the lower one (cell n-1); both when n == 1.  All 26 combinations
-// are unrolled into predicated stores, so nothing lives in local memory.
-template <typename T>
-__device__ __forceinline__ void store_x(const LevelView<T>& L, long c, int i, int j, int k, T v) {
-    L.x[c] = v;
-    const long up0 = (L.per0 && i == 0) ? (long)L.n0 * L.si : 0;
-    const long dn0 = (L.per0 && i == L.n0 - 1) ? -(long)L.n0 * L.si : 0;
-    const long up1 = (L.per1 && j == 0) ? (long)L.n1 * L.sj : 0;
-    const long dn1 = (L.per1 && j == L.n1 - 1) ? -(long)L.n1 * L.sj : 0;
-    const long up2 = (L.per2 && k == 0) ? (long)L.n2 : 0;
-    const long dn2 = (L.per2 && k == L.n2 - 1) ? -(long)L.n2 : 0;
-    if (!(up0 | dn0 | up1 | dn1 | up2 | dn2)) return;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const long o0 = a == 0 ? 0 : a == 1 ? up0 : dn0;
-        if (a && !o0) continue;
-#pragma unroll
-        for (int e = 0; e < 3; ++e) {
-            const long o1 = e == 0 ? 0 : e == 1 ? up1 : dn1;
-            if (e && !o1) continue;
-#pragma unroll
-            for (int f = 0; f < 3; ++f) {
-                const long o2 = f == 0 ? 0 : f == 1 ? up2 : dn2;
-                if (f && !o2) continue;
-                if (a | e | f) L.x[c + o0 + o1 + o2] = v;
-            }
-        }
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Red-black Gauss-Seidel: one colour pass.  Thread per (i, j, k-pair); the
 // pair member of the requested colour is updated.  Colour 0 = (i+j+k) even.
 // Equivalent to one pass of rbgsSmoother.C:65-183 over the whole level.
 // ---------------------------------------------------------------------------
+template <typename T>
+struct Pair;
+template <>
+struct Pair<float> {
+    using type = float2;
+};
+template <>
+struct Pair<double> {
+    using type = double2;
+};
+
+// The thread owns the k-pair (2p, 2p+1) and updates its member of the
+// requested colour.  Neighbour rows and planes are read as whole pairs
+// (8/16-byte loads: rows start on 16-byte boundaries and k0 is even), so a
+// warp's loads fill every L1 wavefront; the k neighbour outside the pair is
+// one scalar load.
 template <typename T, bool VAR>
 __global__ void __launch_bounds__(256) k_colour_pass(LevelView<T> L, int colour) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    using V2 = typename Pair<T>::type;
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = blockIdx.z;
-    if (j >= L.n1) return;
-    const int k = 2 * m + ((colour + i + j) & 1);
+    const int k0 = 2 * p;
+    if (j >= L.n1 || k0 >= L.n2) return;
+    const int e = ((i + j + k0) & 1) == colour ? 0 : 1;
+    const int k = k0 + e;
     if (k >= L.n2) return;
-    const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
-    T w[6], s, d;
+    const long r = L.base + (long)i * L.si + (long)j * L.sj;
+    const T* x = L.x;
+    const long c0 = r + k0;
+    const V2 xm = *reinterpret_cast<const V2*>(x + c0 - L.si);
+    const V2 xp = *reinterpret_cast<const V2*>(x + c0 + L.si);
+    const V2 ym = *reinterpret_cast<const V2*>(x + c0 - L.sj);
+    const V2 yp = *reinterpret_cast<const V2*>(x + c0 + L.sj);
+    const V2 own = *reinterpret_cast<const V2*>(x + c0);
+    const long c = r + k;
+    T w[6];
     couplings<T, VAR>(L, i, j, k, c, w);
-    stencil(L.x, c, L.si, L.sj, w, s, d);
-    const T v = (s - L.b[c]) / d;
-    store_x(L, c, i, j, k, v);
+    const T xn[6] = {e ? xm.y : xm.x, e ? xp.y : xp.x, e ? ym.y : ym.x, e ? yp.y : yp.x,
+                     e ? own.x : x[c0 - 1], e ? x[c0 + 2] : own.y};
+    store_x(L, c, i, j, k, gs_value(w, xn, L.b[c]));
 }
 
 // Damped Jacobi (omega = 0.8, jacSmoother.C:15) into a temporary, then copy.
@@ -247,8 +203,10 @@ __global__ void __launch_bounds__(256) k_residual_out(LevelView<T> L, double* ou
 
 template <int NT>
 __device__ __forceinline__ double block_sum(double v, double* sh) {
+    // NT threads in a block of any shape; the result is valid in thread 0
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int lane = tid & 31, warp = tid >> 5;
     __syncthreads();
     if (lane == 0) sh[warp] = v;
     __syncthreads();
@@ -267,49 +225,55 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
 // row sums of the level-0 operator vanish (all couplings are paired with the
 // centre), so A*mean(x) drops out of the reference's expression.
 // ---------------------------------------------------------------------------
+// One cell per thread over the same (k, j, i) grid as the other cell
+// kernels, one partial sum per block in fixed block order; the finalize
+// kernel adds the partials in a fixed order, so sums are reproducible.
 template <bool VAR>
 __global__ void __launch_bounds__(kReduceThreads) k_residual_norm(LevelView<double> L, int mode,
-                                                                  double* partials, float* b32) {
+                                                                  double* partials, long nblocks,
+                                                                  float* b32) {
     __shared__ double sh[kReduceThreads / 32];
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = blockIdx.z;
     double a1 = 0.0, a2 = 0.0;
-    const int rows = L.n0 * L.n1;
-    for (int q = blockIdx.x; q < rows; q += gridDim.x) {
-        const int i = q / L.n1, j = q % L.n1;
-        const double hij = L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j];
-        for (int k = threadIdx.x; k < L.n2; k += blockDim.x) {
-            const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
-            double w[6], s, d;
-            couplings<double, VAR>(L, i, j, k, c, w);
-            stencil(L.x, c, L.si, L.sj, w, s, d);
-            const double r = L.b[c] + d * L.x[c] - s;
-            const double V = hij * L.tab64[L.to.h[2] + k];
-            const double rr = V * r;
-            a1 += rr * rr;
-            if (mode == 0) {
-                const double bb = V * L.b[c];
-                const double t = fabs(rr - bb) + fabs(bb);
-                a2 += t * t;
-            }
-            if (b32) b32[c] = (float)r;
+    if (j < L.n1 && k < L.n2) {
+        const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
+        double w[6], s, d;
+        couplings<double, VAR>(L, i, j, k, c, w);
+        stencil(L.x, c, L.si, L.sj, w, s, d);
+        const double r = L.b[c] + d * L.x[c] - s;
+        const double V = L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j] * L.tab64[L.to.h[2] + k];
+        const double rr = V * r;
+        a1 = rr * rr;
+        if (mode == 0) {
+            const double bb = V * L.b[c];
+            const double t = fabs(rr - bb) + fabs(bb);
+            a2 = t * t;
         }
+        if (b32) b32[c] = (float)r;
     }
+    const long bid = ((long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
     a1 = block_sum<kReduceThreads>(a1, sh);
     if (mode == 0) a2 = block_sum<kReduceThreads>(a2, sh);
-    if (threadIdx.x == 0) {
-        partials[blockIdx.x] = a1;
-        if (mode == 0) partials[kReduceBlocks + blockIdx.x] = a2;
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        partials[bid] = a1;
+        if (mode == 0) partials[nblocks + bid] = a2;
     }
 }
 
 // solver.C:13-95 on the reduced sums; also decides whether the loop goes on
-// (MG.C:191-195).
-__global__ void __launch_bounds__(kReduceThreads) k_finalize(const double* partials, SolveState* st,
-                                                              int mode) {
+// (MG.C:191-195) and, inside the solve graph, hands that decision to the
+// WHILE node (bounded by maxIter, so the device loop always ends).
+__global__ void __launch_bounds__(kReduceThreads) k_finalize(const double* partials, long nblocks,
+                                                              SolveState* st, int mode,
+                                                              cudaGraphConditionalHandle cond,
+                                                              int setCondition) {
     __shared__ double sh[kReduceThreads / 32];
     double a1 = 0.0, a2 = 0.0;
-    for (int q = threadIdx.x; q < kReduceBlocks; q += blockDim.x) {
+    for (long q = threadIdx.x; q < nblocks; q += blockDim.x) {
         a1 += partials[q];
-        if (mode == 0) a2 += partials[kReduceBlocks + q];
+        if (mode == 0) a2 += partials[nblocks + q];
     }
     a1 = block_sum<kReduceThreads>(a1, sh);
     if (mode == 0) a2 = block_sum<kReduceThreads>(a2, sh);
@@ -333,29 +297,30 @@ __global__ void __launch_bounds__(kReduceThreads) k_finalize(const double* parti
                           (st->cur / (st->init + 1e-20) > st->rel_tol));
         st->keep_going = !st->nan && ((st->iter < st->max_iter && !st->converged) ||
                                       st->iter < st->min_iter);
+        if (setCondition) cudaGraphSetConditional(cond, st->keep_going ? 1u : 0u);
     }
 }
 
 __global__ void __launch_bounds__(kReduceThreads) k_mean_partials(LevelView<double> L, double* partials) {
     __shared__ double sh[kReduceThreads / 32];
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = blockIdx.z;
     double a = 0.0;
-    const int rows = L.n0 * L.n1;
-    for (int q = blockIdx.x; q < rows; q += gridDim.x) {
-        const int i = q / L.n1, j = q % L.n1;
-        const double hij = L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j];
-        for (int k = threadIdx.x; k < L.n2; k += blockDim.x) {
-            const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
-            a += hij * L.tab64[L.to.h[2] + k] * L.x[c];
-        }
+    if (j < L.n1 && k < L.n2) {
+        const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
+        a = L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j] * L.tab64[L.to.h[2] + k] * L.x[c];
     }
     a = block_sum<kReduceThreads>(a, sh);
-    if (threadIdx.x == 0) partials[blockIdx.x] = a;
+    if (threadIdx.x == 0 && threadIdx.y == 0)
+        partials[((long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = a;
 }
 
-__global__ void __launch_bounds__(kReduceThreads) k_mean_finalize(const double* partials, SolveState* st) {
+__global__ void __launch_bounds__(kReduceThreads) k_mean_finalize(const double* partials, long nblocks,
+                                                                  SolveState* st) {
     __shared__ double sh[kReduceThreads / 32];
     double a = 0.0;
-    for (int q = threadIdx.x; q < kReduceBlocks; q += blockDim.x) a += partials[q];
+    for (long q = threadIdx.x; q < nblocks; q += blockDim.x) a += partials[q];
     a = block_sum<kReduceThreads>(a, sh);
     if (threadIdx.x == 0) st->mean = a / st->vol_total;
 }
@@ -452,6 +417,12 @@ inline dim3 block_for(int n2) {
 
 // ---- launchers --------------------------------------------------------------
 
+long reduce_blocks(const LevelView<double>& L) {
+    const dim3 blk = block_for(L.n2);
+    const dim3 g = grid_cells(L.n0, L.n1, L.n2, blk);
+    return (long)g.x * g.y * g.z;
+}
+
 template <typename T, bool VAR>
 void launch_colour_pass(const LevelView<T>& L, int colour, cudaStream_t s) {
     const int pairs = (L.n2 + 1) / 2;
@@ -505,16 +476,20 @@ void launch_residual_out(const LevelView<T>& L, double* out, cudaStream_t s) {
 template <bool VAR>
 void launch_residual_norm(const LevelView<double>& L, int mode, double* partials, float* b32,
                           const LevelView<float>*, cudaStream_t s) {
-    k_residual_norm<VAR><<<kReduceBlocks, kReduceThreads, 0, s>>>(L, mode, partials, b32);
+    const dim3 blk = block_for(L.n2);
+    k_residual_norm<VAR><<<grid_cells(L.n0, L.n1, L.n2, blk), blk, 0, s>>>(L, mode, partials,
+                                                                          reduce_blocks(L), b32);
 }
 
-void launch_finalize(const double* partials, SolveState* st, int mode, cudaStream_t s) {
-    k_finalize<<<1, kReduceThreads, 0, s>>>(partials, st, mode);
+void launch_finalize(const LevelView<double>& L, const double* partials, SolveState* st, int mode,
+                     cudaGraphConditionalHandle cond, int setCondition, cudaStream_t s) {
+    k_finalize<<<1, kReduceThreads, 0, s>>>(partials, reduce_blocks(L), st, mode, cond, setCondition);
 }
 
 void launch_mean(const LevelView<double>& L, double* partials, SolveState* st, cudaStream_t s) {
-    k_mean_partials<<<kReduceBlocks, kReduceThreads, 0, s>>>(L, partials);
-    k_mean_finalize<<<1, kReduceThreads, 0, s>>>(partials, st);
+    const dim3 blk = block_for(L.n2);
+    k_mean_partials<<<grid_cells(L.n0, L.n1, L.n2, blk), blk, 0, s>>>(L, partials);
+    k_mean_finalize<<<1, kReduceThreads, 0, s>>>(partials, reduce_blocks(L), st);
     const long n = L.cells;
     const int blocks = (int)std::min<long>((n + 255) / 256, 148L * 16);
     k_sub_mean<<<blocks, 256, 0, s>>>(L.x, n, st);

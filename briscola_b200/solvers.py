@@ -280,6 +280,13 @@ class Context:
     def coarse_level_index(self) -> int:
         return self._lib.bmg_coarse_level_index(self.h)
 
+    def tuning(self, level: int, precision: int = 0):
+        """(colour stages per fused launch, planes per chunk) on a level."""
+        s, t = ctypes.c_int(), ctypes.c_int()
+        self.check(self._lib.bmg_level_tuning(self.h, level, precision, ctypes.byref(s), ctypes.byref(t)),
+                   "bmg_level_tuning")
+        return s.value, t.value
+
     def colour_pass(self, level, colour, precision=0):
         self.check(self._lib.bmg_op_colour_pass(self.h, level, colour, precision), "colour_pass")
 
@@ -332,6 +339,12 @@ def make_options(d: Dictionary | dict | None = None, **over) -> N.Options:
     o.precision = N.PRECISION[pr]
     o.use_graph = int(_switch(d.get("graph", "on")))
     o.remove_mean = int(_switch(d.get("removeMean", "on")))
+    fused = d.get("fused", "on")
+    try:
+        o.fused = max(0, min(3, int(fused)))
+    except (TypeError, ValueError):
+        o.fused = 3 if _switch(fused) else 0
+    o.autotune = int(_switch(d.get("autotune", "on")))
     o.device = _label(d.get("device", 0))
     o.timeout_ms = _scalar(d.get("timeoutMs", 0))
     return o

@@ -85,6 +85,11 @@ typedef struct bmg_options {
     int precision;      /* precision    (fp64)                                 */
     int use_graph;      /* graph        (1): whole solve as one CUDA graph     */
     int remove_mean;    /* subtract the volume-weighted mean of x (singular)   */
+    int fused;          /* fused (3): up to this many colour passes of a
+                           smoothing step per pass over memory (1..3); 0: one
+                           launch per colour pass                              */
+    int autotune;       /* autotune (1): time the fused smoother's launch
+                           shapes per level at creation and keep the fastest   */
     int device;         /* CUDA device ordinal                                 */
     double timeout_ms;  /* wall-clock budget per solve, <= 0: none             */
 } bmg_options;
@@ -154,6 +159,10 @@ int bmg_op_prolong_correct(struct bmg_ctx* ctx, int level, int precision);
 int bmg_op_coarse_solve(struct bmg_ctx* ctx, int precision);
 /* the configured coarse solve level index */
 int bmg_coarse_level_index(const struct bmg_ctx* ctx);
+/* launch shape of the fused smoother on a level (precision 0: FP64, 1:
+ * FP32): colour stages per launch (0 when the level is smoothed pass by
+ * pass) and planes per CTA chunk, as chosen by the autotuner */
+int bmg_level_tuning(const struct bmg_ctx* ctx, int level, int precision, int* stages, int* chunk);
 
 /* ---- Residual norm without any device allocation ---------------------------
  * No counterpart in the reference: an addition for callers that must not

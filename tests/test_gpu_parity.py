@@ -246,6 +246,22 @@ def test_reference_plugin_path(native):
     assert rep.final_residual / rep.initial_residual <= 1e-10
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_graph_solve_on_legacy_default_stream(native, precision):
+    """The whole-solve graph is captured on a private stream and launched
+    on the caller's, which may be the legacy default stream (torch's)."""
+    mesh, b, _ = workloads.channel(32, seed=6)
+    c = ctx_for(mesh, relTol=1e-8, precision=precision)
+    c.set_stream(0)
+    x = np.zeros_like(b)
+    rep = c.solve(b, x, zero_guess=True)
+    assert rep.status == 0 and rep.rel_residual <= 1e-8
+    c2 = ctx_for(mesh, relTol=1e-8, precision=precision, graph="off")
+    x2 = np.zeros_like(b)
+    rep2 = c2.solve(b, x2, zero_guess=True)
+    assert rep2.cycles == rep.cycles and np.array_equal(x, x2)
+
+
 def test_status_codes(native):
     mesh, b, _ = workloads.cavity(16, seed=3)
     # not converged within maxIter
