@@ -165,6 +165,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-multibrick", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -301,6 +302,36 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item()) / world
 
+    # ---- the seven-brick mesh (2.55 M cells, one launch per level across
+    # bricks, ghost exchange on the device): FP64 and mixed ms per solve ----
+    multibrick = None
+    if not args.no_multibrick:
+        mb_mesh, mb_b, _ = workloads.multibrick(1)
+        mb_bd = torch.from_numpy(mb_b).to(f"cuda:{local}")
+        mb_x = torch.zeros_like(mb_bd)
+        multibrick = {"workload": "7 bricks (128x64x64, 96x96x96, 64x128x32, 128x32x64, 64x64x64, "
+                                  "48x96x48, 32x32x128), h = 1/128, Neumann walls, N(0,1) zero-mean RHS, "
+                                  "V(2,2), coarsest level (622 cells) direct, 1e-8",
+                      "cells": int(mb_b.size)}
+        for prec in ("fp64", "mixed"):
+            cm = bb.Context(mb_mesh, bb.make_options(dict(SOLVER_KEYS, coarseLevel=0, precision=prec,
+                                                          device=local)))
+            cm.set_stream(stream.cuda_stream)
+            for _ in range(3):
+                cm.solve(mb_bd, mb_x, zero_guess=True)
+            barrier()
+            e0.record(stream)
+            for _ in range(args.steps):
+                rep = cm.solve(mb_bd, mb_x, zero_guess=True)
+            e1.record(stream)
+            barrier()
+            if rep.status != 0:
+                raise RuntimeError(f"seven-brick solve failed: status {rep.status}")
+            multibrick[prec] = {"ms_per_solve": round(e0.elapsed_time(e1) / args.steps, 4),
+                                "cycles": rep.cycles, "rel_residual": rep.rel_residual}
+            cm.close()
+        del mb_bd, mb_x
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         times, cycles, threads = cpu_reference(args.size, steps=1)
@@ -337,6 +368,7 @@ def main():
             "e2e": {"value": round(e2e_ms, 4), "unit": "ms/solve", "h2d_bytes_per_step": 8 * n,
                     "d2h_bytes_per_step": 8 * n},
             "gpu_launches": launches, "clocks": clocks,
+            "multibrick": multibrick,
         }
         print(json.dumps(line), flush=True)
     for cc in ctx.values():

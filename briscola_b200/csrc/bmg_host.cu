@@ -1,6 +1,7 @@
-// bmg_host.cu -- host side of the B200 multigrid solver: level hierarchy,
-// geometry tables, the V/W/F cycle driver, mixed-precision refinement and
-// the C ABI declared in include/bmg.h.
+// bmg_host.cu -- host side of the B200 multigrid solver: level hierarchy of
+// one or more bricks, geometry tables, inter-brick ghost lists, the V/W/F
+// cycle driver, mixed-precision refinement, the whole-solve CUDA graph, the
+// launch-shape autotuner and the C ABI declared in include/bmg.h.
 //
 // Reference behaviour followed (paths relative to the Briscola tree, with
 // FV = src/briscolaFiniteVolume):
@@ -13,6 +14,7 @@
 //   pin + coarse solve   FV/solvers/solver/solver.C:201-231, FV/solvers/externalSolvers/APLU/APLU.C:26-128
 //   transfers            linearRestrictionScheme.C:15-187, linearProlongationScheme.C:12-147,
 //                        areaWeightedFaceRestrictionScheme.C:19-57
+//   brick contacts       FV/boundaryConditions/parallelBoundaryCondition/parallelBoundaryCondition.C:84-174
 
 #include "../../include/bmg.h"
 #include "bmg_internal.h"
@@ -35,13 +37,34 @@ struct Axis {
     std::vector<double> h;    // n+2 entries, same indexing
 };
 
-struct HostLevel {
+// one brick on one level
+struct HostBrick {
     int n[3] = {0, 0, 0};
-    int R[3] = {1, 1, 1};  // ratio to the parent level
+    int R[3] = {1, 1, 1};     // ratio to the parent level
+    int origin[3] = {0, 0, 0};  // cell offset in the level's global lattice
     Axis ax[3];
-    long si = 0, sj = 0, base = 0, cells = 0;
-    TabOff to{};
-    std::vector<double> tab;  // host copy of the 1-D tables
+    bool open[6] = {false, false, false, false, false, false};  // periodic or touching another brick
+    int nbr[6] = {-1, -1, -1, -1, -1, -1};  // a brick touching the face (its ghost points come from it)
+    long si = 0, sj = 0;      // strides
+    long off = 0;             // slab offset of the brick's block
+    long base = 0;            // slab index of interior cell (0,0,0)
+    long cells = 0;           // size of the brick's block
+    long cbase = 0;           // offset in compact arrays
+    TabOff to{};              // offsets into the level's table
+    int cpar = 0;
+    std::vector<double> lam_user[3];  // restricted user lambda, block-local indexing
+    long ncell() const { return (long)n[0] * n[1] * n[2]; }
+    long at(int i, int j, int k) const { return base + (long)i * si + (long)j * sj + k; }
+    long loc(int i, int j, int k) const { return at(i, j, k) - off; }
+};
+
+struct HostLevel {
+    std::vector<HostBrick> br;
+    long cells = 0;   // slab size
+    long ncell = 0;   // interior cells of all bricks
+    int planes = 0;   // sum of n0
+    std::vector<double> tab;  // 1-D tables of all bricks
+    std::vector<double> lam_host[3];  // face lambda of the slab (variable coefficient)
     double* x64 = nullptr;
     double* b64 = nullptr;
     float* x32 = nullptr;
@@ -50,20 +73,21 @@ struct HostLevel {
     float* tab32 = nullptr;
     double* lam64[3] = {nullptr, nullptr, nullptr};
     float* lam32[3] = {nullptr, nullptr, nullptr};
-    std::vector<double> lam_host[3];  // ghost-framed face lambda (variable coefficient)
     double* jtmp64 = nullptr;
     float* jtmp32 = nullptr;
     double* x64b = nullptr;  // second x buffers: fused smoothing writes here, then swaps
     float* x32b = nullptr;
-    bool fusedOK = false;    // level large enough for the fused smoother
+    bool fusedOK = false;    // single brick large enough for the fused smoother
     // per precision (0: FP64, 1: FP32), picked by autotune():
     int fusedS[2] = {kFusedMaxStages, kFusedMaxStages};  // colour stages per fused launch
     int fusedTi[2] = {64, 64};                             // planes per CTA chunk
-    long ncell() const { return (long)n[0] * n[1] * n[2]; }
-    long at(int i, int j, int k) const { return base + (long)i * si + (long)j * sj + k; }
+    // ghost refresh between bricks: slab[gdst[q]] = slab[gsrc[q]]
+    int* gdst = nullptr;
+    int* gsrc = nullptr;
+    long nghost = 0;
 };
 
-struct HostTransfer {
+struct BrickTransfer {
     double* ratio64 = nullptr;
     float* ratio32 = nullptr;
     int* pidx = nullptr;
@@ -92,15 +116,18 @@ struct BadArg {
 
 struct bmg_ctx {
     bmg_options opt{};
-    int periodic[3] = {0, 0, 0};
+    int periodic[3] = {0, 0, 0};  // single brick only
+    bool multi = false;           // more than one brick
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     std::vector<HostLevel> lv;
-    std::vector<HostTransfer> tr;
+    std::vector<std::vector<BrickTransfer>> tr;  // [level][brick]
     int lc = 0;  // coarse solve level
     double* ainv = nullptr;
+    int* cidx = nullptr;
     int ncoarse = 0;
-    bool variable = false;
+    bool userLambda = false;  // a variable coefficient was given
+    bool variable = false;    // kernels read face lambdas (user lambda or brick contacts)
     double* partials = nullptr;
     SolveState* st = nullptr;
     SolveState* st_host = nullptr;
@@ -124,16 +151,18 @@ namespace {
 // ---------------------------------------------------------------------------
 // geometry
 // ---------------------------------------------------------------------------
-void finishAxis(Axis& a, int n, bool periodic) {
+// levelPoints.C:198-236 (walls: project by one spacing) and :326-400
+// (periodic: the opposite side's spacing).  A face touching another brick
+// takes the neighbour's point (glo / ghi, NaN where there is none), as the
+// reference's processor-boundary ghost points do.
+void finishAxis(Axis& a, int n, bool periodic, double glo, double ghi) {
     std::vector<double>& p = a.pts;
-    // levelPoints.C:198-236 (walls: project by one spacing) and :326-400
-    // (periodic: the opposite side's spacing)
     if (periodic) {
         p[0] = p[1] - (p[n + 1] - p[n]);
         p[n + 2] = p[n + 1] + (p[2] - p[1]);
     } else {
-        p[0] = p[1] + (p[1] - p[2]);
-        p[n + 2] = p[n + 1] + (p[n + 1] - p[n]);
+        p[0] = std::isnan(glo) ? p[1] + (p[1] - p[2]) : glo;
+        p[n + 2] = std::isnan(ghi) ? p[n + 1] + (p[n + 1] - p[n]) : ghi;
     }
     a.cc.assign(n + 2, 0.0);
     a.h.assign(n + 2, 0.0);
@@ -145,89 +174,123 @@ void finishAxis(Axis& a, int n, bool periodic) {
 
 // Rows of pitch p2 = round_up(n2 + 5, 4) with interior k = 0 at offset 4:
 // rows and interiors start on 16-byte (FP32) / 32-byte (FP64) boundaries so
-// pairs and quads of k-neighbours load as one vector; the k ghosts sit at
-// offsets 3 and n2 + 4.
+// pairs of k-neighbours load as one vector; the k ghosts sit at offsets 3
+// and n2 + 4.  Bricks follow one another in the slab.
 void layout(HostLevel& L) {
-    const long p2 = ((L.n[2] + 5) + 3) / 4 * 4, p1 = L.n[1] + 2, p0 = L.n[0] + 2;
-    L.sj = p2;
-    L.si = p1 * p2;
-    L.base = L.si + L.sj + 4;
-    L.cells = p0 * p1 * p2;
+    long off = 0, coff = 0;
+    int planes = 0;
+    for (auto& B : L.br) {
+        const long p2 = ((B.n[2] + 5) + 3) / 4 * 4, p1 = B.n[1] + 2, p0 = B.n[0] + 2;
+        B.sj = p2;
+        B.si = p1 * p2;
+        B.off = off;
+        B.base = off + B.si + B.sj + 4;
+        B.cells = p0 * p1 * p2;
+        B.cbase = coff;
+        B.cpar = (B.origin[0] + B.origin[1] + B.origin[2]) & 1;
+        off += B.cells;
+        coff += B.ncell();
+        planes += B.n[0];
+    }
+    L.cells = off;
+    L.ncell = coff;
+    L.planes = planes;
 }
 
 // row-scaled couplings (A'/V): lower neighbour delta(i)/h(i), upper
-// delta(i+1)/h(i); zero across a wall, i.e. after the Neumann elimination
-void buildTables(HostLevel& L, const int periodic[3]) {
-    TabOff& to = L.to;
+// delta(i+1)/h(i); zero across a wall face, i.e. after the Neumann
+// elimination.  Faces touching another brick keep their coupling and get
+// their wall parts zeroed through the face lambdas.
+void buildTables(HostLevel& L) {
     int off = 0;
-    for (int d = 0; d < 3; ++d) {
-        to.wl[d] = off;
-        off += L.n[d];
-        to.wh[d] = off;
-        off += L.n[d];
-        to.h[d] = off;
-        off += L.n[d];
-    }
-    to.total = off;
-    L.tab.assign(off, 0.0);
-    for (int d = 0; d < 3; ++d) {
-        const Axis& a = L.ax[d];
-        const int n = L.n[d];
-        for (int i = 0; i < n; ++i) {
-            const double hi = a.h[i + 1];
-            const double dlo = 1.0 / std::fabs(a.cc[i + 1] - a.cc[i]);
-            const double dhi = 1.0 / std::fabs(a.cc[i + 2] - a.cc[i + 1]);
-            double wl = dlo / hi, wh = dhi / hi;
-            if (!periodic[d] && i == 0) wl = 0.0;
-            if (!periodic[d] && i == n - 1) wh = 0.0;
-            L.tab[to.wl[d] + i] = wl;
-            L.tab[to.wh[d] + i] = wh;
-            L.tab[to.h[d] + i] = hi;
+    L.tab.clear();
+    for (auto& B : L.br) {
+        TabOff& to = B.to;
+        for (int d = 0; d < 3; ++d) {
+            to.wl[d] = off;
+            off += B.n[d];
+            to.wh[d] = off;
+            off += B.n[d];
+            to.h[d] = off;
+            off += B.n[d];
+        }
+        to.total = off;
+        L.tab.resize(off, 0.0);
+        for (int d = 0; d < 3; ++d) {
+            const Axis& a = B.ax[d];
+            const int n = B.n[d];
+            for (int i = 0; i < n; ++i) {
+                const double hi = a.h[i + 1];
+                const double dlo = 1.0 / std::fabs(a.cc[i + 1] - a.cc[i]);
+                const double dhi = 1.0 / std::fabs(a.cc[i + 2] - a.cc[i + 1]);
+                double wl = dlo / hi, wh = dhi / hi;
+                if (!B.open[2 * d] && i == 0) wl = 0.0;
+                if (!B.open[2 * d + 1] && i == n - 1) wh = 0.0;
+                L.tab[to.wl[d] + i] = wl;
+                L.tab[to.wh[d] + i] = wh;
+                L.tab[to.h[d] + i] = hi;
+            }
         }
     }
 }
 
 template <typename T>
-LevelView<T> view(const bmg_ctx* c, int l) {
-    const HostLevel& L = c->lv[l];
-    LevelView<T> v{};
-    v.n0 = L.n[0];
-    v.n1 = L.n[1];
-    v.n2 = L.n[2];
-    v.si = L.si;
-    v.sj = L.sj;
-    v.base = L.base;
-    v.cells = L.cells;
-    v.to = L.to;
-    v.tab64 = L.tab64;
-    if constexpr (sizeof(T) == 8) {
-        v.x = reinterpret_cast<T*>(L.x64);
-        v.b = reinterpret_cast<T*>(L.b64);
-        v.tab = reinterpret_cast<const T*>(L.tab64);
-        for (int d = 0; d < 3; ++d) (&v.lam0)[d] = reinterpret_cast<const T*>(L.lam64[d]);
-    } else {
-        v.x = reinterpret_cast<T*>(L.x32);
-        v.b = reinterpret_cast<T*>(L.b32);
-        v.tab = reinterpret_cast<const T*>(L.tab32);
-        for (int d = 0; d < 3; ++d) (&v.lam0)[d] = reinterpret_cast<const T*>(L.lam32[d]);
+Bricks<T> bricks(const bmg_ctx* c, int l) {
+    const HostLevel& H = c->lv[l];
+    Bricks<T> B{};
+    B.nb = (int)H.br.size();
+    int z = 0;
+    for (int b = 0; b < B.nb; ++b) {
+        const HostBrick& K = H.br[b];
+        LevelView<T>& v = B.v[b];
+        v.n0 = K.n[0];
+        v.n1 = K.n[1];
+        v.n2 = K.n[2];
+        v.si = K.si;
+        v.sj = K.sj;
+        v.base = K.base;
+        v.cells = H.cells;
+        v.cbase = K.cbase;
+        v.to = K.to;
+        v.tab64 = H.tab64;
+        if constexpr (sizeof(T) == 8) {
+            v.x = reinterpret_cast<T*>(H.x64);
+            v.b = reinterpret_cast<T*>(H.b64);
+            v.tab = reinterpret_cast<const T*>(H.tab64);
+            for (int d = 0; d < 3; ++d) (&v.lam0)[d] = reinterpret_cast<const T*>(H.lam64[d]);
+        } else {
+            v.x = reinterpret_cast<T*>(H.x32);
+            v.b = reinterpret_cast<T*>(H.b32);
+            v.tab = reinterpret_cast<const T*>(H.tab32);
+            for (int d = 0; d < 3; ++d) (&v.lam0)[d] = reinterpret_cast<const T*>(H.lam32[d]);
+        }
+        v.per0 = c->periodic[0];
+        v.per1 = c->periodic[1];
+        v.per2 = c->periodic[2];
+        v.cpar = K.cpar;
+        B.z0[b] = z;
+        z += K.n[0];
+        B.max1 = std::max(B.max1, K.n[1]);
+        B.max2 = std::max(B.max2, K.n[2]);
     }
-    v.per0 = c->periodic[0];
-    v.per1 = c->periodic[1];
-    v.per2 = c->periodic[2];
-    return v;
+    B.z0[B.nb] = z;
+    return B;
 }
 
-TransferTabs ttabs(const bmg_ctx* c, int l) {
-    const HostTransfer& t = c->tr[l];
-    TransferTabs s{};
-    s.ratio64 = t.ratio64;
-    s.ratio32 = t.ratio32;
-    s.pidx = t.pidx;
-    s.pw64 = t.pw64;
-    s.pw32 = t.pw32;
-    s.R0 = t.R[0];
-    s.R1 = t.R[1];
-    s.R2 = t.R[2];
+TransferSet ttabs(const bmg_ctx* c, int l) {
+    TransferSet s{};
+    for (size_t b = 0; b < c->tr[l].size(); ++b) {
+        const BrickTransfer& t = c->tr[l][b];
+        TransferTabs& u = s.t[b];
+        u.ratio64 = t.ratio64;
+        u.ratio32 = t.ratio32;
+        u.pidx = t.pidx;
+        u.pw64 = t.pw64;
+        u.pw32 = t.pw32;
+        u.R0 = t.R[0];
+        u.R1 = t.R[1];
+        u.R2 = t.R[2];
+    }
     return s;
 }
 
@@ -286,70 +349,123 @@ bool invert(std::vector<double>& M, int n, std::vector<double>& inv) {
     return true;
 }
 
+// brick of a level containing global lattice cell g, with the local cell
+int findBrick(const HostLevel& L, const int g[3], int loc[3]) {
+    for (size_t b = 0; b < L.br.size(); ++b) {
+        const HostBrick& B = L.br[b];
+        bool in = true;
+        for (int d = 0; d < 3; ++d) {
+            loc[d] = g[d] - B.origin[d];
+            in = in && loc[d] >= 0 && loc[d] < B.n[d];
+        }
+        if (in) return (int)b;
+    }
+    return -1;
+}
+
+// coupling of interior cell (b; i,j,k) through stencil slot s (0..5: axis 0
+// lower/upper, axis 1, axis 2), as the kernels form it
+double couplingOf(const bmg_ctx* c, const HostLevel& L, int b, int i, int j, int k, int s) {
+    const HostBrick& B = L.br[b];
+    const int d = s / 2;
+    const bool up = s % 2;
+    const int ijk[3] = {i, j, k};
+    double w = L.tab[(up ? B.to.wh[d] : B.to.wl[d]) + ijk[d]];
+    if (c->variable) {
+        long fc = B.at(i, j, k);
+        if (up) fc += d == 0 ? B.si : d == 1 ? B.sj : 1;
+        w *= L.lam_host[d][fc];
+    }
+    return w;
+}
+
 // Dense row-scaled operator of the coarse solve level with the singularity
-// pin of solver.C:201-231 (row of cell 0 = identity, every coupling to cell
-// 0 removed, periodic images included), inverted once per matrix.
+// pin of solver.C:201-231 (row of the first cell = identity, every coupling
+// to it removed, periodic images included), inverted once per matrix.
+// Unknowns: bricks one after another, k fastest.
 void buildCoarseInverse(bmg_ctx* c) {
     const HostLevel& L = c->lv[c->lc];
-    const int n = (int)L.ncell();
+    const int n = (int)L.ncell;
     std::vector<double> M((size_t)n * n, 0.0);
-    auto num = [&](int i, int j, int k) { return ((long)i * L.n[1] + j) * L.n[2] + k; };
-    for (int i = 0; i < L.n[0]; ++i)
-        for (int j = 0; j < L.n[1]; ++j)
-            for (int k = 0; k < L.n[2]; ++k) {
-                const long row = num(i, j, k);
-                const int ijk[3] = {i, j, k};
-                double diag = 0.0;
-                for (int s = 0; s < 6; ++s) {
-                    const int d = s / 2;
-                    const bool up = s % 2;
-                    double w = L.tab[(up ? L.to.wh[d] : L.to.wl[d]) + ijk[d]];
-                    if (c->variable) {
-                        long fc = L.at(i, j, k);
-                        if (up) fc += d == 0 ? L.si : d == 1 ? L.sj : 1;
-                        w *= L.lam_host[d][fc];
+    std::vector<int> cidx(n);
+    for (int b = 0; b < (int)L.br.size(); ++b) {
+        const HostBrick& B = L.br[b];
+        for (int i = 0; i < B.n[0]; ++i)
+            for (int j = 0; j < B.n[1]; ++j)
+                for (int k = 0; k < B.n[2]; ++k) {
+                    const long row = B.cbase + ((long)i * B.n[1] + j) * B.n[2] + k;
+                    cidx[row] = (int)B.at(i, j, k);
+                    double diag = 0.0;
+                    for (int s = 0; s < 6; ++s) {
+                        const double w = couplingOf(c, L, b, i, j, k, s);
+                        if (w == 0.0) continue;
+                        const int d = s / 2;
+                        int nbl[3] = {i, j, k};
+                        nbl[d] += (s % 2) ? 1 : -1;
+                        long col;
+                        if (nbl[d] >= 0 && nbl[d] < B.n[d]) {
+                            col = B.cbase + ((long)nbl[0] * B.n[1] + nbl[1]) * B.n[2] + nbl[2];
+                        } else if (c->periodic[d]) {
+                            nbl[d] = (nbl[d] + B.n[d]) % B.n[d];
+                            col = B.cbase + ((long)nbl[0] * B.n[1] + nbl[1]) * B.n[2] + nbl[2];
+                        } else {
+                            const int g[3] = {B.origin[0] + nbl[0], B.origin[1] + nbl[1], B.origin[2] + nbl[2]};
+                            int loc[3];
+                            const int nb = findBrick(L, g, loc);
+                            if (nb < 0) continue;  // wall (zero lambda keeps us from getting here)
+                            const HostBrick& N = L.br[nb];
+                            col = N.cbase + ((long)loc[0] * N.n[1] + loc[1]) * N.n[2] + loc[2];
+                        }
+                        diag -= w;
+                        M[(size_t)row * n + col] += w;
                     }
-                    if (w == 0.0) continue;
-                    diag -= w;
-                    int nb[3] = {i, j, k};
-                    nb[d] += up ? 1 : -1;
-                    nb[d] = (nb[d] + L.n[d]) % L.n[d];
-                    M[(size_t)row * n + num(nb[0], nb[1], nb[2])] += w;
+                    M[(size_t)row * n + row] += diag;
                 }
-                M[(size_t)row * n + row] += diag;
-            }
+    }
     for (int j = 0; j < n; ++j) M[j] = j == 0 ? 1.0 : 0.0;
     for (int r = 1; r < n; ++r) M[(size_t)r * n] = 0.0;
     std::vector<double> inv;
     if (!invert(M, n, inv)) throw BadArg{BMG_BAD_ARG, "coarse level matrix is singular"};
     if (!c->ainv || c->ncoarse != n) {
         if (c->ainv) cudaFree(c->ainv);
+        if (c->cidx) cudaFree(c->cidx);
         c->ainv = dalloc<double>((size_t)n * n);
+        c->cidx = dalloc<int>(n);
     }
     c->ncoarse = n;
     upload(c->ainv, inv);
+    upload(c->cidx, cidx);
+}
+
+void destroyGraph(bmg_ctx* c) {
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    c->gexec = nullptr;
+    c->graph = nullptr;
 }
 
 void freeAll(bmg_ctx* c) {
     for (auto& L : c->lv) {
-        for (void* p : {(void*)L.x64, (void*)L.b64, (void*)L.x32, (void*)L.b32, (void*)L.tab64,
-                        (void*)L.tab32, (void*)L.jtmp64, (void*)L.jtmp32, (void*)L.x64b, (void*)L.x32b})
+        for (void* p : {(void*)L.x64, (void*)L.b64, (void*)L.x32, (void*)L.b32, (void*)L.tab64, (void*)L.tab32,
+                        (void*)L.jtmp64, (void*)L.jtmp32, (void*)L.x64b, (void*)L.x32b, (void*)L.gdst,
+                        (void*)L.gsrc})
             if (p) cudaFree(p);
         for (int d = 0; d < 3; ++d) {
             if (L.lam64[d]) cudaFree(L.lam64[d]);
             if (L.lam32[d]) cudaFree(L.lam32[d]);
         }
     }
-    for (auto& t : c->tr)
-        for (void* p : {(void*)t.ratio64, (void*)t.ratio32, (void*)t.pidx, (void*)t.pw64, (void*)t.pw32})
-            if (p) cudaFree(p);
-    for (void* p : {(void*)c->ainv, (void*)c->partials, (void*)c->st, (void*)c->stage_b, (void*)c->stage_x})
+    for (auto& lt : c->tr)
+        for (auto& t : lt)
+            for (void* p : {(void*)t.ratio64, (void*)t.ratio32, (void*)t.pidx, (void*)t.pw64, (void*)t.pw32})
+                if (p) cudaFree(p);
+    for (void* p : {(void*)c->ainv, (void*)c->cidx, (void*)c->partials, (void*)c->st, (void*)c->stage_b,
+                    (void*)c->stage_x})
         if (p) cudaFree(p);
     if (c->st_host) cudaFreeHost(c->st_host);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
-    if (c->gexec) cudaGraphExecDestroy(c->gexec);
-    if (c->graph) cudaGraphDestroy(c->graph);
+    destroyGraph(c);
     if (c->capStream) cudaStreamDestroy(c->capStream);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
 }
@@ -365,134 +481,348 @@ void validateOptions(const bmg_options* o) {
     if (o->fused < 0) throw BadArg{BMG_BAD_ARG, "negative fused stage count"};
 }
 
-void build(bmg_ctx* c, const bmg_mesh_desc* mesh) {
+// Level-0 bricks from the mesh description; contacts between bricks.
+void readBricks(bmg_ctx* c, const bmg_mesh_desc* mesh, HostLevel& L0) {
     if (!mesh || mesh->n_bricks < 1 || !mesh->bricks) throw BadArg{BMG_BAD_ARG, "empty mesh"};
-    if (mesh->n_bricks != 1)
-        throw BadArg{BMG_UNSUPPORTED, "this build solves single-brick meshes"};
-    const bmg_brick& B = mesh->bricks[0];
-    for (int d = 0; d < 3; ++d) {
-        if (B.n[d] < 1) throw BadArg{BMG_BAD_ARG, "brick with fewer than one cell along an axis"};
-        if (!B.points[d]) throw BadArg{BMG_BAD_ARG, "missing vertex coordinates"};
-        for (int q = 0; q < B.n[d]; ++q)
-            if (!(B.points[d][q + 1] > B.points[d][q]))
-                throw BadArg{BMG_BAD_ARG, "vertex coordinates must increase strictly"};
-        const int lo = B.bc[2 * d], hi = B.bc[2 * d + 1];
-        if ((lo == BMG_BC_PERIODIC) != (hi == BMG_BC_PERIODIC))
-            throw BadArg{BMG_BAD_ARG, "periodic faces must come in opposite pairs"};
-        if ((lo != BMG_BC_PERIODIC && lo != BMG_BC_NEUMANN) || (hi != BMG_BC_PERIODIC && hi != BMG_BC_NEUMANN))
-            throw BadArg{BMG_UNSUPPORTED, "boundary condition type not supported"};
-        c->periodic[d] = lo == BMG_BC_PERIODIC;
-    }
-    // mesh.C:19-53: levels while coarsen(N) != N
-    HostLevel L0;
-    for (int d = 0; d < 3; ++d) {
-        L0.n[d] = B.n[d];
-        L0.ax[d].pts.assign(B.n[d] + 3, 0.0);
-        for (int q = 0; q <= B.n[d]; ++q) L0.ax[d].pts[q + 1] = B.points[d][q];
-        finishAxis(L0.ax[d], B.n[d], c->periodic[d]);
-    }
-    c->lv.push_back(std::move(L0));
-    for (;;) {
-        const HostLevel& F = c->lv.back();
-        int nc[3];
-        bool same = true;
+    const int nb = mesh->n_bricks;
+    if (nb > kMaxBricks) throw BadArg{BMG_UNSUPPORTED, "more bricks than this build handles (8)"};
+    c->multi = nb > 1;
+    for (int b = 0; b < nb; ++b) {
+        const bmg_brick& B = mesh->bricks[b];
+        HostBrick K;
         for (int d = 0; d < 3; ++d) {
-            nc[d] = F.n[d] <= 3 ? F.n[d] : F.n[d] / 2;
-            if (F.n[d] > 3 && F.n[d] % 2)
+            if (B.n[d] < 1) throw BadArg{BMG_BAD_ARG, "brick with fewer than one cell along an axis"};
+            if (!B.points[d]) throw BadArg{BMG_BAD_ARG, "missing vertex coordinates"};
+            for (int q = 0; q < B.n[d]; ++q)
+                if (!(B.points[d][q + 1] > B.points[d][q]))
+                    throw BadArg{BMG_BAD_ARG, "vertex coordinates must increase strictly"};
+            const int lo = B.bc[2 * d], hi = B.bc[2 * d + 1];
+            if ((lo == BMG_BC_PERIODIC) != (hi == BMG_BC_PERIODIC))
+                throw BadArg{BMG_BAD_ARG, "periodic faces must come in opposite pairs"};
+            if ((lo != BMG_BC_PERIODIC && lo != BMG_BC_NEUMANN) || (hi != BMG_BC_PERIODIC && hi != BMG_BC_NEUMANN))
+                throw BadArg{BMG_UNSUPPORTED, "boundary condition type not supported"};
+            if (lo == BMG_BC_PERIODIC && c->multi)
+                throw BadArg{BMG_UNSUPPORTED, "periodic faces on multi-brick meshes are not supported"};
+            if (!c->multi) c->periodic[d] = lo == BMG_BC_PERIODIC;
+            K.n[d] = B.n[d];
+            K.origin[d] = c->multi ? B.origin[d] : 0;
+            K.ax[d].pts.assign(B.n[d] + 3, 0.0);
+            for (int q = 0; q <= B.n[d]; ++q) K.ax[d].pts[q + 1] = B.points[d][q];
+            K.open[2 * d] = K.open[2 * d + 1] = c->periodic[d];
+        }
+        L0.br.push_back(std::move(K));
+    }
+    if (!c->multi) return;
+    // bricks must not overlap; faces in the same plane with overlapping
+    // extents are contacts, which need matching vertex coordinates
+    for (int a = 0; a < nb; ++a)
+        for (int b = a + 1; b < nb; ++b) {
+            const HostBrick& A = L0.br[a];
+            const HostBrick& B = L0.br[b];
+            long overlap = 1;
+            for (int d = 0; d < 3; ++d)
+                overlap *= std::max(0, std::min(A.origin[d] + A.n[d], B.origin[d] + B.n[d]) -
+                                           std::max(A.origin[d], B.origin[d]));
+            if (overlap > 0) throw BadArg{BMG_BAD_ARG, "bricks overlap"};
+        }
+    for (int a = 0; a < nb; ++a)
+        for (int b = 0; b < nb; ++b) {
+            if (a == b) continue;
+            HostBrick& A = L0.br[a];
+            const HostBrick& B = L0.br[b];
+            for (int d = 0; d < 3; ++d) {
+                if (A.origin[d] + A.n[d] != B.origin[d]) continue;  // A's upper face meets B's lower face
+                const int t1 = (d + 1) % 3, t2 = (d + 2) % 3;
+                const int lo1 = std::max(A.origin[t1], B.origin[t1]);
+                const int hi1 = std::min(A.origin[t1] + A.n[t1], B.origin[t1] + B.n[t1]);
+                const int lo2 = std::max(A.origin[t2], B.origin[t2]);
+                const int hi2 = std::min(A.origin[t2] + A.n[t2], B.origin[t2] + B.n[t2]);
+                if (hi1 <= lo1 || hi2 <= lo2) continue;
+                const double scale = std::fabs(A.ax[d].pts[A.n[d] + 1] - A.ax[d].pts[1]) + 1.0;
+                const double tol = 1e-12 * scale;
+                if (std::fabs(A.ax[d].pts[A.n[d] + 1] - B.ax[d].pts[1]) > tol)
+                    throw BadArg{BMG_BAD_ARG, "bricks meet on a lattice face but their coordinates differ"};
+                for (int t : {t1, t2}) {
+                    const int lo = t == t1 ? lo1 : lo2, hi = t == t1 ? hi1 : hi2;
+                    for (int g = lo; g <= hi; ++g)
+                        if (std::fabs(A.ax[t].pts[g - A.origin[t] + 1] - B.ax[t].pts[g - B.origin[t] + 1]) > tol)
+                            throw BadArg{BMG_BAD_ARG, "brick contact is not cell-conforming"};
+                }
+                A.open[2 * d + 1] = true;
+                L0.br[b].open[2 * d] = true;
+                if (A.nbr[2 * d + 1] < 0) A.nbr[2 * d + 1] = b;
+                if (L0.br[b].nbr[2 * d] < 0) L0.br[b].nbr[2 * d] = a;
+            }
+        }
+}
+
+// Coarse level: halve every extent (single brick: the reference's rule,
+// dimensions of 3 or fewer cells stay; several bricks: all bricks halve in
+// every direction together, so contacts stay cell-conforming).
+bool coarsenLevel(const bmg_ctx* c, const HostLevel& F, HostLevel& C) {
+    bool anyChange = false;
+    if (!c->multi) {
+        const HostBrick& B = F.br[0];
+        HostBrick K;
+        for (int d = 0; d < 3; ++d) {
+            const int nc = B.n[d] <= 3 ? B.n[d] : B.n[d] / 2;
+            if (B.n[d] > 3 && B.n[d] % 2)
                 throw BadArg{BMG_BAD_ARG, "non-coarsenable brick size (an extent above 3 is odd on some level)"};
-            same = same && nc[d] == F.n[d];
+            anyChange = anyChange || nc != B.n[d];
+            K.n[d] = nc;
+            K.R[d] = B.n[d] / nc;
         }
-        if (same) break;
-        HostLevel C;
+        if (!anyChange) return false;
         for (int d = 0; d < 3; ++d) {
-            C.n[d] = nc[d];
-            C.R[d] = F.n[d] / nc[d];
-            C.ax[d].pts.assign(nc[d] + 3, 0.0);
-            for (int q = 0; q <= nc[d]; ++q) C.ax[d].pts[q + 1] = F.ax[d].pts[q * C.R[d] + 1];
-            finishAxis(C.ax[d], nc[d], c->periodic[d]);
+            K.ax[d].pts.assign(K.n[d] + 3, 0.0);
+            for (int q = 0; q <= K.n[d]; ++q) K.ax[d].pts[q + 1] = B.ax[d].pts[q * K.R[d] + 1];
+            K.open[2 * d] = K.open[2 * d + 1] = c->periodic[d];
         }
+        C.br.push_back(std::move(K));
+        return true;
+    }
+    for (const auto& B : F.br)
+        for (int d = 0; d < 3; ++d)
+            if (B.n[d] < 4 || B.n[d] % 2 || B.origin[d] % 2) return false;
+    for (const auto& B : F.br) {
+        HostBrick K;
+        for (int d = 0; d < 3; ++d) {
+            K.n[d] = B.n[d] / 2;
+            K.R[d] = 2;
+            K.origin[d] = B.origin[d] / 2;
+            K.ax[d].pts.assign(K.n[d] + 3, 0.0);
+            for (int q = 0; q <= K.n[d]; ++q) K.ax[d].pts[q + 1] = B.ax[d].pts[2 * q + 1];
+        }
+        for (int f = 0; f < 6; ++f) {
+            K.open[f] = B.open[f];
+            K.nbr[f] = B.nbr[f];
+        }
+        C.br.push_back(std::move(K));
+    }
+    return true;
+}
+
+// ghost points and cell tables of every brick of a level; every brick
+// touching a face must agree on the ghost point it gives
+void finishLevel(const bmg_ctx* c, HostLevel& L) {
+    for (auto& B : L.br)
+        for (int d = 0; d < 3; ++d) {
+            double g[2] = {NAN, NAN};
+            for (int side = 0; side < 2; ++side) {
+                if (B.nbr[2 * d + side] < 0) continue;
+                const HostBrick& N = L.br[B.nbr[2 * d + side]];
+                g[side] = side ? N.ax[d].pts[2] : N.ax[d].pts[N.n[d]];
+                for (const auto& M : L.br) {
+                    if (&M == &B || &M == &N) continue;
+                    // another brick across the same face plane, overlapping it
+                    const int plane = side ? B.origin[d] + B.n[d] : B.origin[d];
+                    if ((side ? M.origin[d] : M.origin[d] + M.n[d]) != plane) continue;
+                    bool touch = true;
+                    for (int t : {(d + 1) % 3, (d + 2) % 3})
+                        touch = touch && std::min(B.origin[t] + B.n[t], M.origin[t] + M.n[t]) >
+                                             std::max(B.origin[t], M.origin[t]);
+                    if (!touch) continue;
+                    const double gm = side ? M.ax[d].pts[2] : M.ax[d].pts[M.n[d]];
+                    const double h = std::fabs(B.ax[d].pts[side ? B.n[d] + 1 : 1] - g[side]);
+                    if (std::fabs(gm - g[side]) > 1e-9 * h)
+                        throw BadArg{BMG_UNSUPPORTED,
+                                     "bricks touching one face have different cell sizes normal to it"};
+                }
+            }
+            finishAxis(B.ax[d], B.n[d], c->periodic[d], g[0], g[1]);
+        }
+}
+
+// face lambdas of a multi-brick level: 1 inside bricks and where a face
+// touches another brick, 0 on the wall parts of open faces
+void contactMask(const HostLevel& L, std::vector<double> mask[3]) {
+    for (int d = 0; d < 3; ++d) mask[d].assign(L.cells, 1.0);
+    for (const auto& B : L.br)
+        for (int d = 0; d < 3; ++d)
+            for (int side = 0; side < 2; ++side) {
+                if (!B.open[2 * d + side]) continue;
+                const int t1 = (d + 1) % 3, t2 = (d + 2) % 3;
+                for (int u = 0; u < B.n[t1]; ++u)
+                    for (int v = 0; v < B.n[t2]; ++v) {
+                        int cell[3];
+                        cell[d] = side ? B.n[d] - 1 : 0;
+                        cell[t1] = u;
+                        cell[t2] = v;
+                        int g[3] = {B.origin[0] + cell[0], B.origin[1] + cell[1], B.origin[2] + cell[2]};
+                        g[d] += side ? 1 : -1;
+                        int loc[3];
+                        const bool touch = findBrick(L, g, loc) >= 0;
+                        int face[3] = {cell[0], cell[1], cell[2]};
+                        if (side) face[d] += 1;  // upper face = lower face of the next cell
+                        mask[d][B.at(face[0], face[1], face[2])] = touch ? 1.0 : 0.0;
+                    }
+            }
+}
+
+// Ghost frame of every brick: from the brick that owns the position, else a
+// zero-gradient copy of the brick's own nearest cell (what the reference's
+// unset-boundary copies give at walls, meshLevel.C:301-328).
+void ghostList(const HostLevel& L, std::vector<int>& dst, std::vector<int>& src) {
+    dst.clear();
+    src.clear();
+    for (const auto& B : L.br)
+        for (int i = -1; i <= B.n[0]; ++i)
+            for (int j = -1; j <= B.n[1]; ++j)
+                for (int k = -1; k <= B.n[2]; ++k) {
+                    const int l3[3] = {i, j, k};
+                    bool ghost = false;
+                    for (int d = 0; d < 3; ++d) ghost = ghost || l3[d] < 0 || l3[d] >= B.n[d];
+                    if (!ghost) continue;
+                    const int g[3] = {B.origin[0] + i, B.origin[1] + j, B.origin[2] + k};
+                    int loc[3];
+                    const int nb = findBrick(L, g, loc);
+                    long s;
+                    if (nb >= 0) {
+                        s = L.br[nb].at(loc[0], loc[1], loc[2]);
+                    } else {
+                        const int ci = std::min(std::max(i, 0), B.n[0] - 1);
+                        const int cj = std::min(std::max(j, 0), B.n[1] - 1);
+                        const int ck = std::min(std::max(k, 0), B.n[2] - 1);
+                        s = B.at(ci, cj, ck);
+                    }
+                    dst.push_back((int)B.at(i, j, k));
+                    src.push_back((int)s);
+                }
+}
+
+// face lambdas on the device: restricted user lambda (if any) times the
+// contact mask (multi-brick), per level
+void uploadLambda(bmg_ctx* c) {
+    for (auto& L : c->lv) {
+        std::vector<double> mask[3];
+        if (c->multi) contactMask(L, mask);
+        for (int d = 0; d < 3; ++d) {
+            L.lam_host[d].assign(L.cells, c->multi ? 0.0 : 1.0);
+            for (const auto& B : L.br)
+                for (long q = 0; q < B.cells; ++q) {
+                    double v = c->userLambda ? B.lam_user[d][q] : 1.0;
+                    if (c->multi) v *= mask[d][B.off + q];
+                    L.lam_host[d][B.off + q] = v;
+                }
+            if (!L.lam64[d]) L.lam64[d] = dalloc<double>(L.cells);
+            if (!L.lam32[d]) L.lam32[d] = dalloc<float>(L.cells);
+            upload(L.lam64[d], L.lam_host[d]);
+            upload(L.lam32[d], to_f32(L.lam_host[d]));
+        }
+    }
+}
+
+void build(bmg_ctx* c, HostLevel&& L0) {
+    finishLevel(c, L0);
+    c->lv.push_back(std::move(L0));
+    // mesh.C:19-53: levels while coarsen(N) != N
+    for (;;) {
+        HostLevel C;
+        if (!coarsenLevel(c, c->lv.back(), C)) break;
+        finishLevel(c, C);
         c->lv.push_back(std::move(C));
     }
     const int nl = (int)c->lv.size();
     for (auto& L : c->lv)
-        for (int d = 0; d < 3; ++d)
-            if (c->periodic[d] && L.n[d] > 1 && L.n[d] % 2)
-                throw BadArg{BMG_UNSUPPORTED, "odd cell count along a periodic axis on some level"};
+        for (auto& B : L.br)
+            for (int d = 0; d < 3; ++d)
+                if (c->periodic[d] && B.n[d] > 1 && B.n[d] % 2)
+                    throw BadArg{BMG_UNSUPPORTED, "odd cell count along a periodic axis on some level"};
     for (auto& L : c->lv) {
         layout(L);
-        buildTables(L, c->periodic);
+        if (L.cells >= (1L << 31)) throw BadArg{BMG_UNSUPPORTED, "a level above 2^31 cells"};
+        buildTables(L);
         L.x64 = dalloc<double>(L.cells);
         L.b64 = dalloc<double>(L.cells);
         L.x32 = dalloc<float>(L.cells);
         L.b32 = dalloc<float>(L.cells);
         L.tab64 = dalloc<double>(L.tab.size());
         L.tab32 = dalloc<float>(L.tab.size());
-        // the fused smoother marches along axis 0 in chunks and wraps at most
-        // one period there (extent >= 2 * stages)
-        L.fusedOK = L.n[0] >= 16 && L.n[1] >= 16 && L.n[2] >= 16;
+        upload(L.tab64, L.tab);
+        upload(L.tab32, to_f32(L.tab));
+        // the fused smoother handles one brick and marches along axis 0 in
+        // chunks, wrapping at most one period there
+        const HostBrick& B = L.br[0];
+        L.fusedOK = !c->multi && B.n[0] >= 16 && B.n[1] >= 16 && B.n[2] >= 16;
         if (L.fusedOK) {
             L.x64b = dalloc<double>(L.cells);
             L.x32b = dalloc<float>(L.cells);
         }
-        upload(L.tab64, L.tab);
-        upload(L.tab32, to_f32(L.tab));
-    }
-    // transfer tables: restriction shares and prolongation indices/weights
-    c->tr.resize(nl > 1 ? nl - 1 : 0);
-    for (int l = 0; l + 1 < nl; ++l) {
-        const HostLevel& F = c->lv[l];
-        const HostLevel& C = c->lv[l + 1];
-        HostTransfer& t = c->tr[l];
-        std::vector<double> ratio, pw;
-        std::vector<int> pidx;
-        for (int d = 0; d < 3; ++d) {
-            const int R = C.R[d];
-            t.R[d] = R;
-            const Axis& fa = F.ax[d];
-            const Axis& ca = C.ax[d];
-            for (int i = 0; i < F.n[d]; ++i) {
-                const int I0 = i / R;
-                ratio.push_back(R == 1 ? 1.0 : fa.h[i + 1] / ca.h[I0 + 1]);
-                int I1 = I0;
-                double w = 0.0;
-                if (R > 1) {
-                    const int off = (i % 2) ? 1 : -1;
-                    const int In = I0 + off;
-                    // linearProlongationScheme.C:49-104: weight of the coarse
-                    // neighbour on the fine cell's side, ghost centres included
-                    w = (fa.cc[i + 1] - ca.cc[I0 + 1]) / (ca.cc[In + 1] - ca.cc[I0 + 1]);
-                    if (In < 0 || In >= C.n[d]) {
-                        if (c->periodic[d]) {
-                            I1 = (In + C.n[d]) % C.n[d];
-                        } else {
-                            I1 = I0;  // zero-gradient ghost: the value equals the parent's
-                            w = 0.0;
-                        }
-                    } else {
-                        I1 = In;
-                    }
-                }
-                pidx.push_back(I0);
-                pidx.push_back(I1);
-                pw.push_back(w);
-            }
+        if (c->multi) {
+            std::vector<int> dst, src;
+            ghostList(L, dst, src);
+            L.nghost = (long)dst.size();
+            L.gdst = dalloc<int>(dst.size());
+            L.gsrc = dalloc<int>(src.size());
+            upload(L.gdst, dst);
+            upload(L.gsrc, src);
         }
-        t.ratio64 = dalloc<double>(ratio.size());
-        t.ratio32 = dalloc<float>(ratio.size());
-        t.pidx = dalloc<int>(pidx.size());
-        t.pw64 = dalloc<double>(pw.size());
-        t.pw32 = dalloc<float>(pw.size());
-        upload(t.ratio64, ratio);
-        upload(t.ratio32, to_f32(ratio));
-        upload(t.pidx, pidx);
-        upload(t.pw64, pw);
-        upload(t.pw32, to_f32(pw));
     }
-    c->partials = dalloc<double>(2 * reduce_blocks(view<double>(c, 0)));
+    // multi-brick meshes carry face lambdas for their contacts
+    c->variable = c->multi;
+    if (c->multi) uploadLambda(c);
+    // transfer tables per brick: restriction shares and prolongation
+    // indices/weights
+    c->tr.assign(nl > 1 ? nl - 1 : 0, {});
+    for (int l = 0; l + 1 < nl; ++l) {
+        for (size_t b = 0; b < c->lv[l].br.size(); ++b) {
+            const HostBrick& F = c->lv[l].br[b];
+            const HostBrick& C = c->lv[l + 1].br[b];
+            BrickTransfer t;
+            std::vector<double> ratio, pw;
+            std::vector<int> pidx;
+            for (int d = 0; d < 3; ++d) {
+                const int R = C.R[d];
+                t.R[d] = R;
+                const Axis& fa = F.ax[d];
+                const Axis& ca = C.ax[d];
+                for (int i = 0; i < F.n[d]; ++i) {
+                    const int I0 = i / R;
+                    ratio.push_back(R == 1 ? 1.0 : fa.h[i + 1] / ca.h[I0 + 1]);
+                    int I1 = I0;
+                    double w = 0.0;
+                    if (R > 1) {
+                        const int off = (i % 2) ? 1 : -1;
+                        const int In = I0 + off;
+                        // linearProlongationScheme.C:49-104: weight of the coarse
+                        // neighbour on the fine cell's side, ghost centres included
+                        w = (fa.cc[i + 1] - ca.cc[I0 + 1]) / (ca.cc[In + 1] - ca.cc[I0 + 1]);
+                        if (In < 0 || In >= C.n[d]) {
+                            if (c->periodic[d]) {
+                                I1 = (In + C.n[d]) % C.n[d];
+                            } else if (C.open[2 * d + (In >= C.n[d])]) {
+                                I1 = In;  // ghost cell, refreshed from the neighbouring brick
+                            } else {
+                                I1 = I0;  // zero-gradient ghost: the value equals the parent's
+                                w = 0.0;
+                            }
+                        } else {
+                            I1 = In;
+                        }
+                    }
+                    pidx.push_back(I0);
+                    pidx.push_back(I1);
+                    pw.push_back(w);
+                }
+            }
+            t.ratio64 = dalloc<double>(ratio.size());
+            t.ratio32 = dalloc<float>(ratio.size());
+            t.pidx = dalloc<int>(pidx.size());
+            t.pw64 = dalloc<double>(pw.size());
+            t.pw32 = dalloc<float>(pw.size());
+            upload(t.ratio64, ratio);
+            upload(t.ratio32, to_f32(ratio));
+            upload(t.pidx, pidx);
+            upload(t.pw64, pw);
+            upload(t.pw32, to_f32(pw));
+            c->tr[l].push_back(t);
+        }
+    }
+    c->partials = dalloc<double>(2 * reduce_blocks(bricks<double>(c, 0)));
     c->st = dalloc<SolveState>(1);
     BMG_CUDA(cudaMallocHost(&c->st_host, sizeof(SolveState)));
-    c->stage_b = dalloc<double>(c->lv[0].ncell());
-    c->stage_x = dalloc<double>(c->lv[0].ncell());
+    c->stage_b = dalloc<double>(c->lv[0].ncell);
+    c->stage_x = dalloc<double>(c->lv[0].ncell);
     BMG_CUDA(cudaEventCreate(&c->ev0));
     BMG_CUDA(cudaEventCreate(&c->ev1));
     c->visits.assign(nl, 0);
@@ -503,7 +833,7 @@ void configureCoarse(bmg_ctx* c) {
     if (nl < 2 || c->opt.coarse_level > nl - 2)
         throw BadArg{BMG_BAD_ARG, "coarseLevel too high: at most (number of levels - 2)"};
     const int lc = nl - 1 - c->opt.coarse_level;
-    if (c->lv[lc].ncell() > 4096)
+    if (c->lv[lc].ncell > 4096)
         throw BadArg{BMG_UNSUPPORTED, "coarse solve level above 4096 cells; raise coarseLevel"};
     c->lc = lc;
     buildCoarseInverse(c);
@@ -523,8 +853,10 @@ void ensureJacobiBuffers(bmg_ctx* c) {
 // forward odd, then the backward passes whose loop-counter parity maps to
 // colour q = (n0+n1+n2+1) % 2 first (rbgsSmoother.C:125-183, utils.H:736-745).
 // A colour repeated back to back recomputes the same values and is dropped.
+// Several bricks follow the first brick's order.
 std::vector<int> colourSequence(const HostLevel& L, int sweeps) {
-    const int q = (L.n[0] + L.n[1] + L.n[2] + 1) % 2;
+    const HostBrick& B = L.br[0];
+    const int q = (B.n[0] + B.n[1] + B.n[2] + 1) % 2;
     std::vector<int> seq;
     for (int s = 0; s < sweeps; ++s)
         for (int col : {0, 1, q, 1 - q})
@@ -533,21 +865,22 @@ std::vector<int> colourSequence(const HostLevel& L, int sweeps) {
 }
 
 FusedGeom fusedGeom(const bmg_ctx* c, const HostLevel& L, int prec) {
+    const HostBrick& B = L.br[0];
     FusedGeom g{};
     g.m_axis = 0;
-    g.nm = L.n[0];
-    g.na = L.n[1];
-    g.nk = L.n[2];
-    g.sm = L.si;
-    g.sa = L.sj;
+    g.nm = B.n[0];
+    g.na = B.n[1];
+    g.nk = B.n[2];
+    g.sm = B.si;
+    g.sa = B.sj;
     g.perm = c->periodic[0];
     g.pera = c->periodic[1];
     g.perk = c->periodic[2];
-    g.ti = std::min(L.fusedTi[prec], L.n[0]);
-    g.wl_m = L.to.wl[0];
-    g.wh_m = L.to.wh[0];
-    g.wl_a = L.to.wl[1];
-    g.wh_a = L.to.wh[1];
+    g.ti = std::min(L.fusedTi[prec], B.n[0]);
+    g.wl_m = B.to.wl[0];
+    g.wh_m = B.to.wh[0];
+    g.wl_a = B.to.wl[1];
+    g.wh_a = B.to.wh[1];
     return g;
 }
 
@@ -559,22 +892,34 @@ void swapX(HostLevel& L) {
         std::swap(L.x32, L.x32b);
 }
 
+// refresh the ghost frames of a multi-brick level (device-side exchange)
+template <typename T>
+void exchange(bmg_ctx* c, int l) {
+    HostLevel& L = c->lv[l];
+    if (!L.nghost) return;
+    T* x;
+    if constexpr (sizeof(T) == 8)
+        x = reinterpret_cast<T*>(L.x64);
+    else
+        x = reinterpret_cast<T*>(L.x32);
+    c->launches += 1;
+    launch_fill_ghosts<T>(x, L.gdst, L.gsrc, L.nghost, c->stream);
+}
+
 template <typename T>
 void smooth(bmg_ctx* c, int l, int sweeps) {
-    const LevelView<T> L = view<T>(c, l);
     cudaStream_t s = c->stream;
     HostLevel& H = c->lv[l];
-    const int precIdx = sizeof(T) == 8 ? 0 : 1;
-    if (c->opt.smoother == BMG_SMOOTHER_RBGS && c->opt.fused > 0 && H.fusedOK && H.fusedS[precIdx] > 0) {
+    const int prec = sizeof(T) == 8 ? 0 : 1;
+    if (c->opt.smoother == BMG_SMOOTHER_RBGS && c->opt.fused > 0 && H.fusedOK && H.fusedS[prec] > 0) {
         // the colour sequence alternates; run it in launches of up to
         // maxS stages, each writing the other x buffer
         const std::vector<int> seq = colourSequence(H, sweeps);
-        const int prec = sizeof(T) == 8 ? 0 : 1;
         const FusedGeom g = fusedGeom(c, H, prec);
         const size_t maxS = (size_t)std::min({c->opt.fused, H.fusedS[prec], kFusedMaxStages});
         for (size_t p = 0; p < seq.size(); p += maxS) {
             const int stages = (int)std::min<size_t>(maxS, seq.size() - p);
-            const LevelView<T> in = view<T>(c, l);
+            const LevelView<T> in = bricks<T>(c, l).v[0];
             T* out;
             if constexpr (sizeof(T) == 8)
                 out = reinterpret_cast<T*>(H.x64b);
@@ -589,69 +934,74 @@ void smooth(bmg_ctx* c, int l, int sweeps) {
         }
         return;
     }
+    const Bricks<T> B = bricks<T>(c, l);
     if (c->opt.smoother == BMG_SMOOTHER_JACOBI) {
         T* tmp;
         if constexpr (sizeof(T) == 8)
-            tmp = reinterpret_cast<T*>(c->lv[l].jtmp64);
+            tmp = reinterpret_cast<T*>(H.jtmp64);
         else
-            tmp = reinterpret_cast<T*>(c->lv[l].jtmp32);
+            tmp = reinterpret_cast<T*>(H.jtmp32);
         for (int k = 0; k < sweeps; ++k) {
+            exchange<T>(c, l);
             c->launches += 2;
             if (c->variable)
-                launch_jacobi<T, true>(L, tmp, s);
+                launch_jacobi<T, true>(B, tmp, s);
             else
-                launch_jacobi<T, false>(L, tmp, s);
+                launch_jacobi<T, false>(B, tmp, s);
         }
         return;
     }
-    for (int col : colourSequence(c->lv[l], sweeps)) {
+    for (int col : colourSequence(H, sweeps)) {
+        exchange<T>(c, l);
         c->launches += 1;
         if (c->variable)
-            launch_colour_pass<T, true>(L, col, s);
+            launch_colour_pass<T, true>(B, col, s);
         else
-            launch_colour_pass<T, false>(L, col, s);
+            launch_colour_pass<T, false>(B, col, s);
     }
 }
 
 template <typename T>
 void residualRestrict(bmg_ctx* c, int l) {
-    const LevelView<T> F = view<T>(c, l);
-    const LevelView<T> C = view<T>(c, l + 1);
+    exchange<T>(c, l);
+    const Bricks<T> F = bricks<T>(c, l);
+    const Bricks<T> C = bricks<T>(c, l + 1);
     c->launches += 1;
     if (c->variable)
         launch_residual_restrict<T, true>(F, C, ttabs(c, l), c->stream);
     else
         launch_residual_restrict<T, false>(F, C, ttabs(c, l), c->stream);
-    BMG_CUDA(cudaMemsetAsync(C.x, 0, C.cells * sizeof(T), c->stream));
+    BMG_CUDA(cudaMemsetAsync(C.v[0].x, 0, C.v[0].cells * sizeof(T), c->stream));
 }
 
 template <typename T>
 void prolongCorrect(bmg_ctx* c, int l) {
+    exchange<T>(c, l + 1);
     c->launches += 1;
-    launch_prolong_correct<T>(view<T>(c, l), view<T>(c, l + 1), ttabs(c, l), c->stream);
+    launch_prolong_correct<T>(bricks<T>(c, l), bricks<T>(c, l + 1), ttabs(c, l), c->stream);
 }
 
 template <typename T>
 void coarseSolve(bmg_ctx* c) {
     c->launches += 1;
-    launch_coarse_solve<T>(view<T>(c, c->lc), c->ainv, c->ncoarse, c->stream);
+    launch_coarse_solve<T>(bricks<T>(c, c->lc), c->ainv, c->cidx, c->ncoarse, c->stream);
 }
 
-// Launch-shape autotuner: for every level the fused smoother handles, time
-// one smoothing step (the configured sweep count) for each number of colour
-// stages per launch and each plane-chunk length, and keep the fastest.  The
-// tile (16 x 64 cells) is fixed by the kernel's register window; stages and
-// chunk length trade halo recomputation against memory passes and CTA count.
+// Launch-shape autotuner: for every level the fused smoother can handle,
+// time one smoothing step (the configured sweep count) with one launch per
+// colour pass and with the fused smoother at each number of colour stages
+// per launch and plane-chunk length, and keep the fastest.  The tile (16 x
+// 64 cells) is fixed by the fused kernel's register window; stages and chunk
+// length trade halo recomputation against memory passes and CTA count.
 template <typename T>
 void autotuneLevel(bmg_ctx* c, int l, int sweeps, cudaEvent_t e0, cudaEvent_t e1) {
     HostLevel& H = c->lv[l];
     const int prec = sizeof(T) == 8 ? 0 : 1;
     float best = 1e30f;
     int bestS = H.fusedS[prec], bestTi = H.fusedTi[prec];
-    // S = 0: one launch per colour pass (no temporal blocking)
     for (int S = 0; S <= kFusedMaxStages; ++S)
         for (int ti : {32, 64, 128}) {
-            if (ti > 2 * H.n[0] && ti != 32) continue;
+            if (ti > 2 * H.br[0].n[0] && ti != 32) continue;
             if (S == 0 && ti != 32) continue;
             H.fusedS[prec] = S;
             H.fusedTi[prec] = ti;
@@ -729,28 +1079,32 @@ void checkLaunch() {
 // level-0 FP64 residual norm and the convergence decision; inside a graph
 // the decision also sets the WHILE node's condition
 void residualNorm(bmg_ctx* c, int mode, bool setCondition) {
-    const LevelView<double> L = view<double>(c, 0);
+    exchange<double>(c, 0);
+    const Bricks<double> L = bricks<double>(c, 0);
     float* b32 = c->opt.precision == BMG_PRECISION_MIXED ? c->lv[0].b32 : nullptr;
     c->launches += 2;
     if (c->variable)
-        launch_residual_norm<true>(L, mode, c->partials, b32, nullptr, c->stream);
+        launch_residual_norm<true>(L, mode, c->partials, b32, c->stream);
     else
-        launch_residual_norm<false>(L, mode, c->partials, b32, nullptr, c->stream);
+        launch_residual_norm<false>(L, mode, c->partials, b32, c->stream);
     launch_finalize(L, c->partials, c->st, mode, c->cond, setCondition ? 1 : 0, c->stream);
 }
 
 SolveState initialState(const bmg_ctx* c) {
-    const HostLevel& L0 = c->lv[0];
     SolveState init{};
     init.rel_tol = c->opt.rel_tol;
     init.abs_tol = c->opt.abs_tol;
     init.min_iter = c->opt.min_iter;
     init.max_iter = c->opt.max_iter;
-    init.ncells = (double)L0.ncell();
-    double v[3] = {0.0, 0.0, 0.0};
-    for (int d = 0; d < 3; ++d)
-        for (int i = 0; i < L0.n[d]; ++i) v[d] += L0.ax[d].h[i + 1];
-    init.vol_total = v[0] * v[1] * v[2];
+    init.ncells = (double)c->lv[0].ncell;
+    double vol = 0.0;
+    for (const auto& B : c->lv[0].br) {
+        double v[3] = {0.0, 0.0, 0.0};
+        for (int d = 0; d < 3; ++d)
+            for (int i = 0; i < B.n[d]; ++i) v[d] += B.ax[d].h[i + 1];
+        vol += v[0] * v[1] * v[2];
+    }
+    init.vol_total = vol;
     return init;
 }
 
@@ -760,7 +1114,7 @@ SolveState initialState(const bmg_ctx* c) {
 void segInit(bmg_ctx* c, const double* bsrc, const double* xsrc, bool zero, bool setCondition) {
     cudaStream_t s = c->stream;
     HostLevel& L0 = c->lv[0];
-    const LevelView<double> V0 = view<double>(c, 0);
+    const Bricks<double> V0 = bricks<double>(c, 0);
     launch_load_b(V0, bsrc, s);
     BMG_CUDA(cudaMemsetAsync(L0.x64, 0, L0.cells * sizeof(double), s));
     c->launches += 1;
@@ -782,7 +1136,7 @@ void segBody(bmg_ctx* c, bool setCondition) {
     if (c->opt.precision == BMG_PRECISION_MIXED) {
         BMG_CUDA(cudaMemsetAsync(L0.x32, 0, L0.cells * sizeof(float), s));
         cycle<float>(c, 0);
-        launch_add_correction(view<double>(c, 0), view<float>(c, 0), s);
+        launch_add_correction(bricks<double>(c, 0), bricks<float>(c, 0), s);
         c->launches += 1;
     } else {
         cycle<double>(c, 0);
@@ -791,20 +1145,13 @@ void segBody(bmg_ctx* c, bool setCondition) {
 }
 
 void segPost(bmg_ctx* c, double* xdst) {
-    const LevelView<double> V0 = view<double>(c, 0);
+    const Bricks<double> V0 = bricks<double>(c, 0);
     if (c->opt.remove_mean) {
         launch_mean(V0, c->partials, c->st, c->stream);
         c->launches += 3;
     }
     launch_store_x(V0, xdst, c->stream);
     c->launches += 1;
-}
-
-void destroyGraph(bmg_ctx* c) {
-    if (c->gexec) cudaGraphExecDestroy(c->gexec);
-    if (c->graph) cudaGraphDestroy(c->graph);
-    c->gexec = nullptr;
-    c->graph = nullptr;
 }
 
 // Whole solve as one graph: init -> WHILE(keep_going){ cycle, residual,
@@ -873,7 +1220,7 @@ void captureGraph(bmg_ctx* c, bool zero) {
 int solveImpl(bmg_ctx* c, const double* b, double* x, int flags, bmg_report* rep) {
     BMG_CUDA(cudaSetDevice(c->opt.device));
     cudaStream_t s = c->stream;
-    const long n = c->lv[0].ncell();
+    const long n = c->lv[0].ncell;
     const bool dev = flags & BMG_DEVICE_PTRS;
     const bool zero = flags & BMG_ZERO_GUESS;
     if (c->opt.smoother == BMG_SMOOTHER_JACOBI) ensureJacobiBuffers(c);
@@ -956,48 +1303,43 @@ int solveImpl(bmg_ctx* c, const double* b, double* x, int flags, bmg_report* rep
 }
 
 // restrict the level-0 face lambda to every level, area-weighted
-// (areaWeightedFaceRestrictionScheme.C:19-57), into ghost-framed face arrays
+// (areaWeightedFaceRestrictionScheme.C:19-57), per brick
 void restrictLambda(bmg_ctx* c, const double* src[3]) {
     HostLevel& L0 = c->lv[0];
-    for (int fd = 0; fd < 3; ++fd) {
-        L0.lam_host[fd].assign(L0.cells, 0.0);
-        const int e0 = fd == 0, e1 = fd == 1, e2 = fd == 2;
-        long q = 0;
-        for (int i = 0; i < L0.n[0] + e0; ++i)
-            for (int j = 0; j < L0.n[1] + e1; ++j)
-                for (int k = 0; k < L0.n[2] + e2; ++k) L0.lam_host[fd][L0.at(i, j, k)] = src[fd][q++];
-    }
-    for (size_t l = 0; l + 1 < c->lv.size(); ++l) {
-        const HostLevel& F = c->lv[l];
-        HostLevel& C = c->lv[l + 1];
+    long q[3] = {0, 0, 0};
+    for (auto& B : L0.br)
         for (int fd = 0; fd < 3; ++fd) {
-            C.lam_host[fd].assign(C.cells, 0.0);
+            B.lam_user[fd].assign(B.cells, 1.0);
             const int e0 = fd == 0, e1 = fd == 1, e2 = fd == 2;
-            for (int I = 0; I < C.n[0] + e0; ++I)
-                for (int J = 0; J < C.n[1] + e1; ++J)
-                    for (int K = 0; K < C.n[2] + e2; ++K) {
-                        double area = 0.0, value = 0.0;
-                        for (int ox = 0; ox < (fd == 0 ? 1 : C.R[0]); ++ox)
-                            for (int oy = 0; oy < (fd == 1 ? 1 : C.R[1]); ++oy)
-                                for (int oz = 0; oz < (fd == 2 ? 1 : C.R[2]); ++oz) {
-                                    const int fi = I * C.R[0] + ox, fj = J * C.R[1] + oy,
-                                              fk = K * C.R[2] + oz;
-                                    const double a = fd == 0   ? F.ax[1].h[fj + 1] * F.ax[2].h[fk + 1]
-                                                     : fd == 1 ? F.ax[0].h[fi + 1] * F.ax[2].h[fk + 1]
-                                                               : F.ax[0].h[fi + 1] * F.ax[1].h[fj + 1];
-                                    area += a;
-                                    value += a * F.lam_host[fd][F.at(fi, fj, fk)];
-                                }
-                        C.lam_host[fd][C.at(I, J, K)] = value / area;
-                    }
+            for (int i = 0; i < B.n[0] + e0; ++i)
+                for (int j = 0; j < B.n[1] + e1; ++j)
+                    for (int k = 0; k < B.n[2] + e2; ++k) B.lam_user[fd][B.loc(i, j, k)] = src[fd][q[fd]++];
         }
-    }
-    for (auto& L : c->lv)
-        for (int fd = 0; fd < 3; ++fd) {
-            if (!L.lam64[fd]) L.lam64[fd] = dalloc<double>(L.cells);
-            if (!L.lam32[fd]) L.lam32[fd] = dalloc<float>(L.cells);
-            upload(L.lam64[fd], L.lam_host[fd]);
-            upload(L.lam32[fd], to_f32(L.lam_host[fd]));
+    for (size_t l = 0; l + 1 < c->lv.size(); ++l)
+        for (size_t b = 0; b < c->lv[l].br.size(); ++b) {
+            const HostBrick& F = c->lv[l].br[b];
+            HostBrick& C = c->lv[l + 1].br[b];
+            for (int fd = 0; fd < 3; ++fd) {
+                C.lam_user[fd].assign(C.cells, 1.0);
+                const int e0 = fd == 0, e1 = fd == 1, e2 = fd == 2;
+                for (int I = 0; I < C.n[0] + e0; ++I)
+                    for (int J = 0; J < C.n[1] + e1; ++J)
+                        for (int K = 0; K < C.n[2] + e2; ++K) {
+                            double area = 0.0, value = 0.0;
+                            for (int ox = 0; ox < (fd == 0 ? 1 : C.R[0]); ++ox)
+                                for (int oy = 0; oy < (fd == 1 ? 1 : C.R[1]); ++oy)
+                                    for (int oz = 0; oz < (fd == 2 ? 1 : C.R[2]); ++oz) {
+                                        const int fi = I * C.R[0] + ox, fj = J * C.R[1] + oy,
+                                                  fk = K * C.R[2] + oz;
+                                        const double a = fd == 0   ? F.ax[1].h[fj + 1] * F.ax[2].h[fk + 1]
+                                                         : fd == 1 ? F.ax[0].h[fi + 1] * F.ax[2].h[fk + 1]
+                                                                   : F.ax[0].h[fi + 1] * F.ax[1].h[fj + 1];
+                                        area += a;
+                                        value += a * F.lam_user[fd][F.loc(fi, fj, fk)];
+                                    }
+                            C.lam_user[fd][C.loc(I, J, K)] = value / area;
+                        }
+            }
         }
 }
 
@@ -1057,6 +1399,9 @@ int bmg_create(bmg_ctx** out, const bmg_mesh_desc* mesh, const bmg_options* opts
         bmg_default_options(&c->opt);
     const int rc = guarded(c, [&] {
         validateOptions(&c->opt);
+        // the mesh is checked on the host before any device work
+        HostLevel L0;
+        readBricks(c, mesh, L0);
         int ndev = 0;
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= c->opt.device || c->opt.device < 0)
             throw BadArg{BMG_NO_DEVICE, "no CUDA device with the requested ordinal"};
@@ -1068,7 +1413,7 @@ int bmg_create(bmg_ctx** out, const bmg_mesh_desc* mesh, const bmg_options* opts
         c->own_stream = true;
         BMG_CUDA(cudaStreamCreateWithFlags(&c->capStream, cudaStreamNonBlocking));
         configure_fused_kernels();
-        build(c, mesh);
+        build(c, std::move(L0));
         configureCoarse(c);
         if (c->opt.autotune) autotune(c);
         return BMG_OK;
@@ -1115,19 +1460,22 @@ int bmg_set_coefficients(bmg_ctx* c, const double* lx, const double* ly, const d
         BMG_CUDA(cudaStreamSynchronize(c->stream));
         if (!lx || !ly || !lz) {
             if (lx || ly || lz) throw BadArg{BMG_BAD_ARG, "give all three face coefficient arrays or none"};
-            c->variable = false;
+            c->userLambda = false;
         } else {
             const double* src[3] = {lx, ly, lz};
-            for (int fd = 0; fd < 3; ++fd) {
-                const HostLevel& L0 = c->lv[0];
-                long nf = (long)(L0.n[0] + (fd == 0)) * (L0.n[1] + (fd == 1)) * (L0.n[2] + (fd == 2));
-                for (long q = 0; q < nf; ++q)
+            long nf[3] = {0, 0, 0};
+            for (const auto& B : c->lv[0].br)
+                for (int fd = 0; fd < 3; ++fd)
+                    nf[fd] += (long)(B.n[0] + (fd == 0)) * (B.n[1] + (fd == 1)) * (B.n[2] + (fd == 2));
+            for (int fd = 0; fd < 3; ++fd)
+                for (long q = 0; q < nf[fd]; ++q)
                     if (!(src[fd][q] > 0.0) || !std::isfinite(src[fd][q]))
                         throw BadArg{BMG_BAD_ARG, "face coefficients must be positive and finite"};
-            }
             restrictLambda(c, src);
-            c->variable = true;
+            c->userLambda = true;
         }
+        c->variable = c->userLambda || c->multi;
+        if (c->variable) uploadLambda(c);
         buildCoarseInverse(c);
         destroyGraph(c);  // kernels differ between constant and variable coefficients
         return BMG_OK;
@@ -1153,7 +1501,7 @@ int bmg_solve(bmg_ctx* c, const double* b, double* x, int flags, bmg_report* rep
     return rc;
 }
 
-long bmg_num_cells(const bmg_ctx* c) { return c ? c->lv[0].ncell() : 0; }
+long bmg_num_cells(const bmg_ctx* c) { return c ? c->lv[0].ncell : 0; }
 int bmg_num_levels(const bmg_ctx* c) { return c ? (int)c->lv.size() : 0; }
 int bmg_coarse_level_index(const bmg_ctx* c) { return c ? c->lc : -1; }
 
@@ -1162,13 +1510,13 @@ int bmg_level_tuning(const bmg_ctx* c, int l, int prec, int* stages, int* chunk)
     const HostLevel& L = c->lv[l];
     const bool fused = c->opt.smoother == BMG_SMOOTHER_RBGS && c->opt.fused > 0 && L.fusedOK && L.fusedS[prec] > 0;
     *stages = fused ? std::min({c->opt.fused, L.fusedS[prec], kFusedMaxStages}) : 0;
-    *chunk = fused ? std::min(L.fusedTi[prec], L.n[0]) : 0;
+    *chunk = fused ? std::min(L.fusedTi[prec], L.br[0].n[0]) : 0;
     return BMG_OK;
 }
 
 int bmg_level_shape(const bmg_ctx* c, int l, int brick, int n[3]) {
-    if (!validLevel(c, l) || brick != 0 || !n) return BMG_BAD_ARG;
-    for (int d = 0; d < 3; ++d) n[d] = c->lv[l].n[d];
+    if (!validLevel(c, l) || !n || brick < 0 || brick >= (int)c->lv[l].br.size()) return BMG_BAD_ARG;
+    for (int d = 0; d < 3; ++d) n[d] = c->lv[l].br[brick].n[d];
     return BMG_OK;
 }
 
@@ -1194,14 +1542,14 @@ int bmg_level_upload(bmg_ctx* c, int l, int field, int prec, const double* host)
     if (!validLevel(c, l) || !host || field < 0 || field > 1) return BMG_BAD_ARG;
     return guarded(c, [&] {
         BMG_CUDA(cudaSetDevice(c->opt.device));
-        const long n = c->lv[l].ncell();
-        BMG_CUDA(cudaMemcpyAsync(c->stage_b, host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        HostLevel& L = c->lv[l];
+        BMG_CUDA(cudaMemcpyAsync(c->stage_b, host, L.ncell * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         if (prec == 0) {
-            if (field == 0) BMG_CUDA(cudaMemsetAsync(c->lv[l].x64, 0, c->lv[l].cells * sizeof(double), c->stream));
-            launch_load_field<double>(view<double>(c, l), field, c->stage_b, 1, c->stream);
+            if (field == 0) BMG_CUDA(cudaMemsetAsync(L.x64, 0, L.cells * sizeof(double), c->stream));
+            launch_load_field<double>(bricks<double>(c, l), field, c->stage_b, 1, c->stream);
         } else {
-            if (field == 0) BMG_CUDA(cudaMemsetAsync(c->lv[l].x32, 0, c->lv[l].cells * sizeof(float), c->stream));
-            launch_load_field<float>(view<float>(c, l), field, c->stage_b, 1, c->stream);
+            if (field == 0) BMG_CUDA(cudaMemsetAsync(L.x32, 0, L.cells * sizeof(float), c->stream));
+            launch_load_field<float>(bricks<float>(c, l), field, c->stage_b, 1, c->stream);
         }
         checkLaunch();
         BMG_CUDA(cudaStreamSynchronize(c->stream));
@@ -1213,13 +1561,13 @@ int bmg_level_download(bmg_ctx* c, int l, int field, int prec, double* host) {
     if (!validLevel(c, l) || !host || field < 0 || field > 1) return BMG_BAD_ARG;
     return guarded(c, [&] {
         BMG_CUDA(cudaSetDevice(c->opt.device));
-        const long n = c->lv[l].ncell();
         if (prec == 0)
-            launch_store_field<double>(view<double>(c, l), field, c->stage_x, 1, c->stream);
+            launch_store_field<double>(bricks<double>(c, l), field, c->stage_x, 1, c->stream);
         else
-            launch_store_field<float>(view<float>(c, l), field, c->stage_x, 1, c->stream);
+            launch_store_field<float>(bricks<float>(c, l), field, c->stage_x, 1, c->stream);
         checkLaunch();
-        BMG_CUDA(cudaMemcpyAsync(host, c->stage_x, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        BMG_CUDA(cudaMemcpyAsync(host, c->stage_x, c->lv[l].ncell * sizeof(double), cudaMemcpyDeviceToHost,
+                                 c->stream));
         BMG_CUDA(cudaStreamSynchronize(c->stream));
         return BMG_OK;
     });
@@ -1230,11 +1578,13 @@ int bmg_op_colour_pass(bmg_ctx* c, int l, int colour, int prec) {
     return guarded(c, [&] {
         BMG_CUDA(cudaSetDevice(c->opt.device));
         if (prec == 0) {
-            if (c->variable) launch_colour_pass<double, true>(view<double>(c, l), colour, c->stream);
-            else launch_colour_pass<double, false>(view<double>(c, l), colour, c->stream);
+            exchange<double>(c, l);
+            if (c->variable) launch_colour_pass<double, true>(bricks<double>(c, l), colour, c->stream);
+            else launch_colour_pass<double, false>(bricks<double>(c, l), colour, c->stream);
         } else {
-            if (c->variable) launch_colour_pass<float, true>(view<float>(c, l), colour, c->stream);
-            else launch_colour_pass<float, false>(view<float>(c, l), colour, c->stream);
+            exchange<float>(c, l);
+            if (c->variable) launch_colour_pass<float, true>(bricks<float>(c, l), colour, c->stream);
+            else launch_colour_pass<float, false>(bricks<float>(c, l), colour, c->stream);
         }
         checkLaunch();
         BMG_CUDA(cudaStreamSynchronize(c->stream));
@@ -1260,15 +1610,17 @@ int bmg_op_residual(bmg_ctx* c, int l, int prec, double* host_r) {
     return guarded(c, [&] {
         BMG_CUDA(cudaSetDevice(c->opt.device));
         if (prec == 0) {
-            if (c->variable) launch_residual_out<double, true>(view<double>(c, l), c->stage_x, c->stream);
-            else launch_residual_out<double, false>(view<double>(c, l), c->stage_x, c->stream);
+            exchange<double>(c, l);
+            if (c->variable) launch_residual_out<double, true>(bricks<double>(c, l), c->stage_x, c->stream);
+            else launch_residual_out<double, false>(bricks<double>(c, l), c->stage_x, c->stream);
         } else {
-            if (c->variable) launch_residual_out<float, true>(view<float>(c, l), c->stage_x, c->stream);
-            else launch_residual_out<float, false>(view<float>(c, l), c->stage_x, c->stream);
+            exchange<float>(c, l);
+            if (c->variable) launch_residual_out<float, true>(bricks<float>(c, l), c->stage_x, c->stream);
+            else launch_residual_out<float, false>(bricks<float>(c, l), c->stage_x, c->stream);
         }
         checkLaunch();
-        BMG_CUDA(cudaMemcpyAsync(host_r, c->stage_x, c->lv[l].ncell() * sizeof(double),
-                                 cudaMemcpyDeviceToHost, c->stream));
+        BMG_CUDA(cudaMemcpyAsync(host_r, c->stage_x, c->lv[l].ncell * sizeof(double), cudaMemcpyDeviceToHost,
+                                 c->stream));
         BMG_CUDA(cudaStreamSynchronize(c->stream));
         return BMG_OK;
     });

@@ -1,30 +1,44 @@
 // bmg_internal.h -- device-side views and kernel launchers of the B200
-// multigrid solver.  Host driver: bmg_host.cu.  Kernels: bmg_kernels.cu.
+// multigrid solver.  Host driver: bmg_host.cu.  Kernels: bmg_kernels.cu,
+// bmg_smooth_fused.cu.
 //
-// Data layout in HBM (per level, per brick):
-//   every cell field is a ghost-framed block of (n0+2) x (n1+2) x (n2+2)
-//   values, k fastest (the reference's lin(), utils.H:569, with its one-cell
-//   ghost frame, meshDirection.H:35).  Interior cell (i,j,k) sits at
-//   base + i*si + j*sj + k with base = si + sj + 1.
-//   Periodic axes keep their ghost layers (faces, edges, corners) current by
-//   write-through: every kernel that stores an interior value also stores it
-//   into the ghost images of that cell, so stencils read ghosts without
-//   a separate exchange step (the reference exchanges them per sweep,
-//   rbgsSmoother.C:405-428).  Wall (Neumann) ghosts are never read: their
-//   couplings are zero after elimination (NeumannBoundaryCondition.C:19-56).
+// Data layout in HBM (per level):
+//   all bricks of a level live in one slab per field.  Each brick is a
+//   ghost-framed block of (n0+2) x (n1+2) x p2 values, k fastest (the
+//   reference's lin(), utils.H:569, with its one-cell ghost frame,
+//   meshDirection.H:35); rows are padded to p2 = round_up(n2 + 5, 4) so that
+//   interior rows start on 16-byte (FP32) / 32-byte (FP64) boundaries.
+//   Interior cell (i,j,k) of a brick sits at base + i*si + j*sj + k.
+//   Compact (interior-only) arrays list the bricks one after another, each
+//   k fastest, as the C ABI does.
+//
+// Ghosts: on a single brick, periodic axes keep their ghost layers (faces,
+//   edges, corners) current by write-through -- every kernel that stores an
+//   interior value also stores its ghost images -- so stencils read ghosts
+//   without an exchange step (the reference exchanges them per sweep,
+//   rbgsSmoother.C:405-428).  Between bricks, a gather kernel refreshes the
+//   ghost frame from the neighbouring bricks (and zero-gradient copies at
+//   walls) before every stencil pass, the device-side counterpart of the
+//   reference's inter-processor exchange (parallelBoundaryCondition.C:84-174).
+//   Wall couplings are zero after the Neumann elimination
+//   (NeumannBoundaryCondition.C:19-56), so wall ghosts only matter to the
+//   prolongation.
 //
 // The operator is stored row-scaled by the inverse cell volume (A' = A/V,
-// b' = b/V), which leaves every Gauss-Seidel, Jacobi and coarse-solve
-// update unchanged and makes the constant-coefficient couplings pure 1-D
-// tables: coupling to the lower x neighbour = delta_x(i)/h_x(i) (times the
-// face lambda for a variable coefficient).  No 7-coefficient array exists
-// on the device.
+// b' = b/V), which leaves every Gauss-Seidel, Jacobi and coarse-solve update
+// unchanged and makes the constant-coefficient couplings 1-D tables: the
+// coupling to the lower x neighbour is delta_x(i)/h_x(i), times the face
+// lambda for a variable coefficient.  Multi-brick meshes always carry face
+// lambdas: 1 on faces inside a brick and on contact faces, 0 on the wall
+// parts of brick faces.  No 7-coefficient array exists on the device.
 #pragma once
 
 #include <cuda_runtime.h>
 #include <cstdint>
 
 namespace bmg {
+
+constexpr int kMaxBricks = 8;
 
 // 1-D table offsets inside one level's coefficient table
 struct TabOff {
@@ -34,13 +48,15 @@ struct TabOff {
     int total;
 };
 
+// One brick on one level.
 template <typename T>
 struct LevelView {
     int n0, n1, n2;
     long si, sj;       // strides of i and j (k contiguous)
-    long base;         // index of interior cell (0,0,0)
-    long cells;        // size of the ghost-framed block
-    T* x;
+    long base;         // slab index of interior cell (0,0,0)
+    long cells;        // size of the whole slab (all bricks)
+    long cbase;        // offset of the brick in compact arrays
+    T* x;              // slab pointers
     T* b;
     const T* tab;      // 1-D tables (TabOff layout) in precision T
     const double* tab64;  // the same tables in FP64 (norms, volumes)
@@ -48,7 +64,18 @@ struct LevelView {
     const T* lam0;     // face lambda (lower face of the cell, ghost-framed
     const T* lam1;     // indexing), nullptr for a constant coefficient
     const T* lam2;
-    int per0, per1, per2;
+    int per0, per1, per2;  // periodic write-through (single brick only)
+    int cpar;          // parity of the brick origin: colour = (i+j+k+cpar) & 1
+};
+
+// All bricks of a level, for one launch across bricks: the grid's z index
+// runs over the planes of brick 0, then brick 1, ...
+template <typename T>
+struct Bricks {
+    LevelView<T> v[kMaxBricks];
+    int z0[kMaxBricks + 1];  // first plane of each brick; z0[nb] = total planes
+    int nb;
+    int max1, max2;          // largest n1 and n2 (grid extents)
 };
 
 // Transfer tables between level l (fine) and l+1 (coarse), fine-indexed.
@@ -61,6 +88,10 @@ struct TransferTabs {
     const double* pw64;     // [n0f | n1f | n2f]
     const float* pw32;
     int R0, R1, R2;
+};
+
+struct TransferSet {
+    TransferTabs t[kMaxBricks];
 };
 
 // Device-resident solve state: one cache line read back (or tested by the
@@ -83,8 +114,9 @@ struct SolveState {
     int pad[2];
 };
 
-// Geometry of a fused smoothing launch: march axis m (0 or 1), the other
-// non-contiguous axis a, and k (axis 2); see bmg_smooth_fused.cu.
+// Geometry of a fused smoothing launch (single brick): march axis m (0),
+// the other non-contiguous axis a (1), and k (axis 2); see
+// bmg_smooth_fused.cu.
 struct FusedGeom {
     int m_axis;
     int nm, na, nk;
@@ -106,45 +138,44 @@ constexpr int kReduceThreads = 256;
 
 // ---- launchers (bmg_kernels.cu) -------------------------------------------
 template <typename T, bool VAR>
-void launch_colour_pass(const LevelView<T>& L, int colour, cudaStream_t s);
+void launch_colour_pass(const Bricks<T>& B, int colour, cudaStream_t s);
 template <typename T, bool VAR>
-void launch_jacobi(const LevelView<T>& L, T* tmp, cudaStream_t s);
+void launch_jacobi(const Bricks<T>& B, T* tmp, cudaStream_t s);
 template <typename T, bool VAR>
-void launch_residual_restrict(const LevelView<T>& F, const LevelView<T>& C, const TransferTabs& t,
-                              cudaStream_t s);
+void launch_residual_restrict(const Bricks<T>& F, const Bricks<T>& C, const TransferSet& t, cudaStream_t s);
 template <typename T>
-void launch_prolong_correct(const LevelView<T>& F, const LevelView<T>& C, const TransferTabs& t,
-                            cudaStream_t s);
+void launch_prolong_correct(const Bricks<T>& F, const Bricks<T>& C, const TransferSet& t, cudaStream_t s);
+// dense solve on the coarse level; cidx lists the slab index of each unknown
 template <typename T>
-void launch_coarse_solve(const LevelView<T>& C, const double* ainv, int n, cudaStream_t s);
+void launch_coarse_solve(const Bricks<T>& C, const double* ainv, const int* cidx, int n, cudaStream_t s);
 template <typename T, bool VAR>
-void launch_residual_out(const LevelView<T>& L, double* r_unscaled_compact, cudaStream_t s);
+void launch_residual_out(const Bricks<T>& B, double* r_unscaled_compact, cudaStream_t s);
+// x[dst[q]] = x[src[q]]: ghost refresh between bricks
+template <typename T>
+void launch_fill_ghosts(T* x, const int* dst, const int* src, long n, cudaStream_t s);
 
 // residual norms of level 0 in FP64.  mode 0: initial (also the norm-factor
 // sum), 1: current.  When b32 is given the scaled residual is also written
 // there in FP32 (the right-hand side of the next mixed-precision cycle).
 template <bool VAR>
-void launch_residual_norm(const LevelView<double>& L, int mode, double* partials, float* b32,
-                          const LevelView<float>* L32, cudaStream_t s);
-void launch_finalize(const LevelView<double>& L, const double* partials, SolveState* st, int mode,
+void launch_residual_norm(const Bricks<double>& B, int mode, double* partials, float* b32, cudaStream_t s);
+void launch_finalize(const Bricks<double>& B, const double* partials, SolveState* st, int mode,
                      cudaGraphConditionalHandle cond, int setCondition, cudaStream_t s);
+void launch_mean(const Bricks<double>& B, double* partials, SolveState* st, cudaStream_t s);
 // number of per-block partial sums the level-0 reductions write
-long reduce_blocks(const LevelView<double>& L);
+long reduce_blocks(const Bricks<double>& B);
 // sets the dynamic shared memory limits of the fused smoother instances
 void configure_fused_kernels();
-void launch_mean(const LevelView<double>& L, double* partials, SolveState* st, cudaStream_t s);
 
-// compact interior <-> ghost-framed conversions (level 0, FP64)
-void launch_load_b(const LevelView<double>& L, const double* compact, cudaStream_t s);
-void launch_load_x(const LevelView<double>& L, const double* compact, cudaStream_t s);
-void launch_store_x(const LevelView<double>& L, double* compact, cudaStream_t s);
+// compact interior <-> ghost-framed conversions
+void launch_load_b(const Bricks<double>& B, const double* compact, cudaStream_t s);
+void launch_load_x(const Bricks<double>& B, const double* compact, cudaStream_t s);
+void launch_store_x(const Bricks<double>& B, double* compact, cudaStream_t s);
 template <typename T>
-void launch_load_field(const LevelView<T>& L, int field, const double* compact, int unscale,
-                       cudaStream_t s);
+void launch_load_field(const Bricks<T>& B, int field, const double* compact, int unscale, cudaStream_t s);
 template <typename T>
-void launch_store_field(const LevelView<T>& L, int field, double* compact, int unscale,
-                        cudaStream_t s);
+void launch_store_field(const Bricks<T>& B, int field, double* compact, int unscale, cudaStream_t s);
 // x64 += x32 on the interior (write-through)
-void launch_add_correction(const LevelView<double>& L, const LevelView<float>& E, cudaStream_t s);
+void launch_add_correction(const Bricks<double>& B, const Bricks<float>& E, cudaStream_t s);
 
 }  // namespace bmg

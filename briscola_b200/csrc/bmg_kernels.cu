@@ -3,7 +3,9 @@
 // Every kernel here is HBM- (fine levels) or L2-bound (levels up to 128^3
 // fit the 126 MB L2): no tensor cores, coalesced k-fastest access, FP64 or
 // FP32 arithmetic chosen by the template parameter.  Layout and coefficient
-// conventions are described in bmg_internal.h.
+// conventions are described in bmg_internal.h.  Each per-cell kernel runs
+// over all bricks of a level in one launch: the grid's z index walks the
+// planes of brick 0, then brick 1, and so on.
 
 #include "bmg_stencil.cuh"
 
@@ -13,11 +15,6 @@ namespace bmg {
 
 namespace {
 
-// ---------------------------------------------------------------------------
-// Red-black Gauss-Seidel: one colour pass.  Thread per (i, j, k-pair); the
-// pair member of the requested colour is updated.  Colour 0 = (i+j+k) even.
-// Equivalent to one pass of rbgsSmoother.C:65-183 over the whole level.
-// ---------------------------------------------------------------------------
 template <typename T>
 struct Pair;
 template <>
@@ -29,20 +26,34 @@ struct Pair<double> {
     using type = double2;
 };
 
-// The thread owns the k-pair (2p, 2p+1) and updates its member of the
-// requested colour.  Neighbour rows and planes are read as whole pairs
-// (8/16-byte loads: rows start on 16-byte boundaries and k0 is even), so a
+// brick of grid plane z and the plane index inside it
+template <typename T>
+__device__ __forceinline__ int brick_of(const Bricks<T>& B, int z, int& i) {
+    int b = 0;
+    while (b + 1 < B.nb && z >= B.z0[b + 1]) ++b;
+    i = z - B.z0[b];
+    return b;
+}
+
+// ---------------------------------------------------------------------------
+// Red-black Gauss-Seidel: one colour pass (one pass of rbgsSmoother.C:65-183
+// over the whole level).  Colour 0 = (i+j+k+cpar) even, cpar the parity of
+// the brick origin, so colours agree across brick contacts.  The thread owns
+// the k-pair (2p, 2p+1) and updates its member of the requested colour.
+// Neighbour rows and planes are read as whole pairs (8/16-byte loads), so a
 // warp's loads fill every L1 wavefront; the k neighbour outside the pair is
 // one scalar load.
+// ---------------------------------------------------------------------------
 template <typename T, bool VAR>
-__global__ void __launch_bounds__(256) k_colour_pass(LevelView<T> L, int colour) {
+__global__ void __launch_bounds__(256) k_colour_pass(Bricks<T> B, int colour) {
     using V2 = typename Pair<T>::type;
+    int i;
+    const LevelView<T>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
     const int k0 = 2 * p;
     if (j >= L.n1 || k0 >= L.n2) return;
-    const int e = ((i + j + k0) & 1) == colour ? 0 : 1;
+    const int e = ((i + j + k0 + L.cpar) & 1) == colour ? 0 : 1;
     const int k = k0 + e;
     if (k >= L.n2) return;
     const long r = L.base + (long)i * L.si + (long)j * L.sj;
@@ -63,10 +74,11 @@ __global__ void __launch_bounds__(256) k_colour_pass(LevelView<T> L, int colour)
 
 // Damped Jacobi (omega = 0.8, jacSmoother.C:15) into a temporary, then copy.
 template <typename T, bool VAR>
-__global__ void __launch_bounds__(256) k_jacobi(LevelView<T> L, T* tmp) {
+__global__ void __launch_bounds__(256) k_jacobi(Bricks<T> B, T* tmp) {
+    int i;
+    const LevelView<T>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
     if (j >= L.n1 || k >= L.n2) return;
     const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
     T w[6], s, d;
@@ -77,10 +89,11 @@ __global__ void __launch_bounds__(256) k_jacobi(LevelView<T> L, T* tmp) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_copy_interior(LevelView<T> L, const T* src) {
+__global__ void __launch_bounds__(256) k_copy_interior(Bricks<T> B, const T* src) {
+    int i;
+    const LevelView<T>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
     if (j >= L.n1 || k >= L.n2) return;
     const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
     store_x(L, c, i, j, k, src[c]);
@@ -94,22 +107,29 @@ __global__ void __launch_bounds__(256) k_copy_interior(LevelView<T> L, const T* 
 // along an axis is its share of the coarse cell length along that axis.
 // ---------------------------------------------------------------------------
 template <typename T, bool VAR>
-__global__ void __launch_bounds__(256) k_residual_restrict(LevelView<T> F, LevelView<T> C,
-                                                           const T* ratio, int R0, int R1,
-                                                           int R2) {
+__global__ void __launch_bounds__(256) k_residual_restrict(Bricks<T> FB, Bricks<T> CB, TransferSet ts) {
+    int I;
+    const int b = brick_of(CB, blockIdx.z, I);
+    const LevelView<T>& C = CB.v[b];
+    const LevelView<T>& F = FB.v[b];
+    const TransferTabs& t = ts.t[b];
     const int K = blockIdx.x * blockDim.x + threadIdx.x;
     const int J = blockIdx.y * blockDim.y + threadIdx.y;
-    const int I = blockIdx.z;
     if (J >= C.n1 || K >= C.n2) return;
+    const T* ratio;
+    if constexpr (sizeof(T) == 8)
+        ratio = reinterpret_cast<const T*>(t.ratio64);
+    else
+        ratio = reinterpret_cast<const T*>(t.ratio32);
     T acc = T(0);
-    for (int a = 0; a < R0; ++a) {
-        const int i = I * R0 + a;
+    for (int a = 0; a < t.R0; ++a) {
+        const int i = I * t.R0 + a;
         const T ra = ldg(ratio + i);
-        for (int bb = 0; bb < R1; ++bb) {
-            const int j = J * R1 + bb;
+        for (int bb = 0; bb < t.R1; ++bb) {
+            const int j = J * t.R1 + bb;
             const T rab = ra * ldg(ratio + F.n0 + j);
-            for (int e = 0; e < R2; ++e) {
-                const int k = K * R2 + e;
+            for (int e = 0; e < t.R2; ++e) {
+                const int k = K * t.R2 + e;
                 const long c = F.base + (long)i * F.si + (long)j * F.sj + k;
                 T w[6], s, d;
                 couplings<T, VAR>(F, i, j, k, c, w);
@@ -119,25 +139,34 @@ __global__ void __launch_bounds__(256) k_residual_restrict(LevelView<T> F, Level
             }
         }
     }
-    const long cc = C.base + (long)I * C.si + (long)J * C.sj + K;
-    C.b[cc] = acc;
+    C.b[C.base + (long)I * C.si + (long)J * C.sj + K] = acc;
 }
 
 // ---------------------------------------------------------------------------
 // Fused prolongation + correction: x_f += trilinear interpolation of the
 // coarse correction (linearProlongationScheme.C:12-147).  Per fine index the
 // host tables give the two coarse indices (own parent and the neighbour on
-// the fine cell's side, wrapped on periodic axes) and the neighbour's weight;
-// at walls the weight is zero, which equals the reference's use of a
-// zero-gradient ghost there.
+// the fine cell's side) and the neighbour's weight.  On a single brick the
+// neighbour index is wrapped on periodic axes and the weight is zero at
+// walls (the reference's zero-gradient ghost gives the same value); between
+// bricks the neighbour is the coarse ghost cell, refreshed before the call.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) k_prolong_correct(LevelView<T> F, LevelView<T> C,
-                                                         const int* pidx, const T* pw) {
+__global__ void __launch_bounds__(256) k_prolong_correct(Bricks<T> FB, Bricks<T> CB, TransferSet ts) {
+    int i;
+    const int b = brick_of(FB, blockIdx.z, i);
+    const LevelView<T>& F = FB.v[b];
+    const LevelView<T>& C = CB.v[b];
+    const TransferTabs& t = ts.t[b];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
     if (j >= F.n1 || k >= F.n2) return;
+    const int* pidx = t.pidx;
+    const T* pw;
+    if constexpr (sizeof(T) == 8)
+        pw = reinterpret_cast<const T*>(t.pw64);
+    else
+        pw = reinterpret_cast<const T*>(t.pw32);
     const int I0 = ldg(pidx + 2 * i), I1 = ldg(pidx + 2 * i + 1);
     const int J0 = ldg(pidx + 2 * F.n0 + 2 * j), J1 = ldg(pidx + 2 * F.n0 + 2 * j + 1);
     const int K0 = ldg(pidx + 2 * (F.n0 + F.n1) + 2 * k);
@@ -161,17 +190,15 @@ __global__ void __launch_bounds__(256) k_prolong_correct(LevelView<T> F, LevelVi
 // ---------------------------------------------------------------------------
 // Coarse direct solve: x = inverse(A'_pinned) b' with b'(0) = 0 (MG.C:37-40,
 // solver.C:201-231, APLU.C:91-128).  One CTA; the inverse is factored once
-// per matrix on the host in FP64.
+// per matrix on the host in FP64.  cidx gives the slab index of every
+// unknown (bricks one after another, k fastest).
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) k_coarse_solve(LevelView<T> C, const double* __restrict__ ainv,
-                                                      int n) {
+__global__ void __launch_bounds__(256) k_coarse_solve(Bricks<T> CB, const double* __restrict__ ainv,
+                                                      const int* __restrict__ cidx, int n) {
     extern __shared__ double sb[];
-    const int nn = C.n1 * C.n2;
-    for (int q = threadIdx.x; q < n; q += blockDim.x) {
-        const int i = q / nn, j = (q / C.n2) % C.n1, k = q % C.n2;
-        sb[q] = q == 0 ? 0.0 : (double)C.b[C.base + (long)i * C.si + (long)j * C.sj + k];
-    }
+    const T* bsrc = CB.v[0].b;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) sb[q] = q == 0 ? 0.0 : (double)bsrc[cidx[q]];
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int r = warp; r < n; r += nw) {
@@ -179,18 +206,32 @@ __global__ void __launch_bounds__(256) k_coarse_solve(LevelView<T> C, const doub
         for (int l = lane; l < n; l += 32) s += ainv[(long)r * n + l] * sb[l];
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (lane == 0) {
-            const int i = r / nn, j = (r / C.n2) % C.n1, k = r % C.n2;
-            store_x(C, C.base + (long)i * C.si + (long)j * C.sj + k, i, j, k, (T)s);
+            if (CB.nb == 1) {
+                // single brick: also refresh the periodic ghost images
+                const LevelView<T>& C = CB.v[0];
+                const int nn = C.n1 * C.n2;
+                const int i = r / nn, j = (r / C.n2) % C.n1, k = r % C.n2;
+                store_x(C, C.base + (long)i * C.si + (long)j * C.sj + k, i, j, k, (T)s);
+            } else {
+                CB.v[0].x[cidx[r]] = (T)s;
+            }
         }
     }
 }
 
+template <typename T>
+__global__ void k_fill_ghosts(T* x, const int* __restrict__ dst, const int* __restrict__ src, long n) {
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
+        x[dst[q]] = x[src[q]];
+}
+
 // residual r = b - A x of any level, unscaled, into a compact array
 template <typename T, bool VAR>
-__global__ void __launch_bounds__(256) k_residual_out(LevelView<T> L, double* out) {
+__global__ void __launch_bounds__(256) k_residual_out(Bricks<T> B, double* out) {
+    int i;
+    const LevelView<T>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
     if (j >= L.n1 || k >= L.n2) return;
     const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
     T w[6], s, d;
@@ -198,7 +239,7 @@ __global__ void __launch_bounds__(256) k_residual_out(LevelView<T> L, double* ou
     stencil(L.x, c, L.si, L.sj, w, s, d);
     const double r = (double)(L.b[c] + d * L.x[c] - s);
     const double V = L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j] * L.tab64[L.to.h[2] + k];
-    out[((long)i * L.n1 + j) * L.n2 + k] = r * V;
+    out[L.cbase + ((long)i * L.n1 + j) * L.n2 + k] = r * V;
 }
 
 template <int NT>
@@ -218,24 +259,27 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
     return v;
 }
 
+__device__ __forceinline__ long block_id() {
+    return ((long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+}
+
 // ---------------------------------------------------------------------------
 // Level-0 residual norms in FP64 (MG.C:163-174,223-230; solver.C:13-61).
-// Fixed grid and fixed reduction tree: the result does not depend on timing.
-// mode 0 also accumulates the normFactor sum (|r - b| + |b|)^2, where the
-// row sums of the level-0 operator vanish (all couplings are paired with the
-// centre), so A*mean(x) drops out of the reference's expression.
+// One cell per thread over the same grid as the other cell kernels, one
+// partial sum per block; the finalize kernel adds the partials in a fixed
+// order, so sums are reproducible.  mode 0 also accumulates the normFactor
+// sum (|r - b| + |b|)^2: the row sums of the level-0 operator vanish (every
+// coupling is paired with the centre), so A*mean(x) drops out of the
+// reference's expression.
 // ---------------------------------------------------------------------------
-// One cell per thread over the same (k, j, i) grid as the other cell
-// kernels, one partial sum per block in fixed block order; the finalize
-// kernel adds the partials in a fixed order, so sums are reproducible.
 template <bool VAR>
-__global__ void __launch_bounds__(kReduceThreads) k_residual_norm(LevelView<double> L, int mode,
-                                                                  double* partials, long nblocks,
-                                                                  float* b32) {
+__global__ void __launch_bounds__(kReduceThreads) k_residual_norm(Bricks<double> B, int mode, double* partials,
+                                                                  long nblocks, float* b32) {
     __shared__ double sh[kReduceThreads / 32];
+    int i;
+    const LevelView<double>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
     double a1 = 0.0, a2 = 0.0;
     if (j < L.n1 && k < L.n2) {
         const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
@@ -253,7 +297,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_residual_norm(LevelView<doub
         }
         if (b32) b32[c] = (float)r;
     }
-    const long bid = ((long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    const long bid = block_id();
     a1 = block_sum<kReduceThreads>(a1, sh);
     if (mode == 0) a2 = block_sum<kReduceThreads>(a2, sh);
     if (threadIdx.x == 0 && threadIdx.y == 0) {
@@ -301,19 +345,19 @@ __global__ void __launch_bounds__(kReduceThreads) k_finalize(const double* parti
     }
 }
 
-__global__ void __launch_bounds__(kReduceThreads) k_mean_partials(LevelView<double> L, double* partials) {
+__global__ void __launch_bounds__(kReduceThreads) k_mean_partials(Bricks<double> B, double* partials) {
     __shared__ double sh[kReduceThreads / 32];
+    int i;
+    const LevelView<double>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
     double a = 0.0;
     if (j < L.n1 && k < L.n2) {
         const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
         a = L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j] * L.tab64[L.to.h[2] + k] * L.x[c];
     }
     a = block_sum<kReduceThreads>(a, sh);
-    if (threadIdx.x == 0 && threadIdx.y == 0)
-        partials[((long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = a;
+    if (threadIdx.x == 0 && threadIdx.y == 0) partials[block_id()] = a;
 }
 
 __global__ void __launch_bounds__(kReduceThreads) k_mean_finalize(const double* partials, long nblocks,
@@ -333,43 +377,46 @@ __global__ void k_sub_mean(double* x, long n, const SolveState* st) {
         x[q] -= m;
 }
 
-__global__ void __launch_bounds__(256) k_load_b(LevelView<double> L, const double* compact) {
+__global__ void __launch_bounds__(256) k_load_b(Bricks<double> B, const double* compact) {
+    int i;
+    const LevelView<double>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
     if (j >= L.n1 || k >= L.n2) return;
     const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
     const double V = L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j] * L.tab64[L.to.h[2] + k];
-    L.b[c] = compact[((long)i * L.n1 + j) * L.n2 + k] / V;
+    L.b[c] = compact[L.cbase + ((long)i * L.n1 + j) * L.n2 + k] / V;
 }
 
-__global__ void __launch_bounds__(256) k_load_x(LevelView<double> L, const double* compact) {
+__global__ void __launch_bounds__(256) k_load_x(Bricks<double> B, const double* compact) {
+    int i;
+    const LevelView<double>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
     if (j >= L.n1 || k >= L.n2) return;
     const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
-    store_x(L, c, i, j, k, compact[((long)i * L.n1 + j) * L.n2 + k]);
+    store_x(L, c, i, j, k, compact[L.cbase + ((long)i * L.n1 + j) * L.n2 + k]);
 }
 
-__global__ void __launch_bounds__(256) k_store_x(LevelView<double> L, double* compact) {
+__global__ void __launch_bounds__(256) k_store_x(Bricks<double> B, double* compact) {
+    int i;
+    const LevelView<double>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
     if (j >= L.n1 || k >= L.n2) return;
     const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
-    compact[((long)i * L.n1 + j) * L.n2 + k] = L.x[c];
+    compact[L.cbase + ((long)i * L.n1 + j) * L.n2 + k] = L.x[c];
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_load_field(LevelView<T> L, int field, const double* compact,
-                                                    int unscale) {
+__global__ void __launch_bounds__(256) k_load_field(Bricks<T> B, int field, const double* compact, int unscale) {
+    int i;
+    const LevelView<T>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
     if (j >= L.n1 || k >= L.n2) return;
     const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
-    double v = compact[((long)i * L.n1 + j) * L.n2 + k];
+    double v = compact[L.cbase + ((long)i * L.n1 + j) * L.n2 + k];
     if (field == 0) {
         store_x(L, c, i, j, k, (T)v);
     } else {
@@ -379,30 +426,28 @@ __global__ void __launch_bounds__(256) k_load_field(LevelView<T> L, int field, c
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_store_field(LevelView<T> L, int field, double* compact,
-                                                     int unscale) {
+__global__ void __launch_bounds__(256) k_store_field(Bricks<T> B, int field, double* compact, int unscale) {
+    int i;
+    const LevelView<T>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
     if (j >= L.n1 || k >= L.n2) return;
     const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
     double v = field == 0 ? (double)L.x[c] : (double)L.b[c];
     if (field == 1 && unscale)
         v *= L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j] * L.tab64[L.to.h[2] + k];
-    compact[((long)i * L.n1 + j) * L.n2 + k] = v;
+    compact[L.cbase + ((long)i * L.n1 + j) * L.n2 + k] = v;
 }
 
-__global__ void __launch_bounds__(256) k_add_correction(LevelView<double> L, const float* e) {
+__global__ void __launch_bounds__(256) k_add_correction(Bricks<double> B, Bricks<float> E) {
+    int i;
+    const int b = brick_of(B, blockIdx.z, i);
+    const LevelView<double>& L = B.v[b];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
     if (j >= L.n1 || k >= L.n2) return;
     const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
-    store_x(L, c, i, j, k, L.x[c] + (double)e[c]);
-}
-
-inline dim3 grid_cells(int n0, int n1, int n2, dim3 blk) {
-    return dim3((n2 + blk.x - 1) / blk.x, (n1 + blk.y - 1) / blk.y, n0);
+    store_x(L, c, i, j, k, L.x[c] + (double)E.v[b].x[c]);
 }
 
 inline dim3 block_for(int n2) {
@@ -413,147 +458,141 @@ inline dim3 block_for(int n2) {
     return dim3(8, 32, 1);
 }
 
+template <typename T>
+inline dim3 grid_for(const Bricks<T>& B, int nk, dim3 blk) {
+    return dim3((nk + blk.x - 1) / blk.x, (B.max1 + blk.y - 1) / blk.y, B.z0[B.nb]);
+}
+
 }  // namespace
 
 // ---- launchers --------------------------------------------------------------
 
-long reduce_blocks(const LevelView<double>& L) {
-    const dim3 blk = block_for(L.n2);
-    const dim3 g = grid_cells(L.n0, L.n1, L.n2, blk);
+long reduce_blocks(const Bricks<double>& B) {
+    const dim3 blk = block_for(B.max2);
+    const dim3 g = grid_for(B, B.max2, blk);
     return (long)g.x * g.y * g.z;
 }
 
 template <typename T, bool VAR>
-void launch_colour_pass(const LevelView<T>& L, int colour, cudaStream_t s) {
-    const int pairs = (L.n2 + 1) / 2;
+void launch_colour_pass(const Bricks<T>& B, int colour, cudaStream_t s) {
+    const int pairs = (B.max2 + 1) / 2;
     const dim3 blk = pairs >= 32 ? dim3(32, 8, 1) : pairs >= 8 ? dim3(8, 32, 1) : dim3(2, 128, 1);
-    k_colour_pass<T, VAR><<<grid_cells(L.n0, L.n1, pairs, blk), blk, 0, s>>>(L, colour);
+    k_colour_pass<T, VAR><<<grid_for(B, pairs, blk), blk, 0, s>>>(B, colour);
 }
 
 template <typename T, bool VAR>
-void launch_jacobi(const LevelView<T>& L, T* tmp, cudaStream_t s) {
-    const dim3 blk = block_for(L.n2);
-    k_jacobi<T, VAR><<<grid_cells(L.n0, L.n1, L.n2, blk), blk, 0, s>>>(L, tmp);
-    k_copy_interior<T><<<grid_cells(L.n0, L.n1, L.n2, blk), blk, 0, s>>>(L, tmp);
+void launch_jacobi(const Bricks<T>& B, T* tmp, cudaStream_t s) {
+    const dim3 blk = block_for(B.max2);
+    k_jacobi<T, VAR><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, tmp);
+    k_copy_interior<T><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, tmp);
 }
 
 template <typename T, bool VAR>
-void launch_residual_restrict(const LevelView<T>& F, const LevelView<T>& C, const TransferTabs& t,
-                              cudaStream_t s) {
-    const dim3 blk = block_for(C.n2);
-    const T* ratio;
-    if constexpr (sizeof(T) == 8)
-        ratio = reinterpret_cast<const T*>(t.ratio64);
-    else
-        ratio = reinterpret_cast<const T*>(t.ratio32);
-    k_residual_restrict<T, VAR>
-        <<<grid_cells(C.n0, C.n1, C.n2, blk), blk, 0, s>>>(F, C, ratio, t.R0, t.R1, t.R2);
+void launch_residual_restrict(const Bricks<T>& F, const Bricks<T>& C, const TransferSet& t, cudaStream_t s) {
+    const dim3 blk = block_for(C.max2);
+    k_residual_restrict<T, VAR><<<grid_for(C, C.max2, blk), blk, 0, s>>>(F, C, t);
 }
 
 template <typename T>
-void launch_prolong_correct(const LevelView<T>& F, const LevelView<T>& C, const TransferTabs& t,
-                            cudaStream_t s) {
-    const dim3 blk = block_for(F.n2);
-    const T* pw;
-    if constexpr (sizeof(T) == 8)
-        pw = reinterpret_cast<const T*>(t.pw64);
-    else
-        pw = reinterpret_cast<const T*>(t.pw32);
-    k_prolong_correct<T><<<grid_cells(F.n0, F.n1, F.n2, blk), blk, 0, s>>>(F, C, t.pidx, pw);
+void launch_prolong_correct(const Bricks<T>& F, const Bricks<T>& C, const TransferSet& t, cudaStream_t s) {
+    const dim3 blk = block_for(F.max2);
+    k_prolong_correct<T><<<grid_for(F, F.max2, blk), blk, 0, s>>>(F, C, t);
 }
 
 template <typename T>
-void launch_coarse_solve(const LevelView<T>& C, const double* ainv, int n, cudaStream_t s) {
-    k_coarse_solve<T><<<1, 256, n * sizeof(double), s>>>(C, ainv, n);
+void launch_coarse_solve(const Bricks<T>& C, const double* ainv, const int* cidx, int n, cudaStream_t s) {
+    k_coarse_solve<T><<<1, 256, n * sizeof(double), s>>>(C, ainv, cidx, n);
+}
+
+template <typename T>
+void launch_fill_ghosts(T* x, const int* dst, const int* src, long n, cudaStream_t s) {
+    const int blocks = (int)std::min<long>((n + 255) / 256, 148L * 8);
+    k_fill_ghosts<T><<<blocks, 256, 0, s>>>(x, dst, src, n);
 }
 
 template <typename T, bool VAR>
-void launch_residual_out(const LevelView<T>& L, double* out, cudaStream_t s) {
-    const dim3 blk = block_for(L.n2);
-    k_residual_out<T, VAR><<<grid_cells(L.n0, L.n1, L.n2, blk), blk, 0, s>>>(L, out);
+void launch_residual_out(const Bricks<T>& B, double* out, cudaStream_t s) {
+    const dim3 blk = block_for(B.max2);
+    k_residual_out<T, VAR><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, out);
 }
 
 template <bool VAR>
-void launch_residual_norm(const LevelView<double>& L, int mode, double* partials, float* b32,
-                          const LevelView<float>*, cudaStream_t s) {
-    const dim3 blk = block_for(L.n2);
-    k_residual_norm<VAR><<<grid_cells(L.n0, L.n1, L.n2, blk), blk, 0, s>>>(L, mode, partials,
-                                                                          reduce_blocks(L), b32);
+void launch_residual_norm(const Bricks<double>& B, int mode, double* partials, float* b32, cudaStream_t s) {
+    const dim3 blk = block_for(B.max2);
+    k_residual_norm<VAR><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, mode, partials, reduce_blocks(B), b32);
 }
 
-void launch_finalize(const LevelView<double>& L, const double* partials, SolveState* st, int mode,
+void launch_finalize(const Bricks<double>& B, const double* partials, SolveState* st, int mode,
                      cudaGraphConditionalHandle cond, int setCondition, cudaStream_t s) {
-    k_finalize<<<1, kReduceThreads, 0, s>>>(partials, reduce_blocks(L), st, mode, cond, setCondition);
+    k_finalize<<<1, kReduceThreads, 0, s>>>(partials, reduce_blocks(B), st, mode, cond, setCondition);
 }
 
-void launch_mean(const LevelView<double>& L, double* partials, SolveState* st, cudaStream_t s) {
-    const dim3 blk = block_for(L.n2);
-    k_mean_partials<<<grid_cells(L.n0, L.n1, L.n2, blk), blk, 0, s>>>(L, partials);
-    k_mean_finalize<<<1, kReduceThreads, 0, s>>>(partials, reduce_blocks(L), st);
-    const long n = L.cells;
+void launch_mean(const Bricks<double>& B, double* partials, SolveState* st, cudaStream_t s) {
+    const dim3 blk = block_for(B.max2);
+    k_mean_partials<<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, partials);
+    k_mean_finalize<<<1, kReduceThreads, 0, s>>>(partials, reduce_blocks(B), st);
+    const long n = B.v[0].cells;
     const int blocks = (int)std::min<long>((n + 255) / 256, 148L * 16);
-    k_sub_mean<<<blocks, 256, 0, s>>>(L.x, n, st);
+    k_sub_mean<<<blocks, 256, 0, s>>>(B.v[0].x, n, st);
 }
 
-void launch_load_b(const LevelView<double>& L, const double* compact, cudaStream_t s) {
-    const dim3 blk = block_for(L.n2);
-    k_load_b<<<grid_cells(L.n0, L.n1, L.n2, blk), blk, 0, s>>>(L, compact);
+void launch_load_b(const Bricks<double>& B, const double* compact, cudaStream_t s) {
+    const dim3 blk = block_for(B.max2);
+    k_load_b<<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, compact);
 }
 
-void launch_load_x(const LevelView<double>& L, const double* compact, cudaStream_t s) {
-    const dim3 blk = block_for(L.n2);
-    k_load_x<<<grid_cells(L.n0, L.n1, L.n2, blk), blk, 0, s>>>(L, compact);
+void launch_load_x(const Bricks<double>& B, const double* compact, cudaStream_t s) {
+    const dim3 blk = block_for(B.max2);
+    k_load_x<<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, compact);
 }
 
-void launch_store_x(const LevelView<double>& L, double* compact, cudaStream_t s) {
-    const dim3 blk = block_for(L.n2);
-    k_store_x<<<grid_cells(L.n0, L.n1, L.n2, blk), blk, 0, s>>>(L, compact);
-}
-
-template <typename T>
-void launch_load_field(const LevelView<T>& L, int field, const double* compact, int unscale,
-                       cudaStream_t s) {
-    const dim3 blk = block_for(L.n2);
-    k_load_field<T><<<grid_cells(L.n0, L.n1, L.n2, blk), blk, 0, s>>>(L, field, compact, unscale);
+void launch_store_x(const Bricks<double>& B, double* compact, cudaStream_t s) {
+    const dim3 blk = block_for(B.max2);
+    k_store_x<<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, compact);
 }
 
 template <typename T>
-void launch_store_field(const LevelView<T>& L, int field, double* compact, int unscale,
-                        cudaStream_t s) {
-    const dim3 blk = block_for(L.n2);
-    k_store_field<T><<<grid_cells(L.n0, L.n1, L.n2, blk), blk, 0, s>>>(L, field, compact, unscale);
+void launch_load_field(const Bricks<T>& B, int field, const double* compact, int unscale, cudaStream_t s) {
+    const dim3 blk = block_for(B.max2);
+    k_load_field<T><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, field, compact, unscale);
 }
 
-void launch_add_correction(const LevelView<double>& L, const LevelView<float>& E, cudaStream_t s) {
-    const dim3 blk = block_for(L.n2);
-    k_add_correction<<<grid_cells(L.n0, L.n1, L.n2, blk), blk, 0, s>>>(L, E.x);
+template <typename T>
+void launch_store_field(const Bricks<T>& B, int field, double* compact, int unscale, cudaStream_t s) {
+    const dim3 blk = block_for(B.max2);
+    k_store_field<T><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, field, compact, unscale);
+}
+
+void launch_add_correction(const Bricks<double>& B, const Bricks<float>& E, cudaStream_t s) {
+    const dim3 blk = block_for(B.max2);
+    k_add_correction<<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, E);
 }
 
 // explicit instantiations
-#define BMG_INST(T, V)                                                                          \
-    template void launch_colour_pass<T, V>(const LevelView<T>&, int, cudaStream_t);             \
-    template void launch_jacobi<T, V>(const LevelView<T>&, T*, cudaStream_t);                   \
-    template void launch_residual_restrict<T, V>(const LevelView<T>&, const LevelView<T>&,      \
-                                                 const TransferTabs&, cudaStream_t);            \
-    template void launch_residual_out<T, V>(const LevelView<T>&, double*, cudaStream_t);
+#define BMG_INST(T, V)                                                                                   \
+    template void launch_colour_pass<T, V>(const Bricks<T>&, int, cudaStream_t);                         \
+    template void launch_jacobi<T, V>(const Bricks<T>&, T*, cudaStream_t);                               \
+    template void launch_residual_restrict<T, V>(const Bricks<T>&, const Bricks<T>&, const TransferSet&, \
+                                                 cudaStream_t);                                          \
+    template void launch_residual_out<T, V>(const Bricks<T>&, double*, cudaStream_t);
 BMG_INST(double, false)
 BMG_INST(double, true)
 BMG_INST(float, false)
 BMG_INST(float, true)
 #undef BMG_INST
-template void launch_prolong_correct<double>(const LevelView<double>&, const LevelView<double>&,
-                                             const TransferTabs&, cudaStream_t);
-template void launch_prolong_correct<float>(const LevelView<float>&, const LevelView<float>&,
-                                            const TransferTabs&, cudaStream_t);
-template void launch_coarse_solve<double>(const LevelView<double>&, const double*, int, cudaStream_t);
-template void launch_coarse_solve<float>(const LevelView<float>&, const double*, int, cudaStream_t);
-template void launch_residual_norm<false>(const LevelView<double>&, int, double*, float*,
-                                          const LevelView<float>*, cudaStream_t);
-template void launch_residual_norm<true>(const LevelView<double>&, int, double*, float*,
-                                         const LevelView<float>*, cudaStream_t);
-template void launch_load_field<double>(const LevelView<double>&, int, const double*, int, cudaStream_t);
-template void launch_load_field<float>(const LevelView<float>&, int, const double*, int, cudaStream_t);
-template void launch_store_field<double>(const LevelView<double>&, int, double*, int, cudaStream_t);
-template void launch_store_field<float>(const LevelView<float>&, int, double*, int, cudaStream_t);
+template void launch_prolong_correct<double>(const Bricks<double>&, const Bricks<double>&, const TransferSet&,
+                                             cudaStream_t);
+template void launch_prolong_correct<float>(const Bricks<float>&, const Bricks<float>&, const TransferSet&,
+                                            cudaStream_t);
+template void launch_coarse_solve<double>(const Bricks<double>&, const double*, const int*, int, cudaStream_t);
+template void launch_coarse_solve<float>(const Bricks<float>&, const double*, const int*, int, cudaStream_t);
+template void launch_fill_ghosts<double>(double*, const int*, const int*, long, cudaStream_t);
+template void launch_fill_ghosts<float>(float*, const int*, const int*, long, cudaStream_t);
+template void launch_residual_norm<false>(const Bricks<double>&, int, double*, float*, cudaStream_t);
+template void launch_residual_norm<true>(const Bricks<double>&, int, double*, float*, cudaStream_t);
+template void launch_load_field<double>(const Bricks<double>&, int, const double*, int, cudaStream_t);
+template void launch_load_field<float>(const Bricks<float>&, int, const double*, int, cudaStream_t);
+template void launch_store_field<double>(const Bricks<double>&, int, double*, int, cudaStream_t);
+template void launch_store_field<float>(const Bricks<float>&, int, double*, int, cudaStream_t);
 
 }  // namespace bmg

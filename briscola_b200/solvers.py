@@ -195,6 +195,7 @@ class Context:
         self.h = h
         self.opts = opts
         self.n_cells = L.bmg_num_cells(h)
+        self.n_bricks = len(mesh.bricks)
 
     def close(self):
         if getattr(self, "h", None):
@@ -260,17 +261,26 @@ class Context:
                                         a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
         self.check(rc, "bmg_level_upload")
 
+    def _level_array(self, level: int) -> np.ndarray:
+        # one brick: (n0, n1, n2); several: the bricks' cells one after another
+        if self.n_bricks == 1:
+            return np.zeros(self.shape(level))
+        return np.zeros(sum(int(np.prod(s)) for s in self.shapes(level)))
+
     def download(self, level: int, field: str, precision: int = 0) -> np.ndarray:
-        out = np.zeros(self.shape(level))
+        out = self._level_array(level)
         rc = self._lib.bmg_level_download(self.h, level, {"x": 0, "b": 1}[field], precision,
                                           out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
         self.check(rc, "bmg_level_download")
         return out
 
-    def shape(self, level: int):
+    def shape(self, level: int, brick: int = 0):
         n = (ctypes.c_int * 3)()
-        self.check(self._lib.bmg_level_shape(self.h, level, 0, n), "bmg_level_shape")
+        self.check(self._lib.bmg_level_shape(self.h, level, brick, n), "bmg_level_shape")
         return tuple(n)
+
+    def shapes(self, level: int):
+        return [self.shape(level, q) for q in range(self.n_bricks)]
 
     @property
     def num_levels(self) -> int:
@@ -294,7 +304,7 @@ class Context:
         self.check(self._lib.bmg_op_smooth(self.h, level, sweeps, precision), "smooth")
 
     def residual(self, level, precision=0) -> np.ndarray:
-        out = np.zeros(self.shape(level))
+        out = self._level_array(level)
         rc = self._lib.bmg_op_residual(self.h, level, precision,
                                        out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
         self.check(rc, "residual")

@@ -13,6 +13,12 @@ No dataset is involved: every right-hand side is generated from a seed.
   distance ramped over 2 cells, face coefficient lambda = mean of 1/rho of the
   two cells; N(0,1) zero-mean RHS.
 
+* ``multibrick(scale)`` -- seven axis-aligned bricks of uneven sizes
+  (128x64x64, 96x96x96, 64x128x32, 128x32x64, 64x64x64, 48x96x48,
+  32x32x128 cells) joined by cell-conforming contacts, Neumann outer walls,
+  uniform spacing 1/128; every size and origin divided by ``scale`` (1, 2, 4
+  or 8) for smaller cases.  N(0,1) cell RHS, volume-weighted zero mean.
+
 Each returns (mesh, b, lam) with b the system right-hand side
 b_sys = -V f of the reference (linearSystem.C:547-556) as a flat float64
 array and lam None or the three face arrays.
@@ -110,4 +116,33 @@ def sphere(N: int = 256, seed: int = 4000):
     return Mesh([br]), np.ascontiguousarray((-V * f).ravel()), lam
 
 
-CONFIGS = {"cavity": cavity, "channel": channel, "sphere": sphere}
+# (cells, origin) of the seven bricks, in cells of spacing 1/128; origins are
+# multiples of 16 so that the bricks coarsen together four times
+MULTIBRICK_LAYOUT = [
+    ((128, 64, 64), (0, 0, 0)),
+    ((96, 96, 96), (128, 0, 0)),
+    ((64, 128, 32), (0, 64, 0)),
+    ((128, 32, 64), (0, 192, 0)),
+    ((64, 64, 64), (224, 0, 0)),
+    ((48, 96, 48), (64, 64, 0)),
+    ((32, 32, 128), (0, 0, 64)),
+]
+
+
+def multibrick(scale: int = 1, seed: int = 3000):
+    h = scale / 128.0
+    bricks = []
+    for n, o in MULTIBRICK_LAYOUT:
+        n = tuple(v // scale for v in n)
+        o = tuple(v // scale for v in o)
+        pts = [o[d] * h + h * np.arange(n[d] + 1, dtype=np.float64) for d in range(3)]
+        bricks.append(Brick(pts, (NEUMANN,) * 6, o))
+    rng = np.random.default_rng(seed)
+    f = [rng.standard_normal(br.N) for br in bricks]
+    V = [br.cell_volumes() for br in bricks]
+    mean = sum((v * a).sum() for v, a in zip(V, f)) / sum(v.sum() for v in V)
+    b = np.concatenate([(-v * (a - mean)).ravel() for v, a in zip(V, f)])
+    return Mesh(bricks), np.ascontiguousarray(b), None
+
+
+CONFIGS = {"cavity": cavity, "channel": channel, "sphere": sphere, "multibrick": multibrick}

@@ -87,3 +87,102 @@ def vmean(x, V):
 
 def rel(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+# ---------------------------------------------------------------------------
+# multi-brick meshes: the union-domain operator as an independent ground truth
+# ---------------------------------------------------------------------------
+def split_brick(brick, cuts):
+    """Split one brick into the product of the pieces between cut indices
+    (cuts[d] lists interior cell indices along axis d).  The pieces take
+    slices of the same coordinate arrays, so the union is the same mesh."""
+    from briscola_b200.mesh import Brick, Mesh
+
+    edges = [[0] + sorted(cuts[d]) + [brick.N[d]] for d in range(3)]
+    bricks = []
+    for a in range(len(edges[0]) - 1):
+        for b in range(len(edges[1]) - 1):
+            for c in range(len(edges[2]) - 1):
+                lo = (edges[0][a], edges[1][b], edges[2][c])
+                hi = (edges[0][a + 1], edges[1][b + 1], edges[2][c + 1])
+                pts = [brick.points[d][lo[d]:hi[d] + 1] for d in range(3)]
+                bricks.append(Brick(pts, brick.bc, lo))
+    return Mesh(bricks)
+
+
+def brick_to_compact(mesh, full):
+    """A field on the split brick's full (n0, n1, n2) array -> the C ABI's
+    order for the pieces (bricks one after another, k fastest)."""
+    parts = []
+    for br in mesh.bricks:
+        o, n = br.origin, br.N
+        parts.append(full[o[0]:o[0] + n[0], o[1]:o[1] + n[1], o[2]:o[2] + n[2]].ravel())
+    return np.concatenate(parts)
+
+
+def union_operator(mesh):
+    """Sparse FV Laplacian on the union of the bricks' cells: off-diagonal =
+    face area / centre distance (linearGaussLaplacianScheme.C:59-94 with
+    delta = 1/|cc_P - cc_N|), centre = -(sum of the row), Neumann outer walls.
+    Rows in the C ABI's order.  Returns (A, V) with V the cell volumes."""
+    import scipy.sparse as sp
+
+    lo = np.min([br.origin for br in mesh.bricks], axis=0)
+    hi = np.max([np.add(br.origin, br.N) for br in mesh.bricks], axis=0)
+    index = -np.ones(tuple(hi - lo), dtype=np.int64)
+    cc = [[], [], []]
+    hh = [[], [], []]
+    row0 = 0
+    for br in mesh.bricks:
+        n = br.N
+        o = np.subtract(br.origin, lo)
+        index[o[0]:o[0] + n[0], o[1]:o[1] + n[1], o[2]:o[2] + n[2]] = row0 + np.arange(np.prod(n)).reshape(n)
+        grids = np.meshgrid(*[br.cell_centres(d) for d in range(3)], indexing="ij")
+        sizes = np.meshgrid(*[br.cell_sizes(d) for d in range(3)], indexing="ij")
+        for d in range(3):
+            cc[d].append(grids[d].ravel())
+            hh[d].append(sizes[d].ravel())
+        row0 += int(np.prod(n))
+    cc = [np.concatenate(a) for a in cc]
+    hh = [np.concatenate(a) for a in hh]
+    rows, cols, vals = [], [], []
+    for d in range(3):
+        sl_a = [slice(None)] * 3
+        sl_b = [slice(None)] * 3
+        sl_a[d] = slice(0, -1)
+        sl_b[d] = slice(1, None)
+        p = index[tuple(sl_a)].ravel()
+        q = index[tuple(sl_b)].ravel()
+        ok = (p >= 0) & (q >= 0)
+        p, q = p[ok], q[ok]
+        t1, t2 = (d + 1) % 3, (d + 2) % 3
+        w = hh[t1][p] * hh[t2][p] / np.abs(cc[d][q] - cc[d][p])
+        rows += [p, q]
+        cols += [q, p]
+        vals += [w, w]
+    rows = np.concatenate(rows)
+    cols = np.concatenate(cols)
+    vals = np.concatenate(vals)
+    n = row0
+    A = sp.csr_matrix((vals, (rows, cols)), shape=(n, n))
+    A = A - sp.diags(np.asarray(A.sum(axis=1)).ravel())
+    V = hh[0] * hh[1] * hh[2]
+    return A.tocsr(), V
+
+
+def union_solve(mesh, b):
+    """Direct FP64 solve of the union-domain Neumann problem with the
+    reference's pin (first unknown fixed, solver.C:201-231), then the
+    volume-weighted mean removed."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spl
+
+    A, V = union_operator(mesh)
+    A = A.tolil()
+    A[0, :] = 0.0
+    A[:, 0] = 0.0
+    A[0, 0] = 1.0
+    rhs = b.copy()
+    rhs[0] = 0.0
+    x = spl.spsolve(sp.csc_matrix(A), rhs)
+    return vmean(x, V), V
