@@ -18,6 +18,7 @@ BC_NEUMANN, BC_PERIODIC = 0, 1
 CYCLE = {"V": 0, "W": 1, "F": 2}
 SMOOTHER = {"rbgs": 0, "jac": 1, "jacobi": 1}
 PRECISION = {"fp64": 0, "mixed": 1}
+KRYLOV = {"none": 0, "fcg": 1}
 DEVICE_PTRS, ZERO_GUESS = 1, 2
 
 # Every function the header declares; the loader checks they are exported.
@@ -62,6 +63,7 @@ class Options(ctypes.Structure):
         ("autotune", ctypes.c_int),
         ("device", ctypes.c_int),
         ("timeout_ms", ctypes.c_double),
+        ("krylov", ctypes.c_int),
     ]
 
 

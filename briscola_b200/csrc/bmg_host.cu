@@ -133,6 +133,13 @@ struct bmg_ctx {
     SolveState* st_host = nullptr;
     double* stage_b = nullptr;
     double* stage_x = nullptr;
+    // flexible CG outer loop (level-0 slabs): solution, scaled right-hand
+    // side, residual, direction p and q = A'p
+    double* fx = nullptr;
+    double* fb = nullptr;
+    double* fr = nullptr;
+    double* fp = nullptr;
+    double* fq = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::string err;
     long launches = 0;  // kernels launched by the current solve
@@ -460,7 +467,7 @@ void freeAll(bmg_ctx* c) {
             for (void* p : {(void*)t.ratio64, (void*)t.ratio32, (void*)t.pidx, (void*)t.pw64, (void*)t.pw32})
                 if (p) cudaFree(p);
     for (void* p : {(void*)c->ainv, (void*)c->cidx, (void*)c->partials, (void*)c->st, (void*)c->stage_b,
-                    (void*)c->stage_x})
+                    (void*)c->stage_x, (void*)c->fx, (void*)c->fb, (void*)c->fr, (void*)c->fp, (void*)c->fq})
         if (p) cudaFree(p);
     if (c->st_host) cudaFreeHost(c->st_host);
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -479,6 +486,7 @@ void validateOptions(const bmg_options* o) {
     if (o->precision < 0 || o->precision > 1) throw BadArg{BMG_BAD_ARG, "unknown precision"};
     if (o->coarse_level < 0) throw BadArg{BMG_BAD_ARG, "negative coarseLevel"};
     if (o->fused < 0) throw BadArg{BMG_BAD_ARG, "negative fused stage count"};
+    if (o->krylov < 0 || o->krylov > 1) throw BadArg{BMG_BAD_ARG, "unknown krylov"};
 }
 
 // Level-0 bricks from the mesh description; contacts between bricks.
@@ -839,6 +847,12 @@ void configureCoarse(bmg_ctx* c) {
     buildCoarseInverse(c);
 }
 
+void ensureKrylovBuffers(bmg_ctx* c) {
+    const long n = c->lv[0].cells;
+    for (double** p : {&c->fx, &c->fb, &c->fr, &c->fp, &c->fq})
+        if (!*p) *p = dalloc<double>(n);
+}
+
 void ensureJacobiBuffers(bmg_ctx* c) {
     for (auto& L : c->lv) {
         if (!L.jtmp64) L.jtmp64 = dalloc<double>(L.cells);
@@ -894,16 +908,20 @@ void swapX(HostLevel& L) {
 
 // refresh the ghost frames of a multi-brick level (device-side exchange)
 template <typename T>
-void exchange(bmg_ctx* c, int l) {
+void exchangeField(bmg_ctx* c, int l, T* x) {
     HostLevel& L = c->lv[l];
     if (!L.nghost) return;
-    T* x;
-    if constexpr (sizeof(T) == 8)
-        x = reinterpret_cast<T*>(L.x64);
-    else
-        x = reinterpret_cast<T*>(L.x32);
     c->launches += 1;
     launch_fill_ghosts<T>(x, L.gdst, L.gsrc, L.nghost, c->stream);
+}
+
+template <typename T>
+void exchange(bmg_ctx* c, int l) {
+    HostLevel& L = c->lv[l];
+    if constexpr (sizeof(T) == 8)
+        exchangeField<T>(c, l, reinterpret_cast<T*>(L.x64));
+    else
+        exchangeField<T>(c, l, reinterpret_cast<T*>(L.x32));
 }
 
 template <typename T>
@@ -1105,13 +1123,19 @@ SolveState initialState(const bmg_ctx* c) {
         vol += v[0] * v[1] * v[2];
     }
     init.vol_total = vol;
+    init.first = 1;
     return init;
 }
 
 // MG.C:144-190: load b (scaled) and x, initial residual, normFactor and the
 // first convergence test.  The state is copied from the pinned host copy,
 // which the caller fills before every solve (also when replayed as a graph).
+void segInitFcg(bmg_ctx* c, const double* bsrc, const double* xsrc, bool zero, bool setCondition);
+void segBodyFcg(bmg_ctx* c, bool setCondition);
+void segPostFcg(bmg_ctx* c, double* xdst);
+
 void segInit(bmg_ctx* c, const double* bsrc, const double* xsrc, bool zero, bool setCondition) {
+    if (c->opt.krylov == BMG_KRYLOV_FCG) return segInitFcg(c, bsrc, xsrc, zero, setCondition);
     cudaStream_t s = c->stream;
     HostLevel& L0 = c->lv[0];
     const Bricks<double> V0 = bricks<double>(c, 0);
@@ -1130,6 +1154,7 @@ void segInit(bmg_ctx* c, const double* bsrc, const double* xsrc, bool zero, bool
 // cycle solves for the correction of the FP64 residual (written in FP32 by
 // the residual kernel), which is then added in FP64.
 void segBody(bmg_ctx* c, bool setCondition) {
+    if (c->opt.krylov == BMG_KRYLOV_FCG) return segBodyFcg(c, setCondition);
     cudaStream_t s = c->stream;
     HostLevel& L0 = c->lv[0];
     std::fill(c->visits.begin(), c->visits.end(), 0);
@@ -1145,12 +1170,98 @@ void segBody(bmg_ctx* c, bool setCondition) {
 }
 
 void segPost(bmg_ctx* c, double* xdst) {
+    if (c->opt.krylov == BMG_KRYLOV_FCG) return segPostFcg(c, xdst);
     const Bricks<double> V0 = bricks<double>(c, 0);
     if (c->opt.remove_mean) {
         launch_mean(V0, c->partials, c->st, c->stream);
         c->launches += 3;
     }
     launch_store_x(V0, xdst, c->stream);
+    c->launches += 1;
+}
+
+// ---- flexible CG outer loop (bmg_krylov.cu) ----------------------------------
+// level-0 FP64 view whose x and b are the outer loop's solution and RHS
+Bricks<double> fcgView(const bmg_ctx* c) {
+    Bricks<double> V = bricks<double>(c, 0);
+    for (int b = 0; b < V.nb; ++b) {
+        V.v[b].x = c->fx;
+        V.v[b].b = c->fb;
+    }
+    return V;
+}
+
+void segInitFcg(bmg_ctx* c, const double* bsrc, const double* xsrc, bool zero, bool setCondition) {
+    cudaStream_t s = c->stream;
+    const Bricks<double> V = fcgView(c);
+    const bool mixed = c->opt.precision == BMG_PRECISION_MIXED;
+    launch_load_b(V, bsrc, s);
+    BMG_CUDA(cudaMemsetAsync(c->fx, 0, c->lv[0].cells * sizeof(double), s));
+    c->launches += 1;
+    if (!zero) {
+        launch_load_x(V, xsrc, s);
+        c->launches += 1;
+    }
+    BMG_CUDA(cudaMemcpyAsync(c->st, c->st_host, sizeof(SolveState), cudaMemcpyHostToDevice, s));
+    exchangeField<double>(c, 0, c->fx);
+    float* pre32 = mixed ? c->lv[0].b32 : nullptr;
+    double* pre64 = mixed ? nullptr : c->lv[0].b64;
+    if (c->variable)
+        launch_fcg_residual<true>(V, 0, c->fr, pre32, pre64, c->partials, s);
+    else
+        launch_fcg_residual<false>(V, 0, c->fr, pre32, pre64, c->partials, s);
+    launch_finalize(V, c->partials, c->st, 0, c->cond, setCondition ? 1 : 0, s);
+    c->launches += 2;
+}
+
+template <typename T>
+void fcgStep(bmg_ctx* c, const T* z, float* pre32, double* pre64, bool setCondition) {
+    cudaStream_t s = c->stream;
+    const Bricks<double> V = fcgView(c);
+    launch_fcg_beta<T>(V, z, c->fr, c->fq, c->partials, c->st, s);
+    if (c->variable)
+        launch_fcg_direction<T, true>(V, z, c->fp, c->fq, c->partials, c->st, s);
+    else
+        launch_fcg_direction<T, false>(V, z, c->fp, c->fq, c->partials, c->st, s);
+    launch_fcg_update(V, c->fp, c->fr, c->fq, pre32, pre64, c->partials, c->st, s);
+    launch_finalize(V, c->partials, c->st, 1, c->cond, setCondition ? 1 : 0, s);
+    c->launches += 6;
+}
+
+// one preconditioning cycle z = cycle(r) from a zero guess, then one FCG step
+void segBodyFcg(bmg_ctx* c, bool setCondition) {
+    cudaStream_t s = c->stream;
+    HostLevel& L0 = c->lv[0];
+    std::fill(c->visits.begin(), c->visits.end(), 0);
+    if (c->opt.precision == BMG_PRECISION_MIXED) {
+        BMG_CUDA(cudaMemsetAsync(L0.x32, 0, L0.cells * sizeof(float), s));
+        cycle<float>(c, 0);
+        exchange<float>(c, 0);
+        fcgStep<float>(c, L0.x32, L0.b32, nullptr, setCondition);
+    } else {
+        BMG_CUDA(cudaMemsetAsync(L0.x64, 0, L0.cells * sizeof(double), s));
+        cycle<double>(c, 0);
+        exchange<double>(c, 0);
+        fcgStep<double>(c, L0.x64, nullptr, L0.b64, setCondition);
+    }
+}
+
+// the true residual of the final x, mean removal and store
+void segPostFcg(bmg_ctx* c, double* xdst) {
+    cudaStream_t s = c->stream;
+    const Bricks<double> V = fcgView(c);
+    exchangeField<double>(c, 0, c->fx);
+    if (c->variable)
+        launch_fcg_residual<true>(V, 2, nullptr, nullptr, nullptr, c->partials, s);
+    else
+        launch_fcg_residual<false>(V, 2, nullptr, nullptr, nullptr, c->partials, s);
+    launch_fcg_true_norm(V, c->partials, c->st, s);
+    c->launches += 2;
+    if (c->opt.remove_mean) {
+        launch_mean(V, c->partials, c->st, s);
+        c->launches += 3;
+    }
+    launch_store_x(V, xdst, s);
     c->launches += 1;
 }
 
@@ -1205,8 +1316,9 @@ void captureGraph(bmg_ctx* c, bool zero) {
     BMG_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     segBody(c, true);
     // the fused smoother swaps x buffers; level-0 x must come back to the
-    // buffer the next iteration (and the post segment) reads
-    if (c->lv[0].x64 != x0) {
+    // buffer the next iteration (and the post segment) reads (the flexible
+    // CG loop keeps its solution elsewhere)
+    if (c->lv[0].x64 != x0 && c->opt.krylov != BMG_KRYLOV_FCG) {
         BMG_CUDA(cudaMemcpyAsync(x0, c->lv[0].x64, c->lv[0].cells * sizeof(double), cudaMemcpyDeviceToDevice, s));
         std::swap(c->lv[0].x64, c->lv[0].x64b);
     }
@@ -1224,6 +1336,7 @@ int solveImpl(bmg_ctx* c, const double* b, double* x, int flags, bmg_report* rep
     const bool dev = flags & BMG_DEVICE_PTRS;
     const bool zero = flags & BMG_ZERO_GUESS;
     if (c->opt.smoother == BMG_SMOOTHER_JACOBI) ensureJacobiBuffers(c);
+    if (c->opt.krylov == BMG_KRYLOV_FCG) ensureKrylovBuffers(c);
     const auto t0 = std::chrono::steady_clock::now();
     *c->st_host = initialState(c);
     int status = BMG_OK;
@@ -1293,8 +1406,10 @@ int solveImpl(bmg_ctx* c, const double* b, double* x, int flags, bmg_report* rep
         rep->outer_iterations = st.iter;
         rep->initial_residual = st.init;
         rep->final_residual = st.cur;
-        rep->rel_residual = st.l2_0 > 0 ? st.l2 / st.l2_0 : 0.0;
-        rep->final_l2 = st.l2;
+        // the flexible CG loop updates r recursively; report the residual of x
+        const double l2 = c->opt.krylov == BMG_KRYLOV_FCG ? st.l2_true : st.l2;
+        rep->rel_residual = st.l2_0 > 0 ? l2 / st.l2_0 : 0.0;
+        rep->final_l2 = l2;
         rep->norm_factor = st.nf;
         rep->ms = ms;
         rep->kernel_launches = useGraph ? c->launchesInitPost + c->launchesBody * st.iter : c->launches;
@@ -1386,6 +1501,7 @@ int bmg_default_options(bmg_options* o) {
     o->autotune = 1;
     o->device = 0;
     o->timeout_ms = 0.0;
+    o->krylov = BMG_KRYLOV_NONE;
     return BMG_OK;
 }
 

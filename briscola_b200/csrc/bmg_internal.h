@@ -111,7 +111,14 @@ struct SolveState {
     int converged;
     int nan;
     int keep_going;
-    int pad[2];
+    int first;         // flexible CG: no previous direction yet
+    int pad;
+    // flexible CG scalars
+    double alpha;      // step length of the last update
+    double gamma;      // (z, V r) of the current direction
+    double beta;
+    double pq;         // (p, V q) of the current direction
+    double l2_true;    // ||b - A x||_2 recomputed from x after the loop
 };
 
 // Geometry of a fused smoothing launch (single brick): march axis m (0),
@@ -166,6 +173,27 @@ void launch_mean(const Bricks<double>& B, double* partials, SolveState* st, cuda
 long reduce_blocks(const Bricks<double>& B);
 // sets the dynamic shared memory limits of the fused smoother instances
 void configure_fused_kernels();
+
+// ---- flexible CG outer loop (bmg_krylov.cu), level 0, FP64 ------------------
+// r = b - A'x into r (and the cycle's right-hand side pre32 or pre64);
+// partials as launch_residual_norm.  mode 2: only ||V r||^2, nothing written.
+template <bool VAR>
+void launch_fcg_residual(const Bricks<double>& B, int mode, double* r, float* pre32, double* pre64,
+                         double* partials, cudaStream_t s);
+// partials of (z, V r) and (z, V q), then beta and gamma (kernel pair)
+template <typename T>
+void launch_fcg_beta(const Bricks<double>& B, const T* z, const double* r, const double* q, double* partials,
+                     SolveState* st, cudaStream_t s);
+// p = z + beta p, q = A'z + beta q, partials of (p, V q), then alpha
+template <typename T, bool VAR>
+void launch_fcg_direction(const Bricks<double>& B, const T* z, double* p, double* q, double* partials,
+                          SolveState* st, cudaStream_t s);
+// x += alpha p (B.x, periodic write-through), r -= alpha q, pre = r,
+// partials of ||V r||^2
+void launch_fcg_update(const Bricks<double>& B, const double* p, double* r, const double* q, float* pre32,
+                       double* pre64, double* partials, const SolveState* st, cudaStream_t s);
+// st->l2_true from the partials of a mode-2 residual
+void launch_fcg_true_norm(const Bricks<double>& B, const double* partials, SolveState* st, cudaStream_t s);
 
 // compact interior <-> ghost-framed conversions
 void launch_load_b(const Bricks<double>& B, const double* compact, cudaStream_t s);

@@ -1,0 +1,247 @@
+// bmg_krylov.cu -- flexible conjugate gradients around the multigrid cycle:
+// the FP64 outer loop of a mixed-precision solve can be Krylov-accelerated
+// instead of taking one cycle per correction (no counterpart in the
+// reference, whose loop is MG.C:191-242).
+//
+// FCG(1) (Y. Notay, "Flexible conjugate gradients", SIAM J. Sci. Comput.
+// 22 (2000)), with the V-weighted inner product (u, w)_V = sum V u w, in
+// which the row-scaled operator A' = A/V is self-adjoint (A is symmetric):
+//   r = b - A'x,  z = cycle(r)
+//   beta = -(z, V q_prev) / (p_prev, V q_prev)        (0 on the first step)
+//   p = z + beta p_prev,  q = A'p = A'z + beta q_prev
+//   alpha = (z, V r) / (p, V q)
+//   x += alpha p,  r -= alpha q
+// The truncated Gram-Schmidt form tolerates a cycle that is not exactly
+// symmetric or linear (red-black smoothing, FP32 arithmetic, restriction
+// and prolongation that are not transposes).  A'p is formed from A'z and
+// the previous q, so p needs no ghost cells.
+//
+// Every kernel streams level 0 once, in FP64, with one partial sum per
+// block; single-block kernels add the partials in a fixed order and derive
+// the scalars on the device, so the loop runs inside the solve graph.
+
+#include "bmg_grid.cuh"
+#include "bmg_stencil.cuh"
+
+namespace bmg {
+
+namespace {
+
+__device__ __forceinline__ double cell_volume(const LevelView<double>& L, int i, int j, int k) {
+    return L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j] * L.tab64[L.to.h[2] + k];
+}
+
+// r = b - A'x (FP64), written to r and to the cycle's right-hand side;
+// partials: ||V r||^2 and, for mode 0, the normFactor sum (as k_residual_norm)
+template <bool VAR>
+__global__ void __launch_bounds__(kReduceThreads) k_fcg_residual(Bricks<double> B, int mode, double* r_out,
+                                                                 float* pre32, double* pre64, double* partials,
+                                                                 long nblocks) {
+    __shared__ double sh[kReduceThreads / 32];
+    int i;
+    const LevelView<double>& L = B.v[brick_of(B, blockIdx.z, i)];
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    double a1 = 0.0, a2 = 0.0;
+    if (j < L.n1 && k < L.n2) {
+        const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
+        double w[6], s, d;
+        couplings<double, VAR>(L, i, j, k, c, w);
+        stencil(L.x, c, L.si, L.sj, w, s, d);
+        const double r = L.b[c] + d * L.x[c] - s;
+        const double V = cell_volume(L, i, j, k);
+        a1 = (V * r) * (V * r);
+        if (mode == 0) {
+            const double bb = V * L.b[c];
+            const double t = fabs(V * r - bb) + fabs(bb);
+            a2 = t * t;
+        }
+        if (mode != 2) {
+            r_out[c] = r;
+            if (pre32) pre32[c] = (float)r;
+            if (pre64) pre64[c] = r;
+        }
+    }
+    const long bid = block_id();
+    a1 = block_sum<kReduceThreads>(a1, sh);
+    if (mode == 0) a2 = block_sum<kReduceThreads>(a2, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        partials[bid] = a1;
+        if (mode == 0) partials[nblocks + bid] = a2;
+    }
+}
+
+// partials of (z, V r) and (z, V q)
+template <typename T>
+__global__ void __launch_bounds__(kReduceThreads) k_fcg_dots(Bricks<double> B, const T* z, const double* r,
+                                                             const double* q, double* partials, long nblocks) {
+    __shared__ double sh[kReduceThreads / 32];
+    int i;
+    const LevelView<double>& L = B.v[brick_of(B, blockIdx.z, i)];
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    double a1 = 0.0, a2 = 0.0;
+    if (j < L.n1 && k < L.n2) {
+        const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
+        const double Vz = cell_volume(L, i, j, k) * (double)z[c];
+        a1 = Vz * r[c];
+        a2 = Vz * q[c];
+    }
+    a1 = block_sum<kReduceThreads>(a1, sh);
+    a2 = block_sum<kReduceThreads>(a2, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        const long bid = block_id();
+        partials[bid] = a1;
+        partials[nblocks + bid] = a2;
+    }
+}
+
+__global__ void __launch_bounds__(kReduceThreads) k_fcg_beta(const double* partials, long nblocks,
+                                                             SolveState* st) {
+    __shared__ double sh[kReduceThreads / 32];
+    double a1 = 0.0, a2 = 0.0;
+    for (long q = threadIdx.x; q < nblocks; q += blockDim.x) {
+        a1 += partials[q];
+        a2 += partials[nblocks + q];
+    }
+    a1 = block_sum<kReduceThreads>(a1, sh);
+    a2 = block_sum<kReduceThreads>(a2, sh);
+    if (threadIdx.x == 0) {
+        st->gamma = a1;
+        st->beta = st->first ? 0.0 : -a2 / st->pq;
+        st->first = 0;
+    }
+}
+
+// p = z + beta p, q = A'z + beta q; partials of (p, V q)
+template <typename T, bool VAR>
+__global__ void __launch_bounds__(kReduceThreads) k_fcg_direction(Bricks<double> B, const T* z, double* p,
+                                                                  double* q, double* partials,
+                                                                  const SolveState* st) {
+    __shared__ double sh[kReduceThreads / 32];
+    int i;
+    const LevelView<double>& L = B.v[brick_of(B, blockIdx.z, i)];
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    double a = 0.0;
+    if (j < L.n1 && k < L.n2) {
+        const double beta = st->beta;
+        const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
+        double w[6];
+        couplings<double, VAR>(L, i, j, k, c, w);
+        const double zc = (double)z[c];
+        const double s = w[0] * (double)z[c - L.si] + w[1] * (double)z[c + L.si] + w[2] * (double)z[c - L.sj] +
+                         w[3] * (double)z[c + L.sj] + w[4] * (double)z[c - 1] + w[5] * (double)z[c + 1];
+        const double d = w[0] + w[1] + w[2] + w[3] + w[4] + w[5];
+        // on the first step p and q hold whatever the last solve left
+        const double pn = beta != 0.0 ? zc + beta * p[c] : zc;
+        const double qn = beta != 0.0 ? (s - d * zc) + beta * q[c] : s - d * zc;
+        p[c] = pn;
+        q[c] = qn;
+        a = cell_volume(L, i, j, k) * pn * qn;
+    }
+    a = block_sum<kReduceThreads>(a, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0) partials[block_id()] = a;
+}
+
+__global__ void __launch_bounds__(kReduceThreads) k_fcg_alpha(const double* partials, long nblocks,
+                                                              SolveState* st) {
+    __shared__ double sh[kReduceThreads / 32];
+    double a = 0.0;
+    for (long q = threadIdx.x; q < nblocks; q += blockDim.x) a += partials[q];
+    a = block_sum<kReduceThreads>(a, sh);
+    if (threadIdx.x == 0) {
+        st->pq = a;
+        st->alpha = st->gamma / a;
+    }
+}
+
+// x += alpha p, r -= alpha q, cycle right-hand side = r; partials ||V r||^2
+__global__ void __launch_bounds__(kReduceThreads) k_fcg_update(Bricks<double> B, const double* p, double* r,
+                                                               const double* q, float* pre32, double* pre64,
+                                                               double* partials, const SolveState* st) {
+    __shared__ double sh[kReduceThreads / 32];
+    int i;
+    const LevelView<double>& L = B.v[brick_of(B, blockIdx.z, i)];
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    double a = 0.0;
+    if (j < L.n1 && k < L.n2) {
+        const double alpha = st->alpha;
+        const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
+        store_x(L, c, i, j, k, L.x[c] + alpha * p[c]);
+        const double rn = r[c] - alpha * q[c];
+        r[c] = rn;
+        if (pre32) pre32[c] = (float)rn;
+        if (pre64) pre64[c] = rn;
+        const double Vr = cell_volume(L, i, j, k) * rn;
+        a = Vr * Vr;
+    }
+    a = block_sum<kReduceThreads>(a, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0) partials[block_id()] = a;
+}
+
+__global__ void __launch_bounds__(kReduceThreads) k_fcg_true_norm(const double* partials, long nblocks,
+                                                                  SolveState* st) {
+    __shared__ double sh[kReduceThreads / 32];
+    double a = 0.0;
+    for (long q = threadIdx.x; q < nblocks; q += blockDim.x) a += partials[q];
+    a = block_sum<kReduceThreads>(a, sh);
+    if (threadIdx.x == 0) st->l2_true = sqrt(a);
+}
+
+}  // namespace
+
+template <bool VAR>
+void launch_fcg_residual(const Bricks<double>& B, int mode, double* r, float* pre32, double* pre64,
+                         double* partials, cudaStream_t s) {
+    const dim3 blk = block_for(B.max2);
+    k_fcg_residual<VAR><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, mode, r, pre32, pre64, partials,
+                                                                   reduce_blocks(B));
+}
+
+template <typename T>
+void launch_fcg_beta(const Bricks<double>& B, const T* z, const double* r, const double* q, double* partials,
+                     SolveState* st, cudaStream_t s) {
+    const dim3 blk = block_for(B.max2);
+    const long nb = reduce_blocks(B);
+    k_fcg_dots<T><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, z, r, q, partials, nb);
+    k_fcg_beta<<<1, kReduceThreads, 0, s>>>(partials, nb, st);
+}
+
+template <typename T, bool VAR>
+void launch_fcg_direction(const Bricks<double>& B, const T* z, double* p, double* q, double* partials,
+                          SolveState* st, cudaStream_t s) {
+    const dim3 blk = block_for(B.max2);
+    k_fcg_direction<T, VAR><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, z, p, q, partials, st);
+    k_fcg_alpha<<<1, kReduceThreads, 0, s>>>(partials, reduce_blocks(B), st);
+}
+
+void launch_fcg_update(const Bricks<double>& B, const double* p, double* r, const double* q, float* pre32,
+                       double* pre64, double* partials, const SolveState* st, cudaStream_t s) {
+    const dim3 blk = block_for(B.max2);
+    k_fcg_update<<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, p, r, q, pre32, pre64, partials, st);
+}
+
+void launch_fcg_true_norm(const Bricks<double>& B, const double* partials, SolveState* st, cudaStream_t s) {
+    k_fcg_true_norm<<<1, kReduceThreads, 0, s>>>(partials, reduce_blocks(B), st);
+}
+
+template void launch_fcg_residual<false>(const Bricks<double>&, int, double*, float*, double*, double*,
+                                         cudaStream_t);
+template void launch_fcg_residual<true>(const Bricks<double>&, int, double*, float*, double*, double*,
+                                        cudaStream_t);
+template void launch_fcg_beta<float>(const Bricks<double>&, const float*, const double*, const double*, double*,
+                                     SolveState*, cudaStream_t);
+template void launch_fcg_beta<double>(const Bricks<double>&, const double*, const double*, const double*,
+                                      double*, SolveState*, cudaStream_t);
+template void launch_fcg_direction<float, false>(const Bricks<double>&, const float*, double*, double*, double*,
+                                                 SolveState*, cudaStream_t);
+template void launch_fcg_direction<float, true>(const Bricks<double>&, const float*, double*, double*, double*,
+                                                SolveState*, cudaStream_t);
+template void launch_fcg_direction<double, false>(const Bricks<double>&, const double*, double*, double*,
+                                                  double*, SolveState*, cudaStream_t);
+template void launch_fcg_direction<double, true>(const Bricks<double>&, const double*, double*, double*,
+                                                 double*, SolveState*, cudaStream_t);
+
+}  // namespace bmg

@@ -357,6 +357,10 @@ def make_options(d: Dictionary | dict | None = None, **over) -> N.Options:
     o.autotune = int(_switch(d.get("autotune", "on")))
     o.device = _label(d.get("device", 0))
     o.timeout_ms = _scalar(d.get("timeoutMs", 0))
+    kr = str(d.get("krylov", "none"))
+    if kr not in N.KRYLOV:
+        raise FatalError(f"unknown krylov {kr}")
+    o.krylov = N.KRYLOV[kr]
     return o
 
 

@@ -51,6 +51,10 @@ enum { BMG_SMOOTHER_RBGS = 0, BMG_SMOOTHER_JACOBI = 1 };
 /* Arithmetic of the cycles: plain FP64, or FP32 cycles inside FP64
  * iterative refinement (FP64 residual, update, coarse solve, mean). */
 enum { BMG_PRECISION_FP64 = 0, BMG_PRECISION_MIXED = 1 };
+/* Outer loop: the reference's one cycle per iteration (MG.C:191-242), or
+ * flexible conjugate gradients (Notay's FCG(1)) on the FP64 residual with
+ * one cycle as the preconditioner.  No counterpart in the reference. */
+enum { BMG_KRYLOV_NONE = 0, BMG_KRYLOV_FCG = 1 };
 
 /* bmg_solve flags */
 enum {
@@ -92,6 +96,7 @@ typedef struct bmg_options {
                            shapes per level at creation and keep the fastest   */
     int device;         /* CUDA device ordinal                                 */
     double timeout_ms;  /* wall-clock budget per solve, <= 0: none             */
+    int krylov;         /* krylov (none): outer loop, BMG_KRYLOV_*             */
 } bmg_options;
 
 typedef struct bmg_report {
@@ -100,7 +105,8 @@ typedef struct bmg_report {
     int outer_iterations;     /* FP64 refinement steps (mixed), else = cycles     */
     double initial_residual;  /* Briscola-normalised (solver.C:13-61)             */
     double final_residual;    /* Briscola-normalised                              */
-    double rel_residual;      /* ||b - A x||_2 / ||b - A x0||_2                    */
+    double rel_residual;      /* ||b - A x||_2 / ||b - A x0||_2 (recomputed from x
+                                 at the end of an FCG solve)                      */
     double final_l2;          /* ||b - A x||_2                                    */
     double norm_factor;       /* normFactor of solver.C:13-61                     */
     float ms;                 /* device time of the solve (CUDA events)           */

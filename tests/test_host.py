@@ -89,6 +89,9 @@ def test_make_options_maps_reference_keys():
         bb.make_options({"smoother": "lexgs"})
     with pytest.raises(bb.FatalError):
         bb.make_options({"cycleType": "X"})
+    assert bb.make_options({}).krylov == 0 and bb.make_options({"krylov": "fcg"}).krylov == 1
+    with pytest.raises(bb.FatalError):
+        bb.make_options({"krylov": "gmres"})
 
 
 def test_geometric_grading_ratio():
