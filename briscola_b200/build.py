@@ -1,8 +1,10 @@
-"""Build the native solver library in-tree for sm_100a.
+"""Build the native libraries in-tree for sm_100a.
 
 ``python -m briscola_b200.build`` (or ``__graft_entry__.build()``) compiles
-``csrc/*.cu`` with nvcc into ``briscola_b200/_lib/libbmg.so``: a plain C ABI
-library (include/bmg.h) with the CUDA runtime linked statically.
+``csrc/*.cu`` with nvcc into two plain C ABI libraries with the CUDA runtime
+linked statically: ``briscola_b200/_lib/libbmg.so`` (the multigrid solver,
+include/bmg.h) and ``briscola_b200/_lib/libbunet.so`` (the U-Net kernels,
+include/bunet.h).
 """
 from __future__ import annotations
 
@@ -16,6 +18,9 @@ OUT = os.path.join(HERE, "_lib", "libbmg.so")
 SOURCES = ["bmg_host.cu", "bmg_kernels.cu", "bmg_smooth_fused.cu", "bmg_krylov.cu", "bmg_noalloc.cu"]
 HEADERS = ["bmg_internal.h", "bmg_stencil.cuh", "bmg_grid.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+UNET_OUT = os.path.join(HERE, "_lib", "libbunet.so")
+UNET_SOURCES = ["bun_api.cu", "bun_conv.cu", "bun_elem.cu"]
+UNET_HEADERS = ["bun_internal.h", "bun_api_internal.h"]
 
 
 def nvcc() -> str:
@@ -25,22 +30,33 @@ def nvcc() -> str:
     return "nvcc"
 
 
-def build_native(force: bool = False, verbose: bool = False) -> str:
-    srcs = [os.path.join(CSRC, s) for s in SOURCES]
-    deps = srcs + [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(HERE, "..", "include", "bmg.h")]
-    if not force and os.path.exists(OUT):
-        t = os.path.getmtime(OUT)
+def _build(out: str, sources, headers, header: str, force: bool, verbose: bool) -> str:
+    srcs = [os.path.join(CSRC, s) for s in sources]
+    deps = srcs + [os.path.join(CSRC, h) for h in headers] + [os.path.join(HERE, "..", "include", header)]
+    if not force and os.path.exists(out):
+        t = os.path.getmtime(out)
         if all(os.path.getmtime(d) <= t for d in deps if os.path.exists(d)):
-            return OUT
-    os.makedirs(os.path.dirname(OUT), exist_ok=True)
+            return out
+    os.makedirs(os.path.dirname(out), exist_ok=True)
     cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-           "-o", OUT + ".tmp", *srcs]
+           "-o", out + ".tmp", *srcs]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
-    os.replace(OUT + ".tmp", OUT)
-    return OUT
+    os.replace(out + ".tmp", out)
+    return out
+
+
+def build_native(force: bool = False, verbose: bool = False) -> str:
+    """libbmg.so (the solver); returns its path."""
+    return _build(OUT, SOURCES, HEADERS, "bmg.h", force, verbose)
+
+
+def build_unet(force: bool = False, verbose: bool = False) -> str:
+    """libbunet.so (the U-Net kernels); returns its path."""
+    return _build(UNET_OUT, UNET_SOURCES, UNET_HEADERS, "bunet.h", force, verbose)
 
 
 if __name__ == "__main__":
     print(build_native(force="--force" in sys.argv, verbose=True))
+    print(build_unet(force="--force" in sys.argv, verbose=True))
