@@ -160,6 +160,81 @@ def workload_config(args):
             "parallelism": "replicas" if args.gpus > 1 else "single GPU"}
 
 
+def profile_region(args, local):
+    """One headline solve (or one U-Net forward at the bench size) after
+    set-up and warm-up, bracketed by the CUDA profiler API."""
+    import torch
+
+    import briscola_b200 as bb
+    from briscola_b200 import workloads
+
+    stream = torch.cuda.current_stream()
+    if args.profile_region == "unet_fwd":
+        from briscola_b200 import unet
+
+        net = unet.UNet((args.size,) * 3)
+        x = torch.randn(args.size ** 3, device=f"cuda:{local}")
+        for _ in range(args.warmup):
+            net.forward(x)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        net.forward(x)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        net.check_errors()
+        return
+    kw = dict(precision="mixed", krylov="fcg") if args.profile_region == "mixed_fcg" else dict(precision="fp64")
+    mesh, b, _ = workloads.channel(args.size)
+    # the same kernels launched one by one (the profiler cannot see into a
+    # graph with a conditional loop)
+    c = bb.Context(mesh, bb.make_options(dict(SOLVER_KEYS, device=local, graph="off", **kw)))
+    c.set_stream(stream.cuda_stream)
+    b_d = torch.from_numpy(b).to(f"cuda:{local}")
+    x_d = torch.zeros_like(b_d)
+    for _ in range(args.warmup):
+        c.solve(b_d, x_d, zero_guess=True)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    rep = c.solve(b_d, x_d, zero_guess=True)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    if rep.status != 0:
+        raise RuntimeError(f"solve failed: status {rep.status}")
+
+
+def unet_timing(args, local, stream):
+    """U-Net forward at the bench size (algorithmic TFLOP/s of the 3x3x3
+    convolutions) and one training step at half the size."""
+    import torch
+
+    from briscola_b200 import unet
+
+    out = {}
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    for size, what in ((args.size, "forward"), (args.size // 2, "train_step")):
+        net = unet.UNet((size,) * 3)
+        x = torch.randn(size ** 3, device=f"cuda:{local}")
+        t = torch.randn(size ** 3, device=f"cuda:{local}")
+        run = (lambda: net.forward(x)) if what == "forward" else (lambda: net.train_step(x, t, lr=1e-4))
+        for _ in range(3):
+            run()
+        torch.cuda.synchronize()
+        reps = 10
+        e0.record(stream)
+        for _ in range(reps):
+            run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        net.check_errors()
+        ms = e0.elapsed_time(e1) / reps
+        flops = unet.forward_flops((size,) * 3) * (1 if what == "forward" else 3)
+        out[what] = {"grid": [size] * 3, "ms": round(ms, 3), "tflops_algorithmic": round(flops / ms / 1e9, 1)}
+        del net
+        torch.cuda.empty_cache()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -169,6 +244,10 @@ def main():
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-multibrick", action="store_true")
+    ap.add_argument("--no-unet", action="store_true")
+    ap.add_argument("--profile-region", choices=["mixed_fcg", "fp64", "unet_fwd"], default=None,
+                    help="set up, warm up, then run one solve (or one U-Net forward) between "
+                         "cudaProfilerStart/Stop for ncu --profile-from-start off; prints no bench line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -195,6 +274,10 @@ def main():
 
     import briscola_b200 as bb
     from briscola_b200 import workloads
+
+    if args.profile_region:
+        profile_region(args, local)
+        return
 
     mesh, b, _ = workloads.channel(args.size)
     n = b.size
@@ -341,6 +424,8 @@ def main():
             cm.close()
         del mb_bd, mb_x
 
+    unet_t = None if args.no_unet else unet_timing(args, local, stream)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         times, cycles, threads = cpu_reference(args.size, steps=1)
@@ -384,6 +469,7 @@ def main():
                     "d2h_bytes_per_step": 8 * n},
             "gpu_launches": launches, "clocks": clocks,
             "multibrick": multibrick,
+            "unet": unet_t,
         }
         print(json.dumps(line), flush=True)
     for cc in ctx.values():
