@@ -127,6 +127,16 @@ def param_layout():
     return out, off
 
 
+def forward_flops(shape) -> float:
+    """algorithmic FLOPs of one forward pass: 2 * 27 * cin * cout per voxel
+    and 3x3x3 convolution, 2 * 16 per voxel for the head"""
+    nvox = [int(np.prod([s >> l for s in shape])) for l in range(4)]
+    f = 2.0 * 27 * 1 * 16 * nvox[0] + 2.0 * 16 * nvox[0]
+    for name, lev, c0, up0, c1, cout in CONVS:
+        f += 2.0 * 27 * (c0 + c1) * cout * nvox[lev]
+    return f
+
+
 def init_params(seed: int = 0) -> np.ndarray:
     """He-normal weights, zero biases (FP32)."""
     layout, n = param_layout()
