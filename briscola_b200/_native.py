@@ -19,6 +19,7 @@ CYCLE = {"V": 0, "W": 1, "F": 2}
 SMOOTHER = {"rbgs": 0, "jac": 1, "jacobi": 1}
 PRECISION = {"fp64": 0, "mixed": 1}
 KRYLOV = {"none": 0, "fcg": 1}
+CRITERION = {"initial": 0, "rhs": 1}
 DEVICE_PTRS, ZERO_GUESS = 1, 2
 
 # Every function the header declares; the loader checks they are exported.
@@ -64,6 +65,7 @@ class Options(ctypes.Structure):
         ("device", ctypes.c_int),
         ("timeout_ms", ctypes.c_double),
         ("krylov", ctypes.c_int),
+        ("criterion", ctypes.c_int),
     ]
 
 
@@ -79,6 +81,7 @@ class Report(ctypes.Structure):
         ("norm_factor", ctypes.c_double),
         ("ms", ctypes.c_float),
         ("kernel_launches", ctypes.c_long),
+        ("rhs_rel_residual", ctypes.c_double),
     ]
 
 

@@ -33,6 +33,25 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
     return v;
 }
 
+constexpr int kFinalThreads = 1024;  // one-block kernels that add per-block partials
+
+// sum of n per-block partials by one block of NT threads: four independent
+// accumulators per thread keep many loads in flight; the assignment and the
+// order are fixed, so the result is reproducible
+template <int NT>
+__device__ __forceinline__ double sum_partials(const double* __restrict__ p, long n, double* sh) {
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    long q = threadIdx.x;
+    for (; q + 3 * NT < n; q += 4 * NT) {
+        a0 += p[q];
+        a1 += p[q + NT];
+        a2 += p[q + 2 * NT];
+        a3 += p[q + 3 * NT];
+    }
+    for (; q < n; q += NT) a0 += p[q];
+    return block_sum<NT>((a0 + a1) + (a2 + a3), sh);
+}
+
 __device__ __forceinline__ long block_id() {
     return ((long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
 }

@@ -487,6 +487,7 @@ void validateOptions(const bmg_options* o) {
     if (o->coarse_level < 0) throw BadArg{BMG_BAD_ARG, "negative coarseLevel"};
     if (o->fused < 0) throw BadArg{BMG_BAD_ARG, "negative fused stage count"};
     if (o->krylov < 0 || o->krylov > 1) throw BadArg{BMG_BAD_ARG, "unknown krylov"};
+    if (o->criterion < 0 || o->criterion > 1) throw BadArg{BMG_BAD_ARG, "unknown criterion"};
 }
 
 // Level-0 bricks from the mesh description; contacts between bricks.
@@ -826,7 +827,7 @@ void build(bmg_ctx* c, HostLevel&& L0) {
             c->tr[l].push_back(t);
         }
     }
-    c->partials = dalloc<double>(2 * reduce_blocks(bricks<double>(c, 0)));
+    c->partials = dalloc<double>(3 * reduce_blocks(bricks<double>(c, 0)));
     c->st = dalloc<SolveState>(1);
     BMG_CUDA(cudaMallocHost(&c->st_host, sizeof(SolveState)));
     c->stage_b = dalloc<double>(c->lv[0].ncell);
@@ -1124,6 +1125,7 @@ SolveState initialState(const bmg_ctx* c) {
     }
     init.vol_total = vol;
     init.first = 1;
+    init.criterion = c->opt.criterion;
     return init;
 }
 
@@ -1410,6 +1412,7 @@ int solveImpl(bmg_ctx* c, const double* b, double* x, int flags, bmg_report* rep
         const double l2 = c->opt.krylov == BMG_KRYLOV_FCG ? st.l2_true : st.l2;
         rep->rel_residual = st.l2_0 > 0 ? l2 / st.l2_0 : 0.0;
         rep->final_l2 = l2;
+        rep->rhs_rel_residual = st.bnorm > 0 ? l2 / st.bnorm : 0.0;
         rep->norm_factor = st.nf;
         rep->ms = ms;
         rep->kernel_launches = useGraph ? c->launchesInitPost + c->launchesBody * st.iter : c->launches;
@@ -1502,6 +1505,7 @@ int bmg_default_options(bmg_options* o) {
     o->device = 0;
     o->timeout_ms = 0.0;
     o->krylov = BMG_KRYLOV_NONE;
+    o->criterion = BMG_CRITERION_INITIAL;
     return BMG_OK;
 }
 

@@ -112,13 +112,14 @@ struct SolveState {
     int nan;
     int keep_going;
     int first;         // flexible CG: no previous direction yet
-    int pad;
+    int criterion;     // 0: relative to the initial residual, 1: relative to ||b||
     // flexible CG scalars
     double alpha;      // step length of the last update
     double gamma;      // (z, V r) of the current direction
     double beta;
     double pq;         // (p, V q) of the current direction
     double l2_true;    // ||b - A x||_2 recomputed from x after the loop
+    double bnorm;      // ||b||_2 (unscaled)
 };
 
 // Geometry of a fused smoothing launch (single brick): march axis m (0),
@@ -162,7 +163,7 @@ template <typename T>
 void launch_fill_ghosts(T* x, const int* dst, const int* src, long n, cudaStream_t s);
 
 // residual norms of level 0 in FP64.  mode 0: initial (also the norm-factor
-// sum), 1: current.  When b32 is given the scaled residual is also written
+// sum and ||b||^2: three partial arrays), 1: current.  When b32 is given the scaled residual is also written
 // there in FP32 (the right-hand side of the next mixed-precision cycle).
 template <bool VAR>
 void launch_residual_norm(const Bricks<double>& B, int mode, double* partials, float* b32, cudaStream_t s);

@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_residual_norm(Bricks<double>
     const LevelView<double>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    double a1 = 0.0, a2 = 0.0;
+    double a1 = 0.0, a2 = 0.0, a3 = 0.0;
     if (j < L.n1 && k < L.n2) {
         const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
         double w[6], s, d;
@@ -265,33 +265,39 @@ __global__ void __launch_bounds__(kReduceThreads) k_residual_norm(Bricks<double>
             const double bb = V * L.b[c];
             const double t = fabs(rr - bb) + fabs(bb);
             a2 = t * t;
+            a3 = bb * bb;
         }
         if (b32) b32[c] = (float)r;
     }
     const long bid = block_id();
     a1 = block_sum<kReduceThreads>(a1, sh);
-    if (mode == 0) a2 = block_sum<kReduceThreads>(a2, sh);
+    if (mode == 0) {
+        a2 = block_sum<kReduceThreads>(a2, sh);
+        a3 = block_sum<kReduceThreads>(a3, sh);
+    }
     if (threadIdx.x == 0 && threadIdx.y == 0) {
         partials[bid] = a1;
-        if (mode == 0) partials[nblocks + bid] = a2;
+        if (mode == 0) {
+            partials[nblocks + bid] = a2;
+            partials[2 * nblocks + bid] = a3;
+        }
     }
 }
 
 // solver.C:13-95 on the reduced sums; also decides whether the loop goes on
 // (MG.C:191-195) and, inside the solve graph, hands that decision to the
 // WHILE node (bounded by maxIter, so the device loop always ends).
-__global__ void __launch_bounds__(kReduceThreads) k_finalize(const double* partials, long nblocks,
-                                                              SolveState* st, int mode,
-                                                              cudaGraphConditionalHandle cond,
-                                                              int setCondition) {
-    __shared__ double sh[kReduceThreads / 32];
-    double a1 = 0.0, a2 = 0.0;
-    for (long q = threadIdx.x; q < nblocks; q += blockDim.x) {
-        a1 += partials[q];
-        if (mode == 0) a2 += partials[nblocks + q];
+__global__ void __launch_bounds__(kFinalThreads) k_finalize(const double* partials, long nblocks,
+                                                             SolveState* st, int mode,
+                                                             cudaGraphConditionalHandle cond,
+                                                             int setCondition) {
+    __shared__ double sh[kFinalThreads / 32];
+    const double a1 = sum_partials<kFinalThreads>(partials, nblocks, sh);
+    double a2 = 0.0, a3 = 0.0;
+    if (mode == 0) {
+        a2 = sum_partials<kFinalThreads>(partials + nblocks, nblocks, sh);
+        a3 = sum_partials<kFinalThreads>(partials + 2 * nblocks, nblocks, sh);
     }
-    a1 = block_sum<kReduceThreads>(a1, sh);
-    if (mode == 0) a2 = block_sum<kReduceThreads>(a2, sh);
     if (threadIdx.x == 0) {
         const double l2 = sqrt(a1);
         if (mode == 0) {
@@ -300,6 +306,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_finalize(const double* parti
             st->init = l2 / st->nf;
             st->cur = st->init;
             st->l2_0 = l2;
+            st->bnorm = sqrt(a3);
             st->iter = 0;
         } else {
             st->cur = l2 / st->nf;
@@ -307,9 +314,13 @@ __global__ void __launch_bounds__(kReduceThreads) k_finalize(const double* parti
         }
         st->l2 = l2;
         st->nan = !isfinite(st->cur);
-        // solver.C:64-95
-        st->converged = !((st->init > 0.0) && (st->cur > st->abs_tol) &&
-                          (st->cur / (st->init + 1e-20) > st->rel_tol));
+        // solver.C:64-95; criterion 1 measures the residual against ||b||
+        // instead of the initial residual
+        if (st->criterion == 1)
+            st->converged = !((st->bnorm > 0.0) && (st->cur > st->abs_tol) && (l2 > st->rel_tol * st->bnorm));
+        else
+            st->converged = !((st->init > 0.0) && (st->cur > st->abs_tol) &&
+                              (st->cur / (st->init + 1e-20) > st->rel_tol));
         st->keep_going = !st->nan && ((st->iter < st->max_iter && !st->converged) ||
                                       st->iter < st->min_iter);
         if (setCondition) cudaGraphSetConditional(cond, st->keep_going ? 1u : 0u);
@@ -331,12 +342,10 @@ __global__ void __launch_bounds__(kReduceThreads) k_mean_partials(Bricks<double>
     if (threadIdx.x == 0 && threadIdx.y == 0) partials[block_id()] = a;
 }
 
-__global__ void __launch_bounds__(kReduceThreads) k_mean_finalize(const double* partials, long nblocks,
-                                                                  SolveState* st) {
-    __shared__ double sh[kReduceThreads / 32];
-    double a = 0.0;
-    for (long q = threadIdx.x; q < nblocks; q += blockDim.x) a += partials[q];
-    a = block_sum<kReduceThreads>(a, sh);
+__global__ void __launch_bounds__(kFinalThreads) k_mean_finalize(const double* partials, long nblocks,
+                                                                 SolveState* st) {
+    __shared__ double sh[kFinalThreads / 32];
+    const double a = sum_partials<kFinalThreads>(partials, nblocks, sh);
     if (threadIdx.x == 0) st->mean = a / st->vol_total;
 }
 
@@ -482,13 +491,13 @@ void launch_residual_norm(const Bricks<double>& B, int mode, double* partials, f
 
 void launch_finalize(const Bricks<double>& B, const double* partials, SolveState* st, int mode,
                      cudaGraphConditionalHandle cond, int setCondition, cudaStream_t s) {
-    k_finalize<<<1, kReduceThreads, 0, s>>>(partials, reduce_blocks(B), st, mode, cond, setCondition);
+    k_finalize<<<1, kFinalThreads, 0, s>>>(partials, reduce_blocks(B), st, mode, cond, setCondition);
 }
 
 void launch_mean(const Bricks<double>& B, double* partials, SolveState* st, cudaStream_t s) {
     const dim3 blk = block_for(B.max2);
     k_mean_partials<<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, partials);
-    k_mean_finalize<<<1, kReduceThreads, 0, s>>>(partials, reduce_blocks(B), st);
+    k_mean_finalize<<<1, kFinalThreads, 0, s>>>(partials, reduce_blocks(B), st);
     const long n = B.v[0].cells;
     const int blocks = (int)std::min<long>((n + 255) / 256, 148L * 16);
     k_sub_mean<<<blocks, 256, 0, s>>>(B.v[0].x, n, st);

@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_residual(Bricks<double> 
     const LevelView<double>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    double a1 = 0.0, a2 = 0.0;
+    double a1 = 0.0, a2 = 0.0, a3 = 0.0;
     if (j < L.n1 && k < L.n2) {
         const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
         double w[6], s, d;
@@ -55,6 +55,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_residual(Bricks<double> 
             const double bb = V * L.b[c];
             const double t = fabs(V * r - bb) + fabs(bb);
             a2 = t * t;
+            a3 = bb * bb;
         }
         if (mode != 2) {
             r_out[c] = r;
@@ -64,10 +65,16 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_residual(Bricks<double> 
     }
     const long bid = block_id();
     a1 = block_sum<kReduceThreads>(a1, sh);
-    if (mode == 0) a2 = block_sum<kReduceThreads>(a2, sh);
+    if (mode == 0) {
+        a2 = block_sum<kReduceThreads>(a2, sh);
+        a3 = block_sum<kReduceThreads>(a3, sh);
+    }
     if (threadIdx.x == 0 && threadIdx.y == 0) {
         partials[bid] = a1;
-        if (mode == 0) partials[nblocks + bid] = a2;
+        if (mode == 0) {
+            partials[nblocks + bid] = a2;
+            partials[2 * nblocks + bid] = a3;
+        }
     }
 }
 
@@ -96,16 +103,11 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_dots(Bricks<double> B, c
     }
 }
 
-__global__ void __launch_bounds__(kReduceThreads) k_fcg_beta(const double* partials, long nblocks,
-                                                             SolveState* st) {
-    __shared__ double sh[kReduceThreads / 32];
-    double a1 = 0.0, a2 = 0.0;
-    for (long q = threadIdx.x; q < nblocks; q += blockDim.x) {
-        a1 += partials[q];
-        a2 += partials[nblocks + q];
-    }
-    a1 = block_sum<kReduceThreads>(a1, sh);
-    a2 = block_sum<kReduceThreads>(a2, sh);
+__global__ void __launch_bounds__(kFinalThreads) k_fcg_beta(const double* partials, long nblocks,
+                                                            SolveState* st) {
+    __shared__ double sh[kFinalThreads / 32];
+    const double a1 = sum_partials<kFinalThreads>(partials, nblocks, sh);
+    const double a2 = sum_partials<kFinalThreads>(partials + nblocks, nblocks, sh);
     if (threadIdx.x == 0) {
         st->gamma = a1;
         st->beta = st->first ? 0.0 : -a2 / st->pq;
@@ -144,12 +146,10 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_direction(Bricks<double>
     if (threadIdx.x == 0 && threadIdx.y == 0) partials[block_id()] = a;
 }
 
-__global__ void __launch_bounds__(kReduceThreads) k_fcg_alpha(const double* partials, long nblocks,
-                                                              SolveState* st) {
-    __shared__ double sh[kReduceThreads / 32];
-    double a = 0.0;
-    for (long q = threadIdx.x; q < nblocks; q += blockDim.x) a += partials[q];
-    a = block_sum<kReduceThreads>(a, sh);
+__global__ void __launch_bounds__(kFinalThreads) k_fcg_alpha(const double* partials, long nblocks,
+                                                             SolveState* st) {
+    __shared__ double sh[kFinalThreads / 32];
+    const double a = sum_partials<kFinalThreads>(partials, nblocks, sh);
     if (threadIdx.x == 0) {
         st->pq = a;
         st->alpha = st->gamma / a;
@@ -181,12 +181,10 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_update(Bricks<double> B,
     if (threadIdx.x == 0 && threadIdx.y == 0) partials[block_id()] = a;
 }
 
-__global__ void __launch_bounds__(kReduceThreads) k_fcg_true_norm(const double* partials, long nblocks,
-                                                                  SolveState* st) {
-    __shared__ double sh[kReduceThreads / 32];
-    double a = 0.0;
-    for (long q = threadIdx.x; q < nblocks; q += blockDim.x) a += partials[q];
-    a = block_sum<kReduceThreads>(a, sh);
+__global__ void __launch_bounds__(kFinalThreads) k_fcg_true_norm(const double* partials, long nblocks,
+                                                                 SolveState* st) {
+    __shared__ double sh[kFinalThreads / 32];
+    const double a = sum_partials<kFinalThreads>(partials, nblocks, sh);
     if (threadIdx.x == 0) st->l2_true = sqrt(a);
 }
 
@@ -206,7 +204,7 @@ void launch_fcg_beta(const Bricks<double>& B, const T* z, const double* r, const
     const dim3 blk = block_for(B.max2);
     const long nb = reduce_blocks(B);
     k_fcg_dots<T><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, z, r, q, partials, nb);
-    k_fcg_beta<<<1, kReduceThreads, 0, s>>>(partials, nb, st);
+    k_fcg_beta<<<1, kFinalThreads, 0, s>>>(partials, nb, st);
 }
 
 template <typename T, bool VAR>
@@ -214,7 +212,7 @@ void launch_fcg_direction(const Bricks<double>& B, const T* z, double* p, double
                           SolveState* st, cudaStream_t s) {
     const dim3 blk = block_for(B.max2);
     k_fcg_direction<T, VAR><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, z, p, q, partials, st);
-    k_fcg_alpha<<<1, kReduceThreads, 0, s>>>(partials, reduce_blocks(B), st);
+    k_fcg_alpha<<<1, kFinalThreads, 0, s>>>(partials, reduce_blocks(B), st);
 }
 
 void launch_fcg_update(const Bricks<double>& B, const double* p, double* r, const double* q, float* pre32,
@@ -224,7 +222,7 @@ void launch_fcg_update(const Bricks<double>& B, const double* p, double* r, cons
 }
 
 void launch_fcg_true_norm(const Bricks<double>& B, const double* partials, SolveState* st, cudaStream_t s) {
-    k_fcg_true_norm<<<1, kReduceThreads, 0, s>>>(partials, reduce_blocks(B), st);
+    k_fcg_true_norm<<<1, kFinalThreads, 0, s>>>(partials, reduce_blocks(B), st);
 }
 
 template void launch_fcg_residual<false>(const Bricks<double>&, int, double*, float*, double*, double*,

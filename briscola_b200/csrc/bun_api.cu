@@ -167,6 +167,16 @@ int bun_scale_to_double(long n, const float* x, double scale, double* y, void* s
     return status(to_double_launch(n, x, scale, y, S(stream)));
 }
 
+int bun_laplace_residual(int n0, int n1, int n2, const float* y, const float* f, float c, float* r, void* stream) {
+    if (!dims_ok(n0, n1, n2) || !y || !f || !r) return BUN_BAD_ARG;
+    return status(lap_residual_launch(n0, n1, n2, y, f, c, r, S(stream)));
+}
+
+int bun_laplace_add(int n0, int n1, int n2, const float* g, float w, float* dy, void* stream) {
+    if (!dims_ok(n0, n1, n2) || !g || !dy) return BUN_BAD_ARG;
+    return status(lap_add_launch(n0, n1, n2, g, w, dy, S(stream)));
+}
+
 int bun_sumsq(long n, const double* x, int nblocks, double* part, double* out, void* stream) {
     if (n < 1 || !x || nblocks < 1 || !part || !out) return BUN_BAD_ARG;
     return status(sumsq_launch(n, x, part, nblocks, out, S(stream)));

@@ -26,6 +26,9 @@ cudaError_t adam_launch(long n, float* w, const float* g, float* m, float* v, fl
                         float eps, int step, cudaStream_t s);
 cudaError_t to_float_launch(long n, const double* x, double scale, float* y, cudaStream_t s);
 cudaError_t to_double_launch(long n, const float* x, double scale, double* y, cudaStream_t s);
+cudaError_t lap_residual_launch(int n0, int n1, int n2, const float* y, const float* f, float c, float* r,
+                                cudaStream_t s);
+cudaError_t lap_add_launch(int n0, int n1, int n2, const float* g, float w, float* dy, cudaStream_t s);
 cudaError_t sumsq_launch(long n, const double* x, double* part, int nblocks, double* out, cudaStream_t s);
 
 }  // namespace bun

@@ -315,6 +315,47 @@ __global__ void k_sum_double(const double* __restrict__ part, int n, double* __r
     }
 }
 
+// r = sum over the (up to six) in-grid neighbours of (y_nb - y) + c * f:
+// the h^2-scaled residual of the uniform-grid Neumann Laplacian for a
+// network output y and the network input f (c: h^2 over the target scale)
+__global__ void __launch_bounds__(kBlock) k_lap_residual(int n0, int n1, int n2, const float* __restrict__ y,
+                                                         const float* __restrict__ f, float c, float* __restrict__ r) {
+    const long V = (long)n0 * n1 * n2;
+    const long v = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    int i, j, k;
+    decode(v, n1, n2, i, j, k);
+    const float yc = y[v];
+    float s = 0.f;
+    if (i > 0) s += y[v - (long)n1 * n2] - yc;
+    if (i < n0 - 1) s += y[v + (long)n1 * n2] - yc;
+    if (j > 0) s += y[v - n2] - yc;
+    if (j < n1 - 1) s += y[v + n2] - yc;
+    if (k > 0) s += y[v - 1] - yc;
+    if (k < n2 - 1) s += y[v + 1] - yc;
+    r[v] = s + c * f[v];
+}
+
+// dy += w * (the same stencil applied to g): the adjoint of the residual's
+// y-part, which is symmetric
+__global__ void __launch_bounds__(kBlock) k_lap_add(int n0, int n1, int n2, const float* __restrict__ g, float w,
+                                                    float* __restrict__ dy) {
+    const long V = (long)n0 * n1 * n2;
+    const long v = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    int i, j, k;
+    decode(v, n1, n2, i, j, k);
+    const float gc = g[v];
+    float s = 0.f;
+    if (i > 0) s += g[v - (long)n1 * n2] - gc;
+    if (i < n0 - 1) s += g[v + (long)n1 * n2] - gc;
+    if (j > 0) s += g[v - n2] - gc;
+    if (j < n1 - 1) s += g[v + n2] - gc;
+    if (k > 0) s += g[v - 1] - gc;
+    if (k < n2 - 1) s += g[v + 1] - gc;
+    dy[v] += w * s;
+}
+
 inline unsigned blocks_for(long n) { return (unsigned)((n + kBlock - 1) / kBlock); }
 
 }  // namespace
@@ -393,6 +434,17 @@ cudaError_t to_float_launch(long n, const double* x, double scale, float* y, cud
 
 cudaError_t to_double_launch(long n, const float* x, double scale, double* y, cudaStream_t s) {
     k_to_double<<<blocks_for(n), kBlock, 0, s>>>(n, x, scale, y);
+    return cudaGetLastError();
+}
+
+cudaError_t lap_residual_launch(int n0, int n1, int n2, const float* y, const float* f, float c, float* r,
+                                cudaStream_t s) {
+    k_lap_residual<<<blocks_for((long)n0 * n1 * n2), kBlock, 0, s>>>(n0, n1, n2, y, f, c, r);
+    return cudaGetLastError();
+}
+
+cudaError_t lap_add_launch(int n0, int n1, int n2, const float* g, float w, float* dy, cudaStream_t s) {
+    k_lap_add<<<blocks_for((long)n0 * n1 * n2), kBlock, 0, s>>>(n0, n1, n2, g, w, dy);
     return cudaGetLastError();
 }
 

@@ -361,6 +361,10 @@ def make_options(d: Dictionary | dict | None = None, **over) -> N.Options:
     if kr not in N.KRYLOV:
         raise FatalError(f"unknown krylov {kr}")
     o.krylov = N.KRYLOV[kr]
+    cr = str(d.get("criterion", "initial"))
+    if cr not in N.CRITERION:
+        raise FatalError(f"unknown criterion {cr}")
+    o.criterion = N.CRITERION[cr]
     return o
 
 

@@ -88,6 +88,8 @@ def load(path: str = LIB_PATH):
         "bun_scale_to_float": [l, vp, d, vp, vp],
         "bun_scale_to_double": [l, vp, d, vp, vp],
         "bun_sumsq": [l, vp, i, vp, vp, vp],
+        "bun_laplace_residual": [i, i, i, vp, vp, f, vp, vp],
+        "bun_laplace_add": [i, i, i, vp, f, vp, vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -101,7 +103,8 @@ def load(path: str = LIB_PATH):
 
 EXPORTED = ("bun_conv3", "bun_conv3_wgrad", "bun_wgrad_part_floats", "bun_pack_weights", "bun_conv_in",
             "bun_conv_in_wgrad", "bun_head", "bun_head_grad", "bun_pool", "bun_unpool_grad", "bun_skip_grad",
-            "bun_mse", "bun_adam", "bun_scale_to_float", "bun_scale_to_double", "bun_sumsq")
+            "bun_mse", "bun_adam", "bun_scale_to_float", "bun_scale_to_double", "bun_sumsq",
+            "bun_laplace_residual", "bun_laplace_add")
 
 
 def _check(rc, what):
@@ -194,6 +197,10 @@ class UNet:
         self.y = torch.zeros(self.nvox[0], dtype=f32, device=dev)
         self.dy = torch.zeros(self.nvox[0], dtype=f32, device=dev)
         self.loss = torch.zeros(1, dtype=f32, device=dev)
+        self.rloss = torch.zeros(1, dtype=f32, device=dev)
+        self.r = torch.zeros(self.nvox[0], dtype=f32, device=dev)
+        self.dr = torch.zeros(self.nvox[0], dtype=f32, device=dev)
+        self.zero = torch.zeros(self.nvox[0], dtype=f32, device=dev)
         self.err = torch.zeros(1, dtype=torch.int32, device=dev)
         # packed BF16 weights: forward and data-gradient layouts
         self.wf, self.wd = {}, {}
@@ -346,15 +353,32 @@ class UNet:
                               self.red_blocks, self.part.data_ptr(), self.loss.data_ptr(), self._s()), "mse")
         return self.loss
 
+    def residual_loss(self, c: float, weight: float):
+        """add weight * mean(r^2), r = h^2 A'y + c x (the operator residual
+        of the output for the current input), to the loss and to dL/dy"""
+        n0, n1, n2 = self.dims[0]
+        s = self._s()
+        _check(self.L.bun_laplace_residual(n0, n1, n2, self.y.data_ptr(), self.x.data_ptr(), c, self.r.data_ptr(),
+                                           s), "laplace_residual")
+        _check(self.L.bun_mse(self.nvox[0], self.r.data_ptr(), self.zero.data_ptr(), self.dr.data_ptr(),
+                              self.red_blocks, self.part.data_ptr(), self.rloss.data_ptr(), s), "mse")
+        _check(self.L.bun_laplace_add(n0, n1, n2, self.dr.data_ptr(), weight, self.dy.data_ptr(), s),
+               "laplace_add")
+        return self.rloss
+
     def adam(self, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8):
         self.step += 1
         _check(self.L.bun_adam(self.nparam, self.p.data_ptr(), self.g.data_ptr(), self.m.data_ptr(),
                                self.v.data_ptr(), lr, b1, b2, eps, self.step, self._s()), "adam")
         self.pack()
 
-    def train_step(self, x, target, lr=1e-3):
+    def train_step(self, x, target, lr=1e-3, res_c: float = 0.0, res_weight: float = 0.0):
+        """one Adam step on mean (y - target)^2 (+ res_weight * the operator
+        residual term of residual_loss with c = res_c)"""
         self.forward(x)
         self.mse(target)
+        if res_weight > 0:
+            self.residual_loss(res_c, res_weight)
         self.backward()
         self.adam(lr)
         return self.loss
@@ -367,9 +391,10 @@ class UNet:
         return self.p.detach().cpu().numpy().copy()
 
     # -- the solver's view ---------------------------------------------------
-    def guess(self, b, V: float, x0):
+    def guess(self, b, V: float, x0, scale: float = 1.0):
         """Initial guess x0 (FP64 device) for the system right-hand side b
-        (FP64 device, b = -V f on a uniform grid of cell volume V)."""
+        (FP64 device, b = -V f on a uniform grid of cell volume V); scale:
+        the factor the training targets were divided by."""
         L, s = self.L, self._s()
         n = self.nvox[0]
         _check(L.bun_sumsq(n, b.data_ptr(), self.red_blocks, self.dpart.data_ptr(), self.dsum.data_ptr(), s), "sumsq")
@@ -380,5 +405,5 @@ class UNet:
         # f = -b / V; input f / rms(f) = -b / rms(b)
         _check(L.bun_scale_to_float(n, b.data_ptr(), -1.0 / rms_b, self.x.data_ptr(), s), "scale")
         self.forward()
-        _check(L.bun_scale_to_double(n, self.y.data_ptr(), rms_b / V, x0.data_ptr(), s), "scale")
+        _check(L.bun_scale_to_double(n, self.y.data_ptr(), scale * rms_b / V, x0.data_ptr(), s), "scale")
         return x0

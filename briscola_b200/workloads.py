@@ -146,3 +146,70 @@ def multibrick(scale: int = 1, seed: int = 3000):
 
 
 CONFIGS = {"cavity": cavity, "channel": channel, "sphere": sphere, "multibrick": multibrick}
+
+
+# ---------------------------------------------------------------------------
+# time sequence of right-hand sides for the learned initial guess
+# ---------------------------------------------------------------------------
+class TaylorGreenSequence:
+    """Right-hand sides b_t = -V div(u_t) on the all-wall unit cube (N^3,
+    uniform): u_0 is the Taylor-Green field (sin pi x cos pi y cos pi z,
+    -cos pi x sin pi y cos pi z, 0) on the cell faces (amplitude 1, zero
+    normal velocity at the walls) plus seeded N(0, noise^2) on the interior
+    faces; every step applies a fixed explicit update -- forward-Euler
+    upwind advection by the constant velocity U0 plus diffusion nu -- and
+    re-imposes zero wall-normal velocity.  Computed in FP64 on a torch
+    device (synthetic data generation, not part of the solve)."""
+
+    def __init__(self, N: int, seed: int, device, noise: float = 0.1, dt: float = 1e-3,
+                 nu: float = 2e-4, U0=(1.0, 0.5, 0.25)):
+        import torch
+
+        self.torch = torch
+        self.N = N
+        self.h = 1.0 / N
+        self.dt, self.nu, self.U0 = dt, nu, U0
+        g = torch.Generator(device="cpu").manual_seed(seed)
+        h = self.h
+        c = (torch.arange(N, dtype=torch.float64) + 0.5) * h      # cell centres
+        f = torch.arange(N + 1, dtype=torch.float64) * h           # face positions
+        pi = np.pi
+        ux = torch.sin(pi * f)[:, None, None] * torch.cos(pi * c)[None, :, None] * torch.cos(pi * c)[None, None, :]
+        uy = -torch.cos(pi * c)[:, None, None] * torch.sin(pi * f)[None, :, None] * torch.cos(pi * c)[None, None, :]
+        uz = torch.zeros(N, N, N + 1, dtype=torch.float64)
+        u = [ux, uy, uz]
+        for d in range(3):
+            u[d] = u[d] + noise * torch.randn(u[d].shape, generator=g, dtype=torch.float64)
+        self.u = [a.to(device) for a in u]
+        self._walls()
+
+    def _walls(self):
+        for d in range(3):
+            idx = [slice(None)] * 3
+            idx[d] = 0
+            self.u[d][tuple(idx)] = 0.0
+            idx[d] = -1
+            self.u[d][tuple(idx)] = 0.0
+
+    def rhs(self):
+        """b = -V div(u) of the current field, flat FP64 (k fastest)"""
+        h = self.h
+        ux, uy, uz = self.u
+        div_flux = ((ux[1:] - ux[:-1]) + (uy[:, 1:] - uy[:, :-1]) + (uz[:, :, 1:] - uz[:, :, :-1])) * h * h
+        return (-div_flux).reshape(-1).contiguous()
+
+    def step(self):
+        torch = self.torch
+        h, dt, nu = self.h, self.dt, self.nu
+        new = []
+        for a in self.u:
+            lap = torch.zeros_like(a)
+            adv = torch.zeros_like(a)
+            for ax in range(3):
+                lo = torch.cat([a.narrow(ax, 0, 1), a.narrow(ax, 0, a.shape[ax] - 1)], dim=ax)
+                hi = torch.cat([a.narrow(ax, 1, a.shape[ax] - 1), a.narrow(ax, a.shape[ax] - 1, 1)], dim=ax)
+                lap += (lo - 2 * a + hi) / (h * h)
+                adv += self.U0[ax] * (a - lo) / h      # upwind, U0 > 0
+            new.append(a + dt * (nu * lap - adv))
+        self.u = new
+        self._walls()

@@ -55,6 +55,11 @@ enum { BMG_PRECISION_FP64 = 0, BMG_PRECISION_MIXED = 1 };
  * flexible conjugate gradients (Notay's FCG(1)) on the FP64 residual with
  * one cycle as the preconditioner.  No counterpart in the reference. */
 enum { BMG_KRYLOV_NONE = 0, BMG_KRYLOV_FCG = 1 };
+/* Convergence test: relTol relative to the initial residual (solver.C:64-95,
+ * the reference's), or relative to ||b||_2, i.e. ||b - A x||_2 <= relTol
+ * ||b||_2 whatever the initial guess (used to compare solves that start from
+ * different guesses).  The absolute tolerance applies in both. */
+enum { BMG_CRITERION_INITIAL = 0, BMG_CRITERION_RHS = 1 };
 
 /* bmg_solve flags */
 enum {
@@ -97,6 +102,7 @@ typedef struct bmg_options {
     int device;         /* CUDA device ordinal                                 */
     double timeout_ms;  /* wall-clock budget per solve, <= 0: none             */
     int krylov;         /* krylov (none): outer loop, BMG_KRYLOV_*             */
+    int criterion;      /* criterion (initial): BMG_CRITERION_*                */
 } bmg_options;
 
 typedef struct bmg_report {
@@ -111,6 +117,7 @@ typedef struct bmg_report {
     double norm_factor;       /* normFactor of solver.C:13-61                     */
     float ms;                 /* device time of the solve (CUDA events)           */
     long kernel_launches;     /* kernels this solve launched (graph nodes count)  */
+    double rhs_rel_residual;  /* ||b - A x||_2 / ||b||_2                            */
 } bmg_report;
 
 int bmg_default_options(bmg_options* opts);

@@ -93,6 +93,12 @@ int bun_mse(long n, const float* y, const float* t, float* dy, int nblocks, floa
 int bun_adam(long n, float* w, const float* g, float* m, float* v, float lr, float b1, float b2, float eps,
              int step, void* stream);
 
+/* Residual term of the training loss on a uniform n0 x n1 x n2 grid with
+ * Neumann walls: r = sum over in-grid neighbours of (y_nb - y) + c f, and
+ * its adjoint in y, dy += w * (the same stencil applied to g). */
+int bun_laplace_residual(int n0, int n1, int n2, const float* y, const float* f, float c, float* r, void* stream);
+int bun_laplace_add(int n0, int n1, int n2, const float* g, float w, float* dy, void* stream);
+
 /* y = scale * x between the solver's FP64 fields and the network's FP32 ones */
 int bun_scale_to_float(long n, const double* x, double scale, float* y, void* stream);
 int bun_scale_to_double(long n, const float* x, double scale, double* y, void* stream);

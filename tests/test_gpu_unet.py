@@ -201,6 +201,32 @@ def test_small_kernels(L):
     assert rel(host(dzh).reshape(dims + (16,)), dy32[..., None] * hw.astype(np.float32) * (d0 > 0)) <= 4e-3
 
 
+def _lap(y):
+    """sum over in-grid neighbours of (y_nb - y)"""
+    out = np.zeros_like(y)
+    for ax in range(3):
+        d = np.diff(y, axis=ax)
+        lo = [slice(None)] * 3
+        hi = [slice(None)] * 3
+        lo[ax] = slice(0, -1)
+        hi[ax] = slice(1, None)
+        out[tuple(lo)] += d
+        out[tuple(hi)] -= d
+    return out
+
+
+def test_laplace_residual_kernels(L):
+    rng = np.random.default_rng(4)
+    dims = (8, 12, 16)
+    y, f, g, dy = (rng.standard_normal(dims) for _ in range(4))
+    yd, fd, gd, dyd = (dev(a, torch.float32) for a in (y, f, g, dy))
+    r = torch.zeros(int(np.prod(dims)), dtype=torch.float32, device="cuda")
+    assert L.bun_laplace_residual(*dims, yd.data_ptr(), fd.data_ptr(), 0.25, r.data_ptr(), S()) == 0
+    assert L.bun_laplace_add(*dims, gd.data_ptr(), 0.5, dyd.data_ptr(), S()) == 0
+    assert rel(host(r).reshape(dims), _lap(y) + 0.25 * f) <= 1e-6
+    assert rel(host(dyd).reshape(dims), dy + 0.5 * _lap(g)) <= 1e-6
+
+
 def test_argument_checks(L):
     t = torch.zeros(4096, dtype=torch.bfloat16, device="cuda")
     # unsupported (kc, cout), misaligned pointer, channel count not a multiple of kc

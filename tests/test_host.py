@@ -92,6 +92,9 @@ def test_make_options_maps_reference_keys():
     assert bb.make_options({}).krylov == 0 and bb.make_options({"krylov": "fcg"}).krylov == 1
     with pytest.raises(bb.FatalError):
         bb.make_options({"krylov": "gmres"})
+    assert bb.make_options({}).criterion == 0 and bb.make_options({"criterion": "rhs"}).criterion == 1
+    with pytest.raises(bb.FatalError):
+        bb.make_options({"criterion": "x"})
 
 
 def test_geometric_grading_ratio():
