@@ -211,15 +211,18 @@ void layout(HostLevel& L) {
 void buildTables(HostLevel& L) {
     int off = 0;
     L.tab.clear();
+    // every sub-table starts on a multiple of 4 entries, so the colour pass
+    // can read 4 consecutive k couplings as one vector
+    auto next = [](int o, int n) { return (o + n + 3) / 4 * 4; };
     for (auto& B : L.br) {
         TabOff& to = B.to;
         for (int d = 0; d < 3; ++d) {
             to.wl[d] = off;
-            off += B.n[d];
+            off = next(off, B.n[d]);
             to.wh[d] = off;
-            off += B.n[d];
+            off = next(off, B.n[d]);
             to.h[d] = off;
-            off += B.n[d];
+            off = next(off, B.n[d]);
         }
         to.total = off;
         L.tab.resize(off, 0.0);
