@@ -245,6 +245,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-multibrick", action="store_true")
     ap.add_argument("--no-unet", action="store_true")
+    ap.add_argument("--no-variable", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--learned-size", type=int, default=128)
+    ap.add_argument("--learned-pairs", type=int, default=2000)
+    ap.add_argument("--learned-steps", type=int, default=2000)
+    ap.add_argument("--learned-held", type=int, default=200)
     ap.add_argument("--profile-region", choices=["mixed_fcg", "fp64", "unet_fwd"], default=None,
                     help="set up, warm up, then run one solve (or one U-Net forward) between "
                          "cudaProfilerStart/Stop for ncu --profile-from-start off; prints no bench line")
@@ -426,6 +432,41 @@ def main():
 
     unet_t = None if args.no_unet else unet_timing(args, local, stream)
 
+    # ---- two-phase variable coefficient (sphere, density ratio 1000) ----
+    variable = None
+    if not args.no_variable:
+        vmesh, vb, vlam = workloads.sphere(args.size)
+        vbd = torch.from_numpy(vb).to(f"cuda:{local}")
+        vx = torch.zeros_like(vbd)
+        variable = {"workload": f"sphere {args.size}^3, all walls, rho 1 / 1000 (radius 0.2, seeded centre), "
+                                "VOF ramp over 2 cells, face coefficient mean of 1/rho, N(0,1) zero-mean RHS, 1e-8"}
+        for arm, kw in (("fp64", dict(precision="fp64")), ("mixed_fcg", dict(precision="mixed", krylov="fcg"))):
+            cv = bb.Context(vmesh, bb.make_options(dict(SOLVER_KEYS, device=local, maxIter=2000, **kw)))
+            cv.set_stream(stream.cuda_stream)
+            cv.set_coefficients(vlam)
+            for _ in range(2):
+                cv.solve(vbd, vx, zero_guess=True)
+            barrier()
+            e0.record(stream)
+            nrep = max(1, args.steps // 2)
+            for _ in range(nrep):
+                rep = cv.solve(vbd, vx, zero_guess=True)
+            e1.record(stream)
+            barrier()
+            variable[arm] = {"ms_per_solve": round(e0.elapsed_time(e1) / nrep, 3), "cycles": rep.cycles,
+                             "status": rep.status, "rel_residual": rep.rel_residual}
+            cv.close()
+        del vbd, vx
+
+    # ---- learned initial guess (config 5) ----
+    learned_t = None
+    if not args.no_learned:
+        from briscola_b200 import learned
+
+        learned_t = learned.benchmark(args.learned_size, args.learned_pairs, args.learned_steps,
+                                      args.learned_held)
+        torch.cuda.empty_cache()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         times, cycles, threads = cpu_reference(args.size, steps=1)
@@ -470,6 +511,8 @@ def main():
             "gpu_launches": launches, "clocks": clocks,
             "multibrick": multibrick,
             "unet": unet_t,
+            "variable_coefficient": variable,
+            "learned": learned_t,
         }
         print(json.dumps(line), flush=True)
     for cc in ctx.values():

@@ -111,78 +111,92 @@ struct Row4<double> {
 };
 
 // ---------------------------------------------------------------------------
-// Red-black colour pass, four cells per thread: the thread owns the k-quad
-// (4p .. 4p+3) of one row and updates its two cells of the requested colour.
-// The five neighbour rows, b and the k couplings are read as whole vectors,
-// the index arithmetic is done once for both updates, and the quad is
-// written back as one vector (the other colour's two values are unchanged
-// during the pass, so writing them back is safe; a quad is never a ghost).
-// The arithmetic is gs_value's, so results are bit-identical to
-// k_colour_pass and the fused smoother.  Needs every brick's n2 % 4 == 0.
+// Red-black colour pass, four cells per thread and row: the thread owns the
+// k-quad (4p .. 4p+3) of R consecutive rows j0 .. j0+R-1 and updates the two
+// cells of the requested colour in each.  The rows j0-1 .. j0+R, the i
+// neighbours, b and the k couplings are read as whole vectors (rows shared
+// between the R updates are read once), the index arithmetic is done once,
+// and every quad is written back as one vector (the other colour's values
+// are unchanged during the pass, so writing them back is safe; a quad is
+// never a ghost).  The arithmetic is gs_value's, so results are
+// bit-identical to k_colour_pass and the fused smoother.  Needs every
+// brick's n2 % 4 == 0.
 // ---------------------------------------------------------------------------
-template <typename T, bool VAR>
+template <typename T, bool VAR, int R>
 __global__ void __launch_bounds__(256) k_colour_quad(Bricks<T> B, int colour) {
     int i;
     const LevelView<T>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int j0 = (blockIdx.y * blockDim.y + threadIdx.y) * R;
     const int k0 = 4 * p;
-    if (j >= L.n1 || k0 >= L.n2) return;
-    const long c0 = L.base + (long)i * L.si + (long)j * L.sj + k0;
+    if (j0 >= L.n1 || k0 >= L.n2) return;
+    const long c0 = L.base + (long)i * L.si + (long)j0 * L.sj + k0;
     const T* x = L.x;
-    T own[4], xm[4], xp[4], ym[4], yp[4], bb[4], wkl[4], wkh[4];
-    Row4<T>::ld(x + c0, own);
-    Row4<T>::ld(x + c0 - L.si, xm);
-    Row4<T>::ld(x + c0 + L.si, xp);
-    Row4<T>::ld(x + c0 - L.sj, ym);
-    Row4<T>::ld(x + c0 + L.sj, yp);
-    Row4<T>::ld(L.b + c0, bb);
+    // rows j0-1 .. j0+R of this plane (the last may be the ghost row)
+    T row[R + 2][4], xm[R][4], xp[R][4], bb[R][4], wkl[4], wkh[4];
+#pragma unroll
+    for (int r = 0; r < R + 2; ++r) Row4<T>::ld(x + c0 + (long)(r - 1) * L.sj, row[r]);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        Row4<T>::ld(x + c0 + r * L.sj - L.si, xm[r]);
+        Row4<T>::ld(x + c0 + r * L.sj + L.si, xp[r]);
+        Row4<T>::ld(L.b + c0 + r * L.sj, bb[r]);
+    }
     Row4<T>::ldg4(L.tab + L.to.wl[2] + k0, wkl);
     Row4<T>::ldg4(L.tab + L.to.wh[2] + k0, wkh);
-    const T left = x[c0 - 1], right = x[c0 + 4];
     const T wil = ldg(L.tab + L.to.wl[0] + i), wih = ldg(L.tab + L.to.wh[0] + i);
-    const T wjl = ldg(L.tab + L.to.wl[1] + j), wjh = ldg(L.tab + L.to.wh[1] + j);
-    // the two cells of the colour: (0, 2) or (1, 3); every array index
-    // below is a compile-time constant picked by a select
-    const bool odd = ((colour ^ (i + j + k0 + L.cpar)) & 1) != 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int j = j0 + r;
+        if (j >= L.n1) break;
+        const long c = c0 + r * L.sj;
+        const T* own = row[r + 1];
+        const T left = x[c - 1], right = x[c + 4];
+        const T wjl = ldg(L.tab + L.to.wl[1] + j), wjh = ldg(L.tab + L.to.wh[1] + j);
+        // the two cells of the colour: (0, 2) or (1, 3); every array index
+        // below is a compile-time constant picked by a select
+        const bool odd = ((colour ^ (i + j + k0 + L.cpar)) & 1) != 0;
 #define BMG_SEL(a, e) (odd ? a[(e) + 1] : a[e])
-    T w0[6] = {wil, wih, wjl, wjh, BMG_SEL(wkl, 0), BMG_SEL(wkh, 0)};
-    T w2[6] = {wil, wih, wjl, wjh, BMG_SEL(wkl, 2), BMG_SEL(wkh, 2)};
-    if (VAR) {
-        T l0[4], l0p[4], l1[4], l1p[4], l2[4];
-        Row4<T>::ldg4(L.lam0 + c0, l0);
-        Row4<T>::ldg4(L.lam0 + c0 + L.si, l0p);
-        Row4<T>::ldg4(L.lam1 + c0, l1);
-        Row4<T>::ldg4(L.lam1 + c0 + L.sj, l1p);
-        Row4<T>::ldg4(L.lam2 + c0, l2);
-        const T l2r = ldg(L.lam2 + c0 + 4);
-        w0[0] *= BMG_SEL(l0, 0);
-        w0[1] *= BMG_SEL(l0p, 0);
-        w0[2] *= BMG_SEL(l1, 0);
-        w0[3] *= BMG_SEL(l1p, 0);
-        w0[4] *= BMG_SEL(l2, 0);
-        w0[5] *= BMG_SEL(l2, 1);
-        w2[0] *= BMG_SEL(l0, 2);
-        w2[1] *= BMG_SEL(l0p, 2);
-        w2[2] *= BMG_SEL(l1, 2);
-        w2[3] *= BMG_SEL(l1p, 2);
-        w2[4] *= BMG_SEL(l2, 2);
-        w2[5] *= odd ? l2r : l2[3];
-    }
-    const T xn0[6] = {BMG_SEL(xm, 0), BMG_SEL(xp, 0), BMG_SEL(ym, 0), BMG_SEL(yp, 0), odd ? own[0] : left,
-                      odd ? own[2] : own[1]};
-    const T xn2[6] = {BMG_SEL(xm, 2), BMG_SEL(xp, 2), BMG_SEL(ym, 2), BMG_SEL(yp, 2), odd ? own[2] : own[1],
-                      odd ? right : own[3]};
-    const T v0 = gs_value(w0, xn0, BMG_SEL(bb, 0));
-    const T v2 = gs_value(w2, xn2, BMG_SEL(bb, 2));
+        T w0[6] = {wil, wih, wjl, wjh, BMG_SEL(wkl, 0), BMG_SEL(wkh, 0)};
+        T w2[6] = {wil, wih, wjl, wjh, BMG_SEL(wkl, 2), BMG_SEL(wkh, 2)};
+        if (VAR) {
+            T l0[4], l0p[4], l1[4], l1p[4], l2[4];
+            Row4<T>::ldg4(L.lam0 + c, l0);
+            Row4<T>::ldg4(L.lam0 + c + L.si, l0p);
+            Row4<T>::ldg4(L.lam1 + c, l1);
+            Row4<T>::ldg4(L.lam1 + c + L.sj, l1p);
+            Row4<T>::ldg4(L.lam2 + c, l2);
+            const T l2r = ldg(L.lam2 + c + 4);
+            w0[0] *= BMG_SEL(l0, 0);
+            w0[1] *= BMG_SEL(l0p, 0);
+            w0[2] *= BMG_SEL(l1, 0);
+            w0[3] *= BMG_SEL(l1p, 0);
+            w0[4] *= BMG_SEL(l2, 0);
+            w0[5] *= BMG_SEL(l2, 1);
+            w2[0] *= BMG_SEL(l0, 2);
+            w2[1] *= BMG_SEL(l0p, 2);
+            w2[2] *= BMG_SEL(l1, 2);
+            w2[3] *= BMG_SEL(l1p, 2);
+            w2[4] *= BMG_SEL(l2, 2);
+            w2[5] *= odd ? l2r : l2[3];
+        }
+        const T* ym = row[r];
+        const T* yp = row[r + 2];
+        const T xn0[6] = {BMG_SEL(xm[r], 0), BMG_SEL(xp[r], 0), BMG_SEL(ym, 0), BMG_SEL(yp, 0),
+                          odd ? own[0] : left, odd ? own[2] : own[1]};
+        const T xn2[6] = {BMG_SEL(xm[r], 2), BMG_SEL(xp[r], 2), BMG_SEL(ym, 2), BMG_SEL(yp, 2),
+                          odd ? own[2] : own[1], odd ? right : own[3]};
+        const T v0 = gs_value(w0, xn0, BMG_SEL(bb[r], 0));
+        const T v2 = gs_value(w2, xn2, BMG_SEL(bb[r], 2));
 #undef BMG_SEL
-    const T out[4] = {odd ? own[0] : v0, odd ? v0 : own[1], odd ? own[2] : v2, odd ? v2 : own[3]};
-    Row4<T>::st(L.x + c0, out);
-    // periodic images of the two updated cells
-    if (L.per0 | L.per1 | L.per2) {
-        const int q0 = odd ? 1 : 0;
-        store_x(L, c0 + q0, i, j, k0 + q0, v0);
-        store_x(L, c0 + q0 + 2, i, j, k0 + q0 + 2, v2);
+        const T out[4] = {odd ? own[0] : v0, odd ? v0 : own[1], odd ? own[2] : v2, odd ? v2 : own[3]};
+        Row4<T>::st(L.x + c, out);
+        // periodic images of the two updated cells
+        if (L.per0 | L.per1 | L.per2) {
+            const int q0 = odd ? 1 : 0;
+            store_x(L, c + q0, i, j, k0 + q0, v0);
+            store_x(L, c + q0 + 2, i, j, k0 + q0 + 2, v2);
+        }
     }
 }
 
@@ -567,9 +581,11 @@ void launch_colour_pass(const Bricks<T>& B, int colour, cudaStream_t s) {
     bool quads = true;
     for (int b = 0; b < B.nb; ++b) quads = quads && B.v[b].n2 % 4 == 0;
     if (quads) {
+        // one row per thread: two rows per thread (R = 2) measured no faster
+        // on the 256^3 level and costs registers in FP64
         const int nq = B.max2 / 4;
         const dim3 blk = nq >= 32 ? dim3(32, 8, 1) : nq >= 8 ? dim3(8, 32, 1) : dim3(2, 128, 1);
-        k_colour_quad<T, VAR><<<grid_for(B, nq, blk), blk, 0, s>>>(B, colour);
+        k_colour_quad<T, VAR, 1><<<grid_for(B, nq, blk), blk, 0, s>>>(B, colour);
         return;
     }
     const int pairs = (B.max2 + 1) / 2;

@@ -41,14 +41,30 @@ __device__ __forceinline__ void couplings(const LevelView<T>& L, int i, int j, i
 // The FP32 smoother divides with the hardware reciprocal (about 2 ulp, two
 // instructions); the FP64 path keeps IEEE division.  Both smoother kernels
 // call this one function, so they stay bit-identical to each other.
+// The sums are written with explicit round-to-nearest intrinsics, so the
+// compiler cannot contract them into fused multiply-adds differently in
+// different kernels: every smoother evaluates the same sequence of roundings.
 __device__ __forceinline__ float gs_div(float a, float b) { return __fdividef(a, b); }
 __device__ __forceinline__ double gs_div(double a, double b) { return a / b; }
+__device__ __forceinline__ float rn_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double rn_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float rn_fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double rn_fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float rn_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double rn_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float rn_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double rn_sub(double a, double b) { return __dsub_rn(a, b); }
 
 template <typename T>
 __device__ __forceinline__ T gs_value(const T w[6], const T xn[6], T b) {
-    const T s = w[0] * xn[0] + w[1] * xn[1] + w[2] * xn[2] + w[3] * xn[3] + w[4] * xn[4] + w[5] * xn[5];
-    const T d = w[0] + w[1] + w[2] + w[3] + w[4] + w[5];
-    return gs_div(s - b, d);
+    T s = rn_mul(w[0], xn[0]);
+    s = rn_fma(w[1], xn[1], s);
+    s = rn_fma(w[2], xn[2], s);
+    s = rn_fma(w[3], xn[3], s);
+    s = rn_fma(w[4], xn[4], s);
+    s = rn_fma(w[5], xn[5], s);
+    const T d = rn_add(rn_add(rn_add(rn_add(rn_add(w[0], w[1]), w[2]), w[3]), w[4]), w[5]);
+    return gs_div(rn_sub(s, b), d);
 }
 
 // sum of couplings times neighbour values, and the sum of couplings

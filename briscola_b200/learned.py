@@ -119,3 +119,58 @@ class LearnedGuess:
         self.guess(b)
         x.copy_(self.x0)
         return self.ctx.solve(b, x, zero_guess=False)
+
+
+def benchmark(N: int, n_pairs: int, steps: int, n_held: int, seed: int = 1, lr: float = 2e-3):
+    """Config 5 as one measurement: train on n_pairs solved pairs of one
+    sequence, then time held-out solves of another sequence from zero and
+    from the learned guess (mixed precision, flexible CG, ||b||-relative
+    1e-8).  Returns a dict of the timings and cycle counts (CUDA events)."""
+    import time
+
+    import torch
+
+    t0 = time.perf_counter()
+    pairs = PairSet(N, n_pairs, seed=seed)
+    t_data = time.perf_counter() - t0
+    net = U.UNet((N,) * 3, seed=seed)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    losses = train(net, pairs, steps, lr=lr)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    scale = pairs.scale
+    del pairs
+    torch.cuda.empty_cache()
+    held = PairSet(N, n_held, seed=seed + 1000, skip=17, every=3)
+    ctx = Context(cube_mesh(N), make_options(dict(TARGET_KEYS, relTol=1e-8)))
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    lg = LearnedGuess(net, ctx, scale)
+    x = torch.zeros(N ** 3, dtype=torch.float64, device=net.dev)
+    for q in range(min(3, n_held)):  # warm-up (graph capture, guess buffers)
+        ctx.solve(held.b[q], x, zero_guess=True)
+        lg.solve(held.b[q], x)
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    cyc0, cyc1 = [], []
+    torch.cuda.synchronize()
+    e[0].record(stream)
+    for q in range(n_held):
+        cyc0.append(ctx.solve(held.b[q], x, zero_guess=True).cycles)
+    e[1].record(stream)
+    for q in range(n_held):
+        cyc1.append(lg.solve(held.b[q], x).cycles)
+    e[2].record(stream)
+    for q in range(n_held):
+        lg.guess(held.b[q])
+    e[3].record(stream)
+    torch.cuda.synchronize()
+    net.check_errors()
+    return {"grid": [N] * 3, "training_pairs": n_pairs, "training_steps": steps, "held_out": n_held,
+            "data_s": round(t_data, 1), "train_s": round(t_train, 1),
+            "final_loss": float(np.mean(losses[-50:])),
+            "zero_guess": {"ms_per_solve": round(e[0].elapsed_time(e[1]) / n_held, 3),
+                           "cycles_mean": float(np.mean(cyc0))},
+            "learned_guess": {"ms_per_solve": round(e[1].elapsed_time(e[2]) / n_held, 3),
+                              "cycles_mean": float(np.mean(cyc1)),
+                              "guess_ms": round(e[2].elapsed_time(e[3]) / n_held, 3)}}

@@ -229,6 +229,7 @@ class Context:
 
     def set_stream(self, stream_ptr: int):
         self.check(self._lib.bmg_set_stream(self.h, ctypes.c_void_p(stream_ptr)), "bmg_set_stream")
+        self._stream = stream_ptr
 
     def solve_ptr(self, b_ptr: int, x_ptr: int, flags: int) -> N.Report:
         rep = N.Report()
@@ -245,6 +246,13 @@ class Context:
         if hasattr(b, "is_cuda") and b.is_cuda:
             if not (x.is_contiguous() and b.is_contiguous()):
                 raise FatalError("device arrays must be contiguous")
+            # queue the solve behind the work that produced b and x: on the
+            # caller's current stream
+            import torch
+
+            cur = torch.cuda.current_stream(b.device).cuda_stream
+            if getattr(self, "_stream", None) != cur:
+                self.set_stream(cur)
             return self.solve_ptr(b.data_ptr(), x.data_ptr(), flags | N.DEVICE_PTRS)
         if not (isinstance(b, np.ndarray) and b.dtype == np.float64 and b.flags["C_CONTIGUOUS"]):
             raise FatalError("b must be a contiguous float64 array")

@@ -311,3 +311,19 @@ def test_semicoarsening_shapes(native):
     xo, orep, _, rc = oracle_for(br).solve(b.reshape(br.N), rel_tol=1e-12, max_iter=400, n_pre=2,
                                            n_post=2, cycle_type="V", coarse_level=0)
     assert rel(vmean(x.reshape(br.N), V), vmean(xo, V)) <= 1e-9
+
+
+def test_device_solve_waits_for_the_producer_of_b(native):
+    """b produced by torch work still queued on the current stream: the
+    solve must run behind it (Context.solve follows torch's current stream)."""
+    import torch
+
+    mesh, b_np, _ = workloads.cavity(64, seed=3)
+    b0 = torch.from_numpy(b_np).cuda()
+    c = ctx_for(mesh, relTol=1e-10, criterion="rhs", krylov="fcg")
+    for q in range(3):
+        torch.cuda._sleep(50_000_000)  # keep the stream busy for tens of ms
+        b = b0 * float(q + 1)          # written only after the sleep
+        x = torch.zeros_like(b)
+        rep = c.solve(b, x, zero_guess=True)
+        assert rep.status == 0 and rep.rhs_rel_residual <= 1e-10
