@@ -62,6 +62,14 @@ int bun_conv3(int n0, int n1, int n2, const void* src0, int c0, int up0, const v
     return status(conv_launch(a, kc, cout, S(stream)));
 }
 
+int bun_conv3_stage_width(int c0, int c1, int cout, int n2) {
+    const int cin = c0 + c1;
+    if (rows_supported(cin, cout, n2) && c0 % 16 == 0 && c1 % 16 == 0) return 16;
+    for (int kc : {64, 32, 16})
+        if (c0 % kc == 0 && c1 % kc == 0 && conv_supported(kc, cout)) return kc;
+    return 0;
+}
+
 size_t bun_wgrad_part_floats(int cin, int cout, int nsplit) {
     if (cin < 8 || cout < 1 || nsplit < 1) return 0;
     const size_t rows_pad = (27 * (size_t)cin + 127) / 128 * 128;

@@ -438,6 +438,211 @@ __global__ void __launch_bounds__(kThreads) k_wgrad(WgradArgs a) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// forward / data-gradient convolution marching along j (n2 % 128 == 0)
+// ---------------------------------------------------------------------------
+// A CTA owns plane i and the 128-voxel k-segment k0 .. k0+127 and walks the
+// rows j of a segment of kJSeg rows.  For output row j it needs the input
+// rows (i+di, j+dj), di, dj in {-1, 0, 1}, over k0-1 .. k0+128; they live in
+// a ring of NR row-sets (a row-set = the three rows di = -1, 0, 1 of one j')
+// filled once per j' by cp.async, laid out per row as [8-channel chunk h]
+// [voxel 0 .. 129] x 16 bytes.  The operand of tap (di, dj, dk) and channels
+// 16u .. 16u+15 is then a K-major no-swizzle matrix starting at
+//   row(j+dj, di) + 2u * 2080 + (dk + 1) * 16
+// with 2080 bytes between channel chunks (leading byte offset) and 128 bytes
+// between groups of 8 voxels (stride byte offset): shifting along k is a
+// change of start address, so every input row is loaded once, not 27 times.
+// All weights stay in shared memory; the TMEM accumulator is double-
+// buffered so the epilogue of row j overlaps the MMAs of row j+1.
+// Warps 0-3: epilogue (thread = voxel = TMEM lane); warps 4-7: row loader;
+// warp 8: TMEM allocation, one thread issues the MMAs.
+constexpr int kRowVox = 130;                 // k0-1 .. k0+128
+constexpr int kRowChunk = kRowVox * 16;      // bytes of one 8-channel chunk of a row
+constexpr int kJSeg = 32;                    // rows per CTA
+constexpr int kRowThreads = 288;
+
+template <int CIN, int NOUT, int NR>
+struct RowShape {
+    static constexpr int ROW = (CIN / 8) * kRowChunk;  // one input row
+    static constexpr int SET = 3 * ROW;                // rows di = -1, 0, 1
+    static constexpr int WBYTES = 27 * CIN * NOUT * 2;
+    static constexpr int NCOLS = NOUT <= 32 ? 32 : NOUT <= 64 ? 64 : 128;
+    static constexpr int smem = NR * SET + WBYTES + (2 * NR + 6) * 8 + 16;
+};
+
+template <int CIN, int NOUT, int NR>
+__global__ void __launch_bounds__(kRowThreads, 1) k_conv_rows(ConvArgs a) {
+    using F = RowShape<CIN, NOUT, NR>;
+    constexpr int NQ = CIN / 16;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t* rows = smem;
+    uint8_t* wts = smem + NR * F::SET;
+    uint64_t* full = reinterpret_cast<uint64_t*>(wts + F::WBYTES);
+    uint64_t* empty = full + NR;
+    uint64_t* wbar = empty + NR;
+    uint64_t* tfull = wbar + 1;   // [2]
+    uint64_t* tempty = tfull + 2; // [2]
+    uint64_t* fin = tempty + 2;   // every MMA of the CTA has completed
+    uint32_t* slot = reinterpret_cast<uint32_t*>(fin + 1);
+
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int n0 = a.n0, n1 = a.n1, n2 = a.n2;
+    const int k0 = blockIdx.x * kTile;
+    const int i = blockIdx.y;
+    const int js = blockIdx.z * kJSeg;
+    const int je = min(js + kJSeg, n1);
+    const int nsteps = je - js;
+
+    if (tid == 0) {
+        for (int r = 0; r < NR; ++r) {
+            mbar_init(&full[r], kProducers);
+            mbar_init(&empty[r], 1);
+        }
+        mbar_init(wbar, kProducers);
+        for (int q = 0; q < 2; ++q) {
+            mbar_init(&tfull[q], 1);
+            mbar_init(&tempty[q], kProducers);
+        }
+        mbar_init(fin, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 8) tmem_alloc(slot, 2 * F::NCOLS);
+    tc_before();
+    __syncthreads();
+    tc_after();
+    const uint32_t tmem = *slot;
+    bool ok = true;
+    const uint32_t base = smem_u32(smem);
+
+    if (warp >= 4 && warp < 8) {
+        // ---- loader: weights once, then the row-sets js-1 .. je
+        const int lt = tid - 128;
+        const uint32_t wb = base + NR * F::SET;
+        for (int c = lt; c < F::WBYTES / 16; c += kProducers) cp16(wb + c * 16, a.wpack + c * 8, true);
+        cp_arrive(wbar);
+        for (int jj = js - 1; jj <= je; ++jj) {
+            const int q = jj - (js - 1);
+            const int r = q % NR;
+            const uint32_t use = (uint32_t)(q / NR);
+            if (!mbar_wait(&empty[r], (use & 1) ^ 1)) {
+                ok = false;
+                break;
+            }
+            const uint32_t sb = base + r * F::SET;
+            const bool jok = jj >= 0 && jj < n1;
+            // 3 rows x 130 voxels x CIN/8 chunks
+            for (int e = lt; e < 3 * kRowVox * (CIN / 8); e += kProducers) {
+                const int di = e / (kRowVox * (CIN / 8));
+                const int rem = e - di * (kRowVox * (CIN / 8));
+                const int h = rem / kRowVox, kk = rem - h * kRowVox;
+                const int ii = i + di - 1, k = k0 - 1 + kk;
+                const bool valid = jok && ii >= 0 && ii < n0 && k >= 0 && k < n2;
+                const bf16* src = valid ? in_ptr(a.in, n1, n2, ii, jj, k, h * 8) : a.wpack;
+                cp16(sb + di * F::ROW + h * kRowChunk + kk * 16, src, valid);
+            }
+            cp_arrive(&full[r]);
+        }
+    } else if (tid == 256) {
+        // ---- MMA issue
+        constexpr uint32_t idesc = idesc_bf16(kTile, NOUT, false, false);
+        const uint32_t wb = base + NR * F::SET;
+        if (!mbar_wait(wbar, 0)) ok = false;
+        for (int st = 0; ok && st < nsteps; ++st) {
+            const int acc = st & 1;
+            const uint32_t ause = (uint32_t)(st >> 1);
+            if (!mbar_wait(&tempty[acc], (ause & 1) ^ 1)) {
+                ok = false;
+                break;
+            }
+            // row-sets st-1+1 .. st+1+1 in ring order (q = jj - (js-1))
+            for (int q = (st == 0 ? 0 : st + 2); q <= st + 2; ++q) {
+                if (!mbar_wait(&full[q % NR], (uint32_t)(q / NR) & 1)) ok = false;
+            }
+            if (!ok) break;
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            tc_after();
+            const uint32_t d = tmem + (uint32_t)(acc * F::NCOLS);
+            bool first = true;
+#pragma unroll 1
+            for (int dj = 0; dj < 3; ++dj) {
+                const uint32_t set = base + ((st + dj) % NR) * F::SET;
+#pragma unroll 1
+                for (int di = 0; di < 3; ++di) {
+#pragma unroll
+                    for (int dk = 0; dk < 3; ++dk) {
+                        const int t = di * 9 + dj * 3 + dk;
+#pragma unroll
+                        for (int u = 0; u < NQ; ++u) {
+                            const uint32_t as = set + di * F::ROW + 2 * u * kRowChunk + dk * 16;
+                            const uint32_t bs = wb + (uint32_t)((t * NQ + u) * NOUT * 32);
+                            umma(d, sdesc(as, kRowChunk, 128), sdesc(bs, 128, 256), idesc, first ? 0u : 1u);
+                            first = false;
+                        }
+                    }
+                }
+            }
+            umma_commit(&tfull[acc]);
+            umma_commit(&empty[st % NR]);  // row-set js-1+st is not needed again
+        }
+        umma_commit(fin);  // one phase, after every MMA issued above
+    }
+
+    if (warp < 4) {
+        // ---- epilogue
+        for (int st = 0; st < nsteps; ++st) {
+            const int acc = st & 1;
+            bool done = mbar_wait(&tfull[acc], (uint32_t)(st >> 1) & 1);
+            done = __all_sync(0xffffffffu, done);
+            if (!done) {
+                ok = false;
+                break;
+            }
+            tc_after();
+            const int j = js + st;
+            const long v = ((long)i * n1 + j) * n2 + k0 + tid;
+#pragma unroll 1
+            for (int c0 = 0; c0 < NOUT; c0 += 16) {
+                float accv[16];
+                tmem_ld16(tmem + (uint32_t)(acc * F::NCOLS) + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, accv);
+                if (a.bias) {
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) accv[q] += a.bias[c0 + q];
+                }
+                if (a.relu) {
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) accv[q] = fmaxf(accv[q], 0.f);
+                }
+                if (a.mask) {
+                    const uint4* mp = reinterpret_cast<const uint4*>(a.mask + v * NOUT + c0);
+                    uint4 mv[2] = {mp[0], mp[1]};
+                    const bf16* m = reinterpret_cast<const bf16*>(mv);
+#pragma unroll
+                    for (int q = 0; q < 16; ++q)
+                        if (!(__bfloat162float(m[q]) > 0.f)) accv[q] = 0.f;
+                }
+                uint4 ov[2];
+                __nv_bfloat162* o = reinterpret_cast<__nv_bfloat162*>(ov);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) o[q] = __floats2bfloat162_rn(accv[2 * q], accv[2 * q + 1]);
+                uint4* op = reinterpret_cast<uint4*>(a.out + v * NOUT + c0);
+                op[0] = ov[0];
+                op[1] = ov[1];
+            }
+            tc_before();
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&tempty[acc])) : "memory");
+        }
+    }
+
+    if (!ok && a.err) atomicExch(a.err, kErrTimeout);
+    tc_before();
+    __syncthreads();
+    if (warp == 8) {
+        tc_after();
+        mbar_wait(fin, 0);  // no MMA may still write the accumulators
+        tmem_free(tmem, 2 * F::NCOLS);
+    }
+}
+
 constexpr int conv_stages(int kc, int nout) {
     return (96 * 1024) / (kc * 2 * (kTile + nout)) > 6   ? 6
            : (96 * 1024) / (kc * 2 * (kTile + nout)) < 2 ? 2
@@ -465,7 +670,39 @@ cudaError_t wgrad_inst(const WgradArgs& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+template <int CIN, int NOUT>
+cudaError_t rows_inst(const ConvArgs& a, cudaStream_t s) {
+    constexpr int NR = RowShape<CIN, NOUT, 4>::smem <= 200 * 1024 ? 4 : 3;
+    constexpr int smem = RowShape<CIN, NOUT, NR>::smem;
+    static_assert(smem <= 227 * 1024, "row kernel does not fit shared memory");
+    cudaError_t e = cudaFuncSetAttribute(k_conv_rows<CIN, NOUT, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         smem);
+    if (e != cudaSuccess) return e;
+    const dim3 grid((unsigned)(a.n2 / kTile), (unsigned)a.n0, (unsigned)((a.n1 + kJSeg - 1) / kJSeg));
+    k_conv_rows<CIN, NOUT, NR><<<grid, kRowThreads, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
 }  // namespace
+
+// the row-marching kernel covers these (input channels, output channels)
+// on grids with n2 % 128 == 0; other shapes use k_conv
+bool rows_supported(int cin, int nout, int n2) {
+    if (n2 % 128) return false;
+    return (cin == 16 && (nout == 16 || nout == 32 || nout == 48)) || (cin == 32 && (nout == 16 || nout == 32)) ||
+           (cin == 48 && nout == 16);
+}
+
+cudaError_t rows_launch(const ConvArgs& a, int nout, cudaStream_t s) {
+    const int cin = a.in.c0 + a.in.c1;
+    if (cin == 16 && nout == 16) return rows_inst<16, 16>(a, s);
+    if (cin == 16 && nout == 32) return rows_inst<16, 32>(a, s);
+    if (cin == 16 && nout == 48) return rows_inst<16, 48>(a, s);
+    if (cin == 32 && nout == 16) return rows_inst<32, 16>(a, s);
+    if (cin == 32 && nout == 32) return rows_inst<32, 32>(a, s);
+    if (cin == 48 && nout == 16) return rows_inst<48, 16>(a, s);
+    return cudaErrorInvalidValue;
+}
 
 bool conv_supported(int kc, int nout) {
     switch (kc) {
@@ -482,6 +719,8 @@ bool wgrad_supported(int cout) { return cout == 16 || cout == 32 || cout == 64; 
     if (kc == KC && nout == N) return conv_inst<KC, N>(a, s);
 
 cudaError_t conv_launch(const ConvArgs& a, int kc, int nout, cudaStream_t s) {
+    // rows of 128 voxels with 16-channel weight blocks: the row-marching kernel
+    if (kc == 16 && rows_supported(a.in.c0 + a.in.c1, nout, a.n2)) return rows_launch(a, nout, s);
     BUN_CONV_CASE(16, 16)
     BUN_CONV_CASE(16, 32)
     BUN_CONV_CASE(16, 48)

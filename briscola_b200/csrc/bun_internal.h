@@ -61,6 +61,8 @@ constexpr int kErrTimeout = 1;
 cudaError_t conv_launch(const ConvArgs& a, int kc, int nout, cudaStream_t s);
 cudaError_t wgrad_launch(const WgradArgs& a, int cout, cudaStream_t s);
 bool conv_supported(int kc, int nout);
+bool rows_supported(int cin, int nout, int n2);
+cudaError_t rows_launch(const ConvArgs& a, int nout, cudaStream_t s);
 bool wgrad_supported(int cout);
 
 }  // namespace bun

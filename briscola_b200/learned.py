@@ -121,7 +121,7 @@ class LearnedGuess:
         return self.ctx.solve(b, x, zero_guess=False)
 
 
-def benchmark(N: int, n_pairs: int, steps: int, n_held: int, seed: int = 1, lr: float = 2e-3):
+def benchmark(N: int, n_pairs: int, steps: int, n_held: int, seed: int = 1, lr: float = 1e-3):
     """Config 5 as one measurement: train on n_pairs solved pairs of one
     sequence, then time held-out solves of another sequence from zero and
     from the learned guess (mixed precision, flexible CG, ||b||-relative

@@ -49,14 +49,6 @@ CONVS = (
 )
 
 
-def _kc(*cs):
-    """largest stage width in {64, 32, 16} dividing every nonzero channel count"""
-    for kc in (64, 32, 16):
-        if all(c % kc == 0 for c in cs if c):
-            return kc
-    raise ValueError(cs)
-
-
 class UNetError(RuntimeError):
     pass
 
@@ -90,6 +82,7 @@ def load(path: str = LIB_PATH):
         "bun_sumsq": [l, vp, i, vp, vp, vp],
         "bun_laplace_residual": [i, i, i, vp, vp, f, vp, vp],
         "bun_laplace_add": [i, i, i, vp, f, vp, vp],
+        "bun_conv3_stage_width": [i, i, i, i],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -104,7 +97,7 @@ def load(path: str = LIB_PATH):
 EXPORTED = ("bun_conv3", "bun_conv3_wgrad", "bun_wgrad_part_floats", "bun_pack_weights", "bun_conv_in",
             "bun_conv_in_wgrad", "bun_head", "bun_head_grad", "bun_pool", "bun_unpool_grad", "bun_skip_grad",
             "bun_mse", "bun_adam", "bun_scale_to_float", "bun_scale_to_double", "bun_sumsq",
-            "bun_laplace_residual", "bun_laplace_add")
+            "bun_laplace_residual", "bun_laplace_add", "bun_conv3_stage_width")
 
 
 def _check(rc, what):
@@ -202,10 +195,16 @@ class UNet:
         self.dr = torch.zeros(self.nvox[0], dtype=f32, device=dev)
         self.zero = torch.zeros(self.nvox[0], dtype=f32, device=dev)
         self.err = torch.zeros(1, dtype=torch.int32, device=dev)
-        # packed BF16 weights: forward and data-gradient layouts
-        self.wf, self.wd = {}, {}
+        # packed BF16 weights: forward and data-gradient layouts, for the
+        # stage width the library picks for each layer's grid
+        self.wf, self.wd, self.kcf, self.kcd = {}, {}, {}, {}
         for name, lev, c0, up0, c1, cout in CONVS:
             n = 27 * (c0 + c1) * cout
+            n2 = self.dims[lev][2]
+            self.kcf[name] = self.L.bun_conv3_stage_width(c0, c1, cout, n2)
+            self.kcd[name] = self.L.bun_conv3_stage_width(cout, 0, c0 + c1, n2)
+            if not (self.kcf[name] and self.kcd[name]):
+                raise UNetError(f"no convolution kernel for layer {name}")
             self.wf[name] = torch.zeros(n, dtype=bf, device=dev)
             self.wd[name] = torch.zeros(n, dtype=bf, device=dev)
         # scratch for the reductions
@@ -237,10 +236,10 @@ class UNet:
         s = self._s()
         for name, lev, c0, up0, c1, cout in CONVS:
             w = self._w(name + ".w")
-            _check(self.L.bun_pack_weights(w.data_ptr(), c0 + c1, cout, _kc(c0, c1), 0, self.wf[name].data_ptr(),
-                                           s), "pack")
-            _check(self.L.bun_pack_weights(w.data_ptr(), c0 + c1, cout, _kc(cout), 1, self.wd[name].data_ptr(),
-                                           s), "pack")
+            _check(self.L.bun_pack_weights(w.data_ptr(), c0 + c1, cout, self.kcf[name], 0,
+                                           self.wf[name].data_ptr(), s), "pack")
+            _check(self.L.bun_pack_weights(w.data_ptr(), c0 + c1, cout, self.kcd[name], 1,
+                                           self.wd[name].data_ptr(), s), "pack")
 
     def _inputs(self, name):
         a = self.a
@@ -278,7 +277,7 @@ class UNet:
                 m0, m1, m2 = self.dims[lev - 1]
                 _check(L.bun_pool(m0, m1, m2, c, self.a[src].data_ptr(), self.a[dst].data_ptr(), s), "pool")
             src0, src1 = self._inputs(name)
-            self._conv(spec, src0, src1, self.wf[name], _kc(c0, c1), cout, 1, None, self.a[self._OUT[name]],
+            self._conv(spec, src0, src1, self.wf[name], self.kcf[name], cout, 1, None, self.a[self._OUT[name]],
                        self.dims[lev])
         _check(L.bun_head(self.nvox[0], self.a["d0"].data_ptr(), self._w("head.w").data_ptr(),
                           self._w("head.b").data_ptr(), self.y.data_ptr(), s), "head")
@@ -298,9 +297,9 @@ class UNet:
     def _dgrad(self, spec, dz, out, mask):
         name, lev, c0, up0, c1, cout = spec
         n0, n1, n2 = self.dims[lev]
-        _check(self.L.bun_conv3(n0, n1, n2, dz.data_ptr(), cout, 0, None, 0, self.wd[name].data_ptr(), _kc(cout),
-                                c0 + c1, None, 0, mask.data_ptr() if mask is not None else None, out.data_ptr(),
-                                self.err.data_ptr(), self._s()), f"dgrad {name}")
+        _check(self.L.bun_conv3(n0, n1, n2, dz.data_ptr(), cout, 0, None, 0, self.wd[name].data_ptr(),
+                                self.kcd[name], c0 + c1, None, 0, mask.data_ptr() if mask is not None else None,
+                                out.data_ptr(), self.err.data_ptr(), self._s()), f"dgrad {name}")
 
     def backward(self):
         """gradients of the loss whose dL/dy is in self.dy, into self.g"""

@@ -40,10 +40,19 @@ enum {
  *      (mask != NULL: a BF16 tensor of cout channels on the output grid).
  * kc: input channels per pipeline stage (16, 32 or 64), dividing c0 and c1.
  * Supported (kc, cout): (16: 16/32/48/64), (32: 16/32/64/96), (64: 32/64/128).
+ * With kc = 16 on grids with n2 % 128 == 0 the row-marching kernel runs
+ * (see bun_conv3_stage_width); the result is the same convolution.
  * err: device int set to nonzero if a CTA gave up waiting (never expected). */
 int bun_conv3(int n0, int n1, int n2, const void* src0, int c0, int up0, const void* src1, int c1,
               const void* wpack, int kc, int cout, const float* bias, int relu, const void* mask, void* out,
               int* err, void* stream);
+
+/* The stage width kc to pack weights for and pass to bun_conv3 for a
+ * convolution with inputs (c0, c1), cout outputs on grids of extent n2
+ * along k: 16 where the row-marching kernel applies (n2 % 128 == 0 and
+ * (cin, cout) in {(16,16), (16,32), (16,48), (32,16), (32,32), (48,16)}),
+ * otherwise the widest of 64/32/16 the tile kernel supports; 0: none. */
+int bun_conv3_stage_width(int c0, int c1, int cout, int n2);
 
 /* Weight gradient of a tensor-core convolution with the inputs of bun_conv3
  * and the output gradient dz (cout channels, 16/32/64):

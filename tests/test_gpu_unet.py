@@ -52,6 +52,13 @@ CONV_CASES = [
     ((8, 8, 8), 64, 1, 64, 64, 64),    # decoder: upsampled + skip
     ((8, 16, 8), 64, 1, 32, 32, 32),
     ((16, 8, 8), 32, 1, 16, 16, 16),
+    # rows of 128 voxels with kc = 16: the row-marching kernel
+    ((2, 3, 128), 16, 0, 0, 16, 16),
+    ((4, 4, 128), 16, 0, 0, 32, 16),
+    ((2, 4, 128), 32, 1, 16, 16, 16),   # upsampled + skip, 48 channels
+    ((2, 2, 128), 32, 0, 0, 32, 16),
+    ((2, 2, 256), 32, 0, 0, 16, 16),    # two k-segments
+    ((1, 40, 128), 16, 0, 0, 16, 16),   # two j-segments (32 + 8 rows)
 ]
 
 
@@ -90,7 +97,9 @@ def test_conv_forward(L, dims, c0, up0, c1, cout, kc, relu):
 
 @pytest.mark.parametrize("dims,cin,cout,kc", [((8, 8, 8), 48, 16, 16), ((8, 8, 8), 128, 64, 64),
                                                ((8, 8, 8), 96, 32, 32), ((8, 8, 8), 16, 32, 32),
-                                               ((8, 8, 8), 32, 64, 64)])
+                                               ((8, 8, 8), 32, 64, 64),
+                                               ((2, 3, 128), 48, 16, 16), ((2, 3, 128), 16, 32, 16),
+                                               ((2, 3, 128), 32, 32, 16)])
 def test_conv_data_gradient_with_mask(L, dims, cin, cout, kc):
     rng = np.random.default_rng(cin * 7 + cout)
     W = rng.standard_normal((27, cin, cout)) / np.sqrt(27 * cout)
@@ -277,6 +286,35 @@ def test_network_matches_reference(L):
         assert e <= 1e-1, (name, e)
     loss = float(net.loss.item())
     assert abs(loss - np.mean((host(y).reshape(dims) - target.astype(np.float32)) ** 2)) <= 1e-4 * loss
+
+
+def test_network_row_kernels_match_reference(L):
+    """level 0 on 128-voxel rows runs the row-marching kernel"""
+    from briscola_b200 import unet
+
+    rng = np.random.default_rng(6)
+    dims = (8, 8, 128)
+    p = unet.init_params(12)
+    net = unet.UNet(dims, params=p)
+    assert net.kcf["e0b"] == 16 and net.kcf["d0a"] == 16 and net.kcd["d0a"] == 16
+    x = rng.standard_normal(dims)
+    target = rng.standard_normal(dims)
+    y = net.forward(dev(x, torch.float32).reshape(-1))
+    net.mse(dev(target, torch.float32).reshape(-1))
+    net.backward()
+    torch.cuda.synchronize()
+    net.check_errors()
+    P = R.unpack(p.astype(np.float64))
+    x32 = x.astype(np.float32).astype(np.float64)
+    yr, act = R.forward(P, x32)
+    assert rel(host(y).reshape(dims), yr) <= 3e-2
+    dy = 2.0 * (host(y).reshape(dims) - target.astype(np.float32)) / x.size
+    G = R.flat(R.backward(P, x32, act, dy))
+    g = host(net.g)
+    layout, n = unet.param_layout()
+    for name, shape, off in layout:
+        size = int(np.prod(shape))
+        assert rel(g[off:off + size], G[off:off + size]) <= 1e-1, name
 
 
 def test_training_reduces_loss(L):

@@ -204,3 +204,77 @@ def test_descriptor_reads_stay_inside_the_stage():
         for q in range(TILE // 16):
             assert mnmajor(q * 256, 128, 2048, mm, kk).max() + 2 <= a_bytes
             assert mnmajor(a_bytes + q * 256, 128, 2048, nn, kb).max() + 2 <= stage
+
+
+ROW_VOX, ROW_CHUNK = 130, 130 * 16
+
+
+def emulate_rows(dims, src0, c0, up0, src1, c1, W):
+    """bun_conv.cu k_conv_rows: row-sets of 3 rows x 130 voxels laid out
+    [chunk][voxel] x 16 B, tap operands by start-address shifts"""
+    n0, n1, n2 = dims
+    cin, cout = c0 + c1, W.shape[2]
+    nq = cin // 16
+    wp = pack(W, 16, False)
+    row_b = (cin // 8) * ROW_CHUNK
+    set_b = 3 * row_b
+    out = np.zeros((n0, n1, n2, cout))
+    mm, kk_ = np.meshgrid(np.arange(TILE), np.arange(16), indexing="ij")
+    nn, kb = np.meshgrid(np.arange(cout), np.arange(16), indexing="ij")
+    for k0 in range(0, n2, TILE):
+        for i in range(n0):
+            for j in range(n1):
+                # the three row-sets j-1, j, j+1 (one value per BF16 slot)
+                smem = np.zeros(3 * set_b // 2)
+                wbase = 3 * set_b
+                for dj in range(3):
+                    jj = j + dj - 1
+                    for di in range(3):
+                        ii = i + di - 1
+                        for kk in range(ROW_VOX):
+                            k = k0 - 1 + kk
+                            if not (0 <= jj < n1 and 0 <= ii < n0 and 0 <= k < n2):
+                                continue
+                            for h in range(cin // 8):
+                                a = (dj * set_b + di * row_b + h * ROW_CHUNK + kk * 16) // 2
+                                for e in range(8):
+                                    smem[a + e] = in_value(src0, c0, up0, src1, ii, jj, k, h * 8 + e)
+                wsm = wp  # weights follow the ring in shared memory
+                acc = np.zeros((TILE, cout))
+                for dj in range(3):
+                    for di in range(3):
+                        for dk in range(3):
+                            t = di * 9 + dj * 3 + dk
+                            for u in range(nq):
+                                st = dj * set_b + di * row_b + 2 * u * ROW_CHUNK + dk * 16
+                                A = smem[kmajor(st, ROW_CHUNK, 128, mm, kk_) // 2]
+                                bs = (t * nq + u) * cout * 32
+                                B = wsm[kmajor(bs, 128, 256, nn, kb) // 2]
+                                acc += A @ B.T
+                out[i, j, k0:k0 + TILE] = acc
+    return out
+
+
+@pytest.mark.parametrize("dims,c0,up0,c1,cout", [((2, 3, 128), 16, 0, 0, 16), ((2, 2, 128), 32, 1, 16, 16),
+                                                  ((2, 2, 128), 16, 0, 0, 48)])
+def test_row_kernel_tiles_reproduce_convolution(dims, c0, up0, c1, cout):
+    rng = np.random.default_rng(10)
+    src0, src1, x = _case(rng, dims, c0, up0, c1)
+    W = rng.standard_normal((27, c0 + c1, cout))
+    got = emulate_rows(dims, src0, c0, up0, src1, c1, W)
+    assert np.allclose(got, R.conv3(x, W), rtol=1e-12, atol=1e-10)
+
+
+def test_row_kernel_reads_stay_inside_the_ring():
+    """the farthest operand element of the last row-set slot (row di = +1,
+    last channel pair, tap dk = +1) lies inside the ring, and an operand
+    never reads past voxel 129 of its row"""
+    mm, kk = np.meshgrid(np.arange(128), np.arange(16), indexing="ij")
+    for cin in (16, 32, 48):
+        row_b = (cin // 8) * ROW_CHUNK
+        for nr in (3, 4):
+            start = (nr - 1) * 3 * row_b + 2 * row_b + 2 * (cin // 16 - 1) * ROW_CHUNK + 2 * 16
+            assert kmajor(start, ROW_CHUNK, 128, mm, kk).max() + 2 <= nr * 3 * row_b
+    # within one channel chunk (k < 8): voxel 2 + 127 = 129 at most
+    m8, k8 = np.meshgrid(np.arange(128), np.arange(8), indexing="ij")
+    assert (kmajor(2 * 16, ROW_CHUNK, 128, m8, k8) // 16).max() == 129
