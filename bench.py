@@ -183,7 +183,11 @@ def profile_region(args, local):
         torch.cuda.profiler.stop()
         net.check_errors()
         return
-    kw = dict(precision="mixed", krylov="fcg") if args.profile_region == "mixed_fcg" else dict(precision="fp64")
+    kw = dict(precision="fp64")
+    if args.profile_region.startswith("mixed_fcg"):
+        kw = dict(precision="mixed", krylov="fcg")
+    if args.profile_region == "mixed_fcg_fused":
+        kw.update(autotune="off")  # the fused smoother on every level it fits (3 stages, 64-plane chunks)
     mesh, b, _ = workloads.channel(args.size)
     # the same kernels launched one by one (the profiler cannot see into a
     # graph with a conditional loop)
@@ -251,7 +255,7 @@ def main():
     ap.add_argument("--learned-pairs", type=int, default=2000)
     ap.add_argument("--learned-steps", type=int, default=2000)
     ap.add_argument("--learned-held", type=int, default=200)
-    ap.add_argument("--profile-region", choices=["mixed_fcg", "fp64", "unet_fwd"], default=None,
+    ap.add_argument("--profile-region", choices=["mixed_fcg", "mixed_fcg_fused", "fp64", "unet_fwd"], default=None,
                     help="set up, warm up, then run one solve (or one U-Net forward) between "
                          "cudaProfilerStart/Stop for ncu --profile-from-start off; prints no bench line")
     args = ap.parse_args()

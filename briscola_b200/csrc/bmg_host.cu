@@ -1015,6 +1015,51 @@ void coarseSolve(bmg_ctx* c) {
 // per launch and plane-chunk length, and keep the fastest.  The tile (16 x
 // 64 cells) is fixed by the fused kernel's register window; stages and chunk
 // length trade halo recomputation against memory passes and CTA count.
+// Each candidate is timed as a captured graph of kTuneReps smoothing steps,
+// the way the solve graph launches it (stream launches would charge the
+// per-colour passes launch costs the solve does not pay).
+constexpr int kTuneReps = 4;
+
+template <typename T>
+float timeSmoothGraph(bmg_ctx* c, int l, int sweeps, cudaEvent_t e0, cudaEvent_t e1) {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    {
+        // capture on the private stream; an exception ends the capture and
+        // gives the context its stream back
+        struct Capture {
+            bmg_ctx* c;
+            cudaStream_t user;
+            ~Capture() {
+                cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+                if (cudaStreamIsCapturing(c->capStream, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+                    cudaGraph_t dropped = nullptr;
+                    cudaStreamEndCapture(c->capStream, &dropped);
+                    if (dropped) cudaGraphDestroy(dropped);
+                }
+                c->stream = user;
+            }
+        } guard{c, c->stream};
+        c->stream = c->capStream;
+        BMG_CUDA(cudaStreamBeginCapture(c->capStream, cudaStreamCaptureModeThreadLocal));
+        for (int r = 0; r < kTuneReps; ++r) smooth<T>(c, l, sweeps);
+        BMG_CUDA(cudaStreamEndCapture(c->capStream, &g));
+    }
+    cudaError_t err = cudaSuccess;
+    float ms = 0.f;
+    err = cudaGraphInstantiate(&ge, g, 0);
+    if (err == cudaSuccess) err = cudaGraphLaunch(ge, c->stream);  // warm-up
+    if (err == cudaSuccess) err = cudaEventRecord(e0, c->stream);
+    if (err == cudaSuccess) err = cudaGraphLaunch(ge, c->stream);
+    if (err == cudaSuccess) err = cudaEventRecord(e1, c->stream);
+    if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+    if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+    if (ge) cudaGraphExecDestroy(ge);
+    cudaGraphDestroy(g);
+    BMG_CUDA(err);
+    return ms;
+}
+
 template <typename T>
 void autotuneLevel(bmg_ctx* c, int l, int sweeps, cudaEvent_t e0, cudaEvent_t e1) {
     HostLevel& H = c->lv[l];
@@ -1027,13 +1072,7 @@ void autotuneLevel(bmg_ctx* c, int l, int sweeps, cudaEvent_t e0, cudaEvent_t e1
             if (S == 0 && ti != 32) continue;
             H.fusedS[prec] = S;
             H.fusedTi[prec] = ti;
-            smooth<T>(c, l, sweeps);  // warm-up
-            BMG_CUDA(cudaEventRecord(e0, c->stream));
-            for (int r = 0; r < 3; ++r) smooth<T>(c, l, sweeps);
-            BMG_CUDA(cudaEventRecord(e1, c->stream));
-            BMG_CUDA(cudaEventSynchronize(e1));
-            float ms = 0.f;
-            BMG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            const float ms = timeSmoothGraph<T>(c, l, sweeps, e0, e1);
             if (ms < best) {
                 best = ms;
                 bestS = S;
