@@ -316,6 +316,141 @@ __global__ void __launch_bounds__(256) k_prolong_correct(Bricks<T> FB, Bricks<T>
 }
 
 // ---------------------------------------------------------------------------
+// The same two transfers for factor-2 coarsening along every axis with
+// n2 % 4 == 0 (fine) -- the shape of every level the solver builds from
+// even brick extents: a thread owns four fine cells along k.  Prolongation:
+// the coarse i/j indices and weights are set up once for the four cells and
+// the fine quad is read and written as one vector.  Restriction: the thread
+// owns the two coarse cells over those four fine cells and evaluates the
+// residual of each of its four fine rows from whole-vector loads.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_prolong_quad(Bricks<T> FB, Bricks<T> CB, TransferSet ts) {
+    int i;
+    const int b = brick_of(FB, blockIdx.z, i);
+    const LevelView<T>& F = FB.v[b];
+    const LevelView<T>& C = CB.v[b];
+    const TransferTabs& t = ts.t[b];
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k0 = 4 * p;
+    if (j >= F.n1 || k0 >= F.n2) return;
+    const int* pidx = t.pidx;
+    const T* pw;
+    if constexpr (sizeof(T) == 8)
+        pw = reinterpret_cast<const T*>(t.pw64);
+    else
+        pw = reinterpret_cast<const T*>(t.pw32);
+    const int I0 = ldg(pidx + 2 * i), I1 = ldg(pidx + 2 * i + 1);
+    const int J0 = ldg(pidx + 2 * F.n0 + 2 * j), J1 = ldg(pidx + 2 * F.n0 + 2 * j + 1);
+    const T wi = ldg(pw + i), wj = ldg(pw + F.n0 + j);
+    const T ui = T(1) - wi, uj = T(1) - wj;
+    const T* X = C.x;
+    const long r00 = C.base + (long)I0 * C.si + (long)J0 * C.sj;
+    const long r01 = C.base + (long)I0 * C.si + (long)J1 * C.sj;
+    const long r10 = C.base + (long)I1 * C.si + (long)J0 * C.sj;
+    const long r11 = C.base + (long)I1 * C.si + (long)J1 * C.sj;
+    const long c0 = F.base + (long)i * F.si + (long)j * F.sj + k0;
+    T xf[4];
+    Row4<T>::ld(F.x + c0, xf);
+    const int* pk = pidx + 2 * (F.n0 + F.n1);
+    const T* wk = pw + F.n0 + F.n1;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int k = k0 + q;
+        const int K0 = ldg(pk + 2 * k), K1 = ldg(pk + 2 * k + 1);
+        const T w = ldg(wk + k), u = T(1) - w;
+        const T v00 = u * X[r00 + K0] + w * X[r00 + K1];
+        const T v01 = u * X[r01 + K0] + w * X[r01 + K1];
+        const T v10 = u * X[r10 + K0] + w * X[r10 + K1];
+        const T v11 = u * X[r11 + K0] + w * X[r11 + K1];
+        xf[q] += ui * (uj * v00 + wj * v01) + wi * (uj * v10 + wj * v11);
+    }
+    Row4<T>::st(F.x + c0, xf);
+    if (F.per0 | F.per1 | F.per2) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) store_x(F, c0 + q, i, j, k0 + q, xf[q]);
+    }
+}
+
+template <typename T, bool VAR>
+__global__ void __launch_bounds__(256) k_restrict_quad(Bricks<T> FB, Bricks<T> CB, TransferSet ts) {
+    int I;
+    const int b = brick_of(CB, blockIdx.z, I);
+    const LevelView<T>& C = CB.v[b];
+    const LevelView<T>& F = FB.v[b];
+    const TransferTabs& t = ts.t[b];
+    const int P = blockIdx.x * blockDim.x + threadIdx.x;  // coarse k-pair
+    const int J = blockIdx.y * blockDim.y + threadIdx.y;
+    const int K0 = 2 * P;
+    if (J >= C.n1 || K0 >= C.n2) return;
+    const T* ratio;
+    if constexpr (sizeof(T) == 8)
+        ratio = reinterpret_cast<const T*>(t.ratio64);
+    else
+        ratio = reinterpret_cast<const T*>(t.ratio32);
+    const int k0 = 2 * K0;
+    T rk[4], wkl[4], wkh[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) rk[q] = ldg(ratio + F.n0 + F.n1 + k0 + q);
+    Row4<T>::ldg4(F.tab + F.to.wl[2] + k0, wkl);
+    Row4<T>::ldg4(F.tab + F.to.wh[2] + k0, wkh);
+    T acc0 = T(0), acc1 = T(0);
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+        const int i = 2 * I + a;
+        const T ra = ldg(ratio + i);
+        const T wil = ldg(F.tab + F.to.wl[0] + i), wih = ldg(F.tab + F.to.wh[0] + i);
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int j = 2 * J + e;
+            const T rab = ra * ldg(ratio + F.n0 + j);
+            const T wjl = ldg(F.tab + F.to.wl[1] + j), wjh = ldg(F.tab + F.to.wh[1] + j);
+            const long c = F.base + (long)i * F.si + (long)j * F.sj + k0;
+            T own[4], xm[4], xp[4], ym[4], yp[4], bb[4];
+            Row4<T>::ld(F.x + c, own);
+            Row4<T>::ld(F.x + c - F.si, xm);
+            Row4<T>::ld(F.x + c + F.si, xp);
+            Row4<T>::ld(F.x + c - F.sj, ym);
+            Row4<T>::ld(F.x + c + F.sj, yp);
+            Row4<T>::ld(F.b + c, bb);
+            const T left = F.x[c - 1], right = F.x[c + 4];
+            T l0[4], l0p[4], l1[4], l1p[4], l2[4], l2r = T(1);
+            if (VAR) {
+                Row4<T>::ldg4(F.lam0 + c, l0);
+                Row4<T>::ldg4(F.lam0 + c + F.si, l0p);
+                Row4<T>::ldg4(F.lam1 + c, l1);
+                Row4<T>::ldg4(F.lam1 + c + F.sj, l1p);
+                Row4<T>::ldg4(F.lam2 + c, l2);
+                l2r = ldg(F.lam2 + c + 4);
+            }
+            T r[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                T w[6] = {wil, wih, wjl, wjh, wkl[q], wkh[q]};
+                if (VAR) {
+                    w[0] *= l0[q];
+                    w[1] *= l0p[q];
+                    w[2] *= l1[q];
+                    w[3] *= l1p[q];
+                    w[4] *= l2[q];
+                    w[5] *= q < 3 ? l2[q + 1] : l2r;
+                }
+                const T km = q > 0 ? own[q - 1] : left, kp = q < 3 ? own[q + 1] : right;
+                const T sv = w[0] * xm[q] + w[1] * xp[q] + w[2] * ym[q] + w[3] * yp[q] + w[4] * km + w[5] * kp;
+                const T d = w[0] + w[1] + w[2] + w[3] + w[4] + w[5];
+                r[q] = bb[q] + d * own[q] - sv;
+            }
+            acc0 += rab * (rk[0] * r[0] + rk[1] * r[1]);
+            acc1 += rab * (rk[2] * r[2] + rk[3] * r[3]);
+        }
+    }
+    const long cc = C.base + (long)I * C.si + (long)J * C.sj + K0;
+    C.b[cc] = acc0;
+    C.b[cc + 1] = acc1;
+}
+
+// ---------------------------------------------------------------------------
 // Coarse direct solve: x = inverse(A'_pinned) b' with b'(0) = 0 (MG.C:37-40,
 // solver.C:201-231, APLU.C:91-128).  One CTA; the inverse is factored once
 // per matrix on the host in FP64.  cidx gives the slab index of every
@@ -600,14 +735,34 @@ void launch_jacobi(const Bricks<T>& B, T* tmp, cudaStream_t s) {
     k_copy_interior<T><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, tmp);
 }
 
+// factor-2 coarsening along every axis and n2 % 4 == 0 on the fine level
+template <typename T>
+bool quad_transfers(const Bricks<T>& F, const TransferSet& t) {
+    for (int b = 0; b < F.nb; ++b)
+        if (t.t[b].R0 != 2 || t.t[b].R1 != 2 || t.t[b].R2 != 2 || F.v[b].n2 % 4) return false;
+    return true;
+}
+
 template <typename T, bool VAR>
 void launch_residual_restrict(const Bricks<T>& F, const Bricks<T>& C, const TransferSet& t, cudaStream_t s) {
+    if (quad_transfers(F, t)) {
+        const int np = C.max2 / 2;
+        const dim3 blk = np >= 32 ? dim3(32, 8, 1) : np >= 8 ? dim3(8, 32, 1) : dim3(2, 128, 1);
+        k_restrict_quad<T, VAR><<<grid_for(C, np, blk), blk, 0, s>>>(F, C, t);
+        return;
+    }
     const dim3 blk = block_for(C.max2);
     k_residual_restrict<T, VAR><<<grid_for(C, C.max2, blk), blk, 0, s>>>(F, C, t);
 }
 
 template <typename T>
 void launch_prolong_correct(const Bricks<T>& F, const Bricks<T>& C, const TransferSet& t, cudaStream_t s) {
+    if (quad_transfers(F, t)) {
+        const int nq = F.max2 / 4;
+        const dim3 blk = nq >= 32 ? dim3(32, 8, 1) : nq >= 8 ? dim3(8, 32, 1) : dim3(2, 128, 1);
+        k_prolong_quad<T><<<grid_for(F, nq, blk), blk, 0, s>>>(F, C, t);
+        return;
+    }
     const dim3 blk = block_for(F.max2);
     k_prolong_correct<T><<<grid_for(F, F.max2, blk), blk, 0, s>>>(F, C, t);
 }
