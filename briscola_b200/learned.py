@@ -97,18 +97,30 @@ def train(net: U.UNet, pairs: PairSet, steps: int, lr: float = 1e-3, seed: int =
     return [float(v.item()) for v in losses]
 
 
+def save(net: U.UNet, pairs_scale: float, path: str, N: int) -> None:
+    """checkpoint with what LearnedGuess needs: the target scale and grid"""
+    net.save(path, meta={"target_scale": pairs_scale, "training_grid": N})
+
+
 class LearnedGuess:
     """A trained network in front of a solver context on the same N^3 cube."""
 
-    def __init__(self, net: U.UNet, ctx: Context, scale: float):
+    def __init__(self, net: U.UNet, ctx: Context, scale: float, h: float | None = None, h_train: float | None = None):
+        """scale: the target scale of the training pairs; h: the cell size of
+        the grids solved (default 1/N, the unit cube); h_train: the cell
+        size trained on (default h).  The network learned the solution of
+        unit-size sources on the training grid; the solution grows with h^2,
+        hence the factor (h / h_train)^2."""
         import torch
 
         self.torch = torch
         self.net = net
         self.ctx = ctx
         self.N = net.shape[0]
-        self.V = (1.0 / self.N) ** 3
-        self.scale = scale
+        h = 1.0 / self.N if h is None else h
+        h_train = h if h_train is None else h_train
+        self.V = h ** 3
+        self.scale = scale * (h / h_train) ** 2
         self.x0 = torch.zeros(self.N ** 3, dtype=torch.float64, device=net.dev)
 
     def guess(self, b):

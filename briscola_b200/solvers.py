@@ -393,9 +393,41 @@ class GPUMG(solver):
             if str(cs.lookupOrDefault("type", "APLU")) != "APLU":
                 raise FatalError("GPUMG coarse solver is the on-device direct solve (APLU)")
         self.options = make_options(dict_)
+        # learned initial guess: "learned guess;" with "learnedWeights <file>;"
+        # (a U-Net checkpoint); the stopping test then measures against ||b||
+        self.learned = str(dict_.lookupOrDefault("learned", "off"))
+        if self.learned not in ("off", "guess"):
+            raise FatalError(f"unknown learned mode {self.learned} (off or guess)")
+        if self.learned == "guess":
+            self.options.criterion = N.CRITERION["rhs"]
         self.context = Context(mesh, self.options)
         self._lam_id = None
         self.last_report = None
+        self._guess = None
+        if self.learned == "guess":
+            self._guess = self._make_guess(dict_, mesh)
+
+    def _make_guess(self, dict_, mesh):
+        from . import learned, unet
+
+        if not dict_.found("learnedWeights"):
+            raise FatalError("learned guess needs learnedWeights <checkpoint file>")
+        if len(mesh.bricks) != 1:
+            raise FatalError("learned guess: one brick only")
+        br = mesh.bricks[0]
+        n = br.N
+        if any(v % 8 for v in n):
+            raise FatalError("learned guess: every extent a multiple of 8")
+        for d in range(3):
+            h = np.diff(br.points[d])
+            if np.max(np.abs(h - h[0])) > 1e-12 * h[0] or abs(h[0] - br.cell_sizes(0)[0]) > 1e-12 * h[0]:
+                raise FatalError("learned guess: uniform cubic cells only")
+        net, meta = unet.UNet.from_file(str(dict_.lookup("learnedWeights")), n)
+        if "target_scale" not in meta or "training_grid" not in meta:
+            raise FatalError("learned guess: the checkpoint has no target scale or training grid")
+        h = float(br.cell_sizes(0)[0])
+        return learned.LearnedGuess(net, self.context, float(meta["target_scale"]), h=h,
+                                    h_train=1.0 / float(meta["training_grid"]))
 
     def solve(self, sys: LinearSystem, constMatrix: bool = False):
         lam_key = None if sys.lam is None else tuple(id(a) for a in sys.lam)
@@ -403,7 +435,10 @@ class GPUMG(solver):
             if sys.lam is not None or self._lam_id is not None:
                 self.context.set_coefficients(sys.lam)
             self._lam_id = lam_key
-        rep = self.context.solve(sys.b, sys.x, zero_guess=sys.zero_guess)
+        if self._guess is not None:
+            rep = self._learned_solve(sys)
+        else:
+            rep = self.context.solve(sys.b, sys.x, zero_guess=sys.zero_guess)
         self.last_report = rep
         print(f"{self.typeName}: Solving for colocated x, initial residual = {rep.initial_residual:g}, "
               f"final residual = {rep.final_residual:g}, nIter = {rep.cycles}")
@@ -411,4 +446,17 @@ class GPUMG(solver):
             raise FatalError("GPUMG: residual became NaN or Inf")
         if rep.status == N.TIMEOUT:
             raise FatalError("GPUMG: solve exceeded its time budget")
+        return rep
+
+    def _learned_solve(self, sys: LinearSystem):
+        """the network's guess for b, then the multigrid solve from it"""
+        import torch
+
+        dev = self._guess.net.dev
+        on_dev = hasattr(sys.b, "is_cuda") and sys.b.is_cuda
+        b = sys.b if on_dev else torch.from_numpy(np.ascontiguousarray(sys.b)).to(dev)
+        x = sys.x if on_dev else torch.empty_like(b)
+        rep = self._guess.solve(b, x)
+        if not on_dev:
+            sys.x[...] = x.cpu().numpy().reshape(sys.x.shape)
         return rep

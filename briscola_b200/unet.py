@@ -147,6 +147,60 @@ def init_params(seed: int = 0) -> np.ndarray:
     return p
 
 
+# ---------------------------------------------------------------------------
+# checkpoint file: magic, version, JSON header, then FP32 arrays
+# ---------------------------------------------------------------------------
+MAGIC = b"BUNETCK1"
+VERSION = 1
+
+
+def save_state(path: str, params, m=None, v=None, step: int = 0, meta: dict | None = None) -> None:
+    """Write parameters (and Adam moments) as a versioned binary file:
+    8-byte magic, uint32 header length, UTF-8 JSON header (version, layout,
+    step, caller metadata such as the target scale), then the FP32 arrays
+    params, m, v back to back."""
+    import json
+
+    layout, n = param_layout()
+    arrays = [np.asarray(a, dtype=np.float32).ravel() for a in (params, m, v) if a is not None]
+    if any(a.size != n for a in arrays):
+        raise UNetError("parameter arrays of the wrong length")
+    header = {"version": VERSION, "nparam": n, "layout": [[nm, list(sh), off] for nm, sh, off in layout],
+              "step": int(step), "has_moments": m is not None and v is not None, "meta": meta or {}}
+    blob = json.dumps(header).encode()
+    with open(path, "wb") as f:
+        f.write(MAGIC)
+        f.write(np.uint32(len(blob)).tobytes())
+        f.write(blob)
+        for a in arrays:
+            f.write(a.tobytes())
+
+
+def load_state(path: str):
+    """(params, m, v, step, meta) from save_state's file; m and v are None
+    when the file holds no moments.  Rejects other files and layouts."""
+    import json
+
+    with open(path, "rb") as f:
+        if f.read(8) != MAGIC:
+            raise UNetError(f"{path}: not a U-Net checkpoint")
+        hlen = int(np.frombuffer(f.read(4), dtype=np.uint32)[0])
+        header = json.loads(f.read(hlen).decode())
+        if header.get("version") != VERSION:
+            raise UNetError(f"{path}: checkpoint version {header.get('version')} (expected {VERSION})")
+        layout, n = param_layout()
+        if header["nparam"] != n or header["layout"] != [[nm, list(sh), off] for nm, sh, off in layout]:
+            raise UNetError(f"{path}: parameter layout differs from this network")
+        data = np.frombuffer(f.read(), dtype=np.float32)
+    count = 3 if header["has_moments"] else 1
+    if data.size != count * n:
+        raise UNetError(f"{path}: truncated checkpoint")
+    p = data[:n].copy()
+    m = data[n:2 * n].copy() if count == 3 else None
+    v = data[2 * n:].copy() if count == 3 else None
+    return p, m, v, header["step"], header["meta"]
+
+
 class UNet:
     """The network on one grid shape (each extent divisible by 8), its
     activations, gradients and optimiser state on the current CUDA device."""
@@ -388,6 +442,23 @@ class UNet:
 
     def params(self) -> np.ndarray:
         return self.p.detach().cpu().numpy().copy()
+
+    def save(self, path: str, meta: dict | None = None) -> None:
+        """parameters and Adam state to a checkpoint file"""
+        save_state(path, self.params(), self.m.cpu().numpy(), self.v.cpu().numpy(), self.step, meta)
+
+    @classmethod
+    def from_file(cls, path: str, shape):
+        """a network on grid `shape` from a checkpoint (any training grid:
+        the layers are convolutions), with its optimiser state; returns
+        (net, meta)"""
+        p, m, v, step, meta = load_state(path)
+        net = cls(shape, params=p)
+        if m is not None:
+            net.m.copy_(net.torch.from_numpy(m))
+            net.v.copy_(net.torch.from_numpy(v))
+        net.step = step
+        return net, meta
 
     # -- the solver's view ---------------------------------------------------
     def guess(self, b, V: float, x0, scale: float = 1.0):

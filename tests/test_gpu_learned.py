@@ -42,7 +42,17 @@ def test_rhs_criterion(native, krylov):
     assert rb.cycles < ra.cycles and rb.rhs_rel_residual <= 1e-8
 
 
-def test_learned_guess_gain(native, built):
+@pytest.fixture(scope="module")
+def trained(built):
+    """a network trained on 96 pairs of one 32^3 sequence"""
+    N = 32
+    train_set = learned.PairSet(N, 96, seed=1, every=2)
+    net = unet.UNet((N,) * 3, seed=0)
+    losses = learned.train(net, train_set, steps=2000, lr=2e-3)
+    return net, train_set.scale, losses
+
+
+def test_learned_guess_gain(native, trained):
     """Trained on 96 pairs of one sequence, judged on 8 pairs of another: the
     guess must be much closer to the solution than zero (the zero guess has
     relative error 1), leave no more residual than zero does, and never cost
@@ -50,13 +60,11 @@ def test_learned_guess_gain(native, built):
     of every error component per cycle, so the guess saves no whole cycle;
     the numbers are printed."""
     N = 32
-    train_set = learned.PairSet(N, 96, seed=1, every=2)
+    net, scale, losses = trained
     held = learned.PairSet(N, 8, seed=2, skip=40, every=5)
-    net = unet.UNet((N,) * 3, seed=0)
-    losses = learned.train(net, train_set, steps=2000, lr=2e-3)
     assert np.mean(losses[-50:]) < 0.2 * np.mean(losses[:20]), (losses[:5], losses[-5:])
     ctx = bb.Context(learned.cube_mesh(N), bb.make_options(dict(learned.TARGET_KEYS, relTol=1e-8)))
-    lg = learned.LearnedGuess(net, ctx, train_set.scale)
+    lg = learned.LearnedGuess(net, ctx, scale)
     n = N ** 3
     x = torch.zeros(n, dtype=torch.float64, device="cuda")
     cyc0, cyc1, err, res = [], [], [], []
@@ -79,3 +87,34 @@ def test_learned_guess_gain(native, built):
     assert np.mean(err) < 0.3
     assert np.mean(res) < 1.1
     assert all(c1 <= c0 for c0, c1 in zip(cyc0, cyc1))
+
+
+def test_plugin_learned_guess_from_checkpoint(native, trained, tmp_path):
+    """the GPUMG plugin with "learned guess;" loads the checkpoint and
+    solves host arrays and device tensors to tolerance, on the training grid
+    and on a finer one (the guess is scaled by (h / h_train)^2)"""
+    net, scale, _ = trained
+    path = str(tmp_path / "net.bunet")
+    learned.save(net, scale, path, 32)
+    for N in (32, 64):
+        mesh = learned.cube_mesh(N)
+        seq = workloads.TaylorGreenSequence(N, 7, torch.device("cuda", 0))
+        b = seq.rhs()
+        keys = dict(relTol=1e-8, tolerance=0, cycleType="V", nSweepsPre=2, nSweepsPost=2, coarseLevel=1,
+                    precision="mixed", krylov="fcg")
+        s_off = bb.solver.New(bb.Dictionary(dict(keys, type="GPUMG")), mesh)
+        s_on = bb.solver.New(bb.Dictionary(dict(keys, type="GPUMG", learned="guess", learnedWeights=path)), mesh)
+        x0 = torch.zeros_like(b)
+        r0 = s_off.solve(bb.LinearSystem(mesh, x0, b, zero_guess=True))
+        x1 = torch.zeros_like(b)
+        r1 = s_on.solve(bb.LinearSystem(mesh, x1, b))
+        bh = b.cpu().numpy()
+        xh = np.zeros_like(bh)
+        r2 = s_on.solve(bb.LinearSystem(mesh, xh, bh))
+        for r in (r0, r1, r2):
+            assert r.status == 0 and r.rhs_rel_residual <= 1e-8
+        assert r1.cycles <= r0.cycles + 1 and r2.cycles == r1.cycles
+        # the guess's own residual against ||b||: about that of zero on the
+        # training grid; still of that order on the finer one (a guess
+        # scaled wrongly by (h / h_train)^2 would leave several times ||b||)
+        assert r1.rhs_rel_residual / r1.rel_residual < (1.5 if N == 32 else 3.0)

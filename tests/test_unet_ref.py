@@ -2,6 +2,7 @@
 hand-written backward pass agrees with finite differences, its operators
 with their definitions, and the parameter layout matches the network."""
 import numpy as np
+import pytest
 
 from briscola_b200 import unet
 from tests import unet_ref as R
@@ -67,3 +68,31 @@ def test_bf16_rounding():
     assert r[2] == 1.0 + 2 ** -7
     assert r[3] == -2.5
     assert abs(r[4] - 3.0e-3) <= 3.0e-3 * 2 ** -8
+
+
+def test_checkpoint_roundtrip_and_checks(tmp_path):
+    layout, n = unet.param_layout()
+    rng = np.random.default_rng(2)
+    p = rng.standard_normal(n).astype(np.float32)
+    m = rng.standard_normal(n).astype(np.float32)
+    v = rng.random(n).astype(np.float32)
+    f = tmp_path / "w.bunet"
+    unet.save_state(str(f), p, m, v, step=17, meta={"target_scale": 0.5, "training_grid": 64})
+    p2, m2, v2, step, meta = unet.load_state(str(f))
+    assert np.array_equal(p, p2) and np.array_equal(m, m2) and np.array_equal(v, v2)
+    assert step == 17 and meta == {"target_scale": 0.5, "training_grid": 64}
+    # parameters only
+    unet.save_state(str(f), p)
+    p3, m3, v3, _, _ = unet.load_state(str(f))
+    assert np.array_equal(p, p3) and m3 is None and v3 is None
+    # wrong magic, truncated file, wrong length
+    bad = tmp_path / "bad"
+    bad.write_bytes(b"NOTACKPT" + bytes(16))
+    with pytest.raises(unet.UNetError):
+        unet.load_state(str(bad))
+    raw = f.read_bytes()
+    (tmp_path / "cut").write_bytes(raw[:-8])
+    with pytest.raises(unet.UNetError):
+        unet.load_state(str(tmp_path / "cut"))
+    with pytest.raises(unet.UNetError):
+        unet.save_state(str(f), p[:-1])
