@@ -160,6 +160,17 @@ def workload_config(args):
             "parallelism": "replicas" if args.gpus > 1 else "single GPU"}
 
 
+def tuning_string(c):
+    """The autotuner's smoother launch shapes, level:precision:stages:chunk
+    (stages 0: pass by pass), in the form --tuning takes."""
+    out = []
+    for lvl in range(c.num_levels):
+        for prec in (0, 1):
+            stages, chunk = c.tuning(lvl, prec)
+            out.append(f"{lvl}:{prec}:{stages}:{chunk or 64}")
+    return ",".join(out)
+
+
 def profile_region(args, local):
     """One headline solve (or one U-Net forward at the bench size) after
     set-up and warm-up, bracketed by the CUDA profiler API."""
@@ -191,8 +202,14 @@ def profile_region(args, local):
     mesh, b, _ = workloads.channel(args.size)
     # the same kernels launched one by one (the profiler cannot see into a
     # graph with a conditional loop)
+    if args.tuning:
+        kw.update(autotune="off")
     c = bb.Context(mesh, bb.make_options(dict(SOLVER_KEYS, device=local, graph="off", **kw)))
     c.set_stream(stream.cuda_stream)
+    if args.tuning:
+        for item in args.tuning.split(","):
+            lvl, prec, stages, chunk = (int(v) for v in item.split(":"))
+            c.set_tuning(lvl, prec, stages, chunk)
     b_d = torch.from_numpy(b).to(f"cuda:{local}")
     x_d = torch.zeros_like(b_d)
     for _ in range(args.warmup):
@@ -258,6 +275,10 @@ def main():
     ap.add_argument("--profile-region", choices=["mixed_fcg", "mixed_fcg_fused", "fp64", "unet_fwd"], default=None,
                     help="set up, warm up, then run one solve (or one U-Net forward) between "
                          "cudaProfilerStart/Stop for ncu --profile-from-start off; prints no bench line")
+    ap.add_argument("--tuning", default=None,
+                    help="with --profile-region: smoother launch shapes to pin instead of autotuning "
+                         "(level:precision:stages:chunk,...; the bench line's 'tuning' field), since "
+                         "the profiler's per-launch overhead skews the autotuner's timings")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -373,11 +394,15 @@ def main():
     alg_bytes = (12.0 if stages_per_launch >= 2 else 6.0) * cells
     hbm, peak_kind = peaks()
     achieved = alg_bytes / t_pass / 1e9
+    # DRAM bytes per launch from the committed ncu summary of this kernel
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    tp = os.path.join(ROOT, "profiles", "k_sweep_fp32_channel256.md" if stages_per_launch else
+                      "k_colour_pass_fp32_channel256.md")
     if os.path.exists(tp):
-        with open(tp) as f:
-            traffic = json.load(f).get("smooth_fused_fp32_s5_256", None)
+        import re
+
+        m = re.search(r"^traffic per launch \(bytes\): ([0-9.e+]+)", open(tp).read(), re.M)
+        traffic = float(m.group(1)) if m else None
 
     # ---- end to end through the plugin call with host buffers ----
     d = bb.Dictionary(dict(SOLVER_KEYS, type="GPUMG", precision="mixed", krylov="fcg", device=local))
@@ -500,8 +525,8 @@ def main():
             "rel_residual": rep_head.rel_residual,
             "hbm_gbs_fp64_cycle_algorithmic": round(hbm_gbs_fp64, 1),
             "roofline": {"bound": "hbm",
-                         "kernel": (f"k_smooth_fused<float,S={stages_per_launch}> level 0 "
-                                    f"({launches_per_step} launches per 2-sweep step, {chunk}-plane chunks)"
+                         "kernel": (f"k_sweep<float> level 0 ({launches_per_step} launches of up to "
+                                    f"{stages_per_launch} colour stages per 2-sweep step, {chunk}-plane chunks)"
                                     if stages_per_launch else
                                     f"k_colour_pass<float> level 0 ({launches_per_step} passes per "
                                     "2-sweep step; autotuner's choice)"),
@@ -513,6 +538,7 @@ def main():
             "e2e": {"value": round(e2e_ms, 4), "unit": "ms/solve", "h2d_bytes_per_step": 8 * n,
                     "d2h_bytes_per_step": 8 * n},
             "gpu_launches": launches, "clocks": clocks,
+            "tuning": tuning_string(ctx["mixed_fcg"]),
             "multibrick": multibrick,
             "unet": unet_t,
             "variable_coefficient": variable,

@@ -29,7 +29,7 @@ EXPORTED = (
     "bmg_status_string", "bmg_last_error", "bmg_level_upload", "bmg_level_download",
     "bmg_op_colour_pass", "bmg_op_smooth", "bmg_op_residual", "bmg_op_residual_restrict",
     "bmg_op_prolong_correct", "bmg_op_coarse_solve", "bmg_coarse_level_index",
-    "bmg_residual_norm_noalloc", "bmg_level_tuning",
+    "bmg_residual_norm_noalloc", "bmg_level_tuning", "bmg_set_level_tuning",
 )
 
 
@@ -66,6 +66,7 @@ class Options(ctypes.Structure):
         ("timeout_ms", ctypes.c_double),
         ("krylov", ctypes.c_int),
         ("criterion", ctypes.c_int),
+        ("fused_chunk", ctypes.c_int),
     ]
 
 
@@ -130,6 +131,7 @@ def load(path: str = LIB_PATH):
     L.bmg_coarse_level_index.argtypes = [vp]
     L.bmg_residual_norm_noalloc.argtypes = [vp, vp, ip, vp, vp, vp, ip, vp, vp]
     L.bmg_level_tuning.argtypes = [vp, ctypes.c_int, ctypes.c_int, ip, ip]
+    L.bmg_set_level_tuning.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     _lib = L
     return L
 

@@ -489,6 +489,7 @@ void validateOptions(const bmg_options* o) {
     if (o->precision < 0 || o->precision > 1) throw BadArg{BMG_BAD_ARG, "unknown precision"};
     if (o->coarse_level < 0) throw BadArg{BMG_BAD_ARG, "negative coarseLevel"};
     if (o->fused < 0) throw BadArg{BMG_BAD_ARG, "negative fused stage count"};
+    if (o->fused_chunk < 1 || o->fused_chunk > 128) throw BadArg{BMG_BAD_ARG, "fusedChunk outside 1..128"};
     if (o->krylov < 0 || o->krylov > 1) throw BadArg{BMG_BAD_ARG, "unknown krylov"};
     if (o->criterion < 0 || o->criterion > 1) throw BadArg{BMG_BAD_ARG, "unknown criterion"};
 }
@@ -753,9 +754,13 @@ void build(bmg_ctx* c, HostLevel&& L0) {
         upload(L.tab64, L.tab);
         upload(L.tab32, to_f32(L.tab));
         // the fused smoother handles one brick and marches along axis 0 in
-        // chunks, wrapping at most one period there
+        // chunks, wrapping at most one period there; its threads own k-quads,
+        // and it relies on periodic extents being even (a wrapped neighbour
+        // then has the other colour, as an interior one does)
         const HostBrick& B = L.br[0];
-        L.fusedOK = !c->multi && B.n[0] >= 16 && B.n[1] >= 16 && B.n[2] >= 16;
+        L.fusedOK = !c->multi && B.n[0] >= 16 && B.n[1] >= 16 && B.n[2] >= 16 && B.n[2] % 4 == 0;
+        for (int d = 0; d < 3; ++d)
+            if (c->periodic[d] && B.n[d] % 2) L.fusedOK = false;
         if (L.fusedOK) {
             L.x64b = dalloc<double>(L.cells);
             L.x32b = dalloc<float>(L.cells);
@@ -1012,8 +1017,8 @@ void coarseSolve(bmg_ctx* c) {
 // Launch-shape autotuner: for every level the fused smoother can handle,
 // time one smoothing step (the configured sweep count) with one launch per
 // colour pass and with the fused smoother at each number of colour stages
-// per launch and plane-chunk length, and keep the fastest.  The tile (16 x
-// 64 cells) is fixed by the fused kernel's register window; stages and chunk
+// per launch and plane-chunk length, and keep the fastest.  The tile (8 x
+// 64 cells) is fixed by the fused kernel's thread block; stages and chunk
 // length trade halo recomputation against memory passes and CTA count.
 // Each candidate is timed as a captured graph of kTuneReps smoothing steps,
 // the way the solve graph launches it (stream launches would charge the
@@ -1066,10 +1071,15 @@ void autotuneLevel(bmg_ctx* c, int l, int sweeps, cudaEvent_t e0, cudaEvent_t e1
     const int prec = sizeof(T) == 8 ? 0 : 1;
     float best = 1e30f;
     int bestS = H.fusedS[prec], bestTi = H.fusedTi[prec];
-    for (int S = 0; S <= kFusedMaxStages; ++S)
-        for (int ti : {32, 64, 128}) {
-            if (ti > 2 * H.br[0].n[0] && ti != 32) continue;
-            if (S == 0 && ti != 32) continue;
+    const int n0 = H.br[0].n[0];
+    for (int S = 0; S <= kFusedMaxStages; ++S) {
+        bool whole = false;  // chunks at least as long as the level are all one launch shape
+        for (int ti : {16, 24, 32, 48, 64, 128}) {
+            if (S == 0 && ti != 16) continue;
+            if (ti >= n0) {
+                if (whole) continue;
+                whole = true;
+            }
             H.fusedS[prec] = S;
             H.fusedTi[prec] = ti;
             const float ms = timeSmoothGraph<T>(c, l, sweeps, e0, e1);
@@ -1079,8 +1089,14 @@ void autotuneLevel(bmg_ctx* c, int l, int sweeps, cudaEvent_t e0, cudaEvent_t e1
                 bestTi = ti;
             }
         }
+    }
     H.fusedS[prec] = bestS;
     H.fusedTi[prec] = bestTi;
+}
+
+// planes per chunk of the fused smoother from the options (autotune off)
+void applyChunk(bmg_ctx* c) {
+    for (auto& L : c->lv) L.fusedTi[0] = L.fusedTi[1] = c->opt.fused_chunk;
 }
 
 void autotune(bmg_ctx* c) {
@@ -1548,6 +1564,7 @@ int bmg_default_options(bmg_options* o) {
     o->timeout_ms = 0.0;
     o->krylov = BMG_KRYLOV_NONE;
     o->criterion = BMG_CRITERION_INITIAL;
+    o->fused_chunk = 64;
     return BMG_OK;
 }
 
@@ -1577,6 +1594,7 @@ int bmg_create(bmg_ctx** out, const bmg_mesh_desc* mesh, const bmg_options* opts
         configure_fused_kernels();
         build(c, std::move(L0));
         configureCoarse(c);
+        applyChunk(c);
         if (c->opt.autotune) autotune(c);
         return BMG_OK;
     });
@@ -1610,6 +1628,7 @@ int bmg_set_options(bmg_ctx* c, const bmg_options* o) {
         destroyGraph(c);
         BMG_CUDA(cudaSetDevice(c->opt.device));
         if (coarseChanged) configureCoarse(c);
+        if (!o->autotune) applyChunk(c);
         if (retune) autotune(c);
         return BMG_OK;
     });
@@ -1674,6 +1693,20 @@ int bmg_level_tuning(const bmg_ctx* c, int l, int prec, int* stages, int* chunk)
     *stages = fused ? std::min({c->opt.fused, L.fusedS[prec], kFusedMaxStages}) : 0;
     *chunk = fused ? std::min(L.fusedTi[prec], L.br[0].n[0]) : 0;
     return BMG_OK;
+}
+
+int bmg_set_level_tuning(bmg_ctx* c, int l, int prec, int stages, int chunk) {
+    if (!validLevel(c, l) || prec < 0 || prec > 1 || stages < 0 || stages > kFusedMaxStages || chunk < 1 ||
+        chunk > 128)
+        return BMG_BAD_ARG;
+    HostLevel& L = c->lv[l];
+    if (stages > 0 && !L.fusedOK) return BMG_UNSUPPORTED;
+    return guarded(c, [&] {
+        destroyGraph(c);
+        L.fusedS[prec] = stages;
+        L.fusedTi[prec] = chunk;
+        return BMG_OK;
+    });
 }
 
 int bmg_level_shape(const bmg_ctx* c, int l, int brick, int n[3]) {

@@ -305,6 +305,11 @@ class Context:
                    "bmg_level_tuning")
         return s.value, t.value
 
+    def set_tuning(self, level: int, precision: int, stages: int, chunk: int = 64):
+        """Pin a level's smoother launch shape (stages 0: pass by pass)."""
+        self.check(self._lib.bmg_set_level_tuning(self.h, level, precision, stages, chunk),
+                   "bmg_set_level_tuning")
+
     def colour_pass(self, level, colour, precision=0):
         self.check(self._lib.bmg_op_colour_pass(self.h, level, colour, precision), "colour_pass")
 
@@ -363,6 +368,7 @@ def make_options(d: Dictionary | dict | None = None, **over) -> N.Options:
     except (TypeError, ValueError):
         o.fused = 3 if _switch(fused) else 0
     o.autotune = int(_switch(d.get("autotune", "on")))
+    o.fused_chunk = int(_scalar(d.get("fusedChunk", 64)))
     o.device = _label(d.get("device", 0))
     o.timeout_ms = _scalar(d.get("timeoutMs", 0))
     kr = str(d.get("krylov", "none"))

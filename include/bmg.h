@@ -103,6 +103,8 @@ typedef struct bmg_options {
     double timeout_ms;  /* wall-clock budget per solve, <= 0: none             */
     int krylov;         /* krylov (none): outer loop, BMG_KRYLOV_*             */
     int criterion;      /* criterion (initial): BMG_CRITERION_*                */
+    int fused_chunk;    /* fusedChunk (64): planes along i per CTA of the
+                           fused smoother when autotune is off (1..128)        */
 } bmg_options;
 
 typedef struct bmg_report {
@@ -176,6 +178,10 @@ int bmg_coarse_level_index(const struct bmg_ctx* ctx);
  * FP32): colour stages per launch (0 when the level is smoothed pass by
  * pass) and planes per CTA chunk, as chosen by the autotuner */
 int bmg_level_tuning(const struct bmg_ctx* ctx, int level, int precision, int* stages, int* chunk);
+/* pins that launch shape (stages 0: pass by pass; 1..3 needs a level the
+ * fused smoother handles; chunk 1..128), e.g. to replay a tuning measured
+ * in another process; the solve graph is rebuilt at the next solve */
+int bmg_set_level_tuning(struct bmg_ctx* ctx, int level, int precision, int stages, int chunk);
 
 /* ---- Residual norm without any device allocation ---------------------------
  * No counterpart in the reference: an addition for callers that must not

@@ -93,9 +93,30 @@ def test_autotuner_picks_valid_shapes(native):
         for p in (0, 1):
             s, t = c.tuning(l, p)
             if min(c.shape(l)) >= 16 and s > 0:
-                assert s <= 3 and (t in (32, 64, 128) or t == c.shape(l)[0])
+                assert s <= 3 and (t in (16, 24, 32, 48, 64, 128) or t == c.shape(l)[0])
             else:
                 assert (s, t) == (0, 0)  # smoothed pass by pass
     x = np.zeros_like(b)
     rep = c.solve(b, x, zero_guess=True)
     assert rep.status == 0
+
+
+def test_pinned_launch_shapes(native):
+    mesh, b, _ = workloads.channel(64, seed=10)
+    c = bb.Context(mesh, bb.make_options({"coarseLevel": 1, "autotune": "off", "precision": "mixed"}))
+    c.set_tuning(0, 1, 2, 24)
+    c.set_tuning(0, 0, 0, 64)
+    assert c.tuning(0, 1) == (2, 24) and c.tuning(0, 0) == (0, 0)
+    with pytest.raises(bb.FatalError):
+        c.set_tuning(0, 1, 4, 24)  # more stages than a launch runs
+    with pytest.raises(bb.FatalError):
+        c.set_tuning(0, 1, 3, 0)  # chunk outside 1..128
+    coarsest = c.num_levels - 1
+    with pytest.raises(bb.FatalError):
+        c.set_tuning(coarsest, 1, 3, 16)  # a level the fused smoother does not handle
+    x = np.zeros_like(b)
+    rep = c.solve(b, x, zero_guess=True)
+    ref = bb.Context(mesh, bb.make_options({"coarseLevel": 1, "fused": "off", "precision": "mixed"}))
+    x2 = np.zeros_like(b)
+    rep2 = ref.solve(b, x2, zero_guess=True)
+    assert rep.status == 0 and rep.cycles == rep2.cycles and np.array_equal(x, x2)
