@@ -3,8 +3,9 @@
 ``python -m briscola_b200.build`` (or ``__graft_entry__.build()``) compiles
 ``csrc/*.cu`` with nvcc into two plain C ABI libraries with the CUDA runtime
 linked statically: ``briscola_b200/_lib/libbmg.so`` (the multigrid solver,
-include/bmg.h) and ``briscola_b200/_lib/libbunet.so`` (the U-Net kernels,
-include/bunet.h).
+include/bmg.h), ``briscola_b200/_lib/libbunet.so`` (the U-Net kernels,
+include/bunet.h) and ``briscola_b200/_lib/libbfft.so`` (the FFT Poisson
+solver, include/bfft.h).
 """
 from __future__ import annotations
 
@@ -18,6 +19,8 @@ OUT = os.path.join(HERE, "_lib", "libbmg.so")
 SOURCES = ["bmg_host.cu", "bmg_kernels.cu", "bmg_smooth_fused.cu", "bmg_krylov.cu", "bmg_noalloc.cu"]
 HEADERS = ["bmg_internal.h", "bmg_stencil.cuh", "bmg_grid.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FFT_OUT = os.path.join(HERE, "_lib", "libbfft.so")
+FFT_SOURCES = ["bfft.cu"]
 UNET_OUT = os.path.join(HERE, "_lib", "libbunet.so")
 UNET_SOURCES = ["bun_api.cu", "bun_conv.cu", "bun_elem.cu"]
 UNET_HEADERS = ["bun_internal.h", "bun_api_internal.h"]
@@ -52,6 +55,11 @@ def build_native(force: bool = False, verbose: bool = False) -> str:
     return _build(OUT, SOURCES, HEADERS, "bmg.h", force, verbose)
 
 
+def build_fft(force: bool = False, verbose: bool = False) -> str:
+    """libbfft.so (the FFT Poisson solver, include/bfft.h); returns its path."""
+    return _build(FFT_OUT, FFT_SOURCES, [], "bfft.h", force, verbose)
+
+
 def build_unet(force: bool = False, verbose: bool = False) -> str:
     """libbunet.so (the U-Net kernels); returns its path."""
     return _build(UNET_OUT, UNET_SOURCES, UNET_HEADERS, "bunet.h", force, verbose)
@@ -60,3 +68,4 @@ def build_unet(force: bool = False, verbose: bool = False) -> str:
 if __name__ == "__main__":
     print(build_native(force="--force" in sys.argv, verbose=True))
     print(build_unet(force="--force" in sys.argv, verbose=True))
+    print(build_fft(force="--force" in sys.argv, verbose=True))

@@ -14,6 +14,9 @@ import numpy as np
 
 NEUMANN = "Neumann"
 PERIODIC = "periodic"
+# faces only the FFT Poisson solver takes (briscola_b200.fft)
+DIRICHLET = "Dirichlet"
+EMPTY = "empty"
 
 
 def uniform_points(n: int, length: float = 1.0, start: float = 0.0) -> np.ndarray:
