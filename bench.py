@@ -223,6 +223,68 @@ def profile_region(args, local):
         raise RuntimeError(f"solve failed: status {rep.status}")
 
 
+def fft_timing(args, local, stream, mesh, barrier):
+    """The FFT Poisson solver (briscola_b200.fft) on the bench's channel:
+    Laplacian(x) = -f for a seeded zero-mean f, device-resident, CUDA events;
+    the discrete Laplacian residual is checked on the device."""
+    import torch
+
+    from briscola_b200 import fft
+
+    br = mesh.bricks[0]
+    solver = fft.FFTPoissonSolver(br, device=local)
+    n = br.N
+    g = torch.Generator(device=f"cuda:{local}").manual_seed(11)
+    f = torch.randn(n, dtype=torch.float64, device=f"cuda:{local}", generator=g)
+    # a compatible right-hand side for the walled problem: volume-weighted mean zero
+    V = torch.from_numpy(br.cell_volumes()).to(f.device)
+    f -= (f * V).sum() / V.sum()
+    x = torch.empty_like(f)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    for _ in range(3):
+        solver.solve(x, f)
+    barrier()
+    reps = max(10, args.steps * 4)
+    e0.record(stream)
+    for _ in range(reps):
+        solver.solve(x, f)
+    e1.record(stream)
+    barrier()
+    ms = e0.elapsed_time(e1) / reps
+    # residual of the cell-centred Laplacian (periodic x and z, zero-gradient
+    # walls in y: mirrored ghost cells)
+    h = [torch.from_numpy(br.cell_sizes(d)).to(f.device) for d in range(3)]
+    r = f.clone()
+    for d in range(3):
+        hd = h[d]
+        if br.periodic[d]:
+            hg = torch.cat([hd[-1:], hd, hd[:1]])
+            xm, xp = torch.roll(x, 1, d), torch.roll(x, -1, d)
+        else:
+            hg = torch.cat([hd[:1], hd, hd[-1:]])
+            idx = torch.arange(n[d], device=f.device)
+            xm = x.index_select(d, (idx - 1).clamp(min=0))
+            xp = x.index_select(d, (idx + 1).clamp(max=n[d] - 1))
+        hc = hg[1:-1]
+        dw = (hg[1:-1] + hg[:-2]) / 2
+        de = (hg[1:-1] + hg[2:]) / 2
+        shape = [1, 1, 1]
+        shape[d] = -1
+        hc, dw, de = hc.view(shape), dw.view(shape), de.view(shape)
+        r += (xm - x) / (dw * hc) + (xp - x) / (de * hc)
+    res = float(r.abs().max() / f.abs().max())
+    cells = n[0] * n[1] * n[2]
+    sdir = solver.solve_direction
+    solver.close()
+    return {"workload": "the bench channel, Laplacian(x) = -f, seeded N(0,1) f with zero volume-weighted mean",
+            "ms_per_solve": round(ms, 4), "solve_direction": sdir,
+            "max_residual_over_max_rhs": res,
+            "algorithmic_gb_per_s": round(cells * 8 * 10 / (ms * 1e-3) / 1e9, 1),
+            "algorithmic_bytes_note": "10 passes of 8 B/cell: read+write per transform (4) and "
+                                      "tridiagonal (read+write each way)"}
+
+
 def unet_timing(args, local, stream):
     """U-Net forward at the bench size (algorithmic TFLOP/s of the 3x3x3
     convolutions) and one training step at half the size."""
@@ -267,6 +329,7 @@ def main():
     ap.add_argument("--no-multibrick", action="store_true")
     ap.add_argument("--no-unet", action="store_true")
     ap.add_argument("--no-variable", action="store_true")
+    ap.add_argument("--no-fft", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--learned-size", type=int, default=128)
     ap.add_argument("--learned-pairs", type=int, default=2000)
@@ -487,6 +550,11 @@ def main():
             cv.close()
         del vbd, vx
 
+    # ---- FFT Poisson solver on the same channel (periodic x, z; walls in y) ----
+    fft_t = None
+    if not args.no_fft:
+        fft_t = fft_timing(args, local, stream, mesh, barrier)
+
     # ---- learned initial guess (config 5) ----
     learned_t = None
     if not args.no_learned:
@@ -542,6 +610,7 @@ def main():
             "multibrick": multibrick,
             "unet": unet_t,
             "variable_coefficient": variable,
+            "fft": fft_t,
             "learned": learned_t,
         }
         print(json.dumps(line), flush=True)

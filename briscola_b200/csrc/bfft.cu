@@ -44,7 +44,6 @@ enum Pair { P_EMPTY = 0, P_DD = 1, P_NN = 2, P_DN = 3, P_ND = 4, P_CC = 5 };
 enum Mode { M_R2HC = 0, M_HC2R = 1, M_RE = 2, M_NEG_IM = 3 };
 
 constexpr int kThreads = 256;
-constexpr int kTileComplex = 2048;  // complex values of a transform tile (32 KB)
 constexpr int kMaxN = 512;
 
 // lines along one axis: line l starts at (l / inner) * outer + (l % inner) * inner_stride
@@ -60,9 +59,11 @@ struct Lines {
 
 struct Transform {
     int M, logM, mode;
+    int logN;             // log2 of the line length (transformed extents are powers of two)
+    int logLB;            // log2 of the lines per CTA
     const double2* pre;   // n entries, nullptr: 1
     const double2* post;  // n entries, nullptr: 1
-    const double2* tw;    // M/2 entries: exp(-2 pi i j / M)
+    const double2* tw;    // M entries: exp(-2 pi i q / M)
 };
 
 struct Tri {
@@ -76,7 +77,18 @@ struct Tri {
     const double* ev1;    // eigenvalue / h^2 of the first transform direction
     const double* ev2;
     int dir1_inner;       // the first transform direction is the inner line coordinate
+    // modes with equal eigenvalues share one factorisation: class of each
+    // inner / outer line coordinate, a representative coordinate per class
+    const int* clsI;
+    const int* clsO;
+    const int* repI;
+    const int* repO;
+    int nci, nco;
+    double* mfac;         // [ns][modes]: DL_k / Dh_{k-1}
+    double* rfac;         // [ns][modes]: 1 / Dh_k
 };
+
+constexpr int kTriAhead = 8;  // rows a tridiagonal sweep loads ahead
 
 struct Prep {
     int n0, n1, n2;
@@ -85,117 +97,448 @@ struct Prep {
 };
 
 __device__ __forceinline__ long line_base(const Lines& L, long l) {
-    return (l / L.inner) * L.outer_stride + (l % L.inner) * L.inner_stride;
+    // along axes 0 and 2 the outer stride is inner * inner_stride: no division
+    if (L.outer_stride == L.inner * L.inner_stride) return l * L.inner_stride;
+    const unsigned lu = (unsigned)l, in = (unsigned)L.inner;  // line counts fit 32 bits
+    const unsigned o = lu / in;
+    return (long)o * L.outer_stride + (long)(lu - o * in) * L.inner_stride;
 }
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-// w_out(line) = transform of w_in(line) for LB lines per CTA (in place allowed:
-// a CTA reads all its lines before it writes)
-__global__ void __launch_bounds__(kThreads) k_transform(const double* __restrict__ in, double* __restrict__ out,
-                                                        Lines L, Transform T, int LB) {
-    extern __shared__ double2 sm[];
-    const int M = T.M, n = L.n;
-    double2* a = sm;                        // [LB][M]
-    double2* tw = a + (long)LB * M;         // [M/2]
-    long* base = reinterpret_cast<long*>(tw + M / 2);  // [LB]
-    double* raw = reinterpret_cast<double*>(base + LB); // [LB][n] (HC2R input)
-    const int tid = threadIdx.x;
-    const long l0 = (long)blockIdx.x * LB;
-    const int lines = (int)min((long)LB, L.count - l0);
+// cos and sin of a pi / 8, a = 0..7: the twiddles of the register DFTs (R <= 16)
+__host__ __device__ constexpr double cos8(int a) {
+    return a == 0   ? 1.0
+           : a == 1 ? 0.92387953251128675613
+           : a == 2 ? 0.70710678118654752440
+           : a == 3 ? 0.38268343236508977173
+           : a == 4 ? 0.0
+           : a == 5 ? -0.38268343236508977173
+           : a == 6 ? -0.70710678118654752440
+                    : -0.92387953251128675613;
+}
+__host__ __device__ constexpr double sin8(int a) { return a <= 4 ? cos8(4 - a) : cos8(a - 4); }
 
-    for (int q = tid; q < M / 2; q += kThreads) tw[q] = T.tw[q];
-    for (int t = tid; t < LB; t += kThreads) base[t] = t < lines ? line_base(L, l0 + t) : 0;
-    __syncthreads();
+__host__ __device__ constexpr int brev_c(int i, int logR) {
+    int r = 0;
+    for (int b = 0; b < logR; ++b) r |= ((i >> b) & 1) << (logR - 1 - b);
+    return r;
+}
 
-    const int shift = 32 - T.logM;
-    auto brev = [&](int p) { return T.logM ? (int)(__brev((unsigned)p) >> shift) : 0; };
-    // element q of the tile: line-fast order along strided axes
-    auto split = [&](int q, int& t, int& p) {
-        if (L.line_fast) {
-            t = q % LB;
-            p = q / LB;
+// x * exp(-i pi p / h) for compile-time p < h <= 8
+template <int P, int H>
+__device__ __forceinline__ double2 rot(double2 x) {
+    constexpr int a = P * (8 / H);
+    if constexpr (a == 0) {
+        return x;
+    } else if constexpr (a == 4) {
+        return make_double2(x.y, -x.x);
+    } else {
+        constexpr double c = cos8(a), sn = sin8(a);
+        return make_double2(x.x * c + x.y * sn, x.y * c - x.x * sn);
+    }
+}
+
+template <int H, int I, int P, int R>
+__device__ __forceinline__ void bfly(double2 (&v)[R]) {
+    const double2 u = v[I + P];
+    const double2 t = rot<P, H>(v[I + P + H]);
+    v[I + P] = make_double2(u.x + t.x, u.y + t.y);
+    v[I + P + H] = make_double2(u.x - t.x, u.y - t.y);
+}
+
+template <int H, int I, int P, int R>
+__device__ __forceinline__ void bfly_group(double2 (&v)[R]) {
+    if constexpr (P < H) {
+        bfly<H, I, P, R>(v);
+        bfly_group<H, I, P + 1, R>(v);
+    }
+}
+
+template <int H, int I, int R>
+__device__ __forceinline__ void bfly_stage(double2 (&v)[R]) {
+    if constexpr (I < R) {
+        bfly_group<H, I, 0, R>(v);
+        bfly_stage<H, I + 2 * H, R>(v);
+    }
+}
+
+template <int H, int R>
+__device__ __forceinline__ void bfly_stages(double2 (&v)[R]) {
+    if constexpr (H < R) {
+        bfly_stage<H, 0, R>(v);
+        bfly_stages<2 * H, R>(v);
+    }
+}
+
+// in-register DFT of R points (natural order in and out): bit reversal,
+// then radix-2 stages with the exact twiddles of kCos8 / kSin8
+template <int R, int LOGR>
+__device__ __forceinline__ void dft_regs(double2 (&v)[R]) {
+    double2 t[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) t[i] = v[brev_c(i, LOGR)];
+#pragma unroll
+    for (int i = 0; i < R; ++i) v[i] = t[i];
+    bfly_stages<1, R>(v);
+}
+
+constexpr int kTransformThreads = 128;
+constexpr int kTileComplex = 2048;                              // complex values of a tile (LB lines of M)
+constexpr int kPerThread = kTileComplex / kTransformThreads;    // 16 values per thread and pass
+constexpr int kMaxLines = 256;  // lines of a tile (short lines fill less than the tile)
+
+// tile index -> shared-memory slot: one pad slot after every 16, so the
+// first Stockham pass's writes (stride R) do not pile onto one bank group
+__device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
+
+// pad(base + r 2^S) for r = 0..R-1 as pad(base) + r * stride: exact when
+// S >= 4, or when base is a multiple of 16 and R 2^S <= 16
+template <int S>
+__device__ __forceinline__ constexpr int padded_step() {
+    return S >= 4 ? 17 << (S - 4) : 1 << S;
+}
+constexpr int kTileSlots = kTileComplex + kTileComplex / 16;
+constexpr int kTransformSmem = kTileSlots * 16 + kTileComplex * 8;  // tile and staging buffer
+
+// One Stockham radix-R pass (Govindaraju et al., SC 2008) in place over the
+// tile: group j of a line reads points j + r M/R, twiddles them by
+// exp(-2 pi i r (j mod Ns) / (Ns R)), takes their R-point DFT and writes
+// them to (j / Ns) Ns R + (j mod Ns) + r Ns; natural order after the last
+// pass.  Every thread holds its 16 / R groups in registers across the
+// barrier between the reads and the writes.
+template <int R, int LOGR, int LOGM, int LOGNS, int LB>
+__device__ __forceinline__ void stockham_pass(double2* __restrict__ buf, const double2* __restrict__ tw) {
+    constexpr int G = kPerThread / R;
+    constexpr int LOGG = LOGM - LOGR;
+    constexpr int groups = (1 << LOGG) * LB;
+    constexpr int nsMask = (1 << LOGNS) - 1;
+    double2 v[G][R];
+    // a tile of short lines has fewer groups than threads x G: the extra
+    // groups read group 0 and write nothing (predicated, so v stays in
+    // registers)
+    // reads: stride 2^LOGG, affine after padding when LOGG >= 4
+    constexpr bool affineRead = LOGG >= 4;
+    // writes: stride 2^LOGNS from idxD; idxD is a multiple of R when Ns = 1
+    constexpr bool affineWrite = LOGNS >= 4 || (LOGNS == 0 && R <= 16);
+#pragma unroll
+    for (int gi = 0; gi < G; ++gi) {
+        const int g0 = threadIdx.x + gi * kTransformThreads;
+        const int g = (groups >= kTileComplex / R || g0 < groups) ? g0 : 0;
+        const int t = g >> LOGG, j = g & ((1 << LOGG) - 1);
+        const int row = (t << LOGM) + j;
+        if constexpr (affineRead) {
+            const double2* src = buf + pad(row);
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[gi][r] = src[r * padded_step<LOGG>()];
         } else {
-            t = q / n;
-            p = q % n;
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[gi][r] = buf[pad(row + (r << LOGG))];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int gi = 0; gi < G; ++gi) {
+        const int g0 = threadIdx.x + gi * kTransformThreads;
+        const bool ok = groups >= kTileComplex / R || g0 < groups;
+        const int g = ok ? g0 : 0;
+        const int t = g >> LOGG, j = g & ((1 << LOGG) - 1);
+        const int jm = j & nsMask;
+        if constexpr (LOGNS > 0) {
+            const int step = jm << (LOGM - LOGNS - LOGR);
+#pragma unroll
+            for (int r = 1; r < R; ++r) v[gi][r] = cmul(v[gi][r], __ldg(tw + r * step));
+        }
+        dft_regs<R, LOGR>(v[gi]);
+        const int idxD = (t << LOGM) + ((j >> LOGNS) << (LOGNS + LOGR)) + jm;
+        if constexpr (affineWrite) {
+            double2* dst = buf + pad(idxD);
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (ok) dst[r * padded_step<LOGNS>()] = v[gi][r];
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (ok) buf[pad(idxD + (r << LOGNS))] = v[gi][r];
+        }
+    }
+    __syncthreads();
+}
+
+// all passes of an M = 2^LOGM point FFT: radix 16 while 16 points or more
+// remain, then one radix 8, 4 or 2 pass
+template <int LOGM, int LOGNS, int LB>
+__device__ __forceinline__ void stockham_all(double2* __restrict__ buf, const double2* __restrict__ tw) {
+    constexpr int rem = LOGM - LOGNS;
+    if constexpr (rem >= 4) {
+        stockham_pass<16, 4, LOGM, LOGNS, LB>(buf, tw);
+        stockham_all<LOGM, LOGNS + 4, LB>(buf, tw);
+    } else if constexpr (rem == 3) {
+        stockham_pass<8, 3, LOGM, LOGNS, LB>(buf, tw);
+    } else if constexpr (rem == 2) {
+        stockham_pass<4, 2, LOGM, LOGNS, LB>(buf, tw);
+    } else if constexpr (rem == 1) {
+        stockham_pass<2, 1, LOGM, LOGNS, LB>(buf, tw);
+    }
+}
+
+// the prep of the first transform's input: -b - shift x_old - face terms,
+// times 1/normalisation (FFTPoissonSolver.C:116-183)
+struct LoadPrep {
+    int on;
+    int axis;             // the transform axis
+    int n1, n2;
+    const double* xo;     // nullptr: no ddt term
+    Prep P;
+};
+
+__device__ __forceinline__ void cp8(void* smem, const void* gmem, bool valid) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(valid ? 8 : 0)
+                 : "memory");
+}
+// 16 bytes, of which `bytes` (0, 8 or 16) are read and the rest zero-filled
+__device__ __forceinline__ void cp16(void* smem, const void* gmem, int bytes) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+enum Kind { K_R2HC = 0, K_HC2R = 1, K_TRIG = 2 };
+
+// out(line) = transform of in(line), tile by tile (LB = min(2048 / M, 256)
+// lines of n points, M-point FFTs), persistent: while a tile's FFT runs, the
+// next tile's lines are already on their way into a staging buffer by
+// cp.async, so the loads of HBM overlap the arithmetic.  in == out is
+// allowed: every element belongs to one tile, which the same CTA loads
+// before it writes.
+//
+// Element q of a tile is point p of tile line t, with t fastest along the
+// strided axes (LF: a run of lines is a run of consecutive k) and p fastest
+// along k (a tile is then one contiguous block).  Each thread handles the
+// elements q = 2 (tid + u NT) and q + 1: with LF that is one pair of lines
+// for the whole tile, so its addresses are affine in u.  With `pair` the two
+// elements are adjacent in memory and move as one 16-byte copy.
+template <int LOGM, int KIND, bool LF>
+__global__ void __launch_bounds__(kTransformThreads, 3) k_transform(const double* in, double* out, Lines L,
+                                                                    Transform T, LoadPrep LP, long tiles, int pair) {
+    extern __shared__ double2 dsm[];
+    double2* buf = dsm;                                          // [kTileSlots]
+    double* stage = reinterpret_cast<double*>(dsm + kTileSlots);  // [kTileComplex]
+    constexpr int NT = kTransformThreads;
+    constexpr int M = 1 << LOGM;
+    constexpr int LOGN = KIND == K_TRIG ? LOGM - 1 : LOGM;
+    constexpr int N = 1 << LOGN;
+    constexpr int LOGLB = 11 - LOGM < 8 ? 11 - LOGM : 8;
+    constexpr int LB = 1 << LOGLB;
+    constexpr int TOTAL = LB << LOGN;             // elements of a tile
+    constexpr int PAIRS = (TOTAL / 2 + NT - 1) / NT;  // element pairs per thread
+    static_assert(LB >= 2 && TOTAL >= 2, "tiles hold pairs");
+    const int tid = threadIdx.x;
+
+    // element q -> (line t, point p)
+    auto tp = [&](int q, int& t, int& p) {
+        if constexpr (LF) {
+            t = q & (LB - 1);
+            p = q >> LOGLB;
+        } else {
+            t = q >> LOGN;
+            p = q & (N - 1);
         }
     };
-
-    if (T.mode == M_HC2R) {
-        for (int q = tid; q < LB * n; q += kThreads) {
-            int t, p;
-            split(q, t, p);
-            raw[t * n + p] = t < lines ? in[base[t] + p * L.stride] : 0.0;
-        }
-        __syncthreads();
-        // conj(Y_k) of the halfcomplex spectrum, bit-reversed
-        for (int q = tid; q < LB * M; q += kThreads) {
-            const int t = q / M, k = q % M;
-            const double* h = raw + t * n;
-            double re, im;
-            if (k == 0) {
-                re = h[0];
-                im = 0.0;
-            } else if (2 * k < n) {
-                re = h[k];
-                im = -h[n - k];
-            } else if (2 * k == n) {
-                re = h[k];
-                im = 0.0;
-            } else {
-                re = h[n - k];
-                im = h[k];
-            }
-            a[t * M + brev(k)] = make_double2(re, im);
-        }
-    } else {
-        for (int q = tid; q < LB * n; q += kThreads) {
-            int t, p;
-            split(q, t, p);
-            const double x = t < lines ? in[base[t] + p * L.stride] : 0.0;
-            const double2 c = T.pre ? T.pre[p] : make_double2(1.0, 0.0);
-            a[t * M + brev(p)] = make_double2(c.x * x, c.y * x);
-        }
-        if (M > n)  // zero padding
-            for (int q = tid; q < LB * (M - n); q += kThreads) {
-                const int t = q / (M - n), p = n + q % (M - n);
-                a[t * M + brev(p)] = make_double2(0.0, 0.0);
-            }
-    }
-    __syncthreads();
-
-    // radix-2 decimation in time, natural-order output
-    for (int h = 1, ts = M / 2; h < M; h <<= 1, ts >>= 1) {
-        for (int q = tid; q < LB * (M / 2); q += kThreads) {
-            const int t = q / (M / 2), b = q % (M / 2);
-            const int pos = b & (h - 1);
-            const int i0 = t * M + ((b - pos) << 1) + pos, i1 = i0 + h;
-            const double2 u = a[i0];
-            const double2 v = cmul(a[i1], tw[pos * ts]);
-            a[i0] = make_double2(u.x + v.x, u.y + v.y);
-            a[i1] = make_double2(u.x - v.x, u.y - v.y);
-        }
-        __syncthreads();
-    }
-
-    for (int q = tid; q < LB * n; q += kThreads) {
-        int t, k;
-        split(q, t, k);
-        if (t >= lines) continue;
-        const double2* z = a + t * M;
-        double y;
-        if (T.mode == M_R2HC) {
-            y = 2 * k <= n ? z[k].x : z[n - k].y;
-        } else if (T.mode == M_HC2R) {
-            y = z[k].x;
+    // global index of element q of the tile (lb: base of the thread's line
+    // pair along LF axes)
+    auto gidx = [&](long tile, long lb, int q) -> long {
+        if constexpr (LF) {
+            return lb + (long)(q >> LOGLB) * L.stride;
         } else {
-            const double2 c = T.post ? cmul(T.post[k], z[k]) : z[k];
-            y = T.mode == M_RE ? c.x : -c.y;
+            return tile * TOTAL + q;  // axis-2 lines are consecutive rows of n points
         }
-        out[base[t] + k * L.stride] = y;
+    };
+    // the lines of the thread's element pairs: fixed along LF axes
+    auto pair_line = [&](long tile) { return tile * LB + ((2 * tid) & (LB - 1)); };
+    // the first transform forms the right-hand side as it loads b: the face
+    // terms of line l's two fixed coordinates...
+    auto fixed_terms = [&](long l) {
+        if (l >= L.count) return 0.0;
+        const unsigned in = (unsigned)L.inner;
+        const long co = (unsigned)l / in, ci = (unsigned)l - (unsigned)co * in;
+        const int a0 = LP.axis == 0 ? 1 : 0, a1 = LP.axis == 2 ? 1 : 2;
+        const int e0 = a0 == 0 ? LP.P.n0 : LP.P.n1, e1 = a1 == 1 ? LP.P.n1 : LP.P.n2;
+        double f = 0.0;
+        if (co == 0) f += LP.P.corr[2 * a0];
+        if (co == e0 - 1) f += LP.P.corr[2 * a0 + 1];
+        if (ci == 0) f += LP.P.corr[2 * a1];
+        if (ci == e1 - 1) f += LP.P.corr[2 * a1 + 1];
+        return f;
+    };
+    // ... and then those of its varying one (fixed: the line's fixed terms)
+    auto prep = [&](double x, long tile, int t, int p, double fixed) {
+        const long l = tile * LB + t;
+        if (l >= L.count) return 0.0;
+        double v = -x;
+        if (LP.xo) v -= LP.P.shift * LP.xo[line_base(L, l) + (long)p * L.stride];
+        double f = fixed;
+        if (p == 0) f += LP.P.corr[2 * LP.axis];
+        if (p == N - 1) f += LP.P.corr[2 * LP.axis + 1];
+        return (v - f) * LP.P.scale;
+    };
+    auto issue = [&](long tile) {
+        const long l = pair_line(tile);
+        const long lb = LF ? line_base(L, l < L.count ? l : 0) : 0;
+        // elements of the pair that exist: both, the first only (odd line
+        // count), or none
+        const long lines_left = L.count - tile * LB;
+#pragma unroll
+        for (int u = 0; u < PAIRS; ++u) {
+            const int q = 2 * (tid + u * NT);
+            if (q >= TOTAL) break;
+            int t, p;
+            tp(q, t, p);
+            int nvalid;
+            if constexpr (LF || N == 1) {
+                nvalid = (int)min(max(lines_left - t, 0L), 2L);
+            } else {
+                nvalid = t < lines_left ? 2 : 0;
+            }
+            const long g = gidx(tile, lb, q);
+            if (pair) {
+                cp16(stage + q, nvalid ? in + g : in, 8 * nvalid);
+            } else {
+                // the pair's second element is the next line (LF) or point
+                const long g1 = LF ? (nvalid > 1 ? line_base(L, l + 1) + (long)p * L.stride : 0) : g + 1;
+                cp8(stage + q, nvalid > 0 ? in + g : in, nvalid > 0);
+                cp8(stage + q + 1, nvalid > 1 ? in + g1 : in, nvalid > 1);
+            }
+        }
+        cp_commit();
+    };
+
+    long tile = blockIdx.x;
+    if (tile < tiles) issue(tile);
+    for (; tile < tiles; tile += gridDim.x) {
+        const long lines_left = L.count - tile * LB;
+        cp_wait_all();
+        // the staged tile is complete, and the previous tile's output phase
+        // has finished reading buf
+        __syncthreads();
+        if constexpr (KIND == K_HC2R) {
+            // conj(Y_k) of the halfcomplex spectra: element (t, k) of buf
+            // from points k and N - k of the staged line
+            auto h = [&](int t, int p) {
+                const int q = LF ? (p << LOGLB) + t : (t << LOGN) + p;
+                const double x = stage[q];
+                return LP.on ? prep(x, tile, t, p, fixed_terms(tile * LB + t)) : x;
+            };
+            double2 y[2 * PAIRS];
+#pragma unroll
+            for (int u = 0; u < 2 * PAIRS; ++u) {
+                const int q = tid + u * NT;
+                double re = 0.0, im = 0.0;
+                if (q < TOTAL) {
+                    const int t = q >> LOGM, k = q & (M - 1);
+                    if (k == 0) {
+                        re = h(t, 0);
+                    } else if (2 * k < N) {
+                        re = h(t, k);
+                        im = -h(t, N - k);
+                    } else if (2 * k == N) {
+                        re = h(t, k);
+                    } else {
+                        re = h(t, N - k);
+                        im = h(t, k);
+                    }
+                }
+                y[u] = make_double2(re, im);
+            }
+#pragma unroll
+            for (int u = 0; u < 2 * PAIRS; ++u)
+                if (tid + u * NT < TOTAL) buf[pad(tid + u * NT)] = y[u];
+        } else {
+            // along LF axes the thread's line pair is fixed for the tile
+            double fx[2] = {0.0, 0.0};
+            if (LF && LP.on) {
+                fx[0] = fixed_terms(pair_line(tile));
+                fx[1] = fixed_terms(pair_line(tile) + 1);
+            }
+#pragma unroll
+            for (int u = 0; u < PAIRS; ++u) {
+                const int q = 2 * (tid + u * NT);
+                if (q >= TOTAL) break;
+                const double2 x2 = *reinterpret_cast<const double2*>(stage + q);
+                double xs[2] = {x2.x, x2.y};
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    int t, p;
+                    tp(q + e, t, p);
+                    double x = xs[e];
+                    if (LP.on) x = prep(x, tile, t, p, LF ? fx[e] : fixed_terms(tile * LB + t));
+                    double2 c = make_double2(x, 0.0);
+                    if (KIND == K_TRIG && T.pre) {
+                        const double2 w = __ldg(T.pre + p);
+                        c = make_double2(w.x * x, w.y * x);
+                    }
+                    buf[pad((t << LOGM) + p)] = c;
+                }
+            }
+            if constexpr (KIND == K_TRIG) {  // zero padding: points N..2N-1 of every line
+#pragma unroll
+                for (int u = 0; u < 2 * PAIRS; ++u) {
+                    const int q = tid + u * NT;
+                    if (q < TOTAL) buf[pad(((q >> LOGN) << LOGM) + N + (q & (N - 1)))] = make_double2(0.0, 0.0);
+                }
+            }
+        }
+        __syncthreads();
+        // stage is free: the next tile's loads run under this tile's FFT
+        if (tile + gridDim.x < tiles) issue(tile + gridDim.x);
+
+        stockham_all<LOGM, 0, LB>(buf, T.tw);
+
+        // output: element q of the tile from spectrum entry (t, k)
+        const long l = pair_line(tile);
+        const long lb = LF ? line_base(L, l < L.count ? l : 0) : 0;
+#pragma unroll
+        for (int u = 0; u < PAIRS; ++u) {
+            const int q = 2 * (tid + u * NT);
+            if (q >= TOTAL) break;
+            double y[2];
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                int t, k;
+                tp(q + e, t, k);
+                const int row = t << LOGM;
+                if constexpr (KIND == K_R2HC) {
+                    y[e] = 2 * k <= N ? buf[pad(row + k)].x : buf[pad(row + N - k)].y;
+                } else if constexpr (KIND == K_HC2R) {
+                    y[e] = buf[pad(row + k)].x;
+                } else {
+                    const double2 z = buf[pad(row + k)];
+                    const double2 c = T.post ? cmul(__ldg(T.post + k), z) : z;
+                    y[e] = T.mode == M_RE ? c.x : -c.y;
+                }
+            }
+            int t, p;
+            tp(q, t, p);
+            int nvalid;
+            if constexpr (LF || N == 1) {
+                nvalid = (int)min(max(lines_left - t, 0L), 2L);
+            } else {
+                nvalid = t < lines_left ? 2 : 0;
+            }
+            const long g = gidx(tile, lb, q);
+            if (pair && nvalid == 2) {
+                *reinterpret_cast<double2*>(out + g) = make_double2(y[0], y[1]);
+            } else {
+                if (nvalid > 0) out[g] = y[0];
+                if (nvalid > 1) out[LF ? line_base(L, l + 1) + (long)p * L.stride : g + 1] = y[1];
+            }
+        }
     }
+    cp_wait_all();  // no copy outlives the CTA
 }
 
 // Thomas per mode (tridiagonalSolver.C:330-374), or the cyclic form with
@@ -207,7 +550,8 @@ __global__ void __launch_bounds__(kThreads) k_tridiag(double* __restrict__ w, do
     const long base = line_base(L, l);
     const long st = L.stride;
     const int ns = T.ns;
-    const long ci = l % L.inner, co = l / L.inner;
+    const unsigned inner = (unsigned)L.inner;
+    const long co = (unsigned)l / inner, ci = (unsigned)l - (unsigned)co * inner;
     const long c1 = T.dir1_inner ? ci : co, c2 = T.dir1_inner ? co : ci;
     const double e1 = T.ev1[c1], e2 = T.ev2[c2];
     const double e = e1 + e2;
@@ -220,24 +564,51 @@ __global__ void __launch_bounds__(kThreads) k_tridiag(double* __restrict__ w, do
         double Dp = diag(0);
         double fp = w[base];
         dh[base] = Dp;
-#pragma unroll 4
-        for (int k = 1; k < ns; ++k) {
-            const long c = base + k * st;
-            const double m = T.DL[k] / Dp;
-            const double D = diag(k) - m * T.DU[k - 1];
-            const double f = w[c] - m * fp;
-            w[c] = f;
-            dh[c] = D;
-            Dp = D;
-            fp = f;
+        // loads run kTriAhead rows ahead of the elimination
+        double fa[kTriAhead];
+#pragma unroll
+        for (int u = 0; u < kTriAhead; ++u) fa[u] = 1 + u < ns ? w[base + (1 + u) * st] : 0.0;
+        for (int k0 = 1; k0 < ns; k0 += kTriAhead) {
+#pragma unroll
+            for (int u = 0; u < kTriAhead; ++u) {
+                const int k = k0 + u;
+                if (k < ns) {
+                    const long c = base + k * st;
+                    const double fk = fa[u];
+                    const int kn = k + kTriAhead;
+                    fa[u] = kn < ns ? w[base + kn * st] : 0.0;
+                    const double m = T.DL[k] / Dp;
+                    const double D = diag(k) - m * T.DU[k - 1];
+                    const double f = fk - m * fp;
+                    w[c] = f;
+                    dh[c] = D;
+                    Dp = D;
+                    fp = f;
+                }
+            }
         }
         double p = fp / Dp;
         w[base + (ns - 1) * st] = p;
-#pragma unroll 4
-        for (int k = ns - 2; k >= 0; --k) {
-            const long c = base + k * st;
-            p = (w[c] - T.DU[k] * p) / dh[c];
-            w[c] = p;
+        double wa[kTriAhead], da[kTriAhead];
+#pragma unroll
+        for (int u = 0; u < kTriAhead; ++u) {
+            const int k = ns - 2 - u;
+            wa[u] = k >= 0 ? w[base + k * st] : 0.0;
+            da[u] = k >= 0 ? dh[base + k * st] : 1.0;
+        }
+        for (int k0 = ns - 2; k0 >= 0; k0 -= kTriAhead) {
+#pragma unroll
+            for (int u = 0; u < kTriAhead; ++u) {
+                const int k = k0 - u;
+                if (k >= 0) {
+                    const double wk = wa[u], dk = da[u];
+                    const int kn = k - kTriAhead;
+                    wa[u] = kn >= 0 ? w[base + kn * st] : 0.0;
+                    da[u] = kn >= 0 ? dh[base + kn * st] : 1.0;
+                    p = (wk - T.DU[k] * p) / dk;
+                    w[base + k * st] = p;
+                }
+            }
         }
         return;
     }
@@ -282,6 +653,97 @@ __global__ void __launch_bounds__(kThreads) k_tridiag(double* __restrict__ w, do
     }
 }
 
+// Thomas elimination factors of each class of modes (the forward sweep of
+// tridiagonalSolver.C:343-353 without the right-hand side): m_k and 1/Dh_k
+__global__ void k_tri_factor(Tri T) {
+    const int mode = blockIdx.x * blockDim.x + threadIdx.x;
+    const int modes = T.nci * T.nco;
+    if (mode >= modes) return;
+    const int ci = T.repI[mode % T.nci], co = T.repO[mode / T.nci];
+    const int c1 = T.dir1_inner ? ci : co, c2 = T.dir1_inner ? co : ci;
+    const double e1 = T.ev1[c1], e2 = T.ev2[c2];
+    const double e = e1 + e2;
+    const bool singular = e1 == 0.0 && e2 == 0.0;
+    auto diag = [&](int k) {
+        const double d = (k == 0 && singular) ? T.s0 : (e - T.A[k]) - T.B[k];
+        return d - T.shift;
+    };
+    double Dp = diag(0);
+    T.mfac[mode] = 0.0;
+    T.rfac[mode] = 1.0 / Dp;
+    for (int k = 1; k < T.ns; ++k) {
+        const double m = T.DL[k] / Dp;
+        const double D = diag(k) - m * T.DU[k - 1];
+        T.mfac[(long)k * modes + mode] = m;
+        T.rfac[(long)k * modes + mode] = 1.0 / D;
+        Dp = D;
+    }
+}
+
+// the Thomas sweeps with the factors of the line's mode class: one FMA chain
+// forward, one backward, the field read and written once each way
+__global__ void __launch_bounds__(kThreads) k_tri_apply(double* __restrict__ w, Lines L, Tri T) {
+    const long l = (long)blockIdx.x * kThreads + threadIdx.x;
+    if (l >= L.count) return;
+    const long base = line_base(L, l);
+    const long st = L.stride;
+    const int ns = T.ns;
+    const unsigned inner = (unsigned)L.inner;
+    const int co = (int)((unsigned)l / inner), ci = (int)((unsigned)l - (unsigned)co * inner);
+    const int modes = T.nci * T.nco;
+    const int mode = T.clsO[co] * T.nci + T.clsI[ci];
+    const double* mf = T.mfac + mode;
+    const double* rf = T.rfac + mode;
+    // field values and factors run kTriAhead rows ahead of the FMA chains
+    double fp = w[base];
+    double fa[kTriAhead], ma[kTriAhead];
+#pragma unroll
+    for (int u = 0; u < kTriAhead; ++u) {
+        const int k = 1 + u;
+        fa[u] = k < ns ? w[base + k * st] : 0.0;
+        ma[u] = k < ns ? __ldg(mf + (long)k * modes) : 0.0;
+    }
+    for (int k0 = 1; k0 < ns; k0 += kTriAhead) {
+#pragma unroll
+        for (int u = 0; u < kTriAhead; ++u) {
+            const int k = k0 + u;
+            if (k < ns) {
+                const double fk = fa[u], mk = ma[u];
+                const int kn = k + kTriAhead;
+                fa[u] = kn < ns ? w[base + kn * st] : 0.0;
+                ma[u] = kn < ns ? __ldg(mf + (long)kn * modes) : 0.0;
+                fp = fk - mk * fp;
+                w[base + k * st] = fp;
+            }
+        }
+    }
+    double p = fp * __ldg(rf + (long)(ns - 1) * modes);
+    w[base + (ns - 1) * st] = p;
+    double ra[kTriAhead], ua[kTriAhead];
+#pragma unroll
+    for (int u = 0; u < kTriAhead; ++u) {
+        const int k = ns - 2 - u;
+        fa[u] = k >= 0 ? w[base + k * st] : 0.0;
+        ra[u] = k >= 0 ? __ldg(rf + (long)k * modes) : 0.0;
+        ua[u] = k >= 0 ? T.DU[k] : 0.0;
+    }
+    for (int k0 = ns - 2; k0 >= 0; k0 -= kTriAhead) {
+#pragma unroll
+        for (int u = 0; u < kTriAhead; ++u) {
+            const int k = k0 - u;
+            if (k >= 0) {
+                const double wk = fa[u], rk = ra[u], duk = ua[u];
+                const int kn = k - kTriAhead;
+                fa[u] = kn >= 0 ? w[base + kn * st] : 0.0;
+                ra[u] = kn >= 0 ? __ldg(rf + (long)kn * modes) : 0.0;
+                ua[u] = kn >= 0 ? T.DU[kn] : 0.0;
+                p = (wk - duk * p) * rk;
+                w[base + k * st] = p;
+            }
+        }
+    }
+}
+
 // w = (-b - shift x_old - face terms) * scale
 __global__ void k_prep(double* __restrict__ w, const double* __restrict__ b, const double* __restrict__ xo, Prep P) {
     const long total = (long)P.n0 * P.n1 * P.n2;
@@ -299,6 +761,71 @@ __global__ void k_prep(double* __restrict__ w, const double* __restrict__ b, con
         if (k == P.n2 - 1) v -= P.corr[5];
         w[c] = v * P.scale;
     }
+}
+
+template <int LOGM, int KIND, bool LF>
+void launch_one(unsigned grid, cudaStream_t st, const double* in, double* out, const Lines& L, const Transform& T,
+                const LoadPrep& lp, long tiles, int pair) {
+    k_transform<LOGM, KIND, LF><<<grid, kTransformThreads, kTransformSmem, st>>>(in, out, L, T, lp, tiles, pair);
+}
+
+template <int KIND, bool LF>
+void launch_kind(int logM, unsigned grid, cudaStream_t st, const double* in, double* out, const Lines& L,
+                 const Transform& T, const LoadPrep& lp, long tiles, int pair) {
+    switch (logM) {
+        case 1: launch_one<1, KIND, LF>(grid, st, in, out, L, T, lp, tiles, pair); break;
+        case 2: launch_one<2, KIND, LF>(grid, st, in, out, L, T, lp, tiles, pair); break;
+        case 3: launch_one<3, KIND, LF>(grid, st, in, out, L, T, lp, tiles, pair); break;
+        case 4: launch_one<4, KIND, LF>(grid, st, in, out, L, T, lp, tiles, pair); break;
+        case 5: launch_one<5, KIND, LF>(grid, st, in, out, L, T, lp, tiles, pair); break;
+        case 6: launch_one<6, KIND, LF>(grid, st, in, out, L, T, lp, tiles, pair); break;
+        case 7: launch_one<7, KIND, LF>(grid, st, in, out, L, T, lp, tiles, pair); break;
+        case 8: launch_one<8, KIND, LF>(grid, st, in, out, L, T, lp, tiles, pair); break;
+        case 9: launch_one<9, KIND, LF>(grid, st, in, out, L, T, lp, tiles, pair); break;
+        default: launch_one<10, KIND, LF>(grid, st, in, out, L, T, lp, tiles, pair); break;
+    }
+}
+
+void launch_transform(int kind, int logM, unsigned grid, cudaStream_t st, const double* in, double* out,
+                      const Lines& L, const Transform& T, const LoadPrep& lp, long tiles, int pair) {
+    const bool lf = L.line_fast != 0;
+    if (kind == K_R2HC)
+        lf ? launch_kind<K_R2HC, true>(logM, grid, st, in, out, L, T, lp, tiles, pair)
+           : launch_kind<K_R2HC, false>(logM, grid, st, in, out, L, T, lp, tiles, pair);
+    else if (kind == K_HC2R)
+        lf ? launch_kind<K_HC2R, true>(logM, grid, st, in, out, L, T, lp, tiles, pair)
+           : launch_kind<K_HC2R, false>(logM, grid, st, in, out, L, T, lp, tiles, pair);
+    else
+        lf ? launch_kind<K_TRIG, true>(logM, grid, st, in, out, L, T, lp, tiles, pair)
+           : launch_kind<K_TRIG, false>(logM, grid, st, in, out, L, T, lp, tiles, pair);
+}
+
+template <int LOGM, int KIND, bool LF>
+void allow_one() {
+    cudaFuncSetAttribute(k_transform<LOGM, KIND, LF>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTransformSmem);
+}
+
+template <int KIND, bool LF>
+void allow_kind() {
+    allow_one<1, KIND, LF>();
+    allow_one<2, KIND, LF>();
+    allow_one<3, KIND, LF>();
+    allow_one<4, KIND, LF>();
+    allow_one<5, KIND, LF>();
+    allow_one<6, KIND, LF>();
+    allow_one<7, KIND, LF>();
+    allow_one<8, KIND, LF>();
+    allow_one<9, KIND, LF>();
+    allow_one<10, KIND, LF>();
+}
+
+void allow_smem_all() {
+    allow_kind<K_R2HC, true>();
+    allow_kind<K_R2HC, false>();
+    allow_kind<K_HC2R, true>();
+    allow_kind<K_HC2R, false>();
+    allow_kind<K_TRIG, true>();
+    allow_kind<K_TRIG, false>();
 }
 
 struct BadArg {
@@ -323,7 +850,8 @@ struct AxisPlan {
     Lines lines{};
     Transform fwd{}, bwd{};
     int LB = 1;
-    size_t smem = 0;
+    int adjacent = 0;   // the two elements of a thread's pair are adjacent in memory
+    bool identity = false;  // a periodic axis of one cell: nothing to transform
 };
 
 }  // namespace bfft
@@ -332,6 +860,7 @@ using namespace bfft;
 
 struct bfft_ctx {
     int dev = 0;
+    int sms = 148;
     int n[3] = {0, 0, 0};
     int s = 0, dir1 = 0, dir2 = 0;
     AxisPlan ax[3];
@@ -344,6 +873,8 @@ struct bfft_ctx {
     std::vector<void*> owned;
     cudaStream_t stream = nullptr;
     bool ownStream = false;
+    bool factored = false;      // the Thomas factors hold for factorShift
+    double factorShift = 0.0;
     std::string err;
 };
 
@@ -377,15 +908,16 @@ void planTransforms(bfft_ctx* c, int d) {
     const long double pi = 3.141592653589793238462643383279502884L;
     const bool cc = A.pair == P_CC;
     const int M = cc ? N : 2 * N;
-    std::vector<double2> tw(std::max(M / 2, 1));
-    for (int j = 0; j < M / 2; ++j) tw[j] = expi(-2.0L * pi * j / M);
+    std::vector<double2> tw(M);
+    for (int j = 0; j < M; ++j) tw[j] = expi(-2.0L * pi * j / M);
     const double2* twd = upload(c, tw);
     auto table = [&](auto f) {
         std::vector<double2> t(N);
         for (int q = 0; q < N; ++q) t[q] = f(q);
         return upload(c, t);
     };
-    Transform f{M, log2i(M), M_RE, nullptr, nullptr, twd};
+    const int LB = std::min(kTileComplex / M, kMaxLines);
+    Transform f{M, log2i(M), M_RE, log2i(N), log2i(LB), nullptr, nullptr, twd};
     Transform b = f;
     switch (A.pair) {
         case P_CC:
@@ -412,9 +944,12 @@ void planTransforms(bfft_ctx* c, int d) {
     }
     A.fwd = f;
     A.bwd = b;
-    A.LB = std::max(1, std::min(32, kTileComplex / M));
-    A.smem = sizeof(double2) * ((size_t)A.LB * M + std::max(M / 2, 1)) + sizeof(long) * A.LB +
-             (cc ? sizeof(double) * (size_t)A.LB * N : 0);
+    A.LB = LB;
+    A.identity = cc && N == 1;
+    // pairs: consecutive lines along the strided axes (adjacent when the k
+    // rows hold an even number of cells), consecutive points along k
+    const long n1 = c->n[1], n2 = c->n[2];
+    A.adjacent = d == 2 ? 1 : d == 1 ? (n2 % 2 == 0) : ((n1 * n2) % 2 == 0);
 }
 
 Lines linesAlong(const int n[3], int d) {
@@ -519,14 +1054,12 @@ void build(bfft_ctx* c, const bfft_desc* d) {
     if (cudaGetDeviceCount(&count) != cudaSuccess || count <= c->dev || c->dev < 0)
         throw BadArg{BMG_NO_DEVICE, "no usable CUDA device"};
     check(cudaSetDevice(c->dev), "cudaSetDevice");
-    size_t smem = 0;
+    check(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->dev), "cudaDeviceGetAttribute");
+    allow_smem_all();
     for (int a : {c->dir1, c->dir2}) {
         c->ax[a].lines = linesAlong(c->n, a);
         planTransforms(c, a);
-        smem = std::max(smem, c->ax[a].smem);
     }
-    check(cudaFuncSetAttribute(k_transform, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-          "cudaFuncSetAttribute");
 
     // tridiagonal coefficients (tridiagonalSolver.C:117-280), ghost cell
     // sizes from levelPoints.C:198-236 / 326-400
@@ -590,7 +1123,40 @@ void build(bfft_ctx* c, const bfft_desc* d) {
     c->solveLines = linesAlong(c->n, s);
     // the lines' inner coordinate: k for s = 0 and 1, j for s = 2
     const int innerAxis = s == 2 ? 1 : 2;
+    const int outerAxis = s == 0 ? 1 : 0;
     T.dir1_inner = c->dir1 == innerAxis;
+    // classes of equal eigenvalues: frequencies p and N - p of a real
+    // Fourier axis (halfcomplex positions), every position otherwise
+    auto classes = [&](int a, std::vector<int>& cls, std::vector<int>& rep) {
+        const int N = c->n[a];
+        cls.assign(N, 0);
+        rep.clear();
+        if (c->ax[a].pair == P_CC) {
+            for (int q = 0; q < N; ++q) cls[q] = q <= N / 2 ? q : N - q;
+            for (int q = 0; q <= N / 2; ++q) rep.push_back(q);
+        } else {
+            for (int q = 0; q < N; ++q) {
+                cls[q] = q;
+                rep.push_back(q);
+            }
+        }
+    };
+    std::vector<int> cI, rI, cO, rO;
+    classes(innerAxis, cI, rI);
+    classes(outerAxis, cO, rO);
+    T.clsI = upload(c, cI);
+    T.repI = upload(c, rI);
+    T.clsO = upload(c, cO);
+    T.repO = upload(c, rO);
+    T.nci = (int)rI.size();
+    T.nco = (int)rO.size();
+    if (!T.cyclic) {
+        const size_t f = (size_t)T.nci * T.nco * ns;
+        T.mfac = dalloc<double>(f);
+        T.rfac = dalloc<double>(f);
+        c->owned.push_back(T.mfac);
+        c->owned.push_back(T.rfac);
+    }
 
     // right-hand side terms of the faces (FFTPoissonSolver.C:140-183)
     Prep& P = c->prep;
@@ -647,11 +1213,14 @@ int guarded(bfft_ctx* c, F&& f) {
     }
 }
 
-void transform(bfft_ctx* c, int a, bool forward, const double* in, double* out) {
+void transform(bfft_ctx* c, int a, bool forward, const double* in, double* out, const LoadPrep& lp) {
     const AxisPlan& A = c->ax[a];
     const Transform& T = forward ? A.fwd : A.bwd;
-    const long grid = (A.lines.count + A.LB - 1) / A.LB;
-    k_transform<<<(unsigned)grid, kThreads, A.smem, c->stream>>>(in, out, A.lines, T, A.LB);
+    const long tiles = (A.lines.count + A.LB - 1) / A.LB;
+    // persistent: as many CTAs as fit at once (three per SM)
+    const long grid = std::min<long>(tiles, 3L * c->sms);
+    const int kind = T.mode == M_R2HC ? K_R2HC : T.mode == M_HC2R ? K_HC2R : K_TRIG;
+    launch_transform(kind, T.logM, (unsigned)grid, c->stream, in, out, A.lines, T, lp, tiles, A.adjacent);
     check(cudaGetLastError(), "k_transform");
 }
 
@@ -718,24 +1287,52 @@ int bfft_solve(bfft_ctx* c, const double* b, double* x, const double* x_old, dou
         }
         Prep P = c->prep;
         P.shift = shift;
-        const int blocks = (int)std::min<size_t>((cells + kThreads - 1) / kThreads, 148 * 16);
-        k_prep<<<blocks, kThreads, 0, c->stream>>>(c->w, bd, shift != 0.0 ? xo : nullptr, P);
-        check(cudaGetLastError(), "k_prep");
+        std::vector<int> fwd;
         for (int a : {c->dir1, c->dir2})
-            if (c->ax[a].pair != P_EMPTY) transform(c, a, true, c->w, c->w);
+            if (c->ax[a].pair != P_EMPTY && !c->ax[a].identity) fwd.push_back(a);
+        const LoadPrep none{};
+        if (fwd.empty()) {
+            const int blocks = (int)std::min<size_t>((cells + kThreads - 1) / kThreads, 148 * 16);
+            k_prep<<<blocks, kThreads, 0, c->stream>>>(c->w, bd, shift != 0.0 ? xo : nullptr, P);
+            check(cudaGetLastError(), "k_prep");
+        }
+        for (size_t q = 0; q < fwd.size(); ++q) {
+            // the first transform forms the right-hand side as it loads b
+            LoadPrep lp{};
+            if (q == 0) {
+                lp.on = 1;
+                lp.axis = fwd[0];
+                lp.n1 = c->n[1];
+                lp.n2 = c->n[2];
+                lp.xo = shift != 0.0 ? xo : nullptr;
+                lp.P = P;
+            }
+            transform(c, fwd[q], true, q == 0 ? bd : c->w, c->w, q == 0 ? lp : none);
+        }
         Tri T = c->tri;
         T.shift = shift;
+        if (!T.cyclic && (!c->factored || c->factorShift != shift)) {
+            const int modes = T.nci * T.nco;
+            k_tri_factor<<<(modes + 127) / 128, 128, 0, c->stream>>>(T);
+            check(cudaGetLastError(), "k_tri_factor");
+            c->factored = true;
+            c->factorShift = shift;
+        }
         const long lines = c->solveLines.count;
-        k_tridiag<<<(unsigned)((lines + kThreads - 1) / kThreads), kThreads, 0, c->stream>>>(c->w, c->dh, c->vv,
-                                                                                          c->solveLines, T);
+        if (T.cyclic)
+            k_tridiag<<<(unsigned)((lines + kThreads - 1) / kThreads), kThreads, 0, c->stream>>>(c->w, c->dh, c->vv,
+                                                                                              c->solveLines, T);
+        else
+            k_tri_apply<<<(unsigned)((lines + kThreads - 1) / kThreads), kThreads, 0, c->stream>>>(c->w, c->solveLines,
+                                                                                                T);
         check(cudaGetLastError(), "k_tridiag");
         // backward in reverse order; the last one writes the device x
         std::vector<int> back;
         for (int a : {c->dir2, c->dir1})
-            if (c->ax[a].pair != P_EMPTY) back.push_back(a);
+            if (c->ax[a].pair != P_EMPTY && !c->ax[a].identity) back.push_back(a);
         for (size_t q = 0; q < back.size(); ++q) {
             const bool last = q + 1 == back.size();
-            transform(c, back[q], false, c->w, last && dev ? x : c->w);
+            transform(c, back[q], false, c->w, last && dev ? x : c->w, none);
         }
         if (dev && back.empty())
             check(cudaMemcpyAsync(x, c->w, cells * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy x");

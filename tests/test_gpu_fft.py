@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from briscola_b200 import fft
-from briscola_b200.mesh import DIRICHLET, NEUMANN, PERIODIC, Brick, geometric_points, tanh_points, uniform_points
+from briscola_b200.mesh import DIRICHLET, EMPTY, NEUMANN, PERIODIC, Brick, geometric_points, tanh_points, uniform_points
 from oracle import fft_oracle as F
 
 pytestmark = pytest.mark.gpu
@@ -61,6 +61,23 @@ def test_configurations_match_oracle(bc, stretch_axis):
     ref = F.solve(f, pts, bc)
     assert rel(x, ref) <= 1e-12
     assert np.abs(F.laplacian_residual(x, f, pts, bc, (0.0,) * 6)).max() <= 1e-9
+
+
+@pytest.mark.parametrize("bc,n", [
+    ((P, P, EMPTY, EMPTY, N, N), (16, 1, 32)),  # two-dimensional: an empty axis
+    ((N, N, P, P, D, D), (16, 1, 8)),           # a periodic axis of one cell
+    ((D, D, N, D, N, N), (8, 4, 7)),            # stretched z of 7 cells: odd k rows, single-element copies
+])
+def test_thin_and_ragged_shapes(bc, n):
+    pts = [uniform_points(m) for m in n]
+    if n[2] == 7:
+        pts[2] = geometric_points(7, 2.0)
+    rng = np.random.default_rng(13)
+    f = rng.standard_normal(n)
+    s = fft.FFTPoissonSolver(Brick(pts, bc))
+    x = s.solve(None, f)
+    ref = F.solve(f, pts, bc)
+    assert rel(x, ref) <= 1e-12
 
 
 def test_known_answer_ddt():
