@@ -180,6 +180,22 @@ def profile_region(args, local):
     from briscola_b200 import workloads
 
     stream = torch.cuda.current_stream()
+    if args.profile_region == "fft":
+        from briscola_b200 import fft
+
+        mesh, _, _ = workloads.channel(args.size)
+        solver = fft.FFTPoissonSolver(mesh.bricks[0], device=local)
+        f = torch.randn(mesh.bricks[0].N, dtype=torch.float64, device=f"cuda:{local}")
+        x = torch.empty_like(f)
+        for _ in range(args.warmup):
+            solver.solve(x, f)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        solver.solve(x, f)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        solver.close()
+        return
     if args.profile_region == "unet_fwd":
         from briscola_b200 import unet
 
@@ -335,7 +351,8 @@ def main():
     ap.add_argument("--learned-pairs", type=int, default=2000)
     ap.add_argument("--learned-steps", type=int, default=2000)
     ap.add_argument("--learned-held", type=int, default=200)
-    ap.add_argument("--profile-region", choices=["mixed_fcg", "mixed_fcg_fused", "fp64", "unet_fwd"], default=None,
+    ap.add_argument("--profile-region", choices=["mixed_fcg", "mixed_fcg_fused", "fp64", "unet_fwd", "fft"],
+                    default=None,
                     help="set up, warm up, then run one solve (or one U-Net forward) between "
                          "cudaProfilerStart/Stop for ncu --profile-from-start off; prints no bench line")
     ap.add_argument("--tuning", default=None,
