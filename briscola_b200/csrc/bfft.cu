@@ -89,6 +89,7 @@ struct Tri {
 };
 
 constexpr int kTriAhead = 8;  // rows a tridiagonal sweep loads ahead
+constexpr int kSplitBlocks = 592;  // partial maxima of the face coefficients
 
 struct Prep {
     int n0, n1, n2;
@@ -744,6 +745,118 @@ __global__ void __launch_bounds__(kThreads) k_tri_apply(double* __restrict__ w, 
     }
 }
 
+// ---- split Poisson solver -------------------------------------------------
+
+struct SplitGeom {
+    int n[3];
+    const double* h[3];   // cell sizes per axis
+    int bc[6];            // BFFT_BC_* per face
+    double value[6];      // Dirichlet value or Neumann gradient
+};
+
+// largest of the three face arrays: per-block maxima, then one block
+__global__ void k_max3(const double* __restrict__ a, long na, const double* __restrict__ b, long nb,
+                       const double* __restrict__ c, long nc, double* __restrict__ part) {
+    double m = -1e308;
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < na + nb + nc; q += stride) {
+        const double v = q < na ? a[q] : q < na + nb ? b[q - na] : c[q - na - nb];
+        m = fmax(m, v);
+    }
+    __shared__ double sm[kThreads];
+    sm[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = kThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sm[0];
+}
+
+__global__ void k_max_final(double* __restrict__ part, int n) {
+    __shared__ double sm[kThreads];
+    double m = -1e308;
+    for (int q = threadIdx.x; q < n; q += kThreads) m = fmax(m, part[q]);
+    sm[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = kThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[0] = sm[0];
+}
+
+// one face's flux term lambda' (x_nb - x_c) delta, with the neighbour or the
+// ghost the face condition sets (DirichletBoundaryCondition.C:51-71,
+// NeumannBoundaryCondition.C:59-85; mirrored ghost cells: delta = 1/h)
+__device__ __forceinline__ double face_term(const SplitGeom& G, int axis, int side, int idx, double lamp, double xc,
+                                            double xnb, bool boundary, double delta) {
+    if (!boundary) return lamp * (xnb - xc) * delta;
+    const int f = 2 * axis + side;
+    const int bc = G.bc[f];
+    if (bc == BFFT_BC_NEUMANN) return lamp * G.value[f];  // (x_g - x_c) delta = g
+    if (bc == BFFT_BC_DIRICHLET) return lamp * (2.0 * G.value[f] - 2.0 * xc) * delta;
+    return 0.0;  // empty
+}
+
+// bhat = b / lambda0 + div((lambda / lambda0 - 1) faceGrad(x) faceArea)
+__global__ void k_split_source(const double* __restrict__ x, const double* __restrict__ b,
+                               const double* __restrict__ lam0, const double* __restrict__ lam1,
+                               const double* __restrict__ lam2, double lambda0, double* __restrict__ bhat,
+                               SplitGeom G) {
+    const int n0 = G.n[0], n1 = G.n[1], n2 = G.n[2];
+    const long total = (long)n0 * n1 * n2;
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long c = (long)blockIdx.x * blockDim.x + threadIdx.x; c < total; c += stride) {
+        const int k = (int)(c % n2);
+        const long ij = c / n2;
+        const int j = (int)(ij % n1), i = (int)(ij / n1);
+        const int ijk[3] = {i, j, k};
+        const long sx[3] = {(long)n1 * n2, n2, 1};
+        const double xc = x[c];
+        double div = 0.0;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int q = ijk[a], n = G.n[a];
+            const double* h = G.h[a];
+            const bool per = G.bc[2 * a] == BFFT_BC_PERIODIC;
+            const double hc = h[q];
+            // lower and upper faces of the cell along axis a
+            const double hlo = q > 0 ? h[q - 1] : (per ? h[n - 1] : hc);
+            const double hhi = q < n - 1 ? h[q + 1] : (per ? h[0] : hc);
+            const double dw = 0.5 * (hc + hlo), de = 0.5 * (hc + hhi);
+            long flo, fhi;  // face indices in the face array of axis a
+            if (a == 0) {
+                flo = ((long)i * n1 + j) * n2 + k;
+                fhi = ((long)(i + 1) * n1 + j) * n2 + k;
+            } else if (a == 1) {
+                flo = ((long)i * (n1 + 1) + j) * n2 + k;
+                fhi = ((long)i * (n1 + 1) + j + 1) * n2 + k;
+            } else {
+                flo = ((long)i * n1 + j) * (n2 + 1) + k;
+                fhi = flo + 1;
+            }
+            const double* lam = a == 0 ? lam0 : a == 1 ? lam1 : lam2;
+            const double llo = lam[flo] / lambda0 - 1.0, lhi = lam[fhi] / lambda0 - 1.0;
+            const bool blo = q == 0 && !per, bhi = q == n - 1 && !per;
+            double xlo = 0.0, xhi = 0.0;
+            if (!blo) xlo = x[q > 0 ? c - sx[a] : c + (long)(n - 1) * sx[a]];
+            if (!bhi) xhi = x[q < n - 1 ? c + sx[a] : c - (long)(n - 1) * sx[a]];
+            // lower face: outward gradient (x_lo - x_c) delta; upper face enters with a minus sign
+            // of its own outward gradient, i.e. (x_hi - x_c) delta
+            const double tlo = face_term(G, a, 0, q, llo, xc, xlo, blo, 1.0 / dw);
+            const double thi = face_term(G, a, 1, q, lhi, xc, xhi, bhi, 1.0 / de);
+            div += (tlo + thi) / hc;
+        }
+        bhat[c] = b[c] / lambda0 + div;
+    }
+}
+
+__global__ void k_axpby(double a, const double* x, double c, const double* y, double* out, long n) {
+    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
+        out[q] = a * x[q] + c * y[q];
+}
+
 // w = (-b - shift x_old - face terms) * scale
 __global__ void k_prep(double* __restrict__ w, const double* __restrict__ b, const double* __restrict__ xo, Prep P) {
     const long total = (long)P.n0 * P.n1 * P.n2;
@@ -873,6 +986,8 @@ struct bfft_ctx {
     std::vector<void*> owned;
     cudaStream_t stream = nullptr;
     bool ownStream = false;
+    SplitGeom split{};
+    double* part = nullptr;     // reduction partials (split solver)
     bool factored = false;      // the Thomas factors hold for factorShift
     double factorShift = 0.0;
     std::string err;
@@ -1181,6 +1296,18 @@ void build(bfft_ctx* c, const bfft_desc* d) {
             P.corr[f] = d->value[f] * hb / (hb * hb);
     }
 
+    // geometry of the split solver's source kernel
+    for (int a = 0; a < 3; ++a) {
+        c->split.n[a] = c->n[a];
+        c->split.h[a] = upload(c, h[a]);
+    }
+    for (int f = 0; f < 6; ++f) {
+        c->split.bc[f] = d->bc[f];
+        c->split.value[f] = d->value[f];
+    }
+    c->part = dalloc<double>(kSplitBlocks);
+    c->owned.push_back(c->part);
+
     const size_t cells = (size_t)c->n[0] * c->n[1] * c->n[2];
     c->w = dalloc<double>(cells);
     c->dh = dalloc<double>(cells);
@@ -1340,6 +1467,44 @@ int bfft_solve(bfft_ctx* c, const double* b, double* x, const double* x_old, dou
             check(cudaMemcpyAsync(x, c->w, cells * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy x");
             check(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
         }
+        return (int)BMG_OK;
+    });
+}
+
+int bfft_split_lambda0(bfft_ctx* c, const double* lam0, const double* lam1, const double* lam2, double* lambda0) {
+    if (!c || !lam0 || !lam1 || !lam2 || !lambda0) return BMG_BAD_ARG;
+    return guarded(c, [&] {
+        check(cudaSetDevice(c->dev), "cudaSetDevice");
+        const long n0 = c->n[0], n1 = c->n[1], n2 = c->n[2];
+        k_max3<<<kSplitBlocks, kThreads, 0, c->stream>>>(lam0, (n0 + 1) * n1 * n2, lam1, n0 * (n1 + 1) * n2, lam2,
+                                                        n0 * n1 * (n2 + 1), c->part);
+        k_max_final<<<1, kThreads, 0, c->stream>>>(c->part, kSplitBlocks);
+        check(cudaGetLastError(), "k_max3");
+        check(cudaMemcpyAsync(lambda0, c->part, sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy lambda0");
+        check(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+        if (!(*lambda0 > 0.0)) throw BadArg{BMG_BAD_ARG, "face coefficients must be positive"};
+        return (int)BMG_OK;
+    });
+}
+
+int bfft_split_source(bfft_ctx* c, const double* x, const double* b, const double* lam0, const double* lam1,
+                      const double* lam2, double lambda0, double* bhat) {
+    if (!c || !x || !b || !lam0 || !lam1 || !lam2 || !bhat || !(lambda0 > 0.0)) return BMG_BAD_ARG;
+    return guarded(c, [&] {
+        check(cudaSetDevice(c->dev), "cudaSetDevice");
+        k_split_source<<<4 * c->sms, kThreads, 0, c->stream>>>(x, b, lam0, lam1, lam2, lambda0, bhat, c->split);
+        check(cudaGetLastError(), "k_split_source");
+        return (int)BMG_OK;
+    });
+}
+
+int bfft_axpby(bfft_ctx* c, double a, const double* x, double cc, const double* y, double* out) {
+    if (!c || !x || !y || !out) return BMG_BAD_ARG;
+    return guarded(c, [&] {
+        check(cudaSetDevice(c->dev), "cudaSetDevice");
+        const long n = (long)c->n[0] * c->n[1] * c->n[2];
+        k_axpby<<<4 * c->sms, kThreads, 0, c->stream>>>(a, x, cc, y, out, n);
+        check(cudaGetLastError(), "k_axpby");
         return (int)BMG_OK;
     });
 }

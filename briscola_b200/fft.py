@@ -25,7 +25,7 @@ from .solvers import FatalError
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libbfft.so")
 EXPORTED = ("bfft_create", "bfft_destroy", "bfft_set_stream", "bfft_solve", "bfft_solve_direction",
-            "bfft_last_error")
+            "bfft_last_error", "bfft_split_lambda0", "bfft_split_source", "bfft_axpby")
 BC = {DIRICHLET: 0, NEUMANN: 1, PERIODIC: 2, EMPTY: 3}
 DEVICE_PTRS = 1
 
@@ -63,6 +63,9 @@ def load(path: str = LIB_PATH):
     L.bfft_solve_direction.argtypes = [vp]
     L.bfft_last_error.argtypes = [vp]
     L.bfft_last_error.restype = ctypes.c_char_p
+    L.bfft_split_lambda0.argtypes = [vp, vp, vp, vp, ctypes.POINTER(ctypes.c_double)]
+    L.bfft_split_source.argtypes = [vp, vp, vp, vp, vp, vp, ctypes.c_double, vp]
+    L.bfft_axpby.argtypes = [vp, ctypes.c_double, vp, ctypes.c_double, vp, vp]
     _lib = L
     return L
 

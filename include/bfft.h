@@ -61,6 +61,24 @@ int bfft_set_stream(bfft_ctx* ctx, void* stream);
  * 225-231). */
 int bfft_solve(bfft_ctx* ctx, const double* b, double* x, const double* x_old, double shift, int flags);
 
+/* ---- split Poisson solver (splitPoissonSolver.C:53-155) -------------------
+ * Device arrays only.  Face coefficients: lam0 (n0+1) x n1 x n2 (the face
+ * below cell i along x, then the top face), lam1 n0 x (n1+1) x n2, lam2
+ * n0 x n1 x (n2+1), k fastest.
+ *
+ * *lambda0 = the largest face coefficient (splitPoissonSolver.C:97-104). */
+int bfft_split_lambda0(bfft_ctx* ctx, const double* lam0, const double* lam1, const double* lam2, double* lambda0);
+/* bhat = b / lambda0 + div((lambda / lambda0 - 1) faceGrad(x) faceArea), the
+ * modified source of splitPoissonSolver.C:118-138 with the reference's
+ * outward face gradient and flux divergence (linearFaceGradientScheme.C,
+ * divergenceScheme.C:68-96); boundary faces see the ghost values of the
+ * descriptor's face conditions. */
+int bfft_split_source(bfft_ctx* ctx, const double* x, const double* b, const double* lam0, const double* lam1,
+                      const double* lam2, double lambda0, double* bhat);
+/* out = a x + c y (the split solver's prediction from two old levels,
+ * splitPoissonSolver.C:75-84); out may alias x or y. */
+int bfft_axpby(bfft_ctx* ctx, double a, const double* x, double c, const double* y, double* out);
+
 /* the planned solve direction (0, 1, 2) */
 int bfft_solve_direction(const bfft_ctx* ctx);
 /* last error message of the context ("" if none) */

@@ -14,6 +14,11 @@ Follows, for one brick on one process:
                       NeumannBoundaryCondition.C:59-85 (x_g = x_c + g |c_c - c_g|)
   ghost points        src/briscolaMesh/level/levelPoints.C:198-236, 326-400
   known-answer check  applications/test/FFTPoissonSolver/Test-FFTPoissonSolver.C:11-92
+  split solver        src/briscolaFiniteVolume/solvers/PoissonSolvers/splitPoissonSolver/
+                      splitPoissonSolver.C:53-155 (prediction, lambda0, modified source, corrections);
+                      face gradient .../faceGradientSchemes/linearFaceGradientScheme/
+                      linearFaceGradientScheme.C (outward through the lower face), flux divergence
+                      .../divergenceSchemes/divergenceScheme/divergenceScheme.C:68-96
 
 The FFTW r2r kinds are restated with scipy.fft, whose unnormalised DCT/DST
 types 2, 3 and 4 have FFTW's REDFT10/01/11 and RODFT10/01/11 definitions;
@@ -340,3 +345,60 @@ def laplacian_residual(x: np.ndarray, f: np.ndarray, points, bc, bc_values) -> n
         xc, xm, xp = g[tuple(c)], g[tuple(m)], g[tuple(p)]
         r += xm / (dw * hc) - xc / (dw * hc) - xc / (de * hc) + xp / (de * hc)
     return r
+
+
+# ---- split Poisson solver (splitPoissonSolver.C:53-155) --------------------
+
+def face_flux_divergence(x, lamp, points, bc, bc_values):
+    """div(lamp faceGrad(x) faceArea) per cell (volume-divided): faces of
+    axis d carry lamp[d] ((n_d + 1) along d), ghosts from the face
+    conditions (with_ghosts)."""
+    g = with_ghosts(x, points, bc, bc_values)
+    n = x.shape
+    div = np.zeros(n)
+    for d in range(3):
+        if bc[2 * d] == EMPTY:
+            continue
+        h = cell_sizes_with_ghosts(points[d], bc[2 * d] == PERIODIC)
+        delta = 1.0 / ((h[1:] + h[:-1]) / 2.0)  # n+1 faces: between ghost/interior cells
+        shape = [1, 1, 1]
+        shape[d] = -1
+        delta = delta.reshape(shape)
+        # outward gradient through the lower face of cell q (q = 0..n): x[q-1] - x[q]
+        lo = [slice(1, -1)] * 3
+        hi = [slice(1, -1)] * 3
+        lo[d] = slice(0, n[d] + 1)
+        hi[d] = slice(1, n[d] + 2)
+        grad = (g[tuple(lo)] - g[tuple(hi)]) * delta
+        phi = lamp[d] * grad
+        # Div(cell q) += phi(face q); Div(cell q-1) -= phi(face q)
+        a = [slice(None)] * 3
+        b = [slice(None)] * 3
+        a[d] = slice(0, n[d])
+        b[d] = slice(1, n[d] + 1)
+        hc = np.diff(points[d]).reshape(shape)
+        div += (phi[tuple(a)] - phi[tuple(b)]) / hc
+    return div
+
+
+def split_source(x, b, lam, lambda0, points, bc, bc_values=(0.0,) * 6):
+    """bhat = b / lambda0 + div((lambda / lambda0 - 1) faceGrad(x) faceArea)
+    (splitPoissonSolver.C:118-138)."""
+    lamp = [l / lambda0 - 1.0 for l in lam]
+    return b / lambda0 + face_flux_divergence(x, lamp, points, bc, bc_values)
+
+
+def split_solve(x, b, lam, points, bc, bc_values=(0.0,) * 6, n_corr=1):
+    """nCorr corrections of the split solver from the initial x (prediction
+    and preconditioner applied by the caller), FFT inner solver."""
+    lambda0 = max(float(l.max()) for l in lam)
+    for _ in range(n_corr):
+        bhat = split_source(x, b, lam, lambda0, points, bc, bc_values)
+        x = solve(bhat, points, bc, bc_values)
+    return x
+
+
+def variable_residual(x, b, lam, points, bc, bc_values=(0.0,) * 6):
+    """-div(lambda grad x) - b per cell: the equation the split solver
+    approximates."""
+    return -face_flux_divergence(x, lam, points, bc, bc_values) - b

@@ -19,7 +19,7 @@ def test_library_exports_every_header_function():
     lib = ctypes.CDLL(build_fft())
     txt = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "bfft.h")).read(), flags=re.S)
     fns = sorted(set(re.findall(r"\b(bfft_[a-z_0-9]+)\s*\(", txt)))
-    assert len(fns) == 6
+    assert len(fns) == 9
     assert [f for f in fns if not hasattr(lib, f)] == []
     assert set(fns) == set(fft.EXPORTED)
 

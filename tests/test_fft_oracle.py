@@ -133,3 +133,46 @@ def test_shift_keeps_the_singular_mode_pin():
     assert np.abs(r[:, 1:, :]).max() <= 1e-9
     # the residual at j = 0 is the same constant in every cell: the mean mode
     assert np.ptp(r[:, 0, :]) <= 1e-9 and abs(r[0, 0, 0]) > 1e-3
+
+
+def _smooth_lambda(n, ratio, rng, periodic):
+    lam = []
+    for d in range(3):
+        shape = list(n)
+        shape[d] += 1
+        a = 1.0 + (ratio - 1.0) * rng.random(shape)
+        if periodic[d]:
+            idx = [slice(None)] * 3
+            first = [slice(None)] * 3
+            idx[d], first[d] = -1, 0
+            a[tuple(idx)] = a[tuple(first)]
+        lam.append(a)
+    return lam
+
+
+def test_split_divergence_is_the_laplacian_for_unit_lambda():
+    n = (8, 12, 10)
+    pts = [uniform_points(8), geometric_points(12, 2.0), uniform_points(10)]
+    bc = (P, P, N, N, D, N)
+    vals = (0.0, 0.0, 0.5, -0.3, 1.2, 0.7)
+    x = np.random.default_rng(0).standard_normal(n)
+    lam = [np.ones((9, 12, 10)), np.ones((8, 13, 10)), np.ones((8, 12, 11))]
+    div = F.face_flux_divergence(x, lam, pts, bc, vals)
+    assert np.abs(div - F.laplacian_residual(x, np.zeros(n), pts, bc, vals)).max() <= 1e-11
+
+
+def test_split_converges_to_the_variable_coefficient_solution():
+    """splitPoissonSolver.C:110-149: repeated corrections with the lagged
+    variable part converge to -div(lambda grad x) = b (contraction factor
+    about 1 - min lambda / max lambda)."""
+    n = (16, 16, 16)
+    pts = [uniform_points(16), geometric_points(16, 2.0), uniform_points(16)]
+    bc = (P, P, N, N, P, P)
+    rng = np.random.default_rng(1)
+    lam = _smooth_lambda(n, 1.5, rng, (True, False, True))
+    b = rng.standard_normal(n)
+    V = np.diff(pts[0])[:, None, None] * np.diff(pts[1])[None, :, None] * np.diff(pts[2])[None, None, :]
+    b -= (b * V).sum() / V.sum()
+    res = [np.abs(F.variable_residual(F.split_solve(np.zeros(n), b, lam, pts, bc, n_corr=k), b, lam, pts, bc)).max()
+           for k in (1, 5, 20)]
+    assert res[0] > res[1] > res[2] and res[2] <= 1e-9
