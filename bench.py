@@ -301,6 +301,70 @@ def fft_timing(args, local, stream, mesh, barrier):
                                       "tridiagonal (read+write each way)"}
 
 
+def split_timing(args, local, stream, barrier):
+    """The split Poisson solver (briscola_b200.split) on the two-phase sphere
+    coefficient: corrections on the GPU FFT solver, with and without the GPU
+    multigrid as preconditioner; the residual of -div(lambda grad x) = f is
+    evaluated on the device."""
+    import numpy as np
+    import torch
+
+    from briscola_b200 import split, workloads
+
+    mesh, _, lam = workloads.sphere(args.size)
+    br = mesh.bricks[0]
+    dev = torch.device("cuda", local)
+    lamd = [torch.from_numpy(np.ascontiguousarray(l)).to(dev) for l in lam]
+    g = torch.Generator(device=dev).manual_seed(12)
+    f = torch.randn(br.N, dtype=torch.float64, device=dev, generator=g)
+    f -= f.mean()  # uniform cells: a compatible right-hand side for the walled box
+    h = [torch.from_numpy(br.cell_sizes(d)).to(dev) for d in range(3)]
+
+    def residual(x):
+        # -div(lambda grad x) - f with zero-gradient walls (no flux through them)
+        div = torch.zeros_like(x)
+        for d in range(3):
+            n = br.N[d]
+            dx = torch.diff(x, dim=d)  # x[q+1] - x[q] at the n-1 interior faces
+            hc = h[d]
+            dist = 0.5 * (hc[1:] + hc[:-1])
+            shape = [1, 1, 1]
+            shape[d] = -1
+            lf = lamd[d].narrow(d, 1, n - 1)
+            flux = lf * dx / dist.view(shape)
+            zero = torch.zeros_like(flux.narrow(d, 0, 1))
+            fp = torch.cat([zero, flux, zero], dim=d)  # flux through face q (0..n)
+            div += (fp.narrow(d, 1, n) - fp.narrow(d, 0, n)) / hc.view(shape)
+        r = -div - f
+        return float(r.abs().max() / f.abs().max())
+
+    out = {"workload": f"sphere {args.size}^3 coefficient (rho 1 / 1000), all walls, seeded N(0,1) zero-mean f, "
+                       "-div(lambda grad x) = f from x = 0"}
+    arms = (("fft_only_ncorr4", {"nCorr": 4}),
+            ("mg_preconditioned_ncorr2", {"nCorr": 2, "preconditioner": {
+                "type": "GPUMG", "precision": "mixed", "krylov": "fcg", "maxIter": 4, "relTol": 0, "tolerance": 0,
+                "cycleType": "V", "nSweepsPre": 2, "nSweepsPost": 2, "coarseLevel": 1}}))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    for name, extra in arms:
+        s = split.SplitPoissonSolver(mesh, dict({"solver": {"type": "FFT"}, "prediction": "off"}, **extra),
+                                     device=local)
+        x = torch.zeros_like(f)
+        s.solve(x, f, lamd)  # warm-up; sets the preconditioner's coefficients
+        reps = 3
+        barrier()
+        e0.record(stream)
+        for _ in range(reps):
+            x.zero_()
+            s.solve(x, f, lamd, constMatrix=True)
+        e1.record(stream)
+        barrier()
+        out[name] = {"ms_per_solve": round(e0.elapsed_time(e1) / reps, 3),
+                     "max_residual_over_max_rhs": residual(x)}
+        s.close()
+    return out
+
+
 def unet_timing(args, local, stream):
     """U-Net forward at the bench size (algorithmic TFLOP/s of the 3x3x3
     convolutions) and one training step at half the size."""
@@ -346,6 +410,7 @@ def main():
     ap.add_argument("--no-unet", action="store_true")
     ap.add_argument("--no-variable", action="store_true")
     ap.add_argument("--no-fft", action="store_true")
+    ap.add_argument("--no-split", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--learned-size", type=int, default=128)
     ap.add_argument("--learned-pairs", type=int, default=2000)
@@ -572,6 +637,10 @@ def main():
     if not args.no_fft:
         fft_t = fft_timing(args, local, stream, mesh, barrier)
 
+    split_t = None
+    if not args.no_split:
+        split_t = split_timing(args, local, stream, barrier)
+
     # ---- learned initial guess (config 5) ----
     learned_t = None
     if not args.no_learned:
@@ -628,6 +697,7 @@ def main():
             "unet": unet_t,
             "variable_coefficient": variable,
             "fft": fft_t,
+            "split": split_t,
             "learned": learned_t,
         }
         print(json.dumps(line), flush=True)

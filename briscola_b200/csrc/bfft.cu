@@ -804,13 +804,11 @@ __global__ void k_split_source(const double* __restrict__ x, const double* __res
                                const double* __restrict__ lam0, const double* __restrict__ lam1,
                                const double* __restrict__ lam2, double lambda0, double* __restrict__ bhat,
                                SplitGeom G) {
-    const int n0 = G.n[0], n1 = G.n[1], n2 = G.n[2];
-    const long total = (long)n0 * n1 * n2;
-    const long stride = (long)gridDim.x * blockDim.x;
-    for (long c = (long)blockIdx.x * blockDim.x + threadIdx.x; c < total; c += stride) {
-        const int k = (int)(c % n2);
-        const long ij = c / n2;
-        const int j = (int)(ij % n1), i = (int)(ij / n1);
+    const int n1 = G.n[1], n2 = G.n[2];
+    // one CTA row of k per (i, j): grid (k chunks, n1, n0)
+    const int i = blockIdx.z, j = blockIdx.y;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n2; k += gridDim.x * blockDim.x) {
+        const long c = ((long)i * n1 + j) * n2 + k;
         const int ijk[3] = {i, j, k};
         const long sx[3] = {(long)n1 * n2, n2, 1};
         const double xc = x[c];
@@ -1492,7 +1490,8 @@ int bfft_split_source(bfft_ctx* c, const double* x, const double* b, const doubl
     if (!c || !x || !b || !lam0 || !lam1 || !lam2 || !bhat || !(lambda0 > 0.0)) return BMG_BAD_ARG;
     return guarded(c, [&] {
         check(cudaSetDevice(c->dev), "cudaSetDevice");
-        k_split_source<<<4 * c->sms, kThreads, 0, c->stream>>>(x, b, lam0, lam1, lam2, lambda0, bhat, c->split);
+        const dim3 grid((unsigned)std::min((c->n[2] + 127) / 128, 8), (unsigned)c->n[1], (unsigned)c->n[0]);
+        k_split_source<<<grid, 128, 0, c->stream>>>(x, b, lam0, lam1, lam2, lambda0, bhat, c->split);
         check(cudaGetLastError(), "k_split_source");
         return (int)BMG_OK;
     });

@@ -58,6 +58,7 @@ class SplitPoissonSolver:
             self.pre = Context(self.mesh, make_options(dict(opts, device=self.device)))
         self._lib = fft.load()
         self._V = None
+        self._pre_set = False
 
     def close(self):
         self.inner.close()
@@ -68,9 +69,11 @@ class SplitPoissonSolver:
         self.inner._check(rc, what)
 
     def solve(self, x, b, lam, ddt: bool = False, dt: float = 0.0, dtFrac: float = 1.0, dt0: float = 0.0,
-              x_old=None, x_oldold=None):
+              x_old=None, x_oldold=None, constMatrix: bool = False):
         """x <- the split solution; lam: the three face-coefficient arrays
-        ((n0+1, n1, n2), (n0, n1+1, n2), (n0, n1, n2+1))."""
+        ((n0+1, n1, n2), (n0, n1+1, n2), (n0, n1, n2+1)).  constMatrix: the
+        coefficients are those of the previous solve, so the preconditioner
+        keeps its operator (the reference's solve(sys, constMatrix))."""
         import torch
 
         if lam is None:
@@ -108,7 +111,9 @@ class SplitPoissonSolver:
             if self._V is None:
                 self._V = torch.from_numpy(self.brick.cell_volumes()).to(dev)
             self.pre.set_stream(stream)
-            self.pre.set_coefficients([l.cpu().numpy() for l in lams])
+            if not (constMatrix and self._pre_set):
+                self.pre.set_coefficients([l.cpu().numpy() for l in lams])
+                self._pre_set = True
             bsys = -(self._V * bd.view(self.brick.N)).reshape(-1).contiguous()
             self.pre.solve(bsys, xd.view(-1), zero_guess=False)
 
