@@ -20,7 +20,7 @@ SMOOTHER = {"rbgs": 0, "jac": 1, "jacobi": 1}
 PRECISION = {"fp64": 0, "mixed": 1}
 KRYLOV = {"none": 0, "fcg": 1}
 CRITERION = {"initial": 0, "rhs": 1}
-DEVICE_PTRS, ZERO_GUESS = 1, 2
+DEVICE_PTRS, ZERO_GUESS, PER_VOLUME = 1, 2, 4
 
 # Every function the header declares; the loader checks they are exported.
 EXPORTED = (
@@ -29,7 +29,8 @@ EXPORTED = (
     "bmg_status_string", "bmg_last_error", "bmg_level_upload", "bmg_level_download",
     "bmg_op_colour_pass", "bmg_op_smooth", "bmg_op_residual", "bmg_op_residual_restrict",
     "bmg_op_prolong_correct", "bmg_op_coarse_solve", "bmg_coarse_level_index",
-    "bmg_residual_norm_noalloc", "bmg_level_tuning", "bmg_set_level_tuning",
+    "bmg_residual_norm_noalloc", "bmg_level_tuning", "bmg_set_level_tuning", "bmg_project_rhs",
+    "bmg_project_correct",
 )
 
 
@@ -132,6 +133,8 @@ def load(path: str = LIB_PATH):
     L.bmg_residual_norm_noalloc.argtypes = [vp, vp, ip, vp, vp, vp, ip, vp, vp]
     L.bmg_level_tuning.argtypes = [vp, ctypes.c_int, ctypes.c_int, ip, ip]
     L.bmg_set_level_tuning.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.bmg_project_rhs.argtypes = [vp, vp, vp, vp, ctypes.c_double, vp, ctypes.c_int]
+    L.bmg_project_correct.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_double]
     _lib = L
     return L
 

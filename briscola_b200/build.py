@@ -16,7 +16,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_lib", "libbmg.so")
-SOURCES = ["bmg_host.cu", "bmg_kernels.cu", "bmg_smooth_fused.cu", "bmg_krylov.cu", "bmg_noalloc.cu"]
+SOURCES = ["bmg_host.cu", "bmg_kernels.cu", "bmg_smooth_fused.cu", "bmg_krylov.cu", "bmg_noalloc.cu",
+           "bmg_project.cu"]
 HEADERS = ["bmg_internal.h", "bmg_stencil.cuh", "bmg_grid.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FFT_OUT = os.path.join(HERE, "_lib", "libbfft.so")

@@ -1709,6 +1709,51 @@ int bmg_set_level_tuning(bmg_ctx* c, int l, int prec, int stages, int chunk) {
     });
 }
 
+namespace {
+
+ProjGeom projGeom(const bmg_ctx* c) {
+    if (c->multi) throw BadArg{BMG_UNSUPPORTED, "projection steps take a single-brick mesh"};
+    const HostLevel& L = c->lv[0];
+    const HostBrick& B = L.br[0];
+    ProjGeom G{};
+    for (int d = 0; d < 3; ++d) {
+        G.n[d] = B.n[d];
+        G.per[d] = c->periodic[d];
+        G.h[d] = L.tab64 + B.to.h[d];
+    }
+    return G;
+}
+
+}  // namespace
+
+int bmg_project_rhs(bmg_ctx* c, const double* u0, const double* u1, const double* u2, double c_dt, double* out,
+                    int flags) {
+    if (!c || !u0 || !u1 || !u2 || !out || c_dt == 0.0) return BMG_BAD_ARG;
+    return guarded(c, [&] {
+        BMG_CUDA(cudaSetDevice(c->opt.device));
+        ProjGeom G = projGeom(c);
+        G.cdt = c_dt;
+        G.perVolume = (flags & BMG_PER_VOLUME) ? 1 : 0;
+        launch_project_rhs(u0, u1, u2, out, G, c->stream);
+        BMG_CUDA(cudaGetLastError());
+        return BMG_OK;
+    });
+}
+
+int bmg_project_correct(bmg_ctx* c, double* u0, double* u1, double* u2, const double* p, const double* lam0,
+                        const double* lam1, const double* lam2, double c_dt) {
+    if (!c || !u0 || !u1 || !u2 || !p) return BMG_BAD_ARG;
+    if ((lam0 || lam1 || lam2) && !(lam0 && lam1 && lam2)) return BMG_BAD_ARG;
+    return guarded(c, [&] {
+        BMG_CUDA(cudaSetDevice(c->opt.device));
+        ProjGeom G = projGeom(c);
+        G.cdt = c_dt;
+        launch_project_correct(u0, u1, u2, p, lam0, lam1, lam2, G, c->stream);
+        BMG_CUDA(cudaGetLastError());
+        return BMG_OK;
+    });
+}
+
 int bmg_level_shape(const bmg_ctx* c, int l, int brick, int n[3]) {
     if (!validLevel(c, l) || !n || brick < 0 || brick >= (int)c->lv[l].br.size()) return BMG_BAD_ARG;
     for (int d = 0; d < 3; ++d) n[d] = c->lv[l].br[brick].n[d];

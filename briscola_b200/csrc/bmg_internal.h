@@ -34,6 +34,8 @@
 #pragma once
 
 #include <cuda_runtime.h>
+
+#include <algorithm>
 #include <cstdint>
 
 namespace bmg {
@@ -195,6 +197,19 @@ void launch_fcg_update(const Bricks<double>& B, const double* p, double* r, cons
                        double* pre64, double* partials, const SolveState* st, cudaStream_t s);
 // st->l2_true from the partials of a mode-2 residual
 void launch_fcg_true_norm(const Bricks<double>& B, const double* partials, SolveState* st, cudaStream_t s);
+
+// ---- projection steps either side of the pressure solve (bmg_project.cu) ----
+struct ProjGeom {
+    int n[3];
+    int per[3];
+    const double* h[3];  // cell sizes per axis (device)
+    double cdt;          // C dt of the staggered solver's stage
+    int perVolume;       // 1: the Poisson source coloDiv(U) / (-C dt); 0: the system form -V times it
+};
+void launch_project_rhs(const double* u0, const double* u1, const double* u2, double* out, const ProjGeom& G,
+                        cudaStream_t s);
+void launch_project_correct(double* u0, double* u1, double* u2, const double* p, const double* lam0,
+                            const double* lam1, const double* lam2, const ProjGeom& G, cudaStream_t s);
 
 // compact interior <-> ghost-framed conversions
 void launch_load_b(const Bricks<double>& B, const double* compact, cudaStream_t s);

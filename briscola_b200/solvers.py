@@ -227,6 +227,32 @@ class Context:
             rc = self._lib.bmg_set_coefficients(self.h, *ptrs)
         self.check(rc, "bmg_set_coefficients")
 
+    def project_rhs(self, u, c_dt: float, out, per_volume: bool = False):
+        """out <- the pressure right-hand side coloDiv(U) / (-c_dt) of a
+        staggered projection step (system form -V times it unless
+        per_volume); u: three CUDA face arrays, out: CUDA cells."""
+        self._follow(out)
+        flags = N.PER_VOLUME if per_volume else 0
+        self.check(self._lib.bmg_project_rhs(self.h, *(a.data_ptr() for a in u), float(c_dt), out.data_ptr(), flags),
+                   "bmg_project_rhs")
+        return out
+
+    def project_correct(self, u, p, c_dt: float, lam=None):
+        """u <- u - c_dt lambda grad(p) on the faces (stagReconstruct of the
+        Poisson flux); CUDA arrays."""
+        self._follow(p)
+        lp = [None, None, None] if lam is None else [a.data_ptr() for a in lam]
+        self.check(self._lib.bmg_project_correct(self.h, *(a.data_ptr() for a in u), p.data_ptr(), *lp,
+                                                 float(c_dt)), "bmg_project_correct")
+        return u
+
+    def _follow(self, t):
+        import torch
+
+        cur = torch.cuda.current_stream(t.device).cuda_stream
+        if getattr(self, "_stream", None) != cur:
+            self.set_stream(cur)
+
     def set_stream(self, stream_ptr: int):
         self.check(self._lib.bmg_set_stream(self.h, ctypes.c_void_p(stream_ptr)), "bmg_set_stream")
         self._stream = stream_ptr

@@ -64,7 +64,8 @@ enum { BMG_CRITERION_INITIAL = 0, BMG_CRITERION_RHS = 1 };
 /* bmg_solve flags */
 enum {
     BMG_DEVICE_PTRS = 1, /* b and x are device pointers on the context's device */
-    BMG_ZERO_GUESS = 2   /* ignore the incoming x and start from zero           */
+    BMG_ZERO_GUESS = 2,  /* ignore the incoming x and start from zero           */
+    BMG_PER_VOLUME = 4   /* bmg_project_rhs: the Poisson source, not the system form */
 };
 
 typedef struct bmg_brick {
@@ -182,6 +183,26 @@ int bmg_level_tuning(const struct bmg_ctx* ctx, int level, int precision, int* s
  * fused smoother handles; chunk 1..128), e.g. to replay a tuning measured
  * in another process; the solve graph is rebuilt at the next solve */
 int bmg_set_level_tuning(struct bmg_ctx* ctx, int level, int precision, int stages, int chunk);
+
+/* ---- Either side of the solve in a projection step --------------------------
+ * Single-brick contexts, device arrays on the context's stream.  Staggered
+ * face arrays of axis d hold n[d]+1 faces along d (the face below cell q,
+ * then the top face), k fastest: u0 (n0+1) x n1 x n2, u1 n0 x (n1+1) x n2,
+ * u2 n0 x n1 x (n2+1); on a periodic axis the last face repeats the first.
+ *
+ * out (interior cells, k fastest) = the right-hand side of the pressure solve
+ * of a staggered projection, coloDiv(U) / (-c_dt) (briscolaStaggered.C:92,
+ * divergenceScheme.C:116-150), in the system form -V times it that
+ * bmg_solve takes (linearSystem.C:547-556), or as that Poisson source itself
+ * with BMG_PER_VOLUME (for the FFT solver, bfft.h). */
+int bmg_project_rhs(struct bmg_ctx* ctx, const double* u0, const double* u1, const double* u2, double c_dt,
+                    double* out, int flags);
+/* U -= c_dt * stagReconstruct(lambda faceGrad(p) A) = c_dt lambda (p_c - p_below) delta
+ * on every face (briscolaStaggered.C:96, defaultPoissonSolver.C:110-123,
+ * exSchemesReconstruction.H:187-206); lambda arrays as the face arrays of U,
+ * NULL for 1; wall faces (zero gradient) are left unchanged. */
+int bmg_project_correct(struct bmg_ctx* ctx, double* u0, double* u1, double* u2, const double* p,
+                        const double* lam0, const double* lam1, const double* lam2, double c_dt);
 
 /* ---- Residual norm without any device allocation ---------------------------
  * No counterpart in the reference: an addition for callers that must not

@@ -14,6 +14,8 @@ Follows, for one brick on one process:
                       NeumannBoundaryCondition.C:59-85 (x_g = x_c + g |c_c - c_g|)
   ghost points        src/briscolaMesh/level/levelPoints.C:198-236, 326-400
   known-answer check  applications/test/FFTPoissonSolver/Test-FFTPoissonSolver.C:11-92
+  projection steps    divergenceScheme.C:116-150 (coloDiv of a staggered field),
+                      exSchemesReconstruction.H:187-206 (stagReconstruct), briscolaStaggered.C:92-96
   split solver        src/briscolaFiniteVolume/solvers/PoissonSolvers/splitPoissonSolver/
                       splitPoissonSolver.C:53-155 (prediction, lambda0, modified source, corrections);
                       face gradient .../faceGradientSchemes/linearFaceGradientScheme/
@@ -402,3 +404,51 @@ def variable_residual(x, b, lam, points, bc, bc_values=(0.0,) * 6):
     """-div(lambda grad x) - b per cell: the equation the split solver
     approximates."""
     return -face_flux_divergence(x, lam, points, bc, bc_values) - b
+
+
+# ---- projection steps either side of the pressure solve -------------------
+
+def colo_div(u, points):
+    """coloDiv of a staggered field (divergenceScheme.C:116-150): the face
+    arrays u[d] hold n_d + 1 faces along d; sum of U A over the faces / V."""
+    n = tuple(len(p) - 1 for p in points)
+    div = np.zeros(n)
+    for d in range(3):
+        shape = [1, 1, 1]
+        shape[d] = -1
+        hc = np.diff(points[d]).reshape(shape)
+        lo = [slice(None)] * 3
+        hi = [slice(None)] * 3
+        lo[d] = slice(0, n[d])
+        hi[d] = slice(1, n[d] + 1)
+        div += (u[d][tuple(hi)] - u[d][tuple(lo)]) / hc
+    return div
+
+
+def project_correct(u, p, c_dt, points, periodic, lam=None):
+    """U - c_dt stagReconstruct(lambda faceGrad(p) A) (briscolaStaggered.C:96,
+    exSchemesReconstruction.H:187-206): face q of axis d loses
+    c_dt lambda (p_q - p_{q-1}) delta; walls keep their faces (zero
+    gradient), periodic faces wrap."""
+    out = [a.copy() for a in u]
+    n = p.shape
+    for d in range(3):
+        h = cell_sizes_with_ghosts(points[d], periodic[d])
+        delta = 1.0 / ((h[1:] + h[:-1]) / 2.0)  # faces 0..n
+        shape = [1, 1, 1]
+        shape[d] = -1
+        ext = np.concatenate([np.take(p, [n[d] - 1], axis=d), p, np.take(p, [0], axis=d)], axis=d)
+        a = [slice(None)] * 3
+        b = [slice(None)] * 3
+        a[d] = slice(1, n[d] + 2)
+        b[d] = slice(0, n[d] + 1)
+        g = (ext[tuple(a)] - ext[tuple(b)]) * delta.reshape(shape)
+        if not periodic[d]:
+            first = [slice(None)] * 3
+            last = [slice(None)] * 3
+            first[d], last[d] = 0, n[d]
+            g[tuple(first)] = 0.0
+            g[tuple(last)] = 0.0
+        lf = 1.0 if lam is None else lam[d]
+        out[d] = out[d] - c_dt * (lf * g)
+    return out

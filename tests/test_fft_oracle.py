@@ -176,3 +176,24 @@ def test_split_converges_to_the_variable_coefficient_solution():
     res = [np.abs(F.variable_residual(F.split_solve(np.zeros(n), b, lam, pts, bc, n_corr=k), b, lam, pts, bc)).max()
            for k in (1, 5, 20)]
     assert res[0] > res[1] > res[2] and res[2] <= 1e-9
+
+
+def test_projection_step_leaves_a_divergence_free_velocity():
+    """briscolaStaggered.C:92-96 restated: p from coloDiv(U) / (-C dt), then
+    U -= C dt stagReconstruct(faceGrad(p) A); the colocated divergence of the
+    corrected velocity vanishes (the consistency of coloDiv, the solver's
+    Laplacian and the reconstruction)."""
+    n = (16, 24, 16)
+    pts = [uniform_points(16), geometric_points(24, 2.0), uniform_points(16)]
+    bc = (P, P, N, N, P, P)
+    rng = np.random.default_rng(0)
+    u = [rng.standard_normal((17, 24, 16)), rng.standard_normal((16, 25, 16)), rng.standard_normal((16, 24, 17))]
+    u[0][-1] = u[0][0]
+    u[2][:, :, -1] = u[2][:, :, 0]
+    u[1][:, 0, :] = 0.0  # no flux through the walls
+    u[1][:, -1, :] = 0.0
+    cdt = 0.05
+    p = F.solve(F.colo_div(u, pts) / (-cdt), pts, bc)
+    un = F.project_correct(u, p, cdt, pts, (True, False, True))
+    assert np.abs(F.colo_div(u, pts)).max() > 10.0
+    assert np.abs(F.colo_div(un, pts)).max() <= 1e-11
