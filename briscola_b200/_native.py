@@ -68,6 +68,7 @@ class Options(ctypes.Structure):
         ("krylov", ctypes.c_int),
         ("criterion", ctypes.c_int),
         ("fused_chunk", ctypes.c_int),
+        ("fuse_coarse", ctypes.c_int),
     ]
 
 

@@ -123,6 +123,7 @@ struct bmg_ctx {
     std::vector<HostLevel> lv;
     std::vector<std::vector<BrickTransfer>> tr;  // [level][brick]
     int lc = 0;  // coarse solve level
+    int tail = -1;  // first level of the single-CTA coarse cycle, -1: none
     double* ainv = nullptr;
     int* cidx = nullptr;
     int ncoarse = 0;
@@ -1131,8 +1132,60 @@ int levelReps(const bmg_ctx* c, int l) {  // MG.H:106-124
 // MG.C:19-130.  x(l) = 0 for l > 0 is done by the restriction step that
 // produces b(l).  The finest-level residual is always recomputed after
 // pre-smoothing (the reference skips it on the first repetition, MG.C:72).
+// The levels from tailFirst(c) to the coarse solve level run in one CTA
+// (k_tail_cycle) when the cycle is a single-brick V cycle with red-black
+// smoothing and factor-2 quad transfers on every one of them; -1 otherwise.
+int tailFirst(const bmg_ctx* c) {
+    if (!c->opt.fuse_coarse || c->multi || c->opt.cycle_type != BMG_CYCLE_V ||
+        c->opt.smoother != BMG_SMOOTHER_RBGS)
+        return -1;
+    const int lc = c->lc;
+    int first = lc;
+    while (first > 0 && c->lv[first - 1].ncell <= kTailCells) --first;
+    if (first == lc || lc - first + 1 > kMaxTail) return -1;
+    for (int q = first; q < lc; ++q) {
+        const HostBrick& F = c->lv[q].br[0];
+        const HostBrick& C = c->lv[q + 1].br[0];
+        if (F.n[2] % 4 || C.R[0] != 2 || C.R[1] != 2 || C.R[2] != 2) return -1;
+        const int lens[2] = {(int)colourSequence(c->lv[q], c->opt.n_pre).size(),
+                             (int)colourSequence(c->lv[q], c->opt.n_post).size()};
+        if (lens[0] > kMaxSeq || lens[1] > kMaxSeq) return -1;
+    }
+    return first;
+}
+
+template <typename T>
+void tailCycle(bmg_ctx* c, int first) {
+    TailPlan<T> P{};
+    P.nlev = c->lc - first + 1;
+    for (int q = 0; q < P.nlev; ++q) {
+        const int l = first + q;
+        P.v[q] = bricks<T>(c, l).v[0];
+        if (l < c->lc) {
+            P.t[q] = ttabs(c, l).t[0];
+            const std::vector<int> pre = c->opt.n_pre > 0 ? colourSequence(c->lv[l], c->opt.n_pre) : std::vector<int>();
+            const std::vector<int> post =
+                c->opt.n_post > 0 ? colourSequence(c->lv[l], c->opt.n_post) : std::vector<int>();
+            P.npre[q] = (int)pre.size();
+            P.npost[q] = (int)post.size();
+            for (size_t e = 0; e < pre.size(); ++e) P.pre[q][e] = pre[e];
+            for (size_t e = 0; e < post.size(); ++e) P.post[q][e] = post[e];
+        }
+        c->visits[l]++;
+    }
+    P.ainv = c->ainv;
+    P.cidx = c->cidx;
+    P.ncoarse = c->ncoarse;
+    c->launches += 1;
+    if (c->variable)
+        launch_tail_cycle<T, true>(P, c->stream);
+    else
+        launch_tail_cycle<T, false>(P, c->stream);
+}
+
 template <typename T>
 void cycle(bmg_ctx* c, int l) {
+    if (l == c->tail) return tailCycle<T>(c, l);
     if (c->opt.n_pre > 0) smooth<T>(c, l, c->opt.n_pre);
     if (l < c->lc) {
         const int reps = levelReps(c, l);
@@ -1565,6 +1618,7 @@ int bmg_default_options(bmg_options* o) {
     o->krylov = BMG_KRYLOV_NONE;
     o->criterion = BMG_CRITERION_INITIAL;
     o->fused_chunk = 64;
+    o->fuse_coarse = 1;
     return BMG_OK;
 }
 
@@ -1594,6 +1648,7 @@ int bmg_create(bmg_ctx** out, const bmg_mesh_desc* mesh, const bmg_options* opts
         configure_fused_kernels();
         build(c, std::move(L0));
         configureCoarse(c);
+        c->tail = tailFirst(c);
         applyChunk(c);
         if (c->opt.autotune) autotune(c);
         return BMG_OK;
@@ -1628,6 +1683,7 @@ int bmg_set_options(bmg_ctx* c, const bmg_options* o) {
         destroyGraph(c);
         BMG_CUDA(cudaSetDevice(c->opt.device));
         if (coarseChanged) configureCoarse(c);
+        c->tail = tailFirst(c);
         if (!o->autotune) applyChunk(c);
         if (retune) autotune(c);
         return BMG_OK;

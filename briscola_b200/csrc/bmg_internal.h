@@ -146,6 +146,28 @@ constexpr int kFusedMaxStages = 3;
 
 constexpr int kReduceThreads = 256;
 
+// The coarse end of a V-cycle in one CTA (k_tail_cycle): levels v[0] (the
+// first fused level) .. v[nlev-1] (the coarse solve level) of one brick,
+// the transfers between them, and each level's colour sequences.
+constexpr int kMaxTail = 6;
+constexpr int kMaxSeq = 16;
+constexpr int kTailThreads = 512;
+constexpr long kTailCells = 4096;  // levels this small run in the fused tail
+
+template <typename T>
+struct TailPlan {
+    LevelView<T> v[kMaxTail];
+    TransferTabs t[kMaxTail];
+    int pre[kMaxTail][kMaxSeq];
+    int post[kMaxTail][kMaxSeq];
+    int npre[kMaxTail];
+    int npost[kMaxTail];
+    int nlev;
+    const double* ainv;
+    const int* cidx;
+    int ncoarse;
+};
+
 // ---- launchers (bmg_kernels.cu) -------------------------------------------
 template <typename T, bool VAR>
 void launch_colour_pass(const Bricks<T>& B, int colour, cudaStream_t s);
@@ -158,6 +180,8 @@ void launch_prolong_correct(const Bricks<T>& F, const Bricks<T>& C, const Transf
 // dense solve on the coarse level; cidx lists the slab index of each unknown
 template <typename T>
 void launch_coarse_solve(const Bricks<T>& C, const double* ainv, const int* cidx, int n, cudaStream_t s);
+template <typename T, bool VAR>
+void launch_tail_cycle(const TailPlan<T>& P, cudaStream_t s);
 template <typename T, bool VAR>
 void launch_residual_out(const Bricks<T>& B, double* r_unscaled_compact, cudaStream_t s);
 // x[dst[q]] = x[src[q]]: ghost refresh between bricks

@@ -111,93 +111,86 @@ struct Row4<double> {
 };
 
 // ---------------------------------------------------------------------------
-// Red-black colour pass, four cells per thread and row: the thread owns the
-// k-quad (4p .. 4p+3) of R consecutive rows j0 .. j0+R-1 and updates the two
-// cells of the requested colour in each.  The rows j0-1 .. j0+R, the i
-// neighbours, b and the k couplings are read as whole vectors (rows shared
-// between the R updates are read once), the index arithmetic is done once,
-// and every quad is written back as one vector (the other colour's values
-// are unchanged during the pass, so writing them back is safe; a quad is
-// never a ghost).  The arithmetic is gs_value's, so results are
+// Red-black colour pass, four cells per thread: the thread owns the k-quad
+// (4p .. 4p+3) of one row and updates the two cells of the requested colour.
+// The rows j-1, j, j+1, the i neighbours, b and the k couplings are read as
+// whole vectors, and the quad is written back as one vector (the other
+// colour's values are unchanged during the pass, so writing them back is
+// safe; a quad is never a ghost).  colour_quad_item is shared with the
+// single-CTA coarse cycle (k_tail_cycle).  The arithmetic is gs_value's, so results are
 // bit-identical to k_colour_pass and the fused smoother.  Needs every
 // brick's n2 % 4 == 0.
 // ---------------------------------------------------------------------------
-template <typename T, bool VAR, int R>
+template <typename T, bool VAR>
+__device__ __forceinline__ void colour_quad_item(const LevelView<T>& L, int i, int j, int p, int colour) {
+    const int k0 = 4 * p;
+    const long c = L.base + (long)i * L.si + (long)j * L.sj + k0;
+    const T* x = L.x;
+    // rows j-1, j, j+1 of this plane (j+1 may be the ghost row)
+    T ym[4], own[4], yp[4], xm[4], xp[4], bb[4], wkl[4], wkh[4];
+    Row4<T>::ld(x + c - L.sj, ym);
+    Row4<T>::ld(x + c, own);
+    Row4<T>::ld(x + c + L.sj, yp);
+    Row4<T>::ld(x + c - L.si, xm);
+    Row4<T>::ld(x + c + L.si, xp);
+    Row4<T>::ld(L.b + c, bb);
+    Row4<T>::ldg4(L.tab + L.to.wl[2] + k0, wkl);
+    Row4<T>::ldg4(L.tab + L.to.wh[2] + k0, wkh);
+    const T wil = ldg(L.tab + L.to.wl[0] + i), wih = ldg(L.tab + L.to.wh[0] + i);
+    const T left = x[c - 1], right = x[c + 4];
+    const T wjl = ldg(L.tab + L.to.wl[1] + j), wjh = ldg(L.tab + L.to.wh[1] + j);
+    // the two cells of the colour: (0, 2) or (1, 3); every array index
+    // below is a compile-time constant picked by a select
+    const bool odd = ((colour ^ (i + j + k0 + L.cpar)) & 1) != 0;
+#define BMG_SEL(a, e) (odd ? a[(e) + 1] : a[e])
+    T w0[6] = {wil, wih, wjl, wjh, BMG_SEL(wkl, 0), BMG_SEL(wkh, 0)};
+    T w2[6] = {wil, wih, wjl, wjh, BMG_SEL(wkl, 2), BMG_SEL(wkh, 2)};
+    if (VAR) {
+        T l0[4], l0p[4], l1[4], l1p[4], l2[4];
+        Row4<T>::ldg4(L.lam0 + c, l0);
+        Row4<T>::ldg4(L.lam0 + c + L.si, l0p);
+        Row4<T>::ldg4(L.lam1 + c, l1);
+        Row4<T>::ldg4(L.lam1 + c + L.sj, l1p);
+        Row4<T>::ldg4(L.lam2 + c, l2);
+        const T l2r = ldg(L.lam2 + c + 4);
+        w0[0] *= BMG_SEL(l0, 0);
+        w0[1] *= BMG_SEL(l0p, 0);
+        w0[2] *= BMG_SEL(l1, 0);
+        w0[3] *= BMG_SEL(l1p, 0);
+        w0[4] *= BMG_SEL(l2, 0);
+        w0[5] *= BMG_SEL(l2, 1);
+        w2[0] *= BMG_SEL(l0, 2);
+        w2[1] *= BMG_SEL(l0p, 2);
+        w2[2] *= BMG_SEL(l1, 2);
+        w2[3] *= BMG_SEL(l1p, 2);
+        w2[4] *= BMG_SEL(l2, 2);
+        w2[5] *= odd ? l2r : l2[3];
+    }
+    const T xn0[6] = {BMG_SEL(xm, 0), BMG_SEL(xp, 0), BMG_SEL(ym, 0), BMG_SEL(yp, 0), odd ? own[0] : left,
+                      odd ? own[2] : own[1]};
+    const T xn2[6] = {BMG_SEL(xm, 2), BMG_SEL(xp, 2), BMG_SEL(ym, 2), BMG_SEL(yp, 2), odd ? own[2] : own[1],
+                      odd ? right : own[3]};
+    const T v0 = gs_value(w0, xn0, BMG_SEL(bb, 0));
+    const T v2 = gs_value(w2, xn2, BMG_SEL(bb, 2));
+#undef BMG_SEL
+    const T out[4] = {odd ? own[0] : v0, odd ? v0 : own[1], odd ? own[2] : v2, odd ? v2 : own[3]};
+    Row4<T>::st(L.x + c, out);
+    // periodic images of the two updated cells
+    if (L.per0 | L.per1 | L.per2) {
+        const int q0 = odd ? 1 : 0;
+        store_x(L, c + q0, i, j, k0 + q0, v0);
+        store_x(L, c + q0 + 2, i, j, k0 + q0 + 2, v2);
+    }
+}
+
+template <typename T, bool VAR>
 __global__ void __launch_bounds__(256) k_colour_quad(Bricks<T> B, int colour) {
     int i;
     const LevelView<T>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j0 = (blockIdx.y * blockDim.y + threadIdx.y) * R;
-    const int k0 = 4 * p;
-    if (j0 >= L.n1 || k0 >= L.n2) return;
-    const long c0 = L.base + (long)i * L.si + (long)j0 * L.sj + k0;
-    const T* x = L.x;
-    // rows j0-1 .. j0+R of this plane (the last may be the ghost row)
-    T row[R + 2][4], xm[R][4], xp[R][4], bb[R][4], wkl[4], wkh[4];
-#pragma unroll
-    for (int r = 0; r < R + 2; ++r) Row4<T>::ld(x + c0 + (long)(r - 1) * L.sj, row[r]);
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        Row4<T>::ld(x + c0 + r * L.sj - L.si, xm[r]);
-        Row4<T>::ld(x + c0 + r * L.sj + L.si, xp[r]);
-        Row4<T>::ld(L.b + c0 + r * L.sj, bb[r]);
-    }
-    Row4<T>::ldg4(L.tab + L.to.wl[2] + k0, wkl);
-    Row4<T>::ldg4(L.tab + L.to.wh[2] + k0, wkh);
-    const T wil = ldg(L.tab + L.to.wl[0] + i), wih = ldg(L.tab + L.to.wh[0] + i);
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int j = j0 + r;
-        if (j >= L.n1) break;
-        const long c = c0 + r * L.sj;
-        const T* own = row[r + 1];
-        const T left = x[c - 1], right = x[c + 4];
-        const T wjl = ldg(L.tab + L.to.wl[1] + j), wjh = ldg(L.tab + L.to.wh[1] + j);
-        // the two cells of the colour: (0, 2) or (1, 3); every array index
-        // below is a compile-time constant picked by a select
-        const bool odd = ((colour ^ (i + j + k0 + L.cpar)) & 1) != 0;
-#define BMG_SEL(a, e) (odd ? a[(e) + 1] : a[e])
-        T w0[6] = {wil, wih, wjl, wjh, BMG_SEL(wkl, 0), BMG_SEL(wkh, 0)};
-        T w2[6] = {wil, wih, wjl, wjh, BMG_SEL(wkl, 2), BMG_SEL(wkh, 2)};
-        if (VAR) {
-            T l0[4], l0p[4], l1[4], l1p[4], l2[4];
-            Row4<T>::ldg4(L.lam0 + c, l0);
-            Row4<T>::ldg4(L.lam0 + c + L.si, l0p);
-            Row4<T>::ldg4(L.lam1 + c, l1);
-            Row4<T>::ldg4(L.lam1 + c + L.sj, l1p);
-            Row4<T>::ldg4(L.lam2 + c, l2);
-            const T l2r = ldg(L.lam2 + c + 4);
-            w0[0] *= BMG_SEL(l0, 0);
-            w0[1] *= BMG_SEL(l0p, 0);
-            w0[2] *= BMG_SEL(l1, 0);
-            w0[3] *= BMG_SEL(l1p, 0);
-            w0[4] *= BMG_SEL(l2, 0);
-            w0[5] *= BMG_SEL(l2, 1);
-            w2[0] *= BMG_SEL(l0, 2);
-            w2[1] *= BMG_SEL(l0p, 2);
-            w2[2] *= BMG_SEL(l1, 2);
-            w2[3] *= BMG_SEL(l1p, 2);
-            w2[4] *= BMG_SEL(l2, 2);
-            w2[5] *= odd ? l2r : l2[3];
-        }
-        const T* ym = row[r];
-        const T* yp = row[r + 2];
-        const T xn0[6] = {BMG_SEL(xm[r], 0), BMG_SEL(xp[r], 0), BMG_SEL(ym, 0), BMG_SEL(yp, 0),
-                          odd ? own[0] : left, odd ? own[2] : own[1]};
-        const T xn2[6] = {BMG_SEL(xm[r], 2), BMG_SEL(xp[r], 2), BMG_SEL(ym, 2), BMG_SEL(yp, 2),
-                          odd ? own[2] : own[1], odd ? right : own[3]};
-        const T v0 = gs_value(w0, xn0, BMG_SEL(bb[r], 0));
-        const T v2 = gs_value(w2, xn2, BMG_SEL(bb[r], 2));
-#undef BMG_SEL
-        const T out[4] = {odd ? own[0] : v0, odd ? v0 : own[1], odd ? own[2] : v2, odd ? v2 : own[3]};
-        Row4<T>::st(L.x + c, out);
-        // periodic images of the two updated cells
-        if (L.per0 | L.per1 | L.per2) {
-            const int q0 = odd ? 1 : 0;
-            store_x(L, c + q0, i, j, k0 + q0, v0);
-            store_x(L, c + q0 + 2, i, j, k0 + q0 + 2, v2);
-        }
-    }
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (j >= L.n1 || 4 * p >= L.n2) return;
+    colour_quad_item<T, VAR>(L, i, j, p, colour);
 }
 
 // Damped Jacobi (omega = 0.8, jacSmoother.C:15) into a temporary, then copy.
@@ -325,16 +318,9 @@ __global__ void __launch_bounds__(256) k_prolong_correct(Bricks<T> FB, Bricks<T>
 // residual of each of its four fine rows from whole-vector loads.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) k_prolong_quad(Bricks<T> FB, Bricks<T> CB, TransferSet ts) {
-    int i;
-    const int b = brick_of(FB, blockIdx.z, i);
-    const LevelView<T>& F = FB.v[b];
-    const LevelView<T>& C = CB.v[b];
-    const TransferTabs& t = ts.t[b];
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void prolong_quad_item(const LevelView<T>& F, const LevelView<T>& C,
+                                                  const TransferTabs& t, int i, int j, int p) {
     const int k0 = 4 * p;
-    if (j >= F.n1 || k0 >= F.n2) return;
     const int* pidx = t.pidx;
     const T* pw;
     if constexpr (sizeof(T) == 8)
@@ -373,17 +359,20 @@ __global__ void __launch_bounds__(256) k_prolong_quad(Bricks<T> FB, Bricks<T> CB
     }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(256) k_prolong_quad(Bricks<T> FB, Bricks<T> CB, TransferSet ts) {
+    int i;
+    const int b = brick_of(FB, blockIdx.z, i);
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (j >= FB.v[b].n1 || 4 * p >= FB.v[b].n2) return;
+    prolong_quad_item<T>(FB.v[b], CB.v[b], ts.t[b], i, j, p);
+}
+
 template <typename T, bool VAR>
-__global__ void __launch_bounds__(256) k_restrict_quad(Bricks<T> FB, Bricks<T> CB, TransferSet ts) {
-    int I;
-    const int b = brick_of(CB, blockIdx.z, I);
-    const LevelView<T>& C = CB.v[b];
-    const LevelView<T>& F = FB.v[b];
-    const TransferTabs& t = ts.t[b];
-    const int P = blockIdx.x * blockDim.x + threadIdx.x;  // coarse k-pair
-    const int J = blockIdx.y * blockDim.y + threadIdx.y;
-    const int K0 = 2 * P;
-    if (J >= C.n1 || K0 >= C.n2) return;
+__device__ __forceinline__ void restrict_quad_item(const LevelView<T>& F, const LevelView<T>& C,
+                                                   const TransferTabs& t, int I, int J, int P) {
+    const int K0 = 2 * P;  // the thread's coarse k-pair
     const T* ratio;
     if constexpr (sizeof(T) == 8)
         ratio = reinterpret_cast<const T*>(t.ratio64);
@@ -450,16 +439,26 @@ __global__ void __launch_bounds__(256) k_restrict_quad(Bricks<T> FB, Bricks<T> C
     C.b[cc + 1] = acc1;
 }
 
+template <typename T, bool VAR>
+__global__ void __launch_bounds__(256) k_restrict_quad(Bricks<T> FB, Bricks<T> CB, TransferSet ts) {
+    int I;
+    const int b = brick_of(CB, blockIdx.z, I);
+    const int P = blockIdx.x * blockDim.x + threadIdx.x;
+    const int J = blockIdx.y * blockDim.y + threadIdx.y;
+    if (J >= CB.v[b].n1 || 2 * P >= CB.v[b].n2) return;
+    restrict_quad_item<T, VAR>(FB.v[b], CB.v[b], ts.t[b], I, J, P);
+}
+
 // ---------------------------------------------------------------------------
 // Coarse direct solve: x = inverse(A'_pinned) b' with b'(0) = 0 (MG.C:37-40,
 // solver.C:201-231, APLU.C:91-128).  One CTA; the inverse is factored once
 // per matrix on the host in FP64.  cidx gives the slab index of every
 // unknown (bricks one after another, k fastest).
 // ---------------------------------------------------------------------------
+// one CTA (any multiple of 32 threads); sb: n doubles of shared memory
 template <typename T>
-__global__ void __launch_bounds__(256) k_coarse_solve(Bricks<T> CB, const double* __restrict__ ainv,
-                                                      const int* __restrict__ cidx, int n) {
-    extern __shared__ double sb[];
+__device__ __forceinline__ void coarse_solve_block(const Bricks<T>& CB, const double* __restrict__ ainv,
+                                                   const int* __restrict__ cidx, int n, double* sb) {
     const T* bsrc = CB.v[0].b;
     for (int q = threadIdx.x; q < n; q += blockDim.x) sb[q] = q == 0 ? 0.0 : (double)bsrc[cidx[q]];
     __syncthreads();
@@ -479,6 +478,71 @@ __global__ void __launch_bounds__(256) k_coarse_solve(Bricks<T> CB, const double
                 CB.v[0].x[cidx[r]] = (T)s;
             }
         }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_coarse_solve(Bricks<T> CB, const double* __restrict__ ainv,
+                                                      const int* __restrict__ cidx, int n) {
+    extern __shared__ double sb[];
+    coarse_solve_block<T>(CB, ainv, cidx, n, sb);
+}
+
+// ---------------------------------------------------------------------------
+// The coarse end of a V-cycle in one CTA: on the small levels every pass is
+// a few thousand cells, so a launch per pass costs more than the pass.  The
+// levels from P.first down to the coarse solve level run here with a barrier
+// between passes: pre-smoothing colour passes, restriction (and the zeroed
+// coarse x), the dense coarse solve, then prolongation and post-smoothing on
+// the way up -- the same per-item functions as the per-pass kernels, so the
+// result is bit-identical to the per-pass path (MG.C:19-130, V cycle).
+// ---------------------------------------------------------------------------
+template <typename T, bool VAR>
+__global__ void __launch_bounds__(kTailThreads) k_tail_cycle(TailPlan<T> P) {
+    extern __shared__ double sb[];
+    const int nt = blockDim.x;
+    const int nl = P.nlev;
+    auto smooth = [&](int q, const int* seq, int nseq) {
+        const LevelView<T>& L = P.v[q];
+        const int nq = L.n2 / 4;
+        const int items = L.n0 * L.n1 * nq;
+        for (int s = 0; s < nseq; ++s) {
+            for (int it = threadIdx.x; it < items; it += nt) {
+                const int p = it % nq, ij = it / nq;
+                colour_quad_item<T, VAR>(L, ij / L.n1, ij % L.n1, p, seq[s]);
+            }
+            __syncthreads();
+        }
+    };
+    for (int q = 0; q < nl - 1; ++q) {
+        smooth(q, P.pre[q], P.npre[q]);
+        const LevelView<T>& F = P.v[q];
+        const LevelView<T>& C = P.v[q + 1];
+        const int np = C.n2 / 2;
+        const int items = C.n0 * C.n1 * np;
+        for (int it = threadIdx.x; it < items; it += nt) {
+            const int pp = it % np, IJ = it / np;
+            restrict_quad_item<T, VAR>(F, C, P.t[q], IJ / C.n1, IJ % C.n1, pp);
+        }
+        // x(q+1) = 0 over the whole slab (the per-pass path's memset)
+        for (long c = threadIdx.x; c < C.cells; c += nt) C.x[c] = T(0);
+        __syncthreads();
+    }
+    Bricks<T> CB{};
+    CB.v[0] = P.v[nl - 1];
+    CB.nb = 1;
+    coarse_solve_block<T>(CB, P.ainv, P.cidx, P.ncoarse, sb);
+    __syncthreads();
+    for (int q = nl - 2; q >= 0; --q) {
+        const LevelView<T>& F = P.v[q];
+        const int nq = F.n2 / 4;
+        const int items = F.n0 * F.n1 * nq;
+        for (int it = threadIdx.x; it < items; it += nt) {
+            const int p = it % nq, ij = it / nq;
+            prolong_quad_item<T>(F, P.v[q + 1], P.t[q], ij / F.n1, ij % F.n1, p);
+        }
+        __syncthreads();
+        smooth(q, P.post[q], P.npost[q]);
     }
 }
 
@@ -720,7 +784,7 @@ void launch_colour_pass(const Bricks<T>& B, int colour, cudaStream_t s) {
         // on the 256^3 level and costs registers in FP64
         const int nq = B.max2 / 4;
         const dim3 blk = nq >= 32 ? dim3(32, 8, 1) : nq >= 8 ? dim3(8, 32, 1) : dim3(2, 128, 1);
-        k_colour_quad<T, VAR, 1><<<grid_for(B, nq, blk), blk, 0, s>>>(B, colour);
+        k_colour_quad<T, VAR><<<grid_for(B, nq, blk), blk, 0, s>>>(B, colour);
         return;
     }
     const int pairs = (B.max2 + 1) / 2;
@@ -770,6 +834,11 @@ void launch_prolong_correct(const Bricks<T>& F, const Bricks<T>& C, const Transf
 template <typename T>
 void launch_coarse_solve(const Bricks<T>& C, const double* ainv, const int* cidx, int n, cudaStream_t s) {
     k_coarse_solve<T><<<1, 256, n * sizeof(double), s>>>(C, ainv, cidx, n);
+}
+
+template <typename T, bool VAR>
+void launch_tail_cycle(const TailPlan<T>& P, cudaStream_t s) {
+    k_tail_cycle<T, VAR><<<1, kTailThreads, P.ncoarse * sizeof(double), s>>>(P);
 }
 
 template <typename T>
@@ -854,6 +923,10 @@ template void launch_prolong_correct<float>(const Bricks<float>&, const Bricks<f
                                             cudaStream_t);
 template void launch_coarse_solve<double>(const Bricks<double>&, const double*, const int*, int, cudaStream_t);
 template void launch_coarse_solve<float>(const Bricks<float>&, const double*, const int*, int, cudaStream_t);
+template void launch_tail_cycle<double, false>(const TailPlan<double>&, cudaStream_t);
+template void launch_tail_cycle<double, true>(const TailPlan<double>&, cudaStream_t);
+template void launch_tail_cycle<float, false>(const TailPlan<float>&, cudaStream_t);
+template void launch_tail_cycle<float, true>(const TailPlan<float>&, cudaStream_t);
 template void launch_fill_ghosts<double>(double*, const int*, const int*, long, cudaStream_t);
 template void launch_fill_ghosts<float>(float*, const int*, const int*, long, cudaStream_t);
 template void launch_residual_norm<false>(const Bricks<double>&, int, double*, float*, cudaStream_t);

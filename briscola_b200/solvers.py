@@ -395,6 +395,7 @@ def make_options(d: Dictionary | dict | None = None, **over) -> N.Options:
         o.fused = 3 if _switch(fused) else 0
     o.autotune = int(_switch(d.get("autotune", "on")))
     o.fused_chunk = int(_scalar(d.get("fusedChunk", 64)))
+    o.fuse_coarse = int(_switch(d.get("fuseCoarse", "on")))
     o.device = _label(d.get("device", 0))
     o.timeout_ms = _scalar(d.get("timeoutMs", 0))
     kr = str(d.get("krylov", "none"))

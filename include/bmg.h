@@ -106,6 +106,9 @@ typedef struct bmg_options {
     int criterion;      /* criterion (initial): BMG_CRITERION_*                */
     int fused_chunk;    /* fusedChunk (64): planes along i per CTA of the
                            fused smoother when autotune is off (1..128)        */
+    int fuse_coarse;    /* fuseCoarse (1): run the levels of at most 4096
+                           cells and the coarse solve of a single-brick V
+                           cycle in one kernel                                 */
 } bmg_options;
 
 typedef struct bmg_report {
