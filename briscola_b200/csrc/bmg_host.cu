@@ -1337,7 +1337,7 @@ void fcgStep(bmg_ctx* c, const T* z, float* pre32, double* pre64, bool setCondit
     else
         launch_fcg_direction<T, false>(V, z, c->fp, c->fq, c->partials, c->st, s);
     launch_fcg_update(V, c->fp, c->fr, c->fq, pre32, pre64, c->partials, c->st, s);
-    launch_finalize(V, c->partials, c->st, 1, c->cond, setCondition ? 1 : 0, s);
+    launch_finalize_n(c->partials, fcg_partials(V), c->st, 1, c->cond, setCondition ? 1 : 0, s);
     c->launches += 6;
 }
 

@@ -219,6 +219,11 @@ void launch_fcg_direction(const Bricks<double>& B, const T* z, double* p, double
 // partials of ||V r||^2
 void launch_fcg_update(const Bricks<double>& B, const double* p, double* r, const double* q, float* pre32,
                        double* pre64, double* partials, const SolveState* st, cudaStream_t s);
+// number of per-block partials the FCG dots / direction / update kernels write
+long fcg_partials(const Bricks<double>& B);
+// the convergence decision from n partials (as launch_finalize)
+void launch_finalize_n(const double* partials, long n, SolveState* st, int mode, cudaGraphConditionalHandle cond,
+                       int setCondition, cudaStream_t s);
 // st->l2_true from the partials of a mode-2 residual
 void launch_fcg_true_norm(const Bricks<double>& B, const double* partials, SolveState* st, cudaStream_t s);
 

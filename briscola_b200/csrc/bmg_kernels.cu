@@ -864,6 +864,11 @@ void launch_finalize(const Bricks<double>& B, const double* partials, SolveState
     k_finalize<<<1, kFinalThreads, 0, s>>>(partials, reduce_blocks(B), st, mode, cond, setCondition);
 }
 
+void launch_finalize_n(const double* partials, long n, SolveState* st, int mode, cudaGraphConditionalHandle cond,
+                       int setCondition, cudaStream_t s) {
+    k_finalize<<<1, kFinalThreads, 0, s>>>(partials, n, st, mode, cond, setCondition);
+}
+
 void launch_mean(const Bricks<double>& B, double* partials, SolveState* st, cudaStream_t s) {
     const dim3 blk = block_for(B.max2);
     k_mean_partials<<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, partials);

@@ -20,6 +20,8 @@
 // block; single-block kernels add the partials in a fixed order and derive
 // the scalars on the device, so the loop runs inside the solve graph.
 
+#include <algorithm>
+
 #include "bmg_grid.cuh"
 #include "bmg_stencil.cuh"
 
@@ -188,7 +190,185 @@ __global__ void __launch_bounds__(kFinalThreads) k_fcg_true_norm(const double* p
     if (threadIdx.x == 0) st->l2_true = sqrt(a);
 }
 
+// ---- quad versions: a thread owns the k-quad of one row (four cells, vector
+// loads) and the grid strides over the planes, so a reduction leaves few
+// per-block partials for the one-block kernels to add.  Same per-cell
+// arithmetic as the kernels above; used when every brick's n2 % 4 == 0.
+
+constexpr int kQuadPlanes = 64;  // grid z: plane groups
+
+template <typename T>
+struct Quad4;
+template <>
+struct Quad4<double> {
+    static __device__ __forceinline__ void ld(const double* p, double v[4]) {
+        const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+        v[0] = a.x;
+        v[1] = a.y;
+        v[2] = b.x;
+        v[3] = b.y;
+    }
+    static __device__ __forceinline__ void st(double* p, const double v[4]) {
+        reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+        reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+    }
+};
+template <>
+struct Quad4<float> {
+    static __device__ __forceinline__ void ld(const float* p, float v[4]) {
+        const float4 a = *reinterpret_cast<const float4*>(p);
+        v[0] = a.x;
+        v[1] = a.y;
+        v[2] = a.z;
+        v[3] = a.w;
+    }
+    static __device__ __forceinline__ void st(float* p, const float v[4]) {
+        *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    }
+};
+
+// the quad grid: x over k-quads (16 per block), y over rows (16 per block),
+// z over plane groups; every thread visits planes z, z + gridDim.z, ...
+#define BMG_QUAD_LOOP(B, ...)                                                              \
+    {                                                                                      \
+        const int qx = blockIdx.x * blockDim.x + threadIdx.x;                              \
+        const int j = blockIdx.y * blockDim.y + threadIdx.y;                               \
+        for (int zp = blockIdx.z; zp < (B).z0[(B).nb]; zp += gridDim.z) {                  \
+            int i;                                                                         \
+            const LevelView<double>& L = (B).v[brick_of((B), zp, i)];                      \
+            const int k0 = 4 * qx;                                                         \
+            if (j < L.n1 && k0 < L.n2) {                                                   \
+                const long c = L.base + (long)i * L.si + (long)j * L.sj + k0;              \
+                const double hij = L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j];        \
+                double hk[4];                                                              \
+                Quad4<double>::ld(L.tab64 + L.to.h[2] + k0, hk);                           \
+                __VA_ARGS__                                                                \
+            }                                                                              \
+        }                                                                                  \
+    }
+
+template <typename T>
+__global__ void __launch_bounds__(kReduceThreads) k_fcg_dots4(Bricks<double> B, const T* z, const double* r,
+                                                              const double* q, double* partials, long nblocks) {
+    __shared__ double sh[kReduceThreads / 32];
+    double a1 = 0.0, a2 = 0.0;
+    BMG_QUAD_LOOP(B, {
+        T zq[4];
+        double rq[4], qq[4];
+        Quad4<T>::ld(z + c, zq);
+        Quad4<double>::ld(r + c, rq);
+        Quad4<double>::ld(q + c, qq);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const double Vz = (hij * hk[e]) * (double)zq[e];
+            a1 += Vz * rq[e];
+            a2 += Vz * qq[e];
+        }
+    })
+    a1 = block_sum<kReduceThreads>(a1, sh);
+    a2 = block_sum<kReduceThreads>(a2, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        const long bid = block_id();
+        partials[bid] = a1;
+        partials[nblocks + bid] = a2;
+    }
+}
+
+template <typename T, bool VAR>
+__global__ void __launch_bounds__(kReduceThreads) k_fcg_direction4(Bricks<double> B, const T* z, double* p,
+                                                                   double* q, double* partials,
+                                                                   const SolveState* st) {
+    __shared__ double sh[kReduceThreads / 32];
+    const double beta = st->beta;
+    double a = 0.0;
+    BMG_QUAD_LOOP(B, {
+        T zc[4], zim[4], zip[4], zjm[4], zjp[4];
+        Quad4<T>::ld(z + c, zc);
+        Quad4<T>::ld(z + c - L.si, zim);
+        Quad4<T>::ld(z + c + L.si, zip);
+        Quad4<T>::ld(z + c - L.sj, zjm);
+        Quad4<T>::ld(z + c + L.sj, zjp);
+        const T zl = z[c - 1], zr = z[c + 4];
+        double pq[4], qq[4], pn[4], qn[4];
+        Quad4<double>::ld(p + c, pq);
+        Quad4<double>::ld(q + c, qq);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            double w[6];
+            couplings<double, VAR>(L, i, j, k0 + e, c + e, w);
+            const double km = e > 0 ? (double)zc[e - 1] : (double)zl;
+            const double kp = e < 3 ? (double)zc[e + 1] : (double)zr;
+            const double zz = (double)zc[e];
+            const double sv = w[0] * (double)zim[e] + w[1] * (double)zip[e] + w[2] * (double)zjm[e] +
+                              w[3] * (double)zjp[e] + w[4] * km + w[5] * kp;
+            const double d = w[0] + w[1] + w[2] + w[3] + w[4] + w[5];
+            // on the first step p and q hold whatever the last solve left
+            pn[e] = beta != 0.0 ? zz + beta * pq[e] : zz;
+            qn[e] = beta != 0.0 ? (sv - d * zz) + beta * qq[e] : sv - d * zz;
+            a += (hij * hk[e]) * pn[e] * qn[e];
+        }
+        Quad4<double>::st(p + c, pn);
+        Quad4<double>::st(q + c, qn);
+    })
+    a = block_sum<kReduceThreads>(a, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0) partials[block_id()] = a;
+}
+
+__global__ void __launch_bounds__(kReduceThreads) k_fcg_update4(Bricks<double> B, const double* p, double* r,
+                                                                const double* q, float* pre32, double* pre64,
+                                                                double* partials, const SolveState* st) {
+    __shared__ double sh[kReduceThreads / 32];
+    const double alpha = st->alpha;
+    double a = 0.0;
+    BMG_QUAD_LOOP(B, {
+        double xq[4], pq[4], rq[4], qq[4], rn[4];
+        Quad4<double>::ld(L.x + c, xq);
+        Quad4<double>::ld(p + c, pq);
+        Quad4<double>::ld(r + c, rq);
+        Quad4<double>::ld(q + c, qq);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            xq[e] = xq[e] + alpha * pq[e];
+            rn[e] = rq[e] - alpha * qq[e];
+            const double Vr = (hij * hk[e]) * rn[e];
+            a += Vr * Vr;
+        }
+        Quad4<double>::st(L.x + c, xq);
+        if (L.per0 | L.per1 | L.per2) {
+#pragma unroll
+            for (int e = 0; e < 4; ++e) store_x(L, c + e, i, j, k0 + e, xq[e]);
+        }
+        Quad4<double>::st(r + c, rn);
+        if (pre32) {
+            const float f[4] = {(float)rn[0], (float)rn[1], (float)rn[2], (float)rn[3]};
+            Quad4<float>::st(pre32 + c, f);
+        }
+        if (pre64) Quad4<double>::st(pre64 + c, rn);
+    })
+    a = block_sum<kReduceThreads>(a, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0) partials[block_id()] = a;
+}
+
+#undef BMG_QUAD_LOOP
+
+bool fcg_quads(const Bricks<double>& B) {
+    for (int b = 0; b < B.nb; ++b)
+        if (B.v[b].n2 % 4) return false;
+    return true;
+}
+
+dim3 quad_grid(const Bricks<double>& B) {
+    return dim3((unsigned)((B.max2 / 4 + 15) / 16), (unsigned)((B.max1 + 15) / 16),
+                (unsigned)std::min(B.z0[B.nb], kQuadPlanes));
+}
+
 }  // namespace
+
+long fcg_partials(const Bricks<double>& B) {
+    if (!fcg_quads(B)) return reduce_blocks(B);
+    const dim3 g = quad_grid(B);
+    return (long)g.x * g.y * g.z;
+}
 
 template <bool VAR>
 void launch_fcg_residual(const Bricks<double>& B, int mode, double* r, float* pre32, double* pre64,
@@ -201,22 +381,34 @@ void launch_fcg_residual(const Bricks<double>& B, int mode, double* r, float* pr
 template <typename T>
 void launch_fcg_beta(const Bricks<double>& B, const T* z, const double* r, const double* q, double* partials,
                      SolveState* st, cudaStream_t s) {
-    const dim3 blk = block_for(B.max2);
-    const long nb = reduce_blocks(B);
-    k_fcg_dots<T><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, z, r, q, partials, nb);
+    const long nb = fcg_partials(B);
+    if (fcg_quads(B)) {
+        k_fcg_dots4<T><<<quad_grid(B), dim3(16, 16, 1), 0, s>>>(B, z, r, q, partials, nb);
+    } else {
+        const dim3 blk = block_for(B.max2);
+        k_fcg_dots<T><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, z, r, q, partials, nb);
+    }
     k_fcg_beta<<<1, kFinalThreads, 0, s>>>(partials, nb, st);
 }
 
 template <typename T, bool VAR>
 void launch_fcg_direction(const Bricks<double>& B, const T* z, double* p, double* q, double* partials,
                           SolveState* st, cudaStream_t s) {
-    const dim3 blk = block_for(B.max2);
-    k_fcg_direction<T, VAR><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, z, p, q, partials, st);
-    k_fcg_alpha<<<1, kFinalThreads, 0, s>>>(partials, reduce_blocks(B), st);
+    if (fcg_quads(B)) {
+        k_fcg_direction4<T, VAR><<<quad_grid(B), dim3(16, 16, 1), 0, s>>>(B, z, p, q, partials, st);
+    } else {
+        const dim3 blk = block_for(B.max2);
+        k_fcg_direction<T, VAR><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, z, p, q, partials, st);
+    }
+    k_fcg_alpha<<<1, kFinalThreads, 0, s>>>(partials, fcg_partials(B), st);
 }
 
 void launch_fcg_update(const Bricks<double>& B, const double* p, double* r, const double* q, float* pre32,
                        double* pre64, double* partials, const SolveState* st, cudaStream_t s) {
+    if (fcg_quads(B)) {
+        k_fcg_update4<<<quad_grid(B), dim3(16, 16, 1), 0, s>>>(B, p, r, q, pre32, pre64, partials, st);
+        return;
+    }
     const dim3 blk = block_for(B.max2);
     k_fcg_update<<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, p, r, q, pre32, pre64, partials, st);
 }
