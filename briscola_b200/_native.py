@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libbmg.so")
 
 # status codes (bmg_status)
 OK, NOT_CONVERGED, NAN_DETECTED, BAD_ARG, CUDA_ERROR, TIMEOUT, NO_DEVICE, UNSUPPORTED = range(8)
-BC_NEUMANN, BC_PERIODIC = 0, 1
+BC_NEUMANN, BC_PERIODIC, BC_DIRICHLET = 0, 1, 2
 CYCLE = {"V": 0, "W": 1, "F": 2}
 SMOOTHER = {"rbgs": 0, "jac": 1, "jacobi": 1}
 PRECISION = {"fp64": 0, "mixed": 1}
@@ -40,6 +40,7 @@ class Brick(ctypes.Structure):
         ("points", ctypes.POINTER(ctypes.c_double) * 3),
         ("bc", ctypes.c_int * 6),
         ("origin", ctypes.c_int * 3),
+        ("value", ctypes.c_double * 6),
     ]
 
 

@@ -117,6 +117,9 @@ struct BadArg {
 struct bmg_ctx {
     bmg_options opt{};
     int periodic[3] = {0, 0, 0};  // single brick only
+    int dirichlet[6] = {0, 0, 0, 0, 0, 0};  // Dirichlet faces (single brick only)
+    double dval[6] = {0, 0, 0, 0, 0, 0};    // their values
+    bool singular = true;         // no Dirichlet face (linearSystem.H:227-230)
     bool multi = false;           // more than one brick
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -206,10 +209,12 @@ void layout(HostLevel& L) {
 }
 
 // row-scaled couplings (A'/V): lower neighbour delta(i)/h(i), upper
-// delta(i+1)/h(i); zero across a wall face, i.e. after the Neumann
-// elimination.  Faces touching another brick keep their coupling and get
-// their wall parts zeroed through the face lambdas.
-void buildTables(HostLevel& L) {
+// delta(i+1)/h(i); zero across a Neumann wall face (NeumannBoundaryCondition
+// .C:19-56), twice the ghost coupling across a Dirichlet one, whose ghost
+// cells stay zero: A_c -= A_f after A_c = -(sum of all faces)
+// (DirichletBoundaryCondition.C:19-51).  Faces touching another brick keep
+// their coupling and get their wall parts zeroed through the face lambdas.
+void buildTables(HostLevel& L, const int dirichlet[6]) {
     int off = 0;
     L.tab.clear();
     // every sub-table starts on a multiple of 4 entries, so the colour pass
@@ -235,8 +240,8 @@ void buildTables(HostLevel& L) {
                 const double dlo = 1.0 / std::fabs(a.cc[i + 1] - a.cc[i]);
                 const double dhi = 1.0 / std::fabs(a.cc[i + 2] - a.cc[i + 1]);
                 double wl = dlo / hi, wh = dhi / hi;
-                if (!B.open[2 * d] && i == 0) wl = 0.0;
-                if (!B.open[2 * d + 1] && i == n - 1) wh = 0.0;
+                if (!B.open[2 * d] && i == 0) wl = dirichlet[2 * d] ? 2.0 * wl : 0.0;
+                if (!B.open[2 * d + 1] && i == n - 1) wh = dirichlet[2 * d + 1] ? 2.0 * wh : 0.0;
                 L.tab[to.wl[d] + i] = wl;
                 L.tab[to.wh[d] + i] = wh;
                 L.tab[to.h[d] + i] = hi;
@@ -285,6 +290,16 @@ Bricks<T> bricks(const bmg_ctx* c, int l) {
         B.max2 = std::max(B.max2, K.n[2]);
     }
     B.z0[B.nb] = z;
+    B.walls.mask = 0;
+    B.walls.nmask = 0;
+    if (l == 0 && !c->multi) {
+        for (int f = 0; f < 6; ++f) {
+            B.walls.mask |= c->dirichlet[f] << f;
+            B.walls.nmask |= (!c->dirichlet[f] && c->dval[f] != 0.0) << f;
+            B.walls.g[f] = c->dval[f];
+        }
+        B.walls.ybar = c->st ? &c->st->ybar : nullptr;
+    }
     return B;
 }
 
@@ -390,9 +405,10 @@ double couplingOf(const bmg_ctx* c, const HostLevel& L, int b, int i, int j, int
     return w;
 }
 
-// Dense row-scaled operator of the coarse solve level with the singularity
-// pin of solver.C:201-231 (row of the first cell = identity, every coupling
-// to it removed, periodic images included), inverted once per matrix.
+// Dense row-scaled operator of the coarse solve level with, for a singular
+// system, the pin of solver.C:201-231 (row of the first cell = identity,
+// every coupling to it removed, periodic images included), inverted once
+// per matrix.
 // Unknowns: bricks one after another, k fastest.
 void buildCoarseInverse(bmg_ctx* c) {
     const HostLevel& L = c->lv[c->lc];
@@ -423,7 +439,11 @@ void buildCoarseInverse(bmg_ctx* c) {
                             const int g[3] = {B.origin[0] + nbl[0], B.origin[1] + nbl[1], B.origin[2] + nbl[2]};
                             int loc[3];
                             const int nb = findBrick(L, g, loc);
-                            if (nb < 0) continue;  // wall (zero lambda keeps us from getting here)
+                            if (nb < 0) {
+                                // a Dirichlet wall: eliminated coupling, zero ghost
+                                diag -= w;
+                                continue;
+                            }
                             const HostBrick& N = L.br[nb];
                             col = N.cbase + ((long)loc[0] * N.n[1] + loc[1]) * N.n[2] + loc[2];
                         }
@@ -433,10 +453,15 @@ void buildCoarseInverse(bmg_ctx* c) {
                     M[(size_t)row * n + row] += diag;
                 }
     }
-    for (int j = 0; j < n; ++j) M[j] = j == 0 ? 1.0 : 0.0;
-    for (int r = 1; r < n; ++r) M[(size_t)r * n] = 0.0;
+    if (c->singular) {
+        for (int j = 0; j < n; ++j) M[j] = j == 0 ? 1.0 : 0.0;
+        for (int r = 1; r < n; ++r) M[(size_t)r * n] = 0.0;
+    }
     std::vector<double> inv;
     if (!invert(M, n, inv)) throw BadArg{BMG_BAD_ARG, "coarse level matrix is singular"};
+    // MG.C:37-40: the pinned cell's right-hand side is zero
+    if (c->singular)
+        for (int r = 0; r < n; ++r) inv[(size_t)r * n] = 0.0;
     if (!c->ainv || c->ncoarse != n) {
         if (c->ainv) cudaFree(c->ainv);
         if (c->cidx) cudaFree(c->cidx);
@@ -513,8 +538,22 @@ void readBricks(bmg_ctx* c, const bmg_mesh_desc* mesh, HostLevel& L0) {
             const int lo = B.bc[2 * d], hi = B.bc[2 * d + 1];
             if ((lo == BMG_BC_PERIODIC) != (hi == BMG_BC_PERIODIC))
                 throw BadArg{BMG_BAD_ARG, "periodic faces must come in opposite pairs"};
-            if ((lo != BMG_BC_PERIODIC && lo != BMG_BC_NEUMANN) || (hi != BMG_BC_PERIODIC && hi != BMG_BC_NEUMANN))
-                throw BadArg{BMG_UNSUPPORTED, "boundary condition type not supported"};
+            for (int side = 0; side < 2; ++side) {
+                const int t = B.bc[2 * d + side];
+                const double v = B.value[2 * d + side];
+                if (t != BMG_BC_PERIODIC && t != BMG_BC_NEUMANN && t != BMG_BC_DIRICHLET)
+                    throw BadArg{BMG_BAD_ARG, "unknown boundary condition type"};
+                if (t == BMG_BC_PERIODIC) continue;
+                if (!std::isfinite(v)) throw BadArg{BMG_BAD_ARG, "a face value is not finite"};
+                if ((t == BMG_BC_DIRICHLET || v != 0.0) && nb > 1)
+                    throw BadArg{BMG_UNSUPPORTED,
+                                 "Dirichlet faces and Neumann gradients on multi-brick meshes are not supported"};
+                c->dval[2 * d + side] = v;
+                if (t == BMG_BC_DIRICHLET) {
+                    c->dirichlet[2 * d + side] = 1;
+                    c->singular = false;
+                }
+            }
             if (lo == BMG_BC_PERIODIC && c->multi)
                 throw BadArg{BMG_UNSUPPORTED, "periodic faces on multi-brick meshes are not supported"};
             if (!c->multi) c->periodic[d] = lo == BMG_BC_PERIODIC;
@@ -745,7 +784,7 @@ void build(bmg_ctx* c, HostLevel&& L0) {
     for (auto& L : c->lv) {
         layout(L);
         if (L.cells >= (1L << 31)) throw BadArg{BMG_UNSUPPORTED, "a level above 2^31 cells"};
-        buildTables(L);
+        buildTables(L, c->dirichlet);
         L.x64 = dalloc<double>(L.cells);
         L.b64 = dalloc<double>(L.cells);
         L.x32 = dalloc<float>(L.cells);
@@ -810,6 +849,12 @@ void build(bmg_ctx* c, HostLevel&& L0) {
                                 I1 = (In + C.n[d]) % C.n[d];
                             } else if (C.open[2 * d + (In >= C.n[d])]) {
                                 I1 = In;  // ghost cell, refreshed from the neighbouring brick
+                            } else if (c->dirichlet[2 * d + (In >= C.n[d])]) {
+                                // the coarse ghost is -x (DirichletBoundaryCondition.C
+                                // :59-80 above level 0): (1 - w) x + w (-x) = (1 - 2w) x,
+                                // read as weight 2w on the ghost cell, which holds zero
+                                I1 = In;
+                                w = 2.0 * w;
                             } else {
                                 I1 = I0;  // zero-gradient ghost: the value equals the parent's
                                 w = 0.0;
@@ -1260,6 +1305,10 @@ void segInit(bmg_ctx* c, const double* bsrc, const double* xsrc, bool zero, bool
         c->launches += 1;
     }
     BMG_CUDA(cudaMemcpyAsync(c->st, c->st_host, sizeof(SolveState), cudaMemcpyHostToDevice, s));
+    if (!zero && !c->singular) {
+        launch_plain_mean(V0, c->partials, c->st, s);
+        c->launches += 2;
+    }
     residualNorm(c, 0, setCondition);
 }
 
@@ -1285,7 +1334,7 @@ void segBody(bmg_ctx* c, bool setCondition) {
 void segPost(bmg_ctx* c, double* xdst) {
     if (c->opt.krylov == BMG_KRYLOV_FCG) return segPostFcg(c, xdst);
     const Bricks<double> V0 = bricks<double>(c, 0);
-    if (c->opt.remove_mean) {
+    if (c->opt.remove_mean && c->singular) {
         launch_mean(V0, c->partials, c->st, c->stream);
         c->launches += 3;
     }
@@ -1317,6 +1366,10 @@ void segInitFcg(bmg_ctx* c, const double* bsrc, const double* xsrc, bool zero, b
     }
     BMG_CUDA(cudaMemcpyAsync(c->st, c->st_host, sizeof(SolveState), cudaMemcpyHostToDevice, s));
     exchangeField<double>(c, 0, c->fx);
+    if (!zero && !c->singular) {
+        launch_plain_mean(V, c->partials, c->st, s);
+        c->launches += 2;
+    }
     float* pre32 = mixed ? c->lv[0].b32 : nullptr;
     double* pre64 = mixed ? nullptr : c->lv[0].b64;
     if (c->variable)
@@ -1370,7 +1423,7 @@ void segPostFcg(bmg_ctx* c, double* xdst) {
         launch_fcg_residual<false>(V, 2, nullptr, nullptr, nullptr, c->partials, s);
     launch_fcg_true_norm(V, c->partials, c->st, s);
     c->launches += 2;
-    if (c->opt.remove_mean) {
+    if (c->opt.remove_mean && c->singular) {
         launch_mean(V, c->partials, c->st, s);
         c->launches += 3;
     }

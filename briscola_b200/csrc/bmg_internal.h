@@ -70,6 +70,23 @@ struct LevelView {
     int cpar;          // parity of the brick origin: colour = (i+j+k+cpar) & 1
 };
 
+// Wall faces of a single-brick level 0: bit f of mask for a Dirichlet face
+// f (x-lo, x-hi, y-lo, y-hi, z-lo, z-hi; DirichletBoundaryCondition.C:19-80),
+// of nmask for a Neumann face with a nonzero gradient
+// (NeumannBoundaryCondition.C:19-56), g the face values.  On every level the
+// 1-D tables hold the eliminated coupling 2 A_f / V at Dirichlet faces and
+// the ghost cells stay zero, so each stencil kernel applies the eliminated
+// operator as it is; only the right-hand side (b -= 2 A_f g, or A_f g /
+// delta) and the normFactor's A*mean(x) term (solver.C:28-45) need the faces
+// themselves.  ybar: the plain mean of the initial x (SolveState::ybar).
+// Both masks are 0 on coarse levels.
+struct Walls {
+    int mask;
+    int nmask;
+    double g[6];
+    const double* ybar;
+};
+
 // All bricks of a level, for one launch across bricks: the grid's z index
 // runs over the planes of brick 0, then brick 1, ...
 template <typename T>
@@ -78,6 +95,7 @@ struct Bricks {
     int z0[kMaxBricks + 1];  // first plane of each brick; z0[nb] = total planes
     int nb;
     int max1, max2;          // largest n1 and n2 (grid extents)
+    Walls walls;
 };
 
 // Transfer tables between level l (fine) and l+1 (coarse), fine-indexed.
@@ -106,6 +124,7 @@ struct SolveState {
     double l2_0;       // initial ||b - A x0||_2
     double rel_tol, abs_tol;
     double mean;       // volume-weighted mean of x (mean removal)
+    double ybar;       // plain mean of the initial x (normFactor with Dirichlet faces)
     double vol_total;
     double ncells;
     int iter;
@@ -196,6 +215,8 @@ void launch_residual_norm(const Bricks<double>& B, int mode, double* partials, f
 void launch_finalize(const Bricks<double>& B, const double* partials, SolveState* st, int mode,
                      cudaGraphConditionalHandle cond, int setCondition, cudaStream_t s);
 void launch_mean(const Bricks<double>& B, double* partials, SolveState* st, cudaStream_t s);
+// st->ybar = plain mean of the interior x (gAverage, solver.C:24)
+void launch_plain_mean(const Bricks<double>& B, double* partials, SolveState* st, cudaStream_t s);
 // number of per-block partial sums the level-0 reductions write
 long reduce_blocks(const Bricks<double>& B);
 // sets the dynamic shared memory limits of the fused smoother instances

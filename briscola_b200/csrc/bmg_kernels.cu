@@ -451,8 +451,9 @@ __global__ void __launch_bounds__(256) k_restrict_quad(Bricks<T> FB, Bricks<T> C
 
 // ---------------------------------------------------------------------------
 // Coarse direct solve: x = inverse(A'_pinned) b' with b'(0) = 0 (MG.C:37-40,
-// solver.C:201-231, APLU.C:91-128).  One CTA; the inverse is factored once
-// per matrix on the host in FP64.  cidx gives the slab index of every
+// solver.C:201-231, APLU.C:91-128); a singular system's inverse comes with
+// its first column zeroed, which is that b'(0) = 0.  One CTA; the inverse is
+// factored once per matrix on the host in FP64.  cidx gives the slab index of every
 // unknown (bricks one after another, k fastest).
 // ---------------------------------------------------------------------------
 // one CTA (any multiple of 32 threads); sb: n doubles of shared memory
@@ -460,7 +461,7 @@ template <typename T>
 __device__ __forceinline__ void coarse_solve_block(const Bricks<T>& CB, const double* __restrict__ ainv,
                                                    const int* __restrict__ cidx, int n, double* sb) {
     const T* bsrc = CB.v[0].b;
-    for (int q = threadIdx.x; q < n; q += blockDim.x) sb[q] = q == 0 ? 0.0 : (double)bsrc[cidx[q]];
+    for (int q = threadIdx.x; q < n; q += blockDim.x) sb[q] = (double)bsrc[cidx[q]];
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int r = warp; r < n; r += nw) {
@@ -574,9 +575,9 @@ __global__ void __launch_bounds__(256) k_residual_out(Bricks<T> B, double* out) 
 // One cell per thread over the same grid as the other cell kernels, one
 // partial sum per block; the finalize kernel adds the partials in a fixed
 // order, so sums are reproducible.  mode 0 also accumulates the normFactor
-// sum (|r - b| + |b|)^2: the row sums of the level-0 operator vanish (every
-// coupling is paired with the centre), so A*mean(x) drops out of the
-// reference's expression.
+// sum (|r - b + A ybar| + |b - A ybar|)^2, ybar = mean(x): the row sums of
+// the level-0 operator vanish (every coupling is paired with the centre)
+// except in the rows of Dirichlet faces.
 // ---------------------------------------------------------------------------
 template <bool VAR>
 __global__ void __launch_bounds__(kReduceThreads) k_residual_norm(Bricks<double> B, int mode, double* partials,
@@ -598,7 +599,9 @@ __global__ void __launch_bounds__(kReduceThreads) k_residual_norm(Bricks<double>
         a1 = rr * rr;
         if (mode == 0) {
             const double bb = V * L.b[c];
-            const double t = fabs(rr - bb) + fabs(bb);
+            // A*mean(x): nonzero only in the rows of Dirichlet faces
+            const double ay = B.walls.mask ? -V * *B.walls.ybar * wall_sum(L, B.walls, i, j, k, c, false) : 0.0;
+            const double t = fabs(rr - bb + ay) + fabs(bb - ay);
             a2 = t * t;
             a3 = bb * bb;
         }
@@ -684,6 +687,26 @@ __global__ void __launch_bounds__(kFinalThreads) k_mean_finalize(const double* p
     if (threadIdx.x == 0) st->mean = a / st->vol_total;
 }
 
+// plain (unweighted) sum of the interior x per block, then the mean
+__global__ void __launch_bounds__(kReduceThreads) k_plain_partials(Bricks<double> B, double* partials) {
+    __shared__ double sh[kReduceThreads / 32];
+    int i;
+    const LevelView<double>& L = B.v[brick_of(B, blockIdx.z, i)];
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    double a = 0.0;
+    if (j < L.n1 && k < L.n2) a = L.x[L.base + (long)i * L.si + (long)j * L.sj + k];
+    a = block_sum<kReduceThreads>(a, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0) partials[block_id()] = a;
+}
+
+__global__ void __launch_bounds__(kFinalThreads) k_plain_finalize(const double* partials, long nblocks,
+                                                                  SolveState* st) {
+    __shared__ double sh[kFinalThreads / 32];
+    const double a = sum_partials<kFinalThreads>(partials, nblocks, sh);
+    if (threadIdx.x == 0) st->ybar = a / st->ncells;
+}
+
 // subtract the mean everywhere, ghosts included (a constant shift keeps the
 // periodic images consistent)
 __global__ void k_sub_mean(double* x, long n, const SolveState* st) {
@@ -700,7 +723,10 @@ __global__ void __launch_bounds__(256) k_load_b(Bricks<double> B, const double* 
     if (j >= L.n1 || k >= L.n2) return;
     const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
     const double V = L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j] * L.tab64[L.to.h[2] + k];
-    L.b[c] = compact[L.cbase + ((long)i * L.n1 + j) * L.n2 + k] / V;
+    double v = compact[L.cbase + ((long)i * L.n1 + j) * L.n2 + k] / V;
+    // face values: Dirichlet b -= 2 A_f g, Neumann b -= A_f g / delta
+    if (B.walls.mask | B.walls.nmask) v -= wall_sum(L, B.walls, i, j, k, c, true);
+    L.b[c] = v;
 }
 
 __global__ void __launch_bounds__(256) k_load_x(Bricks<double> B, const double* compact) {
@@ -876,6 +902,12 @@ void launch_mean(const Bricks<double>& B, double* partials, SolveState* st, cuda
     const long n = B.v[0].cells;
     const int blocks = (int)std::min<long>((n + 255) / 256, 148L * 16);
     k_sub_mean<<<blocks, 256, 0, s>>>(B.v[0].x, n, st);
+}
+
+void launch_plain_mean(const Bricks<double>& B, double* partials, SolveState* st, cudaStream_t s) {
+    const dim3 blk = block_for(B.max2);
+    k_plain_partials<<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, partials);
+    k_plain_finalize<<<1, kFinalThreads, 0, s>>>(partials, reduce_blocks(B), st);
 }
 
 void launch_load_b(const Bricks<double>& B, const double* compact, cudaStream_t s) {

@@ -55,7 +55,8 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_residual(Bricks<double> 
         a1 = (V * r) * (V * r);
         if (mode == 0) {
             const double bb = V * L.b[c];
-            const double t = fabs(V * r - bb) + fabs(bb);
+            const double ay = B.walls.mask ? -V * *B.walls.ybar * wall_sum(L, B.walls, i, j, k, c, false) : 0.0;
+            const double t = fabs(V * r - bb + ay) + fabs(bb - ay);
             a2 = t * t;
             a3 = bb * bb;
         }

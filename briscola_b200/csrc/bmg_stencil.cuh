@@ -76,6 +76,33 @@ __device__ __forceinline__ void stencil(const T* x, long c, long si, long sj, co
     d = w[0] + w[1] + w[2] + w[3] + w[4] + w[5];
 }
 
+// Wall faces of cell (i,j,k) on level 0 (FP64).  values == false: the sum
+// over its Dirichlet faces of the face coupling (the eliminated 2 A_f / V,
+// times the face lambda), the cell's row sum up to sign.  values == true:
+// the right-hand-side term of the face values, sum over Dirichlet faces of
+// 2 A_f g / V (DirichletBoundaryCondition.C:47-48) plus, over Neumann faces
+// with a gradient g, A_f g / (delta V) = lambda g / h
+// (NeumannBoundaryCondition.C:44-50).
+__device__ __forceinline__ double wall_sum(const LevelView<double>& L, const Walls& W, int i, int j, int k,
+                                           long c, bool values) {
+    double s = 0.0;
+    const int at[6] = {i == 0, i == L.n0 - 1, j == 0, j == L.n1 - 1, k == 0, k == L.n2 - 1};
+    const int q[3] = {i, j, k};
+    const long st[3] = {L.si, L.sj, 1};
+    const int faces = values ? (W.mask | W.nmask) : W.mask;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        if (!((faces >> f) & 1) || !at[f]) continue;
+        const int d = f >> 1, up = f & 1;
+        const bool dir = (W.mask >> f) & 1;
+        double w = dir ? L.tab64[(up ? L.to.wh[d] : L.to.wl[d]) + q[d]] : 1.0 / L.tab64[L.to.h[d] + q[d]];
+        const double* lam = d == 0 ? L.lam0 : d == 1 ? L.lam1 : L.lam2;
+        if (lam) w *= lam[c + (up ? st[d] : 0)];
+        s += values ? w * W.g[f] : w;
+    }
+    return s;
+}
+
 // Store an interior value and its periodic ghost images (faces, edges and
 // corners), replacing the reference's per-sweep periodic ghost copy
 // (periodicBoundaryCondition.C:53-92).  Per axis a cell has up to two

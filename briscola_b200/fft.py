@@ -80,14 +80,15 @@ def _brick(mesh) -> Brick:
 
 class FFTPoissonSolver:
     """The "FFT" Poisson solver of one brick.  ``values``: the Dirichlet
-    value or Neumann gradient of each face (x-lo, x-hi, y-lo, ...)."""
+    value or Neumann gradient of each face (x-lo, x-hi, y-lo, ...); by
+    default the brick's face values."""
 
     typeName = "FFT"
 
-    def __init__(self, mesh, values=(0.0,) * 6, device: int = 0):
+    def __init__(self, mesh, values=None, device: int = 0):
         self.brick = _brick(mesh)
         self.N = self.brick.N
-        self.values = tuple(float(v) for v in values)
+        self.values = tuple(float(v) for v in (self.brick.values if values is None else values))
         for f in self.brick.bc:
             if f not in BC:
                 raise FatalError(f"Incompatible boundary condition {f}")

@@ -14,7 +14,8 @@ import numpy as np
 
 NEUMANN = "Neumann"
 PERIODIC = "periodic"
-# faces only the FFT Poisson solver takes (briscola_b200.fft)
+# Dirichlet faces: both solvers (the multigrid on single-brick meshes);
+# empty axes: the FFT Poisson solver only (briscola_b200.fft)
 DIRICHLET = "Dirichlet"
 EMPTY = "empty"
 
@@ -46,16 +47,18 @@ def tanh_points(n: int, gamma: float, length: float = 1.0, start: float = 0.0) -
 @dataclass
 class Brick:
     """One brick: ``points`` holds the vertex coordinates per axis; ``bc`` the
-    boundary type of faces x-lo, x-hi, y-lo, y-hi, z-lo, z-hi."""
+    boundary type of faces x-lo, x-hi, y-lo, y-hi, z-lo, z-hi; ``values`` the
+    (uniform) value of each Dirichlet face."""
 
     points: list
     bc: tuple = (NEUMANN,) * 6
     origin: tuple = (0, 0, 0)
+    values: tuple = (0.0,) * 6
 
     def __post_init__(self):
         self.points = [np.ascontiguousarray(p, dtype=np.float64) for p in self.points]
-        if len(self.points) != 3 or len(self.bc) != 6:
-            raise ValueError("a brick needs three coordinate arrays and six face conditions")
+        if len(self.points) != 3 or len(self.bc) != 6 or len(self.values) != 6:
+            raise ValueError("a brick needs three coordinate arrays, six face conditions and six face values")
 
     @property
     def N(self):

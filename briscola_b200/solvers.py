@@ -165,6 +165,9 @@ class solver:
         raise NotImplementedError
 
 
+_BC = {"Neumann": N.BC_NEUMANN, "periodic": N.BC_PERIODIC, "Dirichlet": N.BC_DIRICHLET}
+
+
 def _mesh_desc(mesh: Mesh):
     bricks = (N.Brick * len(mesh.bricks))()
     keep = []
@@ -176,7 +179,10 @@ def _mesh_desc(mesh: Mesh):
             bricks[q].points[d] = p.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
             bricks[q].origin[d] = int(br.origin[d])
         for f in range(6):
-            bricks[q].bc[f] = N.BC_PERIODIC if br.bc[f] == "periodic" else N.BC_NEUMANN
+            if br.bc[f] not in _BC:
+                raise FatalError(f"Incompatible boundary condition {br.bc[f]} for the GPU multigrid")
+            bricks[q].bc[f] = _BC[br.bc[f]]
+            bricks[q].value[f] = float(br.values[f])
     desc = N.MeshDesc(len(mesh.bricks), bricks)
     return desc, (bricks, keep)
 

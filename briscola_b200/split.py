@@ -18,6 +18,7 @@ host arrays that are copied to the device.
 from __future__ import annotations
 
 import ctypes
+import dataclasses
 
 import numpy as np
 
@@ -29,11 +30,12 @@ from .solvers import Context, FatalError, _switch, make_options
 class SplitPoissonSolver:
     """``d``: the solver dictionary (``solver`` sub-dictionary of type FFT,
     optional ``preconditioner`` sub-dictionary of a GPUMG solver, ``nCorr``,
-    ``prediction``); ``values``: the face values of the boundary conditions."""
+    ``prediction``); ``values``: the face values of the boundary conditions
+    (Dirichlet values, Neumann gradients; by default the brick's)."""
 
     typeName = "split"
 
-    def __init__(self, mesh, d: dict, values=(0.0,) * 6, device: int = 0):
+    def __init__(self, mesh, d: dict, values=None, device: int = 0):
         d = dict(d)
         sd = d.get("solver")
         if sd is None:
@@ -42,7 +44,12 @@ class SplitPoissonSolver:
             raise FatalError(f"the split solver's inner solver must be of type FFT, not {sd.get('type')}")
         self.mesh = mesh if isinstance(mesh, Mesh) else Mesh([mesh])
         self.brick = self.mesh.bricks[0]
-        self.inner = fft.FFTPoissonSolver(self.brick, values, device)
+        if values is not None:
+            # the face values of both the FFT corrections and the multigrid
+            # preconditioner
+            self.brick = dataclasses.replace(self.brick, values=tuple(float(v) for v in values))
+            self.mesh = Mesh([self.brick])
+        self.inner = fft.FFTPoissonSolver(self.brick, None, device)
         self.device = int(device)
         # splitPoissonSolver.C:31-52
         self.nCorr = int(d.get("nCorr", 1))

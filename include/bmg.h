@@ -42,8 +42,14 @@ typedef enum bmg_status {
     BMG_UNSUPPORTED = 7    /* a valid option this build does not implement                           */
 } bmg_status;
 
-/* Boundary condition of one outer brick face. */
-enum { BMG_BC_NEUMANN = 0, BMG_BC_PERIODIC = 1 };
+/* Boundary condition of one outer brick face.  Dirichlet faces (single-brick
+ * meshes) follow DirichletBoundaryCondition.C:19-80: the ghost coefficient
+ * is eliminated into the centre (A_c -= A_f), the face value g enters the
+ * right-hand side as b -= 2 A_f g at every solve, and the system is not
+ * singular (no pin, no mean removal; linearSystem.H:227-230).  A Neumann
+ * face's value is its gradient g (single-brick meshes): b -= A_f g / delta
+ * (NeumannBoundaryCondition.C:19-56). */
+enum { BMG_BC_NEUMANN = 0, BMG_BC_PERIODIC = 1, BMG_BC_DIRICHLET = 2 };
 
 /* Cycle types (MG.H:106-124) and smoothers (MG.C:313-373). */
 enum { BMG_CYCLE_V = 0, BMG_CYCLE_W = 1, BMG_CYCLE_F = 2 };
@@ -73,6 +79,8 @@ typedef struct bmg_brick {
     const double* points[3];  /* n[d]+1 vertex coordinates along axis d (host memory)  */
     int bc[6];                /* x-lo, x-hi, y-lo, y-hi, z-lo, z-hi: BMG_BC_*          */
     int origin[3];            /* cell offset in the global lattice (multi-brick)       */
+    double value[6];          /* Dirichlet value or Neumann gradient of each face
+                                 (uniform; ignored on periodic faces)             */
 } bmg_brick;
 
 typedef struct bmg_mesh_desc {
@@ -94,7 +102,8 @@ typedef struct bmg_options {
     int smoother;       /* smoother     (rbgs)                                 */
     int precision;      /* precision    (fp64)                                 */
     int use_graph;      /* graph        (1): whole solve as one CUDA graph     */
-    int remove_mean;    /* subtract the volume-weighted mean of x (singular)   */
+    int remove_mean;    /* subtract the volume-weighted mean of x; singular
+                           systems only (no Dirichlet face)                    */
     int fused;          /* fused (3): up to this many colour passes of a
                            smoothing step per pass over memory (1..3); 0: one
                            launch per colour pass                              */

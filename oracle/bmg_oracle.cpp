@@ -131,10 +131,20 @@ struct Level {
 struct bmgo_problem {
     std::vector<Level> lv;
     int periodic[3];
+    int dirichlet[6] = {0, 0, 0, 0, 0, 0};  // walls with a Dirichlet condition
+    double dval[6] = {0, 0, 0, 0, 0, 0};    // their (uniform) boundary values
+    std::vector<double> bdir;               // level-0 right-hand-side term of the Dirichlet values
     bool variable = false;
     Pool pool;
     int coarseLevelIdx = -1;  // level index that carries the pin
     explicit bmgo_problem(int nt) : pool(nt) {}
+    // linearSystem.H:227-230, meshLevel.C:555-583: singular unless a wall
+    // carries a Dirichlet condition
+    bool singular() const {
+        for (int f = 0; f < 6; ++f)
+            if (dirichlet[f]) return false;
+        return true;
+    }
 };
 
 namespace {
@@ -207,42 +217,61 @@ void buildLevels(P& p, const int N[3], const double* pts[3]) {
     }
 }
 
-// Ghost fill of a level field, axis by axis over growing extents, so that
-// edge and corner ghosts hold the composition of the per-axis rules
-// (periodic image, or zero-gradient copy at a wall: NeumannBoundaryCondition.C
-// evaluate with zero gradient, meshLevel.C:301-328 for unset boundaries).
-void fillGhostsAll(const P& p, const Level& L, std::vector<double>& f) {
-    const int N0 = L.N[0], N1 = L.N[1], N2 = L.N[2];
-    for (int j = 0; j < N1; ++j)
-        for (int k = 0; k < N2; ++k) {
-            if (p.periodic[0]) {
-                f[L.at(-1, j, k)] = f[L.at(N0 - 1, j, k)];
-                f[L.at(N0, j, k)] = f[L.at(0, j, k)];
-            } else {
-                f[L.at(-1, j, k)] = f[L.at(0, j, k)];
-                f[L.at(N0, j, k)] = f[L.at(N0 - 1, j, k)];
+// Ghost fill of a level field (meshLevel.C:231-253), axis by axis over
+// growing extents: periodic images, zero-gradient copies at Neumann walls
+// (NeumannBoundaryCondition.C evaluate with zero gradient) and the mirror
+// H 2 g - x at Dirichlet walls (DirichletBoundaryCondition.C:59-80, H = 1 on
+// level 0 only).  Edge and corner ghosts then hold the composition of the
+// per-axis rules, which is what the reference's periodic edge boundaries
+// give.  Where only walls meet (no periodic axis among them), the
+// reference's unset-boundary copy of the diagonal interior cell
+// (meshLevel.C:301-328) applies instead; it differs from the composition
+// only where a Dirichlet wall takes part, so it is written over the
+// composition there.
+void fillGhostsAll(const P& p, const Level& L, std::vector<double>& f, int level) {
+    const double H = level == 0 ? 1.0 : 0.0;
+    int n[3] = {L.N[0], L.N[1], L.N[2]};
+    int lo[3] = {0, 0, 0}, hi[3] = {n[0], n[1], n[2]};
+    for (int d = 0; d < 3; ++d) {
+        const int t1 = (d + 1) % 3, t2 = (d + 2) % 3;
+        for (int u = lo[t1]; u < hi[t1]; ++u)
+            for (int v = lo[t2]; v < hi[t2]; ++v)
+                for (int side = 0; side < 2; ++side) {
+                    int g[3], in[3];
+                    g[t1] = in[t1] = u;
+                    g[t2] = in[t2] = v;
+                    g[d] = side ? n[d] : -1;
+                    if (p.periodic[d])
+                        in[d] = side ? 0 : n[d] - 1;
+                    else
+                        in[d] = side ? n[d] - 1 : 0;
+                    const double val = f[L.at(in[0], in[1], in[2])];
+                    if (!p.periodic[d] && p.dirichlet[2 * d + side])
+                        f[L.at(g[0], g[1], g[2])] = H * 2.0 * p.dval[2 * d + side] - val;
+                    else
+                        f[L.at(g[0], g[1], g[2])] = val;
+                }
+        lo[d] = -1;
+        hi[d] = n[d] + 1;
+    }
+    if (p.singular()) return;
+    // wall-only edges and corners: copy of the diagonal interior cell
+    for (int i = -1; i <= n[0]; ++i)
+        for (int j = -1; j <= n[1]; ++j)
+            for (int k = -1; k <= n[2]; ++k) {
+                const int q[3] = {i, j, k};
+                int out = 0;
+                bool wallOnly = true;
+                int in[3];
+                for (int d = 0; d < 3; ++d) {
+                    const bool o = q[d] < 0 || q[d] >= n[d];
+                    out += o;
+                    if (o && p.periodic[d]) wallOnly = false;
+                    in[d] = std::min(std::max(q[d], 0), n[d] - 1);
+                }
+                if (out < 2 || !wallOnly) continue;
+                f[L.at(i, j, k)] = f[L.at(in[0], in[1], in[2])];
             }
-        }
-    for (int i = -1; i <= N0; ++i)
-        for (int k = 0; k < N2; ++k) {
-            if (p.periodic[1]) {
-                f[L.at(i, -1, k)] = f[L.at(i, N1 - 1, k)];
-                f[L.at(i, N1, k)] = f[L.at(i, 0, k)];
-            } else {
-                f[L.at(i, -1, k)] = f[L.at(i, 0, k)];
-                f[L.at(i, N1, k)] = f[L.at(i, N1 - 1, k)];
-            }
-        }
-    for (int i = -1; i <= N0; ++i)
-        for (int j = -1; j <= N1; ++j) {
-            if (p.periodic[2]) {
-                f[L.at(i, j, -1)] = f[L.at(i, j, N2 - 1)];
-                f[L.at(i, j, N2)] = f[L.at(i, j, 0)];
-            } else {
-                f[L.at(i, j, -1)] = f[L.at(i, j, 0)];
-                f[L.at(i, j, N2)] = f[L.at(i, j, N2 - 1)];
-            }
-        }
 }
 
 // periodicBoundaryCondition.C:53-92: same-rank periodic faces copy the
@@ -332,12 +361,17 @@ void assembleLevel(const P& p, Level& L) {
     }
 }
 
-// NeumannBoundaryCondition.C:19-56 (homogeneous gradient): fold the ghost
-// coefficient into the centre and drop it.
-void eliminateNeumann(const P& p, Level& L) {
+// Wall elimination (linearSystem.C:326-341): NeumannBoundaryCondition.C:19-56
+// folds the ghost coefficient into the centre, DirichletBoundaryCondition.C
+// :19-51 subtracts it; both drop it.  On level 0 the face values enter the
+// right-hand side, -2 A_f g (Dirichlet value g) or -A_f g / delta (Neumann
+// gradient g), kept in bdir and added to b at every solve.
+void eliminateWalls(P& p, Level& L, int level) {
+    if (level == 0) p.bdir.assign(L.cells(), 0.0);
     for (int f = 0; f < 6; ++f) {
         const int fd = f / 2;
         if (p.periodic[fd]) continue;
+        const bool dir = p.dirichlet[f] != 0;
         const int lo[3] = {0, 0, 0};
         int S[3] = {lo[0], lo[1], lo[2]};
         int E[3] = {L.N[0], L.N[1], L.N[2]};
@@ -350,7 +384,20 @@ void eliminateNeumann(const P& p, Level& L) {
                 for (int k = S[2]; k < E[2]; ++k) {
                     const long c = L.at(i, j, k);
                     const double g = L.A[7 * c + f + 1];
-                    L.A[7 * c] += g;
+                    if (dir) {
+                        L.A[7 * c] -= g;
+                        if (level == 0) p.bdir[c] -= g * 2.0 * p.dval[f];
+                    } else {
+                        L.A[7 * c] += g;
+                        // NeumannBoundaryCondition.C:44-50: b -= A_f grad / delta,
+                        // delta of the wall face = 1 / (centre - ghost centre)
+                        if (level == 0 && p.dval[f] != 0.0) {
+                            const int ijk[3] = {i, j, k};
+                            const int gq = ijk[fd] + (f % 2 ? 1 : -1);
+                            const double dist = std::fabs(L.ccen(fd, ijk[fd]) - L.ccen(fd, gq));
+                            p.bdir[c] -= g * p.dval[f] * dist;
+                        }
+                    }
                     L.A[7 * c + f + 1] = 0.0;
                 }
     }
@@ -561,7 +608,7 @@ void prolongLevel(P& p, int lf, std::vector<double>& coarse, std::vector<double>
                   bool fillGhosts = true) {
     const Level& F = p.lv[lf];
     const Level& C = p.lv[lf + 1];
-    if (fillGhosts) fillGhostsAll(p, C, coarse);
+    if (fillGhosts) fillGhostsAll(p, C, coarse, lf + 1);
     const int R0 = C.R[0], R1 = C.R[1], R2 = C.R[2];
     p.pool.run(F.N[0], [&](int ib, int ie) {
         for (int i = ib; i < ie; ++i)
@@ -695,7 +742,7 @@ struct Solver {
     // MG.C:19-130
     void cycle(int l) {
         Level& L = p.lv[l];
-        if (l == coarseLevel) L.b[L.at(0, 0, 0)] = 0.0;
+        if (l == coarseLevel && p.singular()) L.b[L.at(0, 0, 0)] = 0.0;
         if (l > 0) std::fill(L.x.begin(), L.x.end(), 0.0);
         if (o.n_pre > 0) smoothLevel(p, l, o.smoother, o.n_pre);
         if (l < coarseLevel) {
@@ -726,8 +773,8 @@ void assembleAll(P& p, const bmgo_options& o) {
     const int lc = absCoarseLevel(p, o);
     for (size_t l = 0; l < p.lv.size(); ++l) assembleLevel(p, p.lv[l]);
     // MG.C:431-445: pin first (solver.C:201-231), then eliminate ghosts
-    if (lc >= 0 && lc < (int)p.lv.size()) setSingularityConstraint(p, p.lv[lc]);
-    for (size_t l = 0; l < p.lv.size(); ++l) eliminateNeumann(p, p.lv[l]);
+    if (lc >= 0 && lc < (int)p.lv.size() && p.singular()) setSingularityConstraint(p, p.lv[lc]);
+    for (size_t l = 0; l < p.lv.size(); ++l) eliminateWalls(p, p.lv[l], (int)l);
     p.coarseLevelIdx = lc;
 }
 
@@ -768,6 +815,16 @@ bmgo_problem* bmgo_create(const int N[3], const double* px, const double* py, co
     const double* pts[3] = {px, py, pz};
     buildLevels(*p, N, pts);
     return p;
+}
+
+int bmgo_set_faces(bmgo_problem* p, const int dirichlet[6], const double value[6]) {
+    for (int f = 0; f < 6; ++f)
+        if ((dirichlet[f] || (value && value[f] != 0.0)) && p->periodic[f / 2]) return -1;
+    for (int f = 0; f < 6; ++f) {
+        p->dirichlet[f] = dirichlet[f] != 0;
+        p->dval[f] = value ? value[f] : 0.0;
+    }
+    return 0;
 }
 
 void bmgo_destroy(bmgo_problem* p) { delete p; }
@@ -853,8 +910,9 @@ int bmgo_solve(bmgo_problem* pp, const bmgo_options* o, const double* b, double*
         std::fill(L.r.begin(), L.r.end(), 0.0);
     }
     copyIn(L0, b, L0.b);
+    for (long c = 0; c < L0.cells(); ++c) L0.b[c] += p.bdir[c];
     copyIn(L0, x, L0.x);
-    fillGhostsAll(p, L0, L0.x);
+    fillGhostsAll(p, L0, L0.x, 0);
 
     residualLevel(p, L0, false);  // initial residual without boundary correction
 
@@ -909,7 +967,7 @@ void bmgo_residual(bmgo_problem* p, int l, const double* x, const double* b, dou
     std::fill(L.x.begin(), L.x.end(), 0.0);
     copyIn(L, x, L.x);
     copyIn(L, b, L.b);
-    fillGhostsAll(*p, L, L.x);
+    fillGhostsAll(*p, L, L.x, l);
     residualLevel(*p, L, true);
     copyOut(L, L.r, r);
 }
@@ -919,7 +977,7 @@ void bmgo_smooth(bmgo_problem* p, int l, int smoother, int sweeps, double* x, co
     std::fill(L.x.begin(), L.x.end(), 0.0);
     copyIn(L, x, L.x);
     copyIn(L, b, L.b);
-    fillGhostsAll(*p, L, L.x);
+    fillGhostsAll(*p, L, L.x, l);
     smoothLevel(*p, l, smoother, sweeps);
     copyOut(L, L.x, x);
 }
@@ -929,7 +987,7 @@ void bmgo_colour_pass(bmgo_problem* p, int l, int colour, double* x, const doubl
     std::fill(L.x.begin(), L.x.end(), 0.0);
     copyIn(L, x, L.x);
     copyIn(L, b, L.b);
-    fillGhostsAll(*p, L, L.x);
+    fillGhostsAll(*p, L, L.x, l);
     const int S[3] = {1, 1, 1};
     const int E[3] = {1 + L.N[0], 1 + L.N[1], 1 + L.N[2]};
     rbgsPass(*p, L, S, E, colour, false);

@@ -21,6 +21,11 @@
  *   Laplacian assembly          src/briscolaFiniteVolume/schemes/laplacianSchemes/linearGaussLaplacianScheme/linearGaussLaplacianScheme.C:22-102
  *   face deltas                 src/briscolaFiniteVolume/fvMeshMetrics.C:848-893
  *   Neumann elimination         src/briscolaFiniteVolume/boundaryConditions/NeumannBoundaryCondition/NeumannBoundaryCondition.C:19-85
+ *   Dirichlet elimination/ghost src/briscolaFiniteVolume/boundaryConditions/DirichletBoundaryCondition/DirichletBoundaryCondition.C:19-80
+ *   Neumann gradient values     NeumannBoundaryCondition.C:44-50 (b -= A_f g / delta on level 0)
+ *   singularity test            src/briscolaFiniteVolume/linearSystems/linearSystem/linearSystem.H:227-230,
+ *                               src/briscolaFiniteVolume/fields/meshLevels/meshLevel/meshLevel.C:555-583
+ *   ghost fill order            src/briscolaFiniteVolume/fields/meshLevels/meshLevel/meshLevel.C:231-253,301-328
  *   periodic ghost copy         src/briscolaFiniteVolume/boundaryConditions/periodicBoundaryCondition/periodicBoundaryCondition.C:47-92
  *   level sizes                 src/briscolaCore/include/utils.H:1152-1170, src/briscolaMesh/mesh/mesh.C:19-53,
  *                               src/briscolaMesh/level/level.H:144-147
@@ -33,8 +38,9 @@
  *     transfer operators factor into per-axis weights, which are computed
  *     on the fly instead of being cached per cell;
  *   - edge and corner ghosts of a level are filled axis by axis (periodic
- *     image or zero-gradient copy), which is what the reference's unset-BC
- *     copies and periodic edge boundaries give for the face-linked cases here;
+ *     image, zero-gradient copy or Dirichlet mirror), which is what the
+ *     reference's periodic edge boundaries give; where only walls meet, the
+ *     reference's unset-boundary copy of the diagonal interior cell;
  *   - sums that the reference performs with gSum are done per i-plane and
  *     combined in plane order, so results are independent of the thread count.
  */
@@ -74,11 +80,20 @@ void bmgo_default_options(bmgo_options* o);
 
 /* One brick with N[d] cells; pts_d holds N[d]+1 vertex coordinates along
  * axis d.  periodic[d] != 0 makes both faces of axis d periodic, otherwise
- * both are homogeneous Neumann walls.  nthreads <= 0 uses all cores. */
+ * both are homogeneous Neumann walls (bmgo_set_faces makes walls Dirichlet).
+ * nthreads <= 0 uses all cores. */
 bmgo_problem* bmgo_create(const int N[3], const double* pts_x,
                           const double* pts_y, const double* pts_z,
                           const int periodic[3], int nthreads);
 void bmgo_destroy(bmgo_problem* p);
+/* Wall conditions: dirichlet[f] != 0 turns wall face f (x-lo, x-hi, y-lo,
+ * y-hi, z-lo, z-hi) into a Dirichlet face with the uniform value value[f];
+ * on the other walls value[f] is the Neumann gradient (NULL: homogeneous
+ * everywhere).  A Dirichlet face makes the system non-singular: no pin, no
+ * forced coarse cell (linearSystem.H:227-230).  Returns -1 (and changes
+ * nothing) for a Dirichlet face or a nonzero value on a periodic axis.
+ * Takes effect at the next assembly. */
+int  bmgo_set_faces(bmgo_problem* p, const int dirichlet[6], const double* value);
 
 int  bmgo_num_levels(const bmgo_problem* p);
 void bmgo_level_shape(const bmgo_problem* p, int l, int N[3]);
@@ -98,8 +113,8 @@ void bmgo_set_lambda(bmgo_problem* p, const double* lx, const double* ly,
 /* lambda of one level, face direction fd, shape as above for that level */
 void bmgo_get_lambda(const bmgo_problem* p, int l, int fd, double* out);
 
-/* Build A on every level (Laplacian + Neumann elimination + singular pin on
- * the coarsest solve level given by opts->coarse_level). */
+/* Build A on every level (Laplacian + wall elimination + singular pin on
+ * the coarsest solve level given by opts->coarse_level, when singular). */
 void bmgo_assemble(bmgo_problem* p, const bmgo_options* o);
 /* 7 coefficients per interior cell {c,l,r,b,t,a,f}, k fastest */
 void bmgo_get_matrix(const bmgo_problem* p, int l, double* out7);

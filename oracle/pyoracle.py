@@ -67,6 +67,7 @@ def lib():
         L.bmgo_create.restype = vp
         L.bmgo_create.argtypes = [ip, dp, dp, dp, ip, ctypes.c_int]
         L.bmgo_destroy.argtypes = [vp]
+        L.bmgo_set_faces.argtypes = [vp, ip, dp]
         L.bmgo_num_levels.argtypes = [vp]
         L.bmgo_level_shape.argtypes = [vp, ctypes.c_int, ip]
         L.bmgo_level_ratio.argtypes = [vp, ctypes.c_int, ip]
@@ -110,13 +111,24 @@ class Oracle:
     """One rectilinear brick: ``points`` is a list of three vertex-coordinate
     arrays (N_d + 1 each); ``periodic`` flags per axis (walls otherwise)."""
 
-    def __init__(self, points, periodic=(False, False, False), nthreads: int = 0):
+    def __init__(self, points, periodic=(False, False, False), nthreads: int = 0, dirichlet=None,
+                 values=None):
         self.points = [np.ascontiguousarray(p, dtype=np.float64) for p in points]
         self.N = tuple(len(p) - 1 for p in self.points)
         N = (ctypes.c_int * 3)(*self.N)
         per = (ctypes.c_int * 3)(*[int(bool(x)) for x in periodic])
         self.periodic = tuple(bool(x) for x in periodic)
         self._p = lib().bmgo_create(N, *[_dp(p) for p in self.points], per, int(nthreads))
+        if dirichlet is not None:
+            self.set_faces(dirichlet, values)
+
+    def set_faces(self, dirichlet, values=None):
+        """Dirichlet walls (flags per face x-lo, x-hi, y-lo, ...) with uniform
+        values; the other walls stay Neumann."""
+        self._dval = np.ascontiguousarray(values if values is not None else np.zeros(6), dtype=np.float64)
+        flags = (ctypes.c_int * 6)(*[int(bool(x)) for x in dirichlet])
+        if lib().bmgo_set_faces(self._p, flags, _dp(self._dval)) != 0:
+            raise ValueError("a Dirichlet face on a periodic axis")
 
     def __del__(self):
         if getattr(self, "_p", None):

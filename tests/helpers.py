@@ -186,3 +186,90 @@ def union_solve(mesh, b):
     rhs[0] = 0.0
     x = spl.spsolve(sp.csc_matrix(A), rhs)
     return vmean(x, V), V
+
+
+def brick_operator(points, bc, values=(0.0,) * 6, lam=None):
+    """Sparse FV Laplacian of one brick with periodic, Neumann and Dirichlet
+    faces, written from the reference's rules independently of the oracle:
+    off-diagonal area * delta * lambda (delta = 1/|cc_P - cc_N|, a wall's
+    ghost centre one first spacing beyond the wall, levelPoints.C:198-236),
+    centre minus the row; a Neumann wall drops its face and moves
+    -A_f g / delta to the right-hand side (gradient g,
+    NeumannBoundaryCondition.C:19-56), a Dirichlet wall adds its coefficient
+    once more to the centre and moves -2 A_f g there (value g,
+    DirichletBoundaryCondition.C:19-51).  bc: "periodic",
+    "Neumann" or "Dirichlet" per face (x-lo, x-hi, y-lo, ...).  Returns
+    (A, V, bdir): rows k fastest, V the cell volumes, bdir the right-hand-side
+    term of the Dirichlet values (add it to b_sys)."""
+    import scipy.sparse as sp
+
+    pts = [np.asarray(p, dtype=np.float64) for p in points]
+    n = tuple(len(p) - 1 for p in pts)
+    ntot = int(np.prod(n))
+    idx = np.arange(ntot).reshape(n)
+    h = [np.diff(p) for p in pts]
+    cc = [0.5 * (p[1:] + p[:-1]) for p in pts]
+    rows, cols, vals = [], [], []
+    diag = np.zeros(ntot)
+    bdir = np.zeros(ntot)
+    for d in range(3):
+        t1, t2 = (d + 1) % 3, (d + 2) % 3
+        area = np.ones(n)
+        shp1 = [1, 1, 1]
+        shp1[t1] = n[t1]
+        shp2 = [1, 1, 1]
+        shp2[t2] = n[t2]
+        area = area * h[t1].reshape(shp1) * h[t2].reshape(shp2)
+        lamd = None if lam is None else np.asarray(lam[d], dtype=np.float64)
+        periodic = bc[2 * d] == "periodic"
+        for q in range(n[d] + 1):  # face below cell q (q = n: the top face)
+            sl_face = [slice(None)] * 3
+            sl_face[d] = slice(q, q + 1)
+            lf = 1.0 if lamd is None else lamd[tuple(sl_face)]
+            if 0 < q < n[d]:
+                dc = abs(cc[d][q] - cc[d][q - 1])
+                sl_p = [slice(None)] * 3
+                sl_p[d] = slice(q - 1, q)
+                sl_q = [slice(None)] * 3
+                sl_q[d] = slice(q, q + 1)
+                a = (area[tuple(sl_q)] / dc * lf).ravel()
+                P, Q = idx[tuple(sl_p)].ravel(), idx[tuple(sl_q)].ravel()
+                rows += [P, Q]
+                cols += [Q, P]
+                vals += [a, a]
+                diag[P] -= a
+                diag[Q] -= a
+                continue
+            side = 0 if q == 0 else 1
+            cell = 0 if q == 0 else n[d] - 1
+            sl_c = [slice(None)] * 3
+            sl_c[d] = slice(cell, cell + 1)
+            C = idx[tuple(sl_c)].ravel()
+            if periodic:
+                if q == n[d]:
+                    continue  # the wrapped face is the q = 0 one
+                dc = abs(0.5 * (h[d][0] + h[d][-1]))
+                sl_o = [slice(None)] * 3
+                sl_o[d] = slice(n[d] - 1, n[d])
+                a = (area[tuple(sl_c)] / dc * lf).ravel()
+                O = idx[tuple(sl_o)].ravel()
+                rows += [C, O]
+                cols += [O, C]
+                vals += [a, a]
+                diag[C] -= a
+                diag[O] -= a
+                continue
+            kind = bc[2 * d + side]
+            if kind == "Neumann":
+                # gradient g: ghost = x + g * distance, b -= A_f g / delta
+                bdir[C] -= (area[tuple(sl_c)] * lf).ravel() * values[2 * d + side]
+                continue
+            a = (area[tuple(sl_c)] / h[d][cell] * lf).ravel()
+            diag[C] -= 2.0 * a
+            bdir[C] -= 2.0 * a * values[2 * d + side]
+    A = sp.csr_matrix((np.concatenate(vals) if vals else np.zeros(0),
+                       (np.concatenate(rows) if rows else np.zeros(0, int),
+                        np.concatenate(cols) if cols else np.zeros(0, int))), shape=(ntot, ntot))
+    A = (A + sp.diags(diag)).tocsr()
+    V = (h[0][:, None, None] * h[1][None, :, None] * h[2][None, None, :]).ravel()
+    return A, V, bdir

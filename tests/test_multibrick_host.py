@@ -102,3 +102,30 @@ def test_too_many_bricks_is_unsupported():
 def test_valid_multibrick_passes_the_host_checks():
     mesh, _, _ = workloads.multibrick(4)
     assert "no usable" in _create_error(mesh)
+
+
+def test_dirichlet_and_gradients_on_multibrick_are_unsupported():
+    bc = ("Dirichlet",) + ("Neumann",) * 5
+    m = Mesh([Brick([_pts(8, 0), _pts(8, 0), _pts(8, 0)], bc, (0, 0, 0)),
+              Brick([_pts(8, 0), _pts(8, 8), _pts(8, 0)], bc, (0, 8, 0))])
+    assert "unsupported" in _create_error(m)
+    vals = (0.0, 0.5, 0.0, 0.0, 0.0, 0.0)
+    m = Mesh([Brick([_pts(8, 0), _pts(8, 0), _pts(8, 0)], ("Neumann",) * 6, (0, 0, 0), vals),
+              Brick([_pts(8, 0), _pts(8, 8), _pts(8, 0)], ("Neumann",) * 6, (0, 8, 0))])
+    assert "unsupported" in _create_error(m)
+
+
+def test_unknown_face_type_and_bad_values_are_rejected():
+    pts = [_pts(8, 0), _pts(8, 0), _pts(8, 0)]
+    with pytest.raises(bb.FatalError, match="Incompatible boundary condition"):
+        bb.Context(Mesh([Brick(pts, ("empty",) * 6)]), bb.make_options({}))
+    bad = Brick(pts, ("Dirichlet",) + ("Neumann",) * 5, (0, 0, 0), (float("nan"),) + (0.0,) * 5)
+    assert "invalid argument" in _create_error(Mesh([bad]))
+
+
+@pytest.mark.skipif(not _no_gpu(), reason="a GPU is present")
+def test_single_brick_dirichlet_passes_the_host_checks():
+    pts = [_pts(8, 0), _pts(8, 0), _pts(8, 0)]
+    m = Mesh([Brick(pts, ("Dirichlet", "Neumann", "periodic", "periodic", "Neumann", "Dirichlet"),
+                    (0, 0, 0), (1.0, 0.5, 0.0, 0.0, 0.0, -2.0))])
+    assert "no usable" in _create_error(m)
