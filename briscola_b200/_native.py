@@ -41,6 +41,7 @@ class Brick(ctypes.Structure):
         ("bc", ctypes.c_int * 6),
         ("origin", ctypes.c_int * 3),
         ("value", ctypes.c_double * 6),
+        ("transform", ctypes.c_int * 3),
     ]
 
 

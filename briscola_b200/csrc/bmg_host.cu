@@ -45,6 +45,10 @@ struct HostBrick {
     Axis ax[3];
     bool open[6] = {false, false, false, false, false, false};  // periodic or touching another brick
     int nbr[6] = {-1, -1, -1, -1, -1, -1};  // a brick touching the face (its ghost points come from it)
+    // orientation of the caller's arrays: local axis d runs along axis
+    // tax[d] of this (global) frame, reversed when tfl[d]
+    int tax[3] = {0, 1, 2};
+    int tfl[3] = {0, 0, 0};
     long si = 0, sj = 0;      // strides
     long off = 0;             // slab offset of the brick's block
     long base = 0;            // slab index of interior cell (0,0,0)
@@ -266,7 +270,20 @@ Bricks<T> bricks(const bmg_ctx* c, int l) {
         v.sj = K.sj;
         v.base = K.base;
         v.cells = H.cells;
-        v.cbase = K.cbase;
+        // compact (caller) index of cell (i,j,k) of this frame: the brick's
+        // own k-fastest order, cbase + i*cs[0] + j*cs[1] + k*cs[2]
+        {
+            long ls[3];
+            ls[2] = 1;
+            ls[1] = K.n[K.tax[2]];
+            ls[0] = ls[1] * K.n[K.tax[1]];
+            long off = 0;
+            for (int d = 0; d < 3; ++d) {
+                v.cs[K.tax[d]] = (int)(K.tfl[d] ? -ls[d] : ls[d]);
+                if (K.tfl[d]) off += (long)(K.n[K.tax[d]] - 1) * ls[d];
+            }
+            v.cbase = K.cbase + off;
+        }
         v.to = K.to;
         v.tab64 = H.tab64;
         if constexpr (sizeof(T) == 8) {
@@ -529,18 +546,49 @@ void readBricks(bmg_ctx* c, const bmg_mesh_desc* mesh, HostLevel& L0) {
     for (int b = 0; b < nb; ++b) {
         const bmg_brick& B = mesh->bricks[b];
         HostBrick K;
+        // Orientation (the transform T of parallelBoundaryCondition.C:148-163
+        // between a brick's frame and its neighbours'): the brick is kept in
+        // the mesh's frame on the device, and only the caller's arrays are
+        // read and written in the brick's own frame.
+        const bool ident = B.transform[0] == 0 && B.transform[1] == 0 && B.transform[2] == 0;
+        int seen = 0;
+        for (int d = 0; d < 3 && !ident; ++d) {
+            const int t = B.transform[d], a = std::abs(t) - 1;
+            if (a < 0 || a > 2 || ((seen >> a) & 1))
+                throw BadArg{BMG_BAD_ARG, "brick transform is not a signed permutation of the axes"};
+            seen |= 1 << a;
+            K.tax[d] = a;
+            K.tfl[d] = t < 0;
+        }
+        // the brick in the mesh's frame: extents, vertex coordinates (given
+        // in local order along each local axis), face conditions and values
+        int gn[3] = {0, 0, 0}, gbc[6];
+        double gval[6];
+        std::vector<double> gp[3];
         for (int d = 0; d < 3; ++d) {
             if (B.n[d] < 1) throw BadArg{BMG_BAD_ARG, "brick with fewer than one cell along an axis"};
             if (!B.points[d]) throw BadArg{BMG_BAD_ARG, "missing vertex coordinates"};
-            for (int q = 0; q < B.n[d]; ++q)
-                if (!(B.points[d][q + 1] > B.points[d][q]))
-                    throw BadArg{BMG_BAD_ARG, "vertex coordinates must increase strictly"};
-            const int lo = B.bc[2 * d], hi = B.bc[2 * d + 1];
+            const int a = K.tax[d], n = B.n[d];
+            gn[a] = n;
+            gp[a].resize(n + 1);
+            for (int q = 0; q <= n; ++q) gp[a][q] = K.tfl[d] ? B.points[d][n - q] : B.points[d][q];
+            for (int side = 0; side < 2; ++side) {
+                const int gs = K.tfl[d] ? 1 - side : side;
+                gbc[2 * a + gs] = B.bc[2 * d + side];
+                gval[2 * a + gs] = B.value[2 * d + side];
+            }
+        }
+        for (int d = 0; d < 3; ++d) {
+            for (int q = 0; q < gn[d]; ++q)
+                if (!(gp[d][q + 1] > gp[d][q]))
+                    throw BadArg{BMG_BAD_ARG, "vertex coordinates must be strictly monotone (increasing along an "
+                                              "axis, decreasing along a reversed one)"};
+            const int lo = gbc[2 * d], hi = gbc[2 * d + 1];
             if ((lo == BMG_BC_PERIODIC) != (hi == BMG_BC_PERIODIC))
                 throw BadArg{BMG_BAD_ARG, "periodic faces must come in opposite pairs"};
             for (int side = 0; side < 2; ++side) {
-                const int t = B.bc[2 * d + side];
-                const double v = B.value[2 * d + side];
+                const int t = gbc[2 * d + side];
+                const double v = gval[2 * d + side];
                 if (t != BMG_BC_PERIODIC && t != BMG_BC_NEUMANN && t != BMG_BC_DIRICHLET)
                     throw BadArg{BMG_BAD_ARG, "unknown boundary condition type"};
                 if (t == BMG_BC_PERIODIC) continue;
@@ -557,10 +605,10 @@ void readBricks(bmg_ctx* c, const bmg_mesh_desc* mesh, HostLevel& L0) {
             if (lo == BMG_BC_PERIODIC && c->multi)
                 throw BadArg{BMG_UNSUPPORTED, "periodic faces on multi-brick meshes are not supported"};
             if (!c->multi) c->periodic[d] = lo == BMG_BC_PERIODIC;
-            K.n[d] = B.n[d];
+            K.n[d] = gn[d];
             K.origin[d] = c->multi ? B.origin[d] : 0;
-            K.ax[d].pts.assign(B.n[d] + 3, 0.0);
-            for (int q = 0; q <= B.n[d]; ++q) K.ax[d].pts[q + 1] = B.points[d][q];
+            K.ax[d].pts.assign(gn[d] + 3, 0.0);
+            for (int q = 0; q <= gn[d]; ++q) K.ax[d].pts[q + 1] = gp[d][q];
             K.open[2 * d] = K.open[2 * d + 1] = c->periodic[d];
         }
         L0.br.push_back(std::move(K));
@@ -627,6 +675,8 @@ bool coarsenLevel(const bmg_ctx* c, const HostLevel& F, HostLevel& C) {
         }
         if (!anyChange) return false;
         for (int d = 0; d < 3; ++d) {
+            K.tax[d] = B.tax[d];
+            K.tfl[d] = B.tfl[d];
             K.ax[d].pts.assign(K.n[d] + 3, 0.0);
             for (int q = 0; q <= K.n[d]; ++q) K.ax[d].pts[q + 1] = B.ax[d].pts[q * K.R[d] + 1];
             K.open[2 * d] = K.open[2 * d + 1] = c->periodic[d];
@@ -649,6 +699,10 @@ bool coarsenLevel(const bmg_ctx* c, const HostLevel& F, HostLevel& C) {
         for (int f = 0; f < 6; ++f) {
             K.open[f] = B.open[f];
             K.nbr[f] = B.nbr[f];
+        }
+        for (int d = 0; d < 3; ++d) {
+            K.tax[d] = B.tax[d];
+            K.tfl[d] = B.tfl[d];
         }
         C.br.push_back(std::move(K));
     }
@@ -1589,14 +1643,23 @@ int solveImpl(bmg_ctx* c, const double* b, double* x, int flags, bmg_report* rep
 void restrictLambda(bmg_ctx* c, const double* src[3]) {
     HostLevel& L0 = c->lv[0];
     long q[3] = {0, 0, 0};
-    for (auto& B : L0.br)
-        for (int fd = 0; fd < 3; ++fd) {
-            B.lam_user[fd].assign(B.cells, 1.0);
-            const int e0 = fd == 0, e1 = fd == 1, e2 = fd == 2;
-            for (int i = 0; i < B.n[0] + e0; ++i)
-                for (int j = 0; j < B.n[1] + e1; ++j)
-                    for (int k = 0; k < B.n[2] + e2; ++k) B.lam_user[fd][B.loc(i, j, k)] = src[fd][q[fd]++];
+    for (auto& B : L0.br) {
+        for (int fd = 0; fd < 3; ++fd) B.lam_user[fd].assign(B.cells, 1.0);
+        // the caller's arrays are in the brick's own frame: local face
+        // direction ld, local face/cell indices l[] in local order
+        for (int ld = 0; ld < 3; ++ld) {
+            int ln[3];
+            for (int d = 0; d < 3; ++d) ln[d] = B.n[B.tax[d]] + (d == ld);
+            int l[3];
+            for (l[0] = 0; l[0] < ln[0]; ++l[0])
+                for (l[1] = 0; l[1] < ln[1]; ++l[1])
+                    for (l[2] = 0; l[2] < ln[2]; ++l[2]) {
+                        int g[3];
+                        for (int d = 0; d < 3; ++d) g[B.tax[d]] = B.tfl[d] ? ln[d] - 1 - l[d] : l[d];
+                        B.lam_user[B.tax[ld]][B.loc(g[0], g[1], g[2])] = src[ld][q[ld]++];
+                    }
         }
+    }
     for (size_t l = 0; l + 1 < c->lv.size(); ++l)
         for (size_t b = 0; b < c->lv[l].br.size(); ++b) {
             const HostBrick& F = c->lv[l].br[b];
@@ -1755,8 +1818,11 @@ int bmg_set_coefficients(bmg_ctx* c, const double* lx, const double* ly, const d
             const double* src[3] = {lx, ly, lz};
             long nf[3] = {0, 0, 0};
             for (const auto& B : c->lv[0].br)
-                for (int fd = 0; fd < 3; ++fd)
-                    nf[fd] += (long)(B.n[0] + (fd == 0)) * (B.n[1] + (fd == 1)) * (B.n[2] + (fd == 2));
+                for (int fd = 0; fd < 3; ++fd) {  // local face direction, local extents
+                    long m = 1;
+                    for (int d = 0; d < 3; ++d) m *= B.n[B.tax[d]] + (d == fd);
+                    nf[fd] += m;
+                }
             for (int fd = 0; fd < 3; ++fd)
                 for (long q = 0; q < nf[fd]; ++q)
                     if (!(src[fd][q] > 0.0) || !std::isfinite(src[fd][q]))
@@ -1824,6 +1890,9 @@ ProjGeom projGeom(const bmg_ctx* c) {
     if (c->multi) throw BadArg{BMG_UNSUPPORTED, "projection steps take a single-brick mesh"};
     const HostLevel& L = c->lv[0];
     const HostBrick& B = L.br[0];
+    for (int d = 0; d < 3; ++d)
+        if (B.tax[d] != d || B.tfl[d])
+            throw BadArg{BMG_UNSUPPORTED, "projection steps take a brick in the mesh's own orientation"};
     ProjGeom G{};
     for (int d = 0; d < 3; ++d) {
         G.n[d] = B.n[d];
@@ -1865,7 +1934,8 @@ int bmg_project_correct(bmg_ctx* c, double* u0, double* u1, double* u2, const do
 
 int bmg_level_shape(const bmg_ctx* c, int l, int brick, int n[3]) {
     if (!validLevel(c, l) || !n || brick < 0 || brick >= (int)c->lv[l].br.size()) return BMG_BAD_ARG;
-    for (int d = 0; d < 3; ++d) n[d] = c->lv[l].br[brick].n[d];
+    const auto& K = c->lv[l].br[brick];
+    for (int d = 0; d < 3; ++d) n[d] = K.n[K.tax[d]];  // in the brick's own frame
     return BMG_OK;
 }
 

@@ -57,7 +57,9 @@ struct LevelView {
     long si, sj;       // strides of i and j (k contiguous)
     long base;         // slab index of interior cell (0,0,0)
     long cells;        // size of the whole slab (all bricks)
-    long cbase;        // offset of the brick in compact arrays
+    long cbase;        // compact index of cell (0,0,0): with cs[], the caller's
+    int cs[3];         // array index cbase + i*cs[0] + j*cs[1] + k*cs[2]
+                       // (the brick's own frame, k fastest there)
     T* x;              // slab pointers
     T* b;
     const T* tab;      // 1-D tables (TabOff layout) in precision T

@@ -567,7 +567,7 @@ __global__ void __launch_bounds__(256) k_residual_out(Bricks<T> B, double* out) 
     stencil(L.x, c, L.si, L.sj, w, s, d);
     const double r = (double)(L.b[c] + d * L.x[c] - s);
     const double V = L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j] * L.tab64[L.to.h[2] + k];
-    out[L.cbase + ((long)i * L.n1 + j) * L.n2 + k] = r * V;
+    out[compact_index(L, i, j, k)] = r * V;
 }
 
 // ---------------------------------------------------------------------------
@@ -723,7 +723,7 @@ __global__ void __launch_bounds__(256) k_load_b(Bricks<double> B, const double* 
     if (j >= L.n1 || k >= L.n2) return;
     const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
     const double V = L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j] * L.tab64[L.to.h[2] + k];
-    double v = compact[L.cbase + ((long)i * L.n1 + j) * L.n2 + k] / V;
+    double v = compact[compact_index(L, i, j, k)] / V;
     // face values: Dirichlet b -= 2 A_f g, Neumann b -= A_f g / delta
     if (B.walls.mask | B.walls.nmask) v -= wall_sum(L, B.walls, i, j, k, c, true);
     L.b[c] = v;
@@ -736,7 +736,7 @@ __global__ void __launch_bounds__(256) k_load_x(Bricks<double> B, const double* 
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (j >= L.n1 || k >= L.n2) return;
     const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
-    store_x(L, c, i, j, k, compact[L.cbase + ((long)i * L.n1 + j) * L.n2 + k]);
+    store_x(L, c, i, j, k, compact[compact_index(L, i, j, k)]);
 }
 
 __global__ void __launch_bounds__(256) k_store_x(Bricks<double> B, double* compact) {
@@ -746,7 +746,7 @@ __global__ void __launch_bounds__(256) k_store_x(Bricks<double> B, double* compa
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (j >= L.n1 || k >= L.n2) return;
     const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
-    compact[L.cbase + ((long)i * L.n1 + j) * L.n2 + k] = L.x[c];
+    compact[compact_index(L, i, j, k)] = L.x[c];
 }
 
 template <typename T>
@@ -757,7 +757,7 @@ __global__ void __launch_bounds__(256) k_load_field(Bricks<T> B, int field, cons
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (j >= L.n1 || k >= L.n2) return;
     const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
-    double v = compact[L.cbase + ((long)i * L.n1 + j) * L.n2 + k];
+    double v = compact[compact_index(L, i, j, k)];
     if (field == 0) {
         store_x(L, c, i, j, k, (T)v);
     } else {
@@ -777,7 +777,7 @@ __global__ void __launch_bounds__(256) k_store_field(Bricks<T> B, int field, dou
     double v = field == 0 ? (double)L.x[c] : (double)L.b[c];
     if (field == 1 && unscale)
         v *= L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j] * L.tab64[L.to.h[2] + k];
-    compact[L.cbase + ((long)i * L.n1 + j) * L.n2 + k] = v;
+    compact[compact_index(L, i, j, k)] = v;
 }
 
 __global__ void __launch_bounds__(256) k_add_correction(Bricks<double> B, Bricks<float> E) {

@@ -103,6 +103,12 @@ __device__ __forceinline__ double wall_sum(const LevelView<double>& L, const Wal
     return s;
 }
 
+// index of cell (i,j,k) in the caller's (compact, brick-frame) arrays
+template <typename T>
+__device__ __forceinline__ long compact_index(const LevelView<T>& L, int i, int j, int k) {
+    return L.cbase + (long)i * L.cs[0] + (long)j * L.cs[1] + (long)k * L.cs[2];
+}
+
 // Store an interior value and its periodic ghost images (faces, edges and
 // corners), replacing the reference's per-sweep periodic ghost copy
 // (periodicBoundaryCondition.C:53-92).  Per axis a cell has up to two

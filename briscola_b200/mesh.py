@@ -48,12 +48,17 @@ def tanh_points(n: int, gamma: float, length: float = 1.0, start: float = 0.0) -
 class Brick:
     """One brick: ``points`` holds the vertex coordinates per axis; ``bc`` the
     boundary type of faces x-lo, x-hi, y-lo, y-hi, z-lo, z-hi; ``values`` the
-    (uniform) value of each Dirichlet face."""
+    (uniform) Dirichlet value or Neumann gradient of each face; ``transform``
+    the orientation of the brick's own frame in the mesh (local axis d runs
+    along mesh axis |t_d| - 1, reversed when t_d < 0; zeros: the mesh's
+    frame).  Points, faces, values and the brick's arrays are in its own
+    frame, ``origin`` in the mesh's."""
 
     points: list
     bc: tuple = (NEUMANN,) * 6
     origin: tuple = (0, 0, 0)
     values: tuple = (0.0,) * 6
+    transform: tuple = (0, 0, 0)
 
     def __post_init__(self):
         self.points = [np.ascontiguousarray(p, dtype=np.float64) for p in self.points]
@@ -69,7 +74,7 @@ class Brick:
         return tuple(self.bc[2 * d] == PERIODIC for d in range(3))
 
     def cell_sizes(self, axis: int) -> np.ndarray:
-        return np.diff(self.points[axis])
+        return np.abs(np.diff(self.points[axis]))  # points decrease along a reversed axis
 
     def cell_centres(self, axis: int) -> np.ndarray:
         p = self.points[axis]

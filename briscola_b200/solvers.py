@@ -183,6 +183,8 @@ def _mesh_desc(mesh: Mesh):
                 raise FatalError(f"Incompatible boundary condition {br.bc[f]} for the GPU multigrid")
             bricks[q].bc[f] = _BC[br.bc[f]]
             bricks[q].value[f] = float(br.values[f])
+        for d in range(3):
+            bricks[q].transform[d] = int(br.transform[d])
     desc = N.MeshDesc(len(mesh.bricks), bricks)
     return desc, (bricks, keep)
 

@@ -81,6 +81,13 @@ typedef struct bmg_brick {
     int origin[3];            /* cell offset in the global lattice (multi-brick)       */
     double value[6];          /* Dirichlet value or Neumann gradient of each face
                                  (uniform; ignored on periodic faces)             */
+    int transform[3];         /* orientation of the brick's own frame: local axis d
+                                 runs along mesh axis |transform[d]|-1, reversed
+                                 when negative (parallelBoundaryCondition.C:148-163's
+                                 T); {0,0,0} = identity.  n, points, bc, value and
+                                 the brick's parts of b, x and lambda are in the
+                                 brick's frame (points in local order, decreasing
+                                 along a reversed axis); origin is in the mesh's. */
 } bmg_brick;
 
 typedef struct bmg_mesh_desc {
