@@ -87,6 +87,12 @@ struct Row4<float> {
     static __device__ __forceinline__ void st(float* p, const float v[4]) {
         *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
     }
+    // two consecutive values from an 8-byte aligned address
+    static __device__ __forceinline__ void ld2(const float* p, float& a, float& b) {
+        const float2 v = *reinterpret_cast<const float2*>(p);
+        a = v.x;
+        b = v.y;
+    }
 };
 template <>
 struct Row4<double> {
@@ -107,6 +113,12 @@ struct Row4<double> {
     static __device__ __forceinline__ void st(double* p, const double v[4]) {
         reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
         reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+    }
+    // two consecutive values from a 16-byte aligned address
+    static __device__ __forceinline__ void ld2(const double* p, double& a, double& b) {
+        const double2 v = *reinterpret_cast<const double2*>(p);
+        a = v.x;
+        b = v.y;
     }
 };
 
@@ -178,8 +190,8 @@ __device__ __forceinline__ void colour_quad_item(const LevelView<T>& L, int i, i
     // periodic images of the two updated cells
     if (L.per0 | L.per1 | L.per2) {
         const int q0 = odd ? 1 : 0;
-        store_x(L, c + q0, i, j, k0 + q0, v0);
-        store_x(L, c + q0 + 2, i, j, k0 + q0 + 2, v2);
+        store_images(L, c + q0, i, j, k0 + q0, v0);
+        store_images(L, c + q0 + 2, i, j, k0 + q0 + 2, v2);
     }
 }
 
@@ -341,21 +353,36 @@ __device__ __forceinline__ void prolong_quad_item(const LevelView<T>& F, const L
     Row4<T>::ld(F.x + c0, xf);
     const int* pk = pidx + 2 * (F.n0 + F.n1);
     const T* wk = pw + F.n0 + F.n1;
+    // Fine cells k0 .. k0+3 (k0 = 4p) have parents 2p, 2p, 2p+1, 2p+1 and
+    // second coarse cells Ka, 2p+1, 2p, Kd: four coarse values per row,
+    // the middle pair (2p, 2p+1) one aligned vector (interior k starts at an
+    // offset of 4 in every row, so 2p sits at an even offset).
+    const int Ka = ldg(pk + 2 * k0 + 1), Kb = ldg(pk + 2 * k0), Kd = ldg(pk + 2 * (k0 + 3) + 1);
+    T w[4], u[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        const int k = k0 + q;
-        const int K0 = ldg(pk + 2 * k), K1 = ldg(pk + 2 * k + 1);
-        const T w = ldg(wk + k), u = T(1) - w;
-        const T v00 = u * X[r00 + K0] + w * X[r00 + K1];
-        const T v01 = u * X[r01 + K0] + w * X[r01 + K1];
-        const T v10 = u * X[r10 + K0] + w * X[r10 + K1];
-        const T v11 = u * X[r11 + K0] + w * X[r11 + K1];
-        xf[q] += ui * (uj * v00 + wj * v01) + wi * (uj * v10 + wj * v11);
+        w[q] = ldg(wk + k0 + q);
+        u[q] = T(1) - w[q];
     }
+    const long rows[4] = {r00, r01, r10, r11};
+    T v[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        T xb, xc;
+        Row4<T>::ld2(X + rows[r] + Kb, xb, xc);
+        const T xa = X[rows[r] + Ka], xd = X[rows[r] + Kd];
+        v[r][0] = u[0] * xb + w[0] * xa;
+        v[r][1] = u[1] * xb + w[1] * xc;
+        v[r][2] = u[2] * xc + w[2] * xb;
+        v[r][3] = u[3] * xc + w[3] * xd;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+        xf[q] += ui * (uj * v[0][q] + wj * v[1][q]) + wi * (uj * v[2][q] + wj * v[3][q]);
     Row4<T>::st(F.x + c0, xf);
     if (F.per0 | F.per1 | F.per2) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) store_x(F, c0 + q, i, j, k0 + q, xf[q]);
+        for (int q = 0; q < 4; ++q) store_images(F, c0 + q, i, j, k0 + q, xf[q]);
     }
 }
 

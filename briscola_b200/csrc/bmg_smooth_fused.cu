@@ -354,10 +354,10 @@ __global__ void __launch_bounds__(SweepShape<T, S, KR>::threads, SweepShape<T, S
                     const long c = (long)rowa + (long)P * sm + k0_raw;
                     Vec<T>::st4(xout + c, q0, q1, q2, q3);
                     if (images) {
-                        store_x(O, c, P, a, k0_raw, q0);
-                        store_x(O, c + 1, P, a, k0_raw + 1, q1);
-                        store_x(O, c + 2, P, a, k0_raw + 2, q2);
-                        store_x(O, c + 3, P, a, k0_raw + 3, q3);
+                        store_images(O, c, P, a, k0_raw, q0);
+                        store_images(O, c + 1, P, a, k0_raw + 1, q1);
+                        store_images(O, c + 2, P, a, k0_raw + 2, q2);
+                        store_images(O, c + 3, P, a, k0_raw + 3, q3);
                     }
                 }
             }

@@ -116,8 +116,18 @@ __device__ __forceinline__ long compact_index(const LevelView<T>& L, int i, int 
 // n-1); both when n == 1.  All combinations are unrolled into predicated
 // stores, so nothing lives in local memory.
 template <typename T>
+__device__ __forceinline__ void store_images(const LevelView<T>& L, long c, int i, int j, int k, T v);
+
+template <typename T>
 __device__ __forceinline__ void store_x(const LevelView<T>& L, long c, int i, int j, int k, T v) {
     L.x[c] = v;
+    store_images(L, c, i, j, k, v);
+}
+
+// the periodic ghost images alone, for kernels that store the interior
+// value themselves (as part of a vector store)
+template <typename T>
+__device__ __forceinline__ void store_images(const LevelView<T>& L, long c, int i, int j, int k, T v) {
     const long up0 = (L.per0 && i == 0) ? (long)L.n0 * L.si : 0;
     const long dn0 = (L.per0 && i == L.n0 - 1) ? -(long)L.n0 * L.si : 0;
     const long up1 = (L.per1 && j == 0) ? (long)L.n1 * L.sj : 0;
