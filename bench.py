@@ -542,7 +542,7 @@ def main():
     # DRAM bytes per launch from the committed ncu summary of this kernel
     traffic = None
     tp = os.path.join(ROOT, "profiles", "k_sweep_fp32_channel256.md" if stages_per_launch else
-                      "k_colour_pass_fp32_channel256.md")
+                      "k_colour_quad_fp32_channel256.md")
     if os.path.exists(tp):
         import re
 
@@ -682,7 +682,7 @@ def main():
                          "kernel": (f"k_sweep<float> level 0 ({launches_per_step} launches of up to "
                                     f"{stages_per_launch} colour stages per 2-sweep step, {chunk}-plane chunks)"
                                     if stages_per_launch else
-                                    f"k_colour_pass<float> level 0 ({launches_per_step} passes per "
+                                    f"k_colour_quad<float> level 0 ({launches_per_step} passes per "
                                     "2-sweep step; autotuner's choice)"),
                          "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                          "frac": round(achieved / hbm, 4), "peak_kind": peak_kind,
