@@ -136,15 +136,15 @@ struct Row4<double> {
 template <typename T, bool VAR>
 __device__ __forceinline__ void colour_quad_item(const LevelView<T>& L, int i, int j, int p, int colour) {
     const int k0 = 4 * p;
-    const long c = L.base + (long)i * L.si + (long)j * L.sj + k0;
+    const int c = cell32(L, i, j, k0), si = (int)L.si, sj = (int)L.sj;
     const T* x = L.x;
     // rows j-1, j, j+1 of this plane (j+1 may be the ghost row)
     T ym[4], own[4], yp[4], xm[4], xp[4], bb[4], wkl[4], wkh[4];
-    Row4<T>::ld(x + c - L.sj, ym);
+    Row4<T>::ld(x + c - sj, ym);
     Row4<T>::ld(x + c, own);
-    Row4<T>::ld(x + c + L.sj, yp);
-    Row4<T>::ld(x + c - L.si, xm);
-    Row4<T>::ld(x + c + L.si, xp);
+    Row4<T>::ld(x + c + sj, yp);
+    Row4<T>::ld(x + c - si, xm);
+    Row4<T>::ld(x + c + si, xp);
     Row4<T>::ld(L.b + c, bb);
     Row4<T>::ldg4(L.tab + L.to.wl[2] + k0, wkl);
     Row4<T>::ldg4(L.tab + L.to.wh[2] + k0, wkh);
@@ -160,9 +160,9 @@ __device__ __forceinline__ void colour_quad_item(const LevelView<T>& L, int i, i
     if (VAR) {
         T l0[4], l0p[4], l1[4], l1p[4], l2[4];
         Row4<T>::ldg4(L.lam0 + c, l0);
-        Row4<T>::ldg4(L.lam0 + c + L.si, l0p);
+        Row4<T>::ldg4(L.lam0 + c + si, l0p);
         Row4<T>::ldg4(L.lam1 + c, l1);
-        Row4<T>::ldg4(L.lam1 + c + L.sj, l1p);
+        Row4<T>::ldg4(L.lam1 + c + sj, l1p);
         Row4<T>::ldg4(L.lam2 + c, l2);
         const T l2r = ldg(L.lam2 + c + 4);
         w0[0] *= BMG_SEL(l0, 0);
@@ -188,7 +188,7 @@ __device__ __forceinline__ void colour_quad_item(const LevelView<T>& L, int i, i
     const T out[4] = {odd ? own[0] : v0, odd ? v0 : own[1], odd ? own[2] : v2, odd ? v2 : own[3]};
     Row4<T>::st(L.x + c, out);
     // periodic images of the two updated cells
-    if (L.per0 | L.per1 | L.per2) {
+    if (quad_has_images(L, i, j, k0)) {
         const int q0 = odd ? 1 : 0;
         store_images(L, c + q0, i, j, k0 + q0, v0);
         store_images(L, c + q0 + 2, i, j, k0 + q0 + 2, v2);
@@ -344,11 +344,9 @@ __device__ __forceinline__ void prolong_quad_item(const LevelView<T>& F, const L
     const T wi = ldg(pw + i), wj = ldg(pw + F.n0 + j);
     const T ui = T(1) - wi, uj = T(1) - wj;
     const T* X = C.x;
-    const long r00 = C.base + (long)I0 * C.si + (long)J0 * C.sj;
-    const long r01 = C.base + (long)I0 * C.si + (long)J1 * C.sj;
-    const long r10 = C.base + (long)I1 * C.si + (long)J0 * C.sj;
-    const long r11 = C.base + (long)I1 * C.si + (long)J1 * C.sj;
-    const long c0 = F.base + (long)i * F.si + (long)j * F.sj + k0;
+    const int r00 = cell32(C, I0, J0, 0), r01 = cell32(C, I0, J1, 0);
+    const int r10 = cell32(C, I1, J0, 0), r11 = cell32(C, I1, J1, 0);
+    const int c0 = cell32(F, i, j, k0);
     T xf[4];
     Row4<T>::ld(F.x + c0, xf);
     const int* pk = pidx + 2 * (F.n0 + F.n1);
@@ -364,7 +362,7 @@ __device__ __forceinline__ void prolong_quad_item(const LevelView<T>& F, const L
         w[q] = ldg(wk + k0 + q);
         u[q] = T(1) - w[q];
     }
-    const long rows[4] = {r00, r01, r10, r11};
+    const int rows[4] = {r00, r01, r10, r11};
     T v[4][4];
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
@@ -380,7 +378,7 @@ __device__ __forceinline__ void prolong_quad_item(const LevelView<T>& F, const L
     for (int q = 0; q < 4; ++q)
         xf[q] += ui * (uj * v[0][q] + wj * v[1][q]) + wi * (uj * v[2][q] + wj * v[3][q]);
     Row4<T>::st(F.x + c0, xf);
-    if (F.per0 | F.per1 | F.per2) {
+    if (quad_has_images(F, i, j, k0)) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) store_images(F, c0 + q, i, j, k0 + q, xf[q]);
     }
@@ -422,21 +420,21 @@ __device__ __forceinline__ void restrict_quad_item(const LevelView<T>& F, const 
             const int j = 2 * J + e;
             const T rab = ra * ldg(ratio + F.n0 + j);
             const T wjl = ldg(F.tab + F.to.wl[1] + j), wjh = ldg(F.tab + F.to.wh[1] + j);
-            const long c = F.base + (long)i * F.si + (long)j * F.sj + k0;
+            const int c = cell32(F, i, j, k0), si = (int)F.si, sj = (int)F.sj;
             T own[4], xm[4], xp[4], ym[4], yp[4], bb[4];
             Row4<T>::ld(F.x + c, own);
-            Row4<T>::ld(F.x + c - F.si, xm);
-            Row4<T>::ld(F.x + c + F.si, xp);
-            Row4<T>::ld(F.x + c - F.sj, ym);
-            Row4<T>::ld(F.x + c + F.sj, yp);
+            Row4<T>::ld(F.x + c - si, xm);
+            Row4<T>::ld(F.x + c + si, xp);
+            Row4<T>::ld(F.x + c - sj, ym);
+            Row4<T>::ld(F.x + c + sj, yp);
             Row4<T>::ld(F.b + c, bb);
             const T left = F.x[c - 1], right = F.x[c + 4];
             T l0[4], l0p[4], l1[4], l1p[4], l2[4], l2r = T(1);
             if (VAR) {
                 Row4<T>::ldg4(F.lam0 + c, l0);
-                Row4<T>::ldg4(F.lam0 + c + F.si, l0p);
+                Row4<T>::ldg4(F.lam0 + c + si, l0p);
                 Row4<T>::ldg4(F.lam1 + c, l1);
-                Row4<T>::ldg4(F.lam1 + c + F.sj, l1p);
+                Row4<T>::ldg4(F.lam1 + c + sj, l1p);
                 Row4<T>::ldg4(F.lam2 + c, l2);
                 l2r = ldg(F.lam2 + c + 4);
             }
@@ -461,7 +459,7 @@ __device__ __forceinline__ void restrict_quad_item(const LevelView<T>& F, const 
             acc1 += rab * (rk[2] * r[2] + rk[3] * r[3]);
         }
     }
-    const long cc = C.base + (long)I * C.si + (long)J * C.sj + K0;
+    const int cc = cell32(C, I, J, K0);
     C.b[cc] = acc0;
     C.b[cc + 1] = acc1;
 }

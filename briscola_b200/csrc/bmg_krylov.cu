@@ -335,7 +335,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_update4(Bricks<double> B
             a += Vr * Vr;
         }
         Quad4<double>::st(L.x + c, xq);
-        if (L.per0 | L.per1 | L.per2) {
+        if (quad_has_images(L, i, j, k0)) {
 #pragma unroll
             for (int e = 0; e < 4; ++e) store_images(L, c + e, i, j, k0 + e, xq[e]);
         }

@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(SweepShape<T, S, KR>::threads, SweepShape<T, S
                     const T q3 = l ? X[sp][0][1] : X[sp][1][1];
                     const long c = (long)rowa + (long)P * sm + k0_raw;
                     Vec<T>::st4(xout + c, q0, q1, q2, q3);
-                    if (images) {
+                    if (images && quad_has_images(O, P, a, k0_raw)) {
                         store_images(O, c, P, a, k0_raw, q0);
                         store_images(O, c + 1, P, a, k0_raw + 1, q1);
                         store_images(O, c + 2, P, a, k0_raw + 2, q2);

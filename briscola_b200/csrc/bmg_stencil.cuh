@@ -103,6 +103,22 @@ __device__ __forceinline__ double wall_sum(const LevelView<double>& L, const Wal
     return s;
 }
 
+// whether any cell of the k-quad (i, j, k0 .. k0+3) has a periodic ghost
+// image (k0 % 4 == 0, n2 % 4 == 0): a cheap test that spares the other
+// quads store_images' per-cell offset arithmetic
+template <typename T>
+__device__ __forceinline__ bool quad_has_images(const LevelView<T>& L, int i, int j, int k0) {
+    return (L.per0 && (i == 0 || i == L.n0 - 1)) || (L.per1 && (j == 0 || j == L.n1 - 1)) ||
+           (L.per2 && (k0 == 0 || k0 + 4 >= L.n2));
+}
+
+// slab index of cell (i,j,k) in 32-bit arithmetic (the host rejects levels
+// of 2^31 cells or more)
+template <typename T>
+__device__ __forceinline__ int cell32(const LevelView<T>& L, int i, int j, int k) {
+    return (int)L.base + i * (int)L.si + j * (int)L.sj + k;
+}
+
 // index of cell (i,j,k) in the caller's (compact, brick-frame) arrays
 template <typename T>
 __device__ __forceinline__ long compact_index(const LevelView<T>& L, int i, int j, int k) {
