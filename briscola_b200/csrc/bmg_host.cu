@@ -64,6 +64,13 @@ struct HostBrick {
 
 struct HostLevel {
     std::vector<HostBrick> br;
+    // multi-brick lattice box: lowest cell lo, extent ext; axes with wrap
+    // set are periodic (a brick face on the box boundary meets the bricks
+    // on the opposite boundary), period = their length in coordinates
+    int lo[3] = {0, 0, 0};
+    int ext[3] = {0, 0, 0};
+    int wrap[3] = {0, 0, 0};
+    double period[3] = {0.0, 0.0, 0.0};
     long cells = 0;   // slab size
     long ncell = 0;   // interior cells of all bricks
     int planes = 0;   // sum of n0
@@ -392,8 +399,12 @@ bool invert(std::vector<double>& M, int n, std::vector<double>& inv) {
     return true;
 }
 
-// brick of a level containing global lattice cell g, with the local cell
-int findBrick(const HostLevel& L, const int g[3], int loc[3]) {
+// brick of a level containing global lattice cell g (wrapped around the
+// box on periodic axes), with the local cell
+int findBrick(const HostLevel& L, const int g0[3], int loc[3]) {
+    int g[3];
+    for (int d = 0; d < 3; ++d)
+        g[d] = L.wrap[d] ? L.lo[d] + (((g0[d] - L.lo[d]) % L.ext[d]) + L.ext[d]) % L.ext[d] : g0[d];
     for (size_t b = 0; b < L.br.size(); ++b) {
         const HostBrick& B = L.br[b];
         bool in = true;
@@ -602,8 +613,7 @@ void readBricks(bmg_ctx* c, const bmg_mesh_desc* mesh, HostLevel& L0) {
                     c->singular = false;
                 }
             }
-            if (lo == BMG_BC_PERIODIC && c->multi)
-                throw BadArg{BMG_UNSUPPORTED, "periodic faces on multi-brick meshes are not supported"};
+            if (lo == BMG_BC_PERIODIC && c->multi) L0.wrap[d] |= 1 << b;  // resolved below
             if (!c->multi) c->periodic[d] = lo == BMG_BC_PERIODIC;
             K.n[d] = gn[d];
             K.origin[d] = c->multi ? B.origin[d] : 0;
@@ -614,8 +624,23 @@ void readBricks(bmg_ctx* c, const bmg_mesh_desc* mesh, HostLevel& L0) {
         L0.br.push_back(std::move(K));
     }
     if (!c->multi) return;
+    // the lattice box; an axis is periodic for every brick or for none
+    for (int d = 0; d < 3; ++d) {
+        int lo = L0.br[0].origin[d], hi = lo + L0.br[0].n[d];
+        for (const auto& K : L0.br) {
+            lo = std::min(lo, K.origin[d]);
+            hi = std::max(hi, K.origin[d] + K.n[d]);
+        }
+        L0.lo[d] = lo;
+        L0.ext[d] = hi - lo;
+        const int all = (1 << nb) - 1;
+        if (L0.wrap[d] != 0 && L0.wrap[d] != all)
+            throw BadArg{BMG_BAD_ARG, "on a multi-brick mesh an axis is periodic for every brick or for none"};
+        L0.wrap[d] = L0.wrap[d] != 0;
+    }
     // bricks must not overlap; faces in the same plane with overlapping
-    // extents are contacts, which need matching vertex coordinates
+    // extents are contacts, which need matching vertex coordinates (on a
+    // periodic axis the box's two ends meet, one period apart)
     for (int a = 0; a < nb; ++a)
         for (int b = a + 1; b < nb; ++b) {
             const HostBrick& A = L0.br[a];
@@ -628,11 +653,14 @@ void readBricks(bmg_ctx* c, const bmg_mesh_desc* mesh, HostLevel& L0) {
         }
     for (int a = 0; a < nb; ++a)
         for (int b = 0; b < nb; ++b) {
-            if (a == b) continue;
             HostBrick& A = L0.br[a];
             const HostBrick& B = L0.br[b];
             for (int d = 0; d < 3; ++d) {
-                if (A.origin[d] + A.n[d] != B.origin[d]) continue;  // A's upper face meets B's lower face
+                // A's upper face meets B's lower face, directly or across
+                // the periodic ends of the box (a brick may meet itself)
+                const bool across = L0.wrap[d] && A.origin[d] + A.n[d] == L0.lo[d] + L0.ext[d] &&
+                                    B.origin[d] == L0.lo[d];
+                if (!across && (a == b || A.origin[d] + A.n[d] != B.origin[d])) continue;
                 const int t1 = (d + 1) % 3, t2 = (d + 2) % 3;
                 const int lo1 = std::max(A.origin[t1], B.origin[t1]);
                 const int hi1 = std::min(A.origin[t1] + A.n[t1], B.origin[t1] + B.n[t1]);
@@ -641,8 +669,14 @@ void readBricks(bmg_ctx* c, const bmg_mesh_desc* mesh, HostLevel& L0) {
                 if (hi1 <= lo1 || hi2 <= lo2) continue;
                 const double scale = std::fabs(A.ax[d].pts[A.n[d] + 1] - A.ax[d].pts[1]) + 1.0;
                 const double tol = 1e-12 * scale;
-                if (std::fabs(A.ax[d].pts[A.n[d] + 1] - B.ax[d].pts[1]) > tol)
+                if (across) {
+                    const double P = A.ax[d].pts[A.n[d] + 1] - B.ax[d].pts[1];
+                    if (L0.period[d] == 0.0) L0.period[d] = P;
+                    if (!(P > 0.0) || std::fabs(P - L0.period[d]) > tol)
+                        throw BadArg{BMG_BAD_ARG, "the periodic ends of the bricks are not one period apart"};
+                } else if (std::fabs(A.ax[d].pts[A.n[d] + 1] - B.ax[d].pts[1]) > tol) {
                     throw BadArg{BMG_BAD_ARG, "bricks meet on a lattice face but their coordinates differ"};
+                }
                 for (int t : {t1, t2}) {
                     const int lo = t == t1 ? lo1 : lo2, hi = t == t1 ? hi1 : hi2;
                     for (int g = lo; g <= hi; ++g)
@@ -687,6 +721,12 @@ bool coarsenLevel(const bmg_ctx* c, const HostLevel& F, HostLevel& C) {
     for (const auto& B : F.br)
         for (int d = 0; d < 3; ++d)
             if (B.n[d] < 4 || B.n[d] % 2 || B.origin[d] % 2) return false;
+    for (int d = 0; d < 3; ++d) {
+        C.lo[d] = F.lo[d] / 2;
+        C.ext[d] = F.ext[d] / 2;
+        C.wrap[d] = F.wrap[d];
+        C.period[d] = F.period[d];
+    }
     for (const auto& B : F.br) {
         HostBrick K;
         for (int d = 0; d < 3; ++d) {
@@ -712,24 +752,35 @@ bool coarsenLevel(const bmg_ctx* c, const HostLevel& F, HostLevel& C) {
 // ghost points and cell tables of every brick of a level; every brick
 // touching a face must agree on the ghost point it gives
 void finishLevel(const bmg_ctx* c, HostLevel& L) {
+    // lattice planes a and b coincide, directly or as the two ends of a
+    // periodic axis
+    auto samePlane = [&](int d, int a, int b) {
+        return a == b || (L.wrap[d] && ((a == L.lo[d] && b == L.lo[d] + L.ext[d]) ||
+                                        (b == L.lo[d] && a == L.lo[d] + L.ext[d])));
+    };
     for (auto& B : L.br)
         for (int d = 0; d < 3; ++d) {
             double g[2] = {NAN, NAN};
             for (int side = 0; side < 2; ++side) {
                 if (B.nbr[2 * d + side] < 0) continue;
                 const HostBrick& N = L.br[B.nbr[2 * d + side]];
-                g[side] = side ? N.ax[d].pts[2] : N.ax[d].pts[N.n[d]];
+                // across the periodic ends the neighbour's coordinates are
+                // one period away
+                const bool across = L.wrap[d] && (side ? B.origin[d] + B.n[d] == L.lo[d] + L.ext[d]
+                                                       : B.origin[d] == L.lo[d]);
+                const double shift = across ? (side ? L.period[d] : -L.period[d]) : 0.0;
+                g[side] = (side ? N.ax[d].pts[2] : N.ax[d].pts[N.n[d]]) + shift;
                 for (const auto& M : L.br) {
                     if (&M == &B || &M == &N) continue;
                     // another brick across the same face plane, overlapping it
                     const int plane = side ? B.origin[d] + B.n[d] : B.origin[d];
-                    if ((side ? M.origin[d] : M.origin[d] + M.n[d]) != plane) continue;
+                    if (!samePlane(d, side ? M.origin[d] : M.origin[d] + M.n[d], plane)) continue;
                     bool touch = true;
                     for (int t : {(d + 1) % 3, (d + 2) % 3})
                         touch = touch && std::min(B.origin[t] + B.n[t], M.origin[t] + M.n[t]) >
                                              std::max(B.origin[t], M.origin[t]);
                     if (!touch) continue;
-                    const double gm = side ? M.ax[d].pts[2] : M.ax[d].pts[M.n[d]];
+                    const double gm = (side ? M.ax[d].pts[2] : M.ax[d].pts[M.n[d]]) + shift;
                     const double h = std::fabs(B.ax[d].pts[side ? B.n[d] + 1 : 1] - g[side]);
                     if (std::fabs(gm - g[side]) > 1e-9 * h)
                         throw BadArg{BMG_UNSUPPORTED,
@@ -830,11 +881,16 @@ void build(bmg_ctx* c, HostLevel&& L0) {
         c->lv.push_back(std::move(C));
     }
     const int nl = (int)c->lv.size();
-    for (auto& L : c->lv)
+    for (auto& L : c->lv) {
         for (auto& B : L.br)
             for (int d = 0; d < 3; ++d)
                 if (c->periodic[d] && B.n[d] > 1 && B.n[d] % 2)
                     throw BadArg{BMG_UNSUPPORTED, "odd cell count along a periodic axis on some level"};
+        // red-black colours alternate across the periodic ends of the box
+        for (int d = 0; d < 3; ++d)
+            if (L.wrap[d] && L.ext[d] > 1 && L.ext[d] % 2)
+                throw BadArg{BMG_UNSUPPORTED, "odd cell count along a periodic axis on some level"};
+    }
     for (auto& L : c->lv) {
         layout(L);
         if (L.cells >= (1L << 31)) throw BadArg{BMG_UNSUPPORTED, "a level above 2^31 cells"};

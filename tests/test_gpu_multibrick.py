@@ -15,7 +15,7 @@ import pytest
 
 import briscola_b200 as bb
 from briscola_b200 import workloads
-from briscola_b200.mesh import Brick, Mesh, geometric_points, uniform_points
+from briscola_b200.mesh import NEUMANN, PERIODIC, Brick, Mesh, geometric_points, uniform_points
 from tests.helpers import brick_to_compact, rel, split_brick, union_operator, union_solve, vmean
 
 pytestmark = pytest.mark.gpu
@@ -27,6 +27,12 @@ SPLITS = {
     "xyz8": (lambda: Brick([uniform_points(32)] * 3), ([16], [16], [16])),
     "graded_z": (lambda: Brick([uniform_points(16), geometric_points(16, 2.0), geometric_points(48, 0.5)]),
                  ([], [], [16, 32])),
+    # periodic axes: the pieces meet across the box's periodic ends
+    "periodic_x2": (lambda: Brick([uniform_points(32)] * 3, (PERIODIC, PERIODIC) + (NEUMANN,) * 4), ([16], [], [])),
+    "channel_xz": (lambda: Brick([uniform_points(32), geometric_points(16, 2.0), uniform_points(32)],
+                                 (PERIODIC, PERIODIC, NEUMANN, NEUMANN, PERIODIC, PERIODIC)), ([16], [], [8, 24])),
+    "periodic_spanning": (lambda: Brick([uniform_points(16), uniform_points(32), uniform_points(16)],
+                                        (NEUMANN, NEUMANN, NEUMANN, NEUMANN, PERIODIC, PERIODIC)), ([8], [16], [])),
 }
 
 
@@ -53,7 +59,7 @@ def _to_parts(parts, level, full, whole_shape):
     return np.concatenate(out)
 
 
-@pytest.mark.parametrize("name", ["x2", "y3", "xyz8"])
+@pytest.mark.parametrize("name", ["x2", "y3", "xyz8", "periodic_x2", "channel_xz", "periodic_spanning"])
 @pytest.mark.parametrize("precision", [0, 1])
 def test_split_building_blocks_bit_identical(native, name, precision):
     br, whole, parts = _whole_and_parts(name)

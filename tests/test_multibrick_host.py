@@ -84,11 +84,19 @@ def test_mismatched_contact_coordinates_are_rejected():
     assert "invalid argument" in _create_error(Mesh([a, c]))
 
 
-def test_periodic_multibrick_is_unsupported():
+def test_periodic_axis_must_be_periodic_for_every_brick():
     bc = (PERIODIC, PERIODIC) + ("Neumann",) * 4
     m = Mesh([Brick([_pts(8, 0), _pts(8, 0), _pts(8, 0)], bc, (0, 0, 0)),
-              Brick([_pts(8, 0), _pts(8, 8), _pts(8, 0)], bc, (0, 8, 0))])
-    assert "unsupported" in _create_error(m)
+              Brick([_pts(8, 0), _pts(8, 8), _pts(8, 0)], ("Neumann",) * 6, (0, 8, 0))])
+    assert "invalid argument" in _create_error(m)
+
+
+@pytest.mark.skipif(not _no_gpu(), reason="a GPU is present")
+def test_periodic_multibrick_passes_the_host_checks():
+    bc = (PERIODIC, PERIODIC) + ("Neumann",) * 4
+    m = Mesh([Brick([_pts(8, 0), _pts(8, 0), _pts(8, 0)], bc, (0, 0, 0)),
+              Brick([_pts(8, 8), _pts(8, 0), _pts(8, 0)], bc, (8, 0, 0))])
+    assert "no usable" in _create_error(m)
 
 
 def test_too_many_bricks_is_unsupported():
