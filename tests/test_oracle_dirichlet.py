@@ -129,3 +129,28 @@ def test_prolongation_reads_the_mirrored_coarse_ghosts():
     ref = np.zeros(o.shape(0))
     lib().bmgo_prolong_ghosted(o._p, 0, _dp(np.ascontiguousarray(g)), _dp(ref), 0)
     assert np.array_equal(out, ref)
+
+
+@pytest.mark.parametrize("bc,values", [
+    ((D, N, P, P, N, D), (1.0, 0.5, 0.0, 0.0, -0.25, 2.0)),
+    ((N, D, N, N, P, P), (0.3, -1.0, 0.2, -0.4, 0.0, 0.0)),
+])
+def test_face_value_conventions_match_the_fft_restatement(bc, values):
+    """The multigrid's face values (Dirichlet value, Neumann gradient) mean
+    what the FFT solver's do (FFTPoissonSolver.C, oracle/fft_oracle.py): the
+    same finite-volume system, so the split solver can hand one problem to
+    both.  MG system A x = -V f + face terms; FFT: Laplacian(x) = -f."""
+    import scipy.sparse.linalg as spl
+
+    from briscola_b200.mesh import geometric_points, uniform_points
+    from oracle import fft_oracle as F
+
+    pts = [uniform_points(16), uniform_points(8), geometric_points(12, 2.0)]
+    if bc[4] == P:
+        pts[2] = uniform_points(12)
+    n = tuple(len(p) - 1 for p in pts)
+    f = np.random.default_rng(2).standard_normal(n)
+    x_fft = F.solve(f, pts, bc, values)
+    A, V, bdir = brick_operator(pts, bc, values)
+    x_mg = spl.spsolve(A.tocsc(), -(V * f.ravel()) + bdir)
+    assert rel(x_mg, x_fft.ravel()) <= 1e-10
