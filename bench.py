@@ -132,6 +132,20 @@ def cpu_reference(N: int, steps: int | None = None, warmup: int = 0):
     return times, cycles, threads
 
 
+def max_over_ranks(value: float, dist, device) -> float:
+    """The slowest rank's time: replicas (one independent solve per rank, no
+    collective on the data path) are timed together and the job is as fast
+    as its slowest rank.  dist is torch.distributed (NCCL on the GPUs, gloo
+    in the CPU tests) or None for one rank."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -492,11 +506,7 @@ def main():
             cycles.append(rep.cycles)
         e1.record(stream)
         barrier()
-        ms = e0.elapsed_time(e1)
-        if dist is not None:
-            t = torch.tensor([ms], device=f"cuda:{local}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(e0.elapsed_time(e1), dist, f"cuda:{local}")
         return ms, launches, cycles
 
     clk = Clocks(local)
@@ -568,11 +578,7 @@ def main():
             s.solve(sys_)
         e1.record(stream)
         barrier()
-    e2e_ms = e0.elapsed_time(e1) / args.steps
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item()) / world
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, f"cuda:{local}") / world
 
     # ---- the seven-brick mesh (2.55 M cells, one launch per level across
     # bricks, ghost exchange on the device): FP64 and mixed ms per solve ----
