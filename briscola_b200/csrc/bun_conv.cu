@@ -475,7 +475,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) k_conv_rows(ConvArgs a) {
     using F = RowShape<CIN, NOUT, NR>;
     constexpr int NQ = CIN / 16;
     extern __shared__ __align__(1024) uint8_t smem[];
-    uint8_t* rows = smem;
+    // the NR row slots start at smem (addressed through `base` below)
     uint8_t* wts = smem + NR * F::SET;
     uint64_t* full = reinterpret_cast<uint64_t*>(wts + F::WBYTES);
     uint64_t* empty = full + NR;
