@@ -20,6 +20,7 @@ SMOOTHER = {"rbgs": 0, "jac": 1, "jacobi": 1}
 PRECISION = {"fp64": 0, "mixed": 1}
 KRYLOV = {"none": 0, "fcg": 1}
 CRITERION = {"initial": 0, "rhs": 1}
+COARSE_MODE = {"direct": 0, "smooth": 1}
 DEVICE_PTRS, ZERO_GUESS, PER_VOLUME = 1, 2, 4
 
 # Every function the header declares; the loader checks they are exported.
@@ -71,6 +72,7 @@ class Options(ctypes.Structure):
         ("criterion", ctypes.c_int),
         ("fused_chunk", ctypes.c_int),
         ("fuse_coarse", ctypes.c_int),
+        ("coarse_mode", ctypes.c_int),
     ]
 
 

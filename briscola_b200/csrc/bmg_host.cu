@@ -308,6 +308,9 @@ Bricks<T> bricks(const bmg_ctx* c, int l) {
         v.per1 = c->periodic[1];
         v.per2 = c->periodic[2];
         v.cpar = K.cpar;
+        // a smoothed coarse level of a singular system keeps global cell 0
+        // (brick 0's first cell) at zero
+        v.pin = l == c->lc && b == 0 && c->singular && c->opt.coarse_mode == BMG_COARSE_SMOOTH;
         B.z0[b] = z;
         z += K.n[0];
         B.max1 = std::max(B.max1, K.n[1]);
@@ -501,6 +504,15 @@ void buildCoarseInverse(bmg_ctx* c) {
     upload(c->cidx, cidx);
 }
 
+// the dense inverse exists for coarse levels of at most 4096 cells (the
+// direct coarse solve, and the building block of either coarse mode)
+void refreshCoarseInverse(bmg_ctx* c) {
+    if (c->lv[c->lc].ncell <= 4096)
+        buildCoarseInverse(c);
+    else
+        c->ncoarse = 0;
+}
+
 void destroyGraph(bmg_ctx* c) {
     if (c->gexec) cudaGraphExecDestroy(c->gexec);
     if (c->graph) cudaGraphDestroy(c->graph);
@@ -546,6 +558,7 @@ void validateOptions(const bmg_options* o) {
     if (o->fused_chunk < 1 || o->fused_chunk > 128) throw BadArg{BMG_BAD_ARG, "fusedChunk outside 1..128"};
     if (o->krylov < 0 || o->krylov > 1) throw BadArg{BMG_BAD_ARG, "unknown krylov"};
     if (o->criterion < 0 || o->criterion > 1) throw BadArg{BMG_BAD_ARG, "unknown criterion"};
+    if (o->coarse_mode < 0 || o->coarse_mode > 1) throw BadArg{BMG_BAD_ARG, "unknown coarseMode"};
 }
 
 // Level-0 bricks from the mesh description; contacts between bricks.
@@ -1006,10 +1019,10 @@ void configureCoarse(bmg_ctx* c) {
     if (nl < 2 || c->opt.coarse_level > nl - 2)
         throw BadArg{BMG_BAD_ARG, "coarseLevel too high: at most (number of levels - 2)"};
     const int lc = nl - 1 - c->opt.coarse_level;
-    if (c->lv[lc].ncell > 4096)
+    if (c->lv[lc].ncell > 4096 && c->opt.coarse_mode == BMG_COARSE_DIRECT)
         throw BadArg{BMG_UNSUPPORTED, "coarse solve level above 4096 cells; raise coarseLevel"};
     c->lc = lc;
-    buildCoarseInverse(c);
+    refreshCoarseInverse(c);
 }
 
 void ensureKrylovBuffers(bmg_ctx* c) {
@@ -1094,7 +1107,10 @@ void smooth(bmg_ctx* c, int l, int sweeps) {
     cudaStream_t s = c->stream;
     HostLevel& H = c->lv[l];
     const int prec = sizeof(T) == 8 ? 0 : 1;
-    if (c->opt.smoother == BMG_SMOOTHER_RBGS && c->opt.fused > 0 && H.fusedOK && H.fusedS[prec] > 0) {
+    // (the fused smoother does not keep a pinned cell: a pinned level runs
+    // pass by pass)
+    const bool pinned = l == c->lc && c->singular && c->opt.coarse_mode == BMG_COARSE_SMOOTH;
+    if (c->opt.smoother == BMG_SMOOTHER_RBGS && c->opt.fused > 0 && H.fusedOK && H.fusedS[prec] > 0 && !pinned) {
         // the colour sequence alternates; run it in launches of up to
         // maxS stages, each writing the other x buffer
         const std::vector<int> seq = colourSequence(H, sweeps);
@@ -1292,7 +1308,7 @@ int levelReps(const bmg_ctx* c, int l) {  // MG.H:106-124
 // smoothing and factor-2 quad transfers on every one of them; -1 otherwise.
 int tailFirst(const bmg_ctx* c) {
     if (!c->opt.fuse_coarse || c->multi || c->opt.cycle_type != BMG_CYCLE_V ||
-        c->opt.smoother != BMG_SMOOTHER_RBGS)
+        c->opt.smoother != BMG_SMOOTHER_RBGS || c->opt.coarse_mode != BMG_COARSE_DIRECT)
         return -1;
     const int lc = c->lc;
     int first = lc;
@@ -1350,6 +1366,8 @@ void cycle(bmg_ctx* c, int l) {
             prolongCorrect<T>(c, l);
             if (c->opt.n_post > 0) smooth<T>(c, l, c->opt.n_post);
         }
+    } else if (c->opt.coarse_mode == BMG_COARSE_SMOOTH) {
+        smooth<T>(c, l, std::max(c->opt.n_post, 2));  // MG.C:116-125
     } else {
         coarseSolve<T>(c);
     }
@@ -1791,6 +1809,7 @@ int bmg_default_options(bmg_options* o) {
     o->criterion = BMG_CRITERION_INITIAL;
     o->fused_chunk = 64;
     o->fuse_coarse = 1;
+    o->coarse_mode = BMG_COARSE_DIRECT;
     return BMG_OK;
 }
 
@@ -1848,7 +1867,7 @@ int bmg_set_options(bmg_ctx* c, const bmg_options* o) {
     return guarded(c, [&] {
         validateOptions(o);
         if (o->device != c->opt.device) throw BadArg{BMG_BAD_ARG, "the device of a context is fixed"};
-        const bool coarseChanged = o->coarse_level != c->opt.coarse_level;
+        const bool coarseChanged = o->coarse_level != c->opt.coarse_level || o->coarse_mode != c->opt.coarse_mode;
         const bool retune = o->autotune && (!c->opt.autotune || o->fused != c->opt.fused ||
                                             o->n_pre != c->opt.n_pre || o->n_post != c->opt.n_post);
         c->opt = *o;
@@ -1888,7 +1907,7 @@ int bmg_set_coefficients(bmg_ctx* c, const double* lx, const double* ly, const d
         }
         c->variable = c->userLambda || c->multi;
         if (c->variable) uploadLambda(c);
-        buildCoarseInverse(c);
+        refreshCoarseInverse(c);
         destroyGraph(c);  // kernels differ between constant and variable coefficients
         return BMG_OK;
     });
@@ -2129,6 +2148,7 @@ int bmg_op_coarse_solve(bmg_ctx* c, int prec) {
     if (!c) return BMG_BAD_ARG;
     return guarded(c, [&] {
         BMG_CUDA(cudaSetDevice(c->opt.device));
+        if (c->ncoarse == 0) throw BadArg{BMG_UNSUPPORTED, "no dense coarse solve on a level above 4096 cells"};
         if (prec == 0) coarseSolve<double>(c);
         else coarseSolve<float>(c);
         checkLaunch();

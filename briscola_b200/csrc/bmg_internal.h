@@ -70,6 +70,8 @@ struct LevelView {
     const T* lam2;
     int per0, per1, per2;  // periodic write-through (single brick only)
     int cpar;          // parity of the brick origin: colour = (i+j+k+cpar) & 1
+    int pin;           // smoothers keep cell (0,0,0) at zero: the singularity pin
+                       // of an iteratively smoothed coarse level (solver.C:201-231)
 };
 
 // Wall faces of a single-brick level 0: bit f of mask for a Dirichlet face

@@ -57,6 +57,7 @@ __global__ void __launch_bounds__(256) k_colour_pass(Bricks<T> B, int colour) {
     const V2 yp = *reinterpret_cast<const V2*>(x + c0 + L.sj);
     const V2 own = *reinterpret_cast<const V2*>(x + c0);
     const long c = r + k;
+    if (L.pin && (i | j | k) == 0) return;  // the pinned cell stays zero
     T w[6];
     couplings<T, VAR>(L, i, j, k, c, w);
     const T xn[6] = {e ? xm.y : xm.x, e ? xp.y : xp.x, e ? ym.y : ym.x, e ? yp.y : yp.x,
@@ -182,7 +183,8 @@ __device__ __forceinline__ void colour_quad_item(const LevelView<T>& L, int i, i
                       odd ? own[2] : own[1]};
     const T xn2[6] = {BMG_SEL(xm, 2), BMG_SEL(xp, 2), BMG_SEL(ym, 2), BMG_SEL(yp, 2), odd ? own[2] : own[1],
                       odd ? right : own[3]};
-    const T v0 = gs_value(w0, xn0, BMG_SEL(bb, 0));
+    // the pinned cell (0,0,0), when this pass updates it, stays zero
+    const T v0 = (L.pin && (i | j | k0) == 0 && !odd) ? own[0] : gs_value(w0, xn0, BMG_SEL(bb, 0));
     const T v2 = gs_value(w2, xn2, BMG_SEL(bb, 2));
 #undef BMG_SEL
     const T out[4] = {odd ? own[0] : v0, odd ? v0 : own[1], odd ? own[2] : v2, odd ? v2 : own[3]};
@@ -218,7 +220,7 @@ __global__ void __launch_bounds__(256) k_jacobi(Bricks<T> B, T* tmp) {
     couplings<T, VAR>(L, i, j, k, c, w);
     stencil(L.x, c, L.si, L.sj, w, s, d);
     const T omega = T(0.8);
-    tmp[c] = (T(1) - omega) * L.x[c] + omega * (s - L.b[c]) / d;
+    tmp[c] = (L.pin && (i | j | k) == 0) ? T(0) : (T(1) - omega) * L.x[c] + omega * (s - L.b[c]) / d;
 }
 
 template <typename T>

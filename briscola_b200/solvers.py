@@ -414,6 +414,11 @@ def make_options(d: Dictionary | dict | None = None, **over) -> N.Options:
     if cr not in N.CRITERION:
         raise FatalError(f"unknown criterion {cr}")
     o.criterion = N.CRITERION[cr]
+    # MG.C:277-287 (MGCoarseModeNames)
+    cm = str(d.get("coarseMode", "direct"))
+    if cm not in N.COARSE_MODE:
+        raise FatalError(f"unknown coarseMode {cm}")
+    o.coarse_mode = N.COARSE_MODE[cm]
     return o
 
 
@@ -424,8 +429,6 @@ class GPUMG(solver):
 
     def __init__(self, dict_: Dictionary, mesh: Mesh):
         super().__init__(dict_, mesh)
-        if str(dict_.lookupOrDefault("coarseMode", "direct")) != "direct":
-            raise FatalError("GPUMG supports coarseMode direct only")
         for key in ("prolong", "restrict"):
             if str(dict_.lookupOrDefault(key, "linear")) != "linear":
                 raise FatalError(f"GPUMG supports {key} linear only")

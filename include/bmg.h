@@ -61,6 +61,10 @@ enum { BMG_PRECISION_FP64 = 0, BMG_PRECISION_MIXED = 1 };
  * flexible conjugate gradients (Notay's FCG(1)) on the FP64 residual with
  * one cycle as the preconditioner.  No counterpart in the reference. */
 enum { BMG_KRYLOV_NONE = 0, BMG_KRYLOV_FCG = 1 };
+/* Coarsest level of a cycle (coarseMode, MG.C:110-126): the direct solve
+ * (APLU), or max(nSweepsPost, 2) sweeps of the smoother, with the
+ * singularity pin (solver.C:201-231) kept by the smoothers on that level. */
+enum { BMG_COARSE_DIRECT = 0, BMG_COARSE_SMOOTH = 1 };
 /* Convergence test: relTol relative to the initial residual (solver.C:64-95,
  * the reference's), or relative to ||b||_2, i.e. ||b - A x||_2 <= relTol
  * ||b||_2 whatever the initial guess (used to compare solves that start from
@@ -125,6 +129,7 @@ typedef struct bmg_options {
     int fuse_coarse;    /* fuseCoarse (1): run the levels of at most 4096
                            cells and the coarse solve of a single-brick V
                            cycle in one kernel                                 */
+    int coarse_mode;    /* coarseMode (direct): BMG_COARSE_* (MG.C:110-126)     */
 } bmg_options;
 
 typedef struct bmg_report {
