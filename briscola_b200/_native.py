@@ -21,6 +21,8 @@ PRECISION = {"fp64": 0, "mixed": 1}
 KRYLOV = {"none": 0, "fcg": 1}
 CRITERION = {"initial": 0, "rhs": 1}
 COARSE_MODE = {"direct": 0, "smooth": 1}
+RESTRICT = {"linear": 0, "average": 1}
+PROLONG = {"linear": 0, "injection": 1}
 DEVICE_PTRS, ZERO_GUESS, PER_VOLUME = 1, 2, 4
 
 # Every function the header declares; the loader checks they are exported.
@@ -73,6 +75,8 @@ class Options(ctypes.Structure):
         ("fused_chunk", ctypes.c_int),
         ("fuse_coarse", ctypes.c_int),
         ("coarse_mode", ctypes.c_int),
+        ("restrict_scheme", ctypes.c_int),
+        ("prolong_scheme", ctypes.c_int),
     ]
 
 

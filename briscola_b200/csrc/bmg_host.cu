@@ -520,6 +520,8 @@ void destroyGraph(bmg_ctx* c) {
     c->graph = nullptr;
 }
 
+void freeTransfers(bmg_ctx* c);
+
 void freeAll(bmg_ctx* c) {
     for (auto& L : c->lv) {
         for (void* p : {(void*)L.x64, (void*)L.b64, (void*)L.x32, (void*)L.b32, (void*)L.tab64, (void*)L.tab32,
@@ -531,10 +533,7 @@ void freeAll(bmg_ctx* c) {
             if (L.lam32[d]) cudaFree(L.lam32[d]);
         }
     }
-    for (auto& lt : c->tr)
-        for (auto& t : lt)
-            for (void* p : {(void*)t.ratio64, (void*)t.ratio32, (void*)t.pidx, (void*)t.pw64, (void*)t.pw32})
-                if (p) cudaFree(p);
+    freeTransfers(c);
     for (void* p : {(void*)c->ainv, (void*)c->cidx, (void*)c->partials, (void*)c->st, (void*)c->stage_b,
                     (void*)c->stage_x, (void*)c->fx, (void*)c->fb, (void*)c->fr, (void*)c->fp, (void*)c->fq})
         if (p) cudaFree(p);
@@ -559,6 +558,8 @@ void validateOptions(const bmg_options* o) {
     if (o->krylov < 0 || o->krylov > 1) throw BadArg{BMG_BAD_ARG, "unknown krylov"};
     if (o->criterion < 0 || o->criterion > 1) throw BadArg{BMG_BAD_ARG, "unknown criterion"};
     if (o->coarse_mode < 0 || o->coarse_mode > 1) throw BadArg{BMG_BAD_ARG, "unknown coarseMode"};
+    if (o->restrict_scheme < 0 || o->restrict_scheme > 1) throw BadArg{BMG_BAD_ARG, "unknown restriction scheme"};
+    if (o->prolong_scheme < 0 || o->prolong_scheme > 1) throw BadArg{BMG_BAD_ARG, "unknown prolongation scheme"};
 }
 
 // Level-0 bricks from the mesh description; contacts between bricks.
@@ -883,6 +884,90 @@ void uploadLambda(bmg_ctx* c) {
     }
 }
 
+// transfer tables per brick between levels l and l+1: restriction shares
+// and prolongation indices/weights, for the configured schemes
+void freeTransfers(bmg_ctx* c) {
+    for (auto& lt : c->tr)
+        for (auto& t : lt)
+            for (void* p : {(void*)t.ratio64, (void*)t.ratio32, (void*)t.pidx, (void*)t.pw64, (void*)t.pw32})
+                if (p) cudaFree(p);
+    c->tr.clear();
+}
+
+void buildTransfers(bmg_ctx* c) {
+    freeTransfers(c);
+    const int nl = (int)c->lv.size();
+    c->tr.assign(nl > 1 ? nl - 1 : 0, {});
+    for (int l = 0; l + 1 < nl; ++l) {
+        for (size_t b = 0; b < c->lv[l].br.size(); ++b) {
+            const HostBrick& F = c->lv[l].br[b];
+            const HostBrick& C = c->lv[l + 1].br[b];
+            BrickTransfer t;
+            std::vector<double> ratio, pw;
+            std::vector<int> pidx;
+            for (int d = 0; d < 3; ++d) {
+                const int R = C.R[d];
+                t.R[d] = R;
+                const Axis& fa = F.ax[d];
+                const Axis& ca = C.ax[d];
+                for (int i = 0; i < F.n[d]; ++i) {
+                    const int I0 = i / R;
+                    // linear: the trilinear weight of the coarse centre between
+                    // the two fine centres, h_f / H_c per axis
+                    // (linearRestrictionScheme.C:15-80); average: 1/R per axis
+                    // (averageRestrictionScheme.C:35-77)
+                    ratio.push_back(R == 1 ? 1.0
+                                    : c->opt.restrict_scheme == BMG_RESTRICT_AVERAGE ? 0.5
+                                                                                     : fa.h[i + 1] / ca.h[I0 + 1]);
+                    int I1 = I0;
+                    double w = 0.0;
+                    // injection (injectionProlongationScheme.C:14-33): the
+                    // parent's value, weight 0 on every second coarse cell
+                    if (R > 1 && c->opt.prolong_scheme == BMG_PROLONG_LINEAR) {
+                        const int off = (i % 2) ? 1 : -1;
+                        const int In = I0 + off;
+                        // linearProlongationScheme.C:49-104: weight of the coarse
+                        // neighbour on the fine cell's side, ghost centres included
+                        w = (fa.cc[i + 1] - ca.cc[I0 + 1]) / (ca.cc[In + 1] - ca.cc[I0 + 1]);
+                        if (In < 0 || In >= C.n[d]) {
+                            if (c->periodic[d]) {
+                                I1 = (In + C.n[d]) % C.n[d];
+                            } else if (C.open[2 * d + (In >= C.n[d])]) {
+                                I1 = In;  // ghost cell, refreshed from the neighbouring brick
+                            } else if (c->dirichlet[2 * d + (In >= C.n[d])]) {
+                                // the coarse ghost is -x (DirichletBoundaryCondition.C
+                                // :59-80 above level 0): (1 - w) x + w (-x) = (1 - 2w) x,
+                                // read as weight 2w on the ghost cell, which holds zero
+                                I1 = In;
+                                w = 2.0 * w;
+                            } else {
+                                I1 = I0;  // zero-gradient ghost: the value equals the parent's
+                                w = 0.0;
+                            }
+                        } else {
+                            I1 = In;
+                        }
+                    }
+                    pidx.push_back(I0);
+                    pidx.push_back(I1);
+                    pw.push_back(w);
+                }
+            }
+            t.ratio64 = dalloc<double>(ratio.size());
+            t.ratio32 = dalloc<float>(ratio.size());
+            t.pidx = dalloc<int>(pidx.size());
+            t.pw64 = dalloc<double>(pw.size());
+            t.pw32 = dalloc<float>(pw.size());
+            upload(t.ratio64, ratio);
+            upload(t.ratio32, to_f32(ratio));
+            upload(t.pidx, pidx);
+            upload(t.pw64, pw);
+            upload(t.pw32, to_f32(pw));
+            c->tr[l].push_back(t);
+        }
+    }
+}
+
 void build(bmg_ctx* c, HostLevel&& L0) {
     finishLevel(c, L0);
     c->lv.push_back(std::move(L0));
@@ -941,69 +1026,7 @@ void build(bmg_ctx* c, HostLevel&& L0) {
     // multi-brick meshes carry face lambdas for their contacts
     c->variable = c->multi;
     if (c->multi) uploadLambda(c);
-    // transfer tables per brick: restriction shares and prolongation
-    // indices/weights
-    c->tr.assign(nl > 1 ? nl - 1 : 0, {});
-    for (int l = 0; l + 1 < nl; ++l) {
-        for (size_t b = 0; b < c->lv[l].br.size(); ++b) {
-            const HostBrick& F = c->lv[l].br[b];
-            const HostBrick& C = c->lv[l + 1].br[b];
-            BrickTransfer t;
-            std::vector<double> ratio, pw;
-            std::vector<int> pidx;
-            for (int d = 0; d < 3; ++d) {
-                const int R = C.R[d];
-                t.R[d] = R;
-                const Axis& fa = F.ax[d];
-                const Axis& ca = C.ax[d];
-                for (int i = 0; i < F.n[d]; ++i) {
-                    const int I0 = i / R;
-                    ratio.push_back(R == 1 ? 1.0 : fa.h[i + 1] / ca.h[I0 + 1]);
-                    int I1 = I0;
-                    double w = 0.0;
-                    if (R > 1) {
-                        const int off = (i % 2) ? 1 : -1;
-                        const int In = I0 + off;
-                        // linearProlongationScheme.C:49-104: weight of the coarse
-                        // neighbour on the fine cell's side, ghost centres included
-                        w = (fa.cc[i + 1] - ca.cc[I0 + 1]) / (ca.cc[In + 1] - ca.cc[I0 + 1]);
-                        if (In < 0 || In >= C.n[d]) {
-                            if (c->periodic[d]) {
-                                I1 = (In + C.n[d]) % C.n[d];
-                            } else if (C.open[2 * d + (In >= C.n[d])]) {
-                                I1 = In;  // ghost cell, refreshed from the neighbouring brick
-                            } else if (c->dirichlet[2 * d + (In >= C.n[d])]) {
-                                // the coarse ghost is -x (DirichletBoundaryCondition.C
-                                // :59-80 above level 0): (1 - w) x + w (-x) = (1 - 2w) x,
-                                // read as weight 2w on the ghost cell, which holds zero
-                                I1 = In;
-                                w = 2.0 * w;
-                            } else {
-                                I1 = I0;  // zero-gradient ghost: the value equals the parent's
-                                w = 0.0;
-                            }
-                        } else {
-                            I1 = In;
-                        }
-                    }
-                    pidx.push_back(I0);
-                    pidx.push_back(I1);
-                    pw.push_back(w);
-                }
-            }
-            t.ratio64 = dalloc<double>(ratio.size());
-            t.ratio32 = dalloc<float>(ratio.size());
-            t.pidx = dalloc<int>(pidx.size());
-            t.pw64 = dalloc<double>(pw.size());
-            t.pw32 = dalloc<float>(pw.size());
-            upload(t.ratio64, ratio);
-            upload(t.ratio32, to_f32(ratio));
-            upload(t.pidx, pidx);
-            upload(t.pw64, pw);
-            upload(t.pw32, to_f32(pw));
-            c->tr[l].push_back(t);
-        }
-    }
+    buildTransfers(c);
     c->partials = dalloc<double>(3 * reduce_blocks(bricks<double>(c, 0)));
     c->st = dalloc<SolveState>(1);
     BMG_CUDA(cudaMallocHost(&c->st_host, sizeof(SolveState)));
@@ -1810,6 +1833,8 @@ int bmg_default_options(bmg_options* o) {
     o->fused_chunk = 64;
     o->fuse_coarse = 1;
     o->coarse_mode = BMG_COARSE_DIRECT;
+    o->restrict_scheme = BMG_RESTRICT_LINEAR;
+    o->prolong_scheme = BMG_PROLONG_LINEAR;
     return BMG_OK;
 }
 
@@ -1868,12 +1893,15 @@ int bmg_set_options(bmg_ctx* c, const bmg_options* o) {
         validateOptions(o);
         if (o->device != c->opt.device) throw BadArg{BMG_BAD_ARG, "the device of a context is fixed"};
         const bool coarseChanged = o->coarse_level != c->opt.coarse_level || o->coarse_mode != c->opt.coarse_mode;
+        const bool transfersChanged =
+            o->restrict_scheme != c->opt.restrict_scheme || o->prolong_scheme != c->opt.prolong_scheme;
         const bool retune = o->autotune && (!c->opt.autotune || o->fused != c->opt.fused ||
                                             o->n_pre != c->opt.n_pre || o->n_post != c->opt.n_post);
         c->opt = *o;
         destroyGraph(c);
         BMG_CUDA(cudaSetDevice(c->opt.device));
         if (coarseChanged) configureCoarse(c);
+        if (transfersChanged) buildTransfers(c);
         c->tail = tailFirst(c);
         if (!o->autotune) applyChunk(c);
         if (retune) autotune(c);

@@ -419,6 +419,12 @@ def make_options(d: Dictionary | dict | None = None, **over) -> N.Options:
     if cm not in N.COARSE_MODE:
         raise FatalError(f"unknown coarseMode {cm}")
     o.coarse_mode = N.COARSE_MODE[cm]
+    # restriction and prolongation schemes (MG.C:289-305)
+    for key, table, field in (("restrict", N.RESTRICT, "restrict_scheme"), ("prolong", N.PROLONG, "prolong_scheme")):
+        v = str(d.get(key, "linear"))
+        if v not in table:
+            raise FatalError(f"GPUMG {key} scheme must be one of {sorted(table)}, not {v}")
+        setattr(o, field, table[v])
     return o
 
 
@@ -429,9 +435,6 @@ class GPUMG(solver):
 
     def __init__(self, dict_: Dictionary, mesh: Mesh):
         super().__init__(dict_, mesh)
-        for key in ("prolong", "restrict"):
-            if str(dict_.lookupOrDefault(key, "linear")) != "linear":
-                raise FatalError(f"GPUMG supports {key} linear only")
         if dict_.found("coarseSolver"):
             cs = dict_.subDict("coarseSolver")
             if str(cs.lookupOrDefault("type", "APLU")) != "APLU":

@@ -65,6 +65,13 @@ enum { BMG_KRYLOV_NONE = 0, BMG_KRYLOV_FCG = 1 };
  * (APLU), or max(nSweepsPost, 2) sweeps of the smoother, with the
  * singularity pin (solver.C:201-231) kept by the smoothers on that level. */
 enum { BMG_COARSE_DIRECT = 0, BMG_COARSE_SMOOTH = 1 };
+/* Grid transfers of the cycle (MG.C:289-305): the residual restriction
+ * linear (linearRestrictionScheme.C:15-187) or average
+ * (averageRestrictionScheme.C:17-77), the correction's prolongation linear
+ * (linearProlongationScheme.C:12-147) or injection
+ * (injectionProlongationScheme.C:14-33). */
+enum { BMG_RESTRICT_LINEAR = 0, BMG_RESTRICT_AVERAGE = 1 };
+enum { BMG_PROLONG_LINEAR = 0, BMG_PROLONG_INJECTION = 1 };
 /* Convergence test: relTol relative to the initial residual (solver.C:64-95,
  * the reference's), or relative to ||b||_2, i.e. ||b - A x||_2 <= relTol
  * ||b||_2 whatever the initial guess (used to compare solves that start from
@@ -130,6 +137,8 @@ typedef struct bmg_options {
                            cells and the coarse solve of a single-brick V
                            cycle in one kernel                                 */
     int coarse_mode;    /* coarseMode (direct): BMG_COARSE_* (MG.C:110-126)     */
+    int restrict_scheme;/* restrict (linear): BMG_RESTRICT_*                   */
+    int prolong_scheme; /* prolong (linear): BMG_PROLONG_*                     */
 } bmg_options;
 
 typedef struct bmg_report {

@@ -134,6 +134,8 @@ struct bmgo_problem {
     int dirichlet[6] = {0, 0, 0, 0, 0, 0};  // walls with a Dirichlet condition
     double dval[6] = {0, 0, 0, 0, 0, 0};    // their (uniform) boundary values
     std::vector<double> bdir;               // level-0 right-hand-side term of the Dirichlet values
+    int restrictAverage = 0;                // restriction / prolongation schemes
+    int prolongInjection = 0;
     bool variable = false;
     Pool pool;
     int coarseLevelIdx = -1;  // level index that carries the pin
@@ -572,9 +574,12 @@ void restrictLevel(P& p, int lf, const std::vector<double>& fine, std::vector<do
         for (int I = Ib; I < Ie; ++I)
             for (int J = 0; J < C.N[1]; ++J)
                 for (int K = 0; K < C.N[2]; ++K) {
-                    const double wx = axisWeight(C.ccen(0, I), F.ccen(0, I * R0), F.ccen(0, I * R0 + 1));
-                    const double wy = axisWeight(C.ccen(1, J), F.ccen(1, J * R1), F.ccen(1, J * R1 + 1));
-                    const double wz = axisWeight(C.ccen(2, K), F.ccen(2, K * R2), F.ccen(2, K * R2 + 1));
+                    // averageRestrictionScheme.C:35-77: the children's mean
+                    // (weight 1/2 per coarsened axis)
+                    const bool avg = p.restrictAverage != 0;
+                    const double wx = avg ? 0.5 : axisWeight(C.ccen(0, I), F.ccen(0, I * R0), F.ccen(0, I * R0 + 1));
+                    const double wy = avg ? 0.5 : axisWeight(C.ccen(1, J), F.ccen(1, J * R1), F.ccen(1, J * R1 + 1));
+                    const double wz = avg ? 0.5 : axisWeight(C.ccen(2, K), F.ccen(2, K * R2), F.ccen(2, K * R2 + 1));
                     double w[8] = {(1.0 - wx) * (1.0 - wy) * (1.0 - wz), (wx) * (1.0 - wy) * (1.0 - wz),
                                    (1.0 - wx) * (wy) * (1.0 - wz),       (wx) * (wy) * (1.0 - wz),
                                    (1.0 - wx) * (1.0 - wy) * (wz),       (wx) * (1.0 - wy) * (wz),
@@ -616,9 +621,11 @@ void prolongLevel(P& p, int lf, std::vector<double>& coarse, std::vector<double>
                 for (int k = 0; k < F.N[2]; ++k) {
                     const int o0 = i % 2 ? 1 : -1, o1 = j % 2 ? 1 : -1, o2 = k % 2 ? 1 : -1;
                     const int I = i / R0, J = j / R1, K = k / R2;
-                    const double wx = axisWeight(F.ccen(0, i), C.ccen(0, I), C.ccen(0, I + o0));
-                    const double wy = axisWeight(F.ccen(1, j), C.ccen(1, J), C.ccen(1, J + o1));
-                    const double wz = axisWeight(F.ccen(2, k), C.ccen(2, K), C.ccen(2, K + o2));
+                    // injectionProlongationScheme.C:14-33: the parent's value
+                    const bool inj = p.prolongInjection != 0;
+                    const double wx = inj ? 0.0 : axisWeight(F.ccen(0, i), C.ccen(0, I), C.ccen(0, I + o0));
+                    const double wy = inj ? 0.0 : axisWeight(F.ccen(1, j), C.ccen(1, J), C.ccen(1, J + o1));
+                    const double wz = inj ? 0.0 : axisWeight(F.ccen(2, k), C.ccen(2, K), C.ccen(2, K + o2));
                     double v = 0.0;
                     for (int c = 0; c < 2; ++c)
                         for (int bb = 0; bb < 2; ++bb)
@@ -770,6 +777,8 @@ int absCoarseLevel(const P& p, const bmgo_options& o) {
 }
 
 void assembleAll(P& p, const bmgo_options& o) {
+    p.restrictAverage = o.restrict_average;
+    p.prolongInjection = o.prolong_injection;
     const int lc = absCoarseLevel(p, o);
     for (size_t l = 0; l < p.lv.size(); ++l) assembleLevel(p, p.lv[l]);
     // MG.C:431-445: pin first (solver.C:201-231), then eliminate ghosts
@@ -805,6 +814,8 @@ void bmgo_default_options(bmgo_options* o) {
     o->coarse_direct = 1;
     o->smoother = 0;
     o->stale_residual = 1;
+    o->restrict_average = 0;
+    o->prolong_injection = 0;
 }
 
 bmgo_problem* bmgo_create(const int N[3], const double* px, const double* py, const double* pz,

@@ -17,6 +17,8 @@
  *   row products                src/briscolaFiniteVolume/linearSystems/linearSystem/linearSystemFunctions.H:28-104
  *   linear restriction          src/briscolaFiniteVolume/schemes/restrictionSchemes/linearRestrictionScheme/linearRestrictionScheme.C:15-187
  *   linear prolongation         src/briscolaFiniteVolume/schemes/prolongationSchemes/linearProlongationScheme/linearProlongationScheme.C:12-147
+ *   average restriction         src/briscolaFiniteVolume/schemes/restrictionSchemes/averageRestrictionScheme/averageRestrictionScheme.C:17-77
+ *   injection prolongation      src/briscolaFiniteVolume/schemes/prolongationSchemes/injectionProlongationScheme/injectionProlongationScheme.C:14-33
  *   area-weighted lambda        src/briscolaFiniteVolume/schemes/restrictionSchemes/areaWeightedFaceRestrictionScheme/areaWeightedFaceRestrictionScheme.C:19-57
  *   Laplacian assembly          src/briscolaFiniteVolume/schemes/laplacianSchemes/linearGaussLaplacianScheme/linearGaussLaplacianScheme.C:22-102
  *   face deltas                 src/briscolaFiniteVolume/fvMeshMetrics.C:848-893
@@ -65,6 +67,8 @@ typedef struct bmgo_options {
     int    coarse_direct;  /* 1 = direct (APLU), 0 = smoothing        */
     int    smoother;       /* 0 = rbgs, 1 = jacobi                    */
     int    stale_residual; /* 1 = keep MG.C:72 (skip fine residual on rep 0) */
+    int    restrict_average;  /* restrict average (averageRestrictionScheme.C) instead of linear */
+    int    prolong_injection; /* prolong injection (injectionProlongationScheme.C) instead of linear */
 } bmgo_options;
 
 typedef struct bmgo_report {
@@ -114,7 +118,8 @@ void bmgo_set_lambda(bmgo_problem* p, const double* lx, const double* ly,
 void bmgo_get_lambda(const bmgo_problem* p, int l, int fd, double* out);
 
 /* Build A on every level (Laplacian + wall elimination + singular pin on
- * the coarsest solve level given by opts->coarse_level, when singular). */
+ * the coarsest solve level given by opts->coarse_level, when singular);
+ * also selects the transfer schemes of opts for the building blocks. */
 void bmgo_assemble(bmgo_problem* p, const bmgo_options* o);
 /* 7 coefficients per interior cell {c,l,r,b,t,a,f}, k fastest */
 void bmgo_get_matrix(const bmgo_problem* p, int l, double* out7);

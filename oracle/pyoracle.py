@@ -30,6 +30,8 @@ class Options(ctypes.Structure):
         ("coarse_direct", ctypes.c_int),
         ("smoother", ctypes.c_int),
         ("stale_residual", ctypes.c_int),
+        ("restrict_average", ctypes.c_int),
+        ("prolong_injection", ctypes.c_int),
     ]
 
 
