@@ -11,7 +11,9 @@
 //
 // The arithmetic is the level-0 residual of the solver (the same operator as
 // k_residual_norm in bmg_kernels.cu): row-scaled couplings delta/h per axis,
-// periodic neighbours wrapped, wall couplings zero.
+// periodic neighbours wrapped, Neumann wall couplings zero, Dirichlet wall
+// couplings doubled against a zero ghost (homogeneous: face values belong
+// in b).
 
 #include "../../include/bmg.h"
 
@@ -34,24 +36,34 @@ double* g_scratch[kMaxDevices] = {nullptr};
 std::mutex g_scratch_mutex;
 
 // row-scaled coupling between cell i and its lower (up = 0) or upper (up = 1)
-// neighbour along an axis with vertices p[0..n]: 1 / (centre distance * h_i)
-__device__ __forceinline__ double coupling(const double* p, int n, int i, int up, int periodic) {
+// neighbour along an axis with vertices p[0..n]: 1 / (centre distance * h_i).
+// At a wall the neighbour is a ghost: a Neumann wall drops the coupling, a
+// (homogeneous) Dirichlet wall doubles it, with the ghost one spacing h_i
+// away and read as zero (DirichletBoundaryCondition.C:19-51).  *inner: the
+// neighbour is a cell of the brick (or its periodic image).
+__device__ __forceinline__ double coupling(const double* p, int n, int i, int up, int periodic, int dirichlet,
+                                           bool* inner) {
     const double h = p[i + 1] - p[i];
     double dist;
+    *inner = true;
     if (!up) {
         if (i > 0)
             dist = 0.5 * (p[i + 1] - p[i - 1]);
         else if (periodic)
             dist = 0.5 * (h + (p[n] - p[n - 1]));
-        else
-            return 0.0;
+        else {
+            *inner = false;
+            return dirichlet ? 2.0 / h / h : 0.0;
+        }
     } else {
         if (i < n - 1)
             dist = 0.5 * (p[i + 2] - p[i]);
         else if (periodic)
             dist = 0.5 * (h + (p[1] - p[0]));
-        else
-            return 0.0;
+        else {
+            *inner = false;
+            return dirichlet ? 2.0 / h / h : 0.0;
+        }
     }
     return 1.0 / dist / h;
 }
@@ -61,26 +73,30 @@ __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >=
 __global__ void __launch_bounds__(kThreads) k_rows(const double* __restrict__ x, const double* __restrict__ b,
                                                    int n0, int n1, int n2, const double* __restrict__ p0,
                                                    const double* __restrict__ p1, const double* __restrict__ p2,
-                                                   int per0, int per1, int per2, double* rows) {
+                                                   int per0, int per1, int per2, int dir, double* rows) {
     __shared__ double sh[kThreads / 32];
     const int nrows = n0 * n1;
     for (int q = blockIdx.x; q < nrows; q += gridDim.x) {
         const int i = q / n1, j = q % n1;
-        const double w0 = coupling(p0, n0, i, 0, per0), w1 = coupling(p0, n0, i, 1, per0);
-        const double w2 = coupling(p1, n1, j, 0, per1), w3 = coupling(p1, n1, j, 1, per1);
+        bool in0, in1, in2, in3, in4, in5;
+        const double w0 = coupling(p0, n0, i, 0, per0, dir & 1, &in0);
+        const double w1 = coupling(p0, n0, i, 1, per0, dir & 2, &in1);
+        const double w2 = coupling(p1, n1, j, 0, per1, dir & 4, &in2);
+        const double w3 = coupling(p1, n1, j, 1, per1, dir & 8, &in3);
         const double hij = (p0[i + 1] - p0[i]) * (p1[j + 1] - p1[j]);
         const long rim = (long)wrap(i - 1, n0) * n1 + j, rip = (long)wrap(i + 1, n0) * n1 + j;
         const long rjm = (long)i * n1 + wrap(j - 1, n1), rjp = (long)i * n1 + wrap(j + 1, n1);
         double acc = 0.0;
         for (int k = threadIdx.x; k < n2; k += blockDim.x) {
-            const double w4 = coupling(p2, n2, k, 0, per2), w5 = coupling(p2, n2, k, 1, per2);
+            const double w4 = coupling(p2, n2, k, 0, per2, dir & 16, &in4);
+            const double w5 = coupling(p2, n2, k, 1, per2, dir & 32, &in5);
             const int km = wrap(k - 1, n2), kp = wrap(k + 1, n2);
             const long c = (long)q * n2 + k;
-            // zero couplings never read their (clamped) neighbour
-            const double s = (w0 != 0.0 ? w0 * x[rim * n2 + k] : 0.0) + (w1 != 0.0 ? w1 * x[rip * n2 + k] : 0.0) +
-                             (w2 != 0.0 ? w2 * x[rjm * n2 + k] : 0.0) + (w3 != 0.0 ? w3 * x[rjp * n2 + k] : 0.0) +
-                             (w4 != 0.0 ? w4 * x[(long)q * n2 + km] : 0.0) +
-                             (w5 != 0.0 ? w5 * x[(long)q * n2 + kp] : 0.0);
+            // ghost neighbours (walls) are never read: zero-gradient walls
+            // have no coupling, Dirichlet ghosts are zero
+            const double s = (in0 ? w0 * x[rim * n2 + k] : 0.0) + (in1 ? w1 * x[rip * n2 + k] : 0.0) +
+                             (in2 ? w2 * x[rjm * n2 + k] : 0.0) + (in3 ? w3 * x[rjp * n2 + k] : 0.0) +
+                             (in4 ? w4 * x[(long)q * n2 + km] : 0.0) + (in5 ? w5 * x[(long)q * n2 + kp] : 0.0);
             const double d = w0 + w1 + w2 + w3 + w4 + w5;
             const double V = hij * (p2[k + 1] - p2[k]);
             const double r = b[c] + V * (d * x[c] - s);
@@ -139,9 +155,15 @@ extern "C" int bmg_residual_norm_noalloc(const double* x, const double* b, const
                                          const double* points_z, const int bc[6], double* norm_out,
                                          void* stream) {
     if (!x || !b || !n || !points_x || !points_y || !points_z || !bc || !norm_out) return BMG_BAD_ARG;
+    int dir = 0;
     for (int d = 0; d < 3; ++d) {
         if (n[d] < 1) return BMG_BAD_ARG;
         if ((bc[2 * d] == BMG_BC_PERIODIC) != (bc[2 * d + 1] == BMG_BC_PERIODIC)) return BMG_BAD_ARG;
+        for (int side = 0; side < 2; ++side) {
+            const int t = bc[2 * d + side];
+            if (t != BMG_BC_NEUMANN && t != BMG_BC_PERIODIC && t != BMG_BC_DIRICHLET) return BMG_BAD_ARG;
+            if (t == BMG_BC_DIRICHLET) dir |= 1 << (2 * d + side);
+        }
     }
     const long nrows = (long)n[0] * n[1];
     if (nrows > BMG_NOALLOC_MAX_ROWS) {
@@ -157,7 +179,7 @@ extern "C" int bmg_residual_norm_noalloc(const double* x, const double* b, const
     const int blocks = (int)(nrows < 148L * 8 ? nrows : 148L * 8);
     k_rows<<<blocks, kThreads, 0, s>>>(x, b, n[0], n[1], n[2], points_x, points_y, points_z,
                                        bc[0] == BMG_BC_PERIODIC, bc[2] == BMG_BC_PERIODIC,
-                                       bc[4] == BMG_BC_PERIODIC, rows);
+                                       bc[4] == BMG_BC_PERIODIC, dir, rows);
     k_sum_rows<<<1, kThreads, 0, s>>>(rows, (int)nrows, norm_out);
     return cudaGetLastError() == cudaSuccess ? BMG_OK : BMG_CUDA_ERROR;
 }

@@ -247,7 +247,8 @@ int bmg_project_correct(struct bmg_ctx* ctx, double* u0, double* u1, double* u2,
  * *norm_out = ||b - A x||_2 for one brick with the solver's level-0 operator
  * (constant coefficient).  x, b: device arrays of interior cells, k fastest;
  * points_*: device arrays of n[d]+1 vertex coordinates; bc: host array of
- * BMG_BC_* per face; norm_out: one device double.  Work is queued on
+ * BMG_BC_* per face (Dirichlet faces homogeneous: the eliminated operator,
+ * with any face values already in b); norm_out: one device double.  Work is queued on
  * `stream` (a cudaStream_t, NULL for the default stream); the result is
  * ready once the stream has reached that point.
  *

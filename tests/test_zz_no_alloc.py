@@ -24,11 +24,22 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr())
 
 
-@pytest.mark.parametrize("name,N", [("channel", 32), ("cavity", 24)])
+def _dirichlet_mesh(N):
+    from briscola_b200.mesh import Brick, Mesh, geometric_points, uniform_points
+
+    br = Brick([uniform_points(N), uniform_points(N), geometric_points(N, 2.0)],
+               ("Dirichlet", "Neumann", "periodic", "periodic", "Dirichlet", "Dirichlet"))
+    return Mesh([br]), np.random.default_rng(5).standard_normal(N ** 3), None
+
+
+_BC = {"periodic": NA.BC_PERIODIC, "Neumann": NA.BC_NEUMANN, "Dirichlet": NA.BC_DIRICHLET}
+
+
+@pytest.mark.parametrize("name,N", [("channel", 32), ("cavity", 24), ("dirichlet", 16)])
 def test_noalloc_norm_matches_context_residual(native, name, N):
     import torch
 
-    mesh, b, _ = workloads.CONFIGS[name](N)
+    mesh, b, _ = _dirichlet_mesh(N) if name == "dirichlet" else workloads.CONFIGS[name](N)
     br = mesh.bricks[0]
     rng = np.random.default_rng(17)
     x = rng.standard_normal(b.size)
@@ -45,7 +56,7 @@ def test_noalloc_norm_matches_context_residual(native, name, N):
     pts = [torch.from_numpy(np.ascontiguousarray(p)).to(dev) for p in br.points]
     out = torch.full((1,), -1.0, dtype=torch.float64, device=dev)
     n = (ctypes.c_int * 3)(*br.N)
-    bc = (ctypes.c_int * 6)(*[NA.BC_PERIODIC if f == "periodic" else NA.BC_NEUMANN for f in br.bc])
+    bc = (ctypes.c_int * 6)(*[_BC[f] for f in br.bc])
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     for call in range(2):  # the static scratch is reused by the second call
         out.fill_(-1.0)
