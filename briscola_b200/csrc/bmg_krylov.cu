@@ -259,7 +259,6 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_dots4(Bricks<double> B, 
         Quad4<T>::ld(z + c, zq);
         Quad4<double>::ld(r + c, rq);
         Quad4<double>::ld(q + c, qq);
-        _Pragma("unroll")
         for (int e = 0; e < 4; ++e) {
             const double Vz = (hij * hk[e]) * (double)zq[e];
             a1 += Vz * rq[e];
@@ -293,7 +292,6 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_direction4(Bricks<double
         double pq[4], qq[4], pn[4], qn[4];
         Quad4<double>::ld(p + c, pq);
         Quad4<double>::ld(q + c, qq);
-        _Pragma("unroll")
         for (int e = 0; e < 4; ++e) {
             double w[6];
             couplings<double, VAR>(L, i, j, k0 + e, c + e, w);
@@ -327,7 +325,6 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_update4(Bricks<double> B
         Quad4<double>::ld(p + c, pq);
         Quad4<double>::ld(r + c, rq);
         Quad4<double>::ld(q + c, qq);
-        _Pragma("unroll")
         for (int e = 0; e < 4; ++e) {
             xq[e] = xq[e] + alpha * pq[e];
             rn[e] = rq[e] - alpha * qq[e];
@@ -336,7 +333,6 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_update4(Bricks<double> B
         }
         Quad4<double>::st(L.x + c, xq);
         if (quad_has_images(L, i, j, k0)) {
-            _Pragma("unroll")
             for (int e = 0; e < 4; ++e) store_images(L, c + e, i, j, k0 + e, xq[e]);
         }
         Quad4<double>::st(r + c, rn);
