@@ -95,6 +95,35 @@ def test_make_options_maps_reference_keys():
     assert bb.make_options({}).criterion == 0 and bb.make_options({"criterion": "rhs"}).criterion == 1
     with pytest.raises(bb.FatalError):
         bb.make_options({"criterion": "x"})
+    # MG.C:277-305: coarseMode, restrict, prolong
+    d = bb.make_options({})
+    assert (d.coarse_mode, d.restrict_scheme, d.prolong_scheme) == (0, 0, 0)
+    o = bb.make_options({"coarseMode": "smooth", "restrict": "average", "prolong": "injection"})
+    assert (o.coarse_mode, o.restrict_scheme, o.prolong_scheme) == (1, 1, 1)
+    for bad in ({"coarseMode": "amg"}, {"restrict": "volumeWeighted"}, {"prolong": "cubic"}):
+        with pytest.raises(bb.FatalError):
+            bb.make_options(bad)
+
+
+def _fft_desc():
+    from briscola_b200 import fft
+
+    return fft.Desc
+
+
+@pytest.mark.parametrize("header,name,mirror", [("bmg.h", "bmg_options", lambda: NA.Options),
+                                                ("bmg.h", "bmg_brick", lambda: NA.Brick),
+                                                ("bmg.h", "bmg_report", lambda: NA.Report),
+                                                ("bfft.h", "bfft_desc", _fft_desc)])
+def test_structs_match_the_header(header, name, mirror):
+    """The ctypes mirrors of the C ABI's structs list the header's fields in
+    order (a field missing from a mirror would shift every later one)."""
+    mirror = mirror()
+    txt = open(os.path.join(ROOT, "include", header)).read()
+    body = txt[txt.index(f"typedef struct {name} {{"):txt.index(f"}} {name};")]
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    fields = re.findall(r"\b(?:const\s+)?(?:int|double|float|long)\s*\*?\s+(\w+)\s*(?:\[\d+\])?\s*;", body)
+    assert fields == [f for f, _ in mirror._fields_]
 
 
 def test_geometric_grading_ratio():
