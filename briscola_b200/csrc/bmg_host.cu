@@ -1037,14 +1037,19 @@ void build(bmg_ctx* c, HostLevel&& L0) {
     c->visits.assign(nl, 0);
 }
 
-void configureCoarse(bmg_ctx* c) {
+// the coarse solve level the options ask for, checked against the hierarchy
+int coarseLevelFor(const bmg_ctx* c, const bmg_options& o) {
     const int nl = (int)c->lv.size();
-    if (nl < 2 || c->opt.coarse_level > nl - 2)
+    if (nl < 2 || o.coarse_level > nl - 2)
         throw BadArg{BMG_BAD_ARG, "coarseLevel too high: at most (number of levels - 2)"};
-    const int lc = nl - 1 - c->opt.coarse_level;
-    if (c->lv[lc].ncell > 4096 && c->opt.coarse_mode == BMG_COARSE_DIRECT)
+    const int lc = nl - 1 - o.coarse_level;
+    if (c->lv[lc].ncell > 4096 && o.coarse_mode == BMG_COARSE_DIRECT)
         throw BadArg{BMG_UNSUPPORTED, "coarse solve level above 4096 cells; raise coarseLevel"};
-    c->lc = lc;
+    return lc;
+}
+
+void configureCoarse(bmg_ctx* c) {
+    c->lc = coarseLevelFor(c, c->opt);
     refreshCoarseInverse(c);
 }
 
@@ -1897,6 +1902,8 @@ int bmg_set_options(bmg_ctx* c, const bmg_options* o) {
             o->restrict_scheme != c->opt.restrict_scheme || o->prolong_scheme != c->opt.prolong_scheme;
         const bool retune = o->autotune && (!c->opt.autotune || o->fused != c->opt.fused ||
                                             o->n_pre != c->opt.n_pre || o->n_post != c->opt.n_post);
+        // options the hierarchy cannot take are refused before anything changes
+        if (coarseChanged) coarseLevelFor(c, *o);
         c->opt = *o;
         destroyGraph(c);
         BMG_CUDA(cudaSetDevice(c->opt.device));

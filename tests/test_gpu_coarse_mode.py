@@ -107,3 +107,17 @@ def test_mixed_fcg_with_smoothed_coarse_level(native):
     x = np.zeros_like(b)
     rep = c.solve(b, x, zero_guess=True)
     assert rep.status == 0 and rep.rel_residual <= 1.5e-8
+
+
+def test_refused_options_leave_the_context_unchanged(native):
+    """bmg_set_options refuses a direct coarse solve on a level above 4096
+    cells before it changes anything: the context keeps solving with the
+    options it had."""
+    mesh, b, _ = workloads.cavity(64)
+    c = ctx(mesh, relTol=0.0, maxIter=5, coarseLevel=4)  # smoothed 32^3 coarse level
+    with pytest.raises(bb.FatalError):
+        c.set_options(bb.make_options({"nSweepsPre": 2, "nSweepsPost": 2, "cycleType": "V",
+                                       "coarseMode": "direct", "coarseLevel": 4}))
+    x = np.zeros_like(b)
+    rep = c.solve(b, x, zero_guess=True)
+    assert rep.cycles == 5 and rep.final_residual < 0.5 * rep.initial_residual
