@@ -154,3 +154,24 @@ def test_face_value_conventions_match_the_fft_restatement(bc, values):
     A, V, bdir = brick_operator(pts, bc, values)
     x_mg = spl.spsolve(A.tocsc(), -(V * f.ravel()) + bdir)
     assert rel(x_mg, x_fft.ravel()) <= 1e-10
+
+
+@pytest.mark.parametrize("cycle", ["V", "W", "F"])
+@pytest.mark.parametrize("options", [dict(), dict(coarse_direct=0), dict(restrict_average=1, prolong_injection=1)])
+def test_every_cycle_option_reaches_the_direct_solution(cycle, options):
+    """Cycle type, coarse mode and transfer schemes change how the oracle gets
+    there, not where it goes: each reaches the sparse direct solution."""
+    import scipy.sparse.linalg as spl
+
+    bc, values = (D, N, P, P, N, D), (1.0, 0.0, 0.0, 0.0, 0.5, -1.0)
+    periodic = (False, True, False)
+    pts = geometry(periodic)
+    n = tuple(len(p) - 1 for p in pts)
+    A, V, bdir = brick_operator(pts, bc, values)
+    b = np.random.default_rng(11).standard_normal(int(np.prod(n)))
+    ref = spl.spsolve(A.tocsc(), b + bdir)
+    o = Oracle(pts, periodic, nthreads=2, dirichlet=[f == D for f in bc], values=values)
+    x, rep, hist, rc = o.solve(b.reshape(n), rel_tol=1e-12, cycle_type=cycle, n_pre=2, n_post=2, coarse_level=1,
+                               max_iter=400, **options)
+    assert rc == 0
+    assert rel(x.ravel(), ref) <= 1e-9
