@@ -109,18 +109,26 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_reference(N: int, steps: int | None = None, warmup: int = 0):
-    """Time the oracle (CPU restatement of the reference MG, all host threads)
-    on the benchmark workload: full solves from a zero guess."""
+def cpu_reference(N: int, steps: int | None = None, warmup: int = 0, stale: int = 1,
+                  nthreads: int | None = None):
+    """Time the oracle (CPU restatement of the reference MG) on the benchmark
+    workload: full solves from a zero guess.  nthreads threads (default: all
+    host threads) emulate as many ranks of a slab decomposition of the brick
+    (P, 1, 1): each owns a contiguous range of i-planes in every pass, with a
+    barrier between passes where the reference exchanges halos, and levels
+    with fewer than 2P planes run on one thread, as the reference gathers
+    its coarse levels.  stale: the reference's stale finest-level residual
+    on the first repetition (MG.C:72), on (1, the reference) or off (0)."""
     from briscola_b200 import workloads
     from oracle.pyoracle import Oracle
 
     mesh, b, _ = workloads.channel(N)
     br = mesh.bricks[0]
-    threads = os.cpu_count() or 1
+    threads = nthreads or os.cpu_count() or 1
     o = Oracle(br.points, periodic=br.periodic, nthreads=threads)
     bb = b.reshape(br.N)
-    kw = dict(rel_tol=1e-8, abs_tol=0.0, n_pre=2, n_post=2, cycle_type="V", coarse_level=1)
+    kw = dict(rel_tol=1e-8, abs_tol=0.0, n_pre=2, n_post=2, cycle_type="V", coarse_level=1,
+              stale_residual=stale)
     times, cycles = [], 0
     for s in range(warmup + (steps or 1)):
         t = time.perf_counter()
@@ -130,6 +138,29 @@ def cpu_reference(N: int, steps: int | None = None, warmup: int = 0):
         if s >= warmup:
             times.append(dt)
     return times, cycles, threads
+
+
+def cpu_one_core(N: int, cycles: int):
+    """One core (one reference rank owning the whole brick), a bounded
+    sample: a solve stopped after 1 cycle and one stopped after 3 give the
+    set-up cost and the cost of a cycle; ms per solve = set-up + cycles
+    times the cycle cost."""
+    from briscola_b200 import workloads
+    from oracle.pyoracle import Oracle
+
+    mesh, b, _ = workloads.channel(N)
+    br = mesh.bricks[0]
+    o = Oracle(br.points, periodic=br.periodic, nthreads=1)
+    bb = b.reshape(br.N)
+    kw = dict(rel_tol=0.0, abs_tol=0.0, n_pre=2, n_post=2, cycle_type="V", coarse_level=1)
+    t = {}
+    for m in (1, 3):
+        t0 = time.perf_counter()
+        o.solve(bb, max_iter=m, **kw)
+        t[m] = (time.perf_counter() - t0) * 1e3
+    per_cycle = (t[3] - t[1]) / 2
+    setup = max(t[1] - per_cycle, 0.0)
+    return setup + cycles * per_cycle, per_cycle, setup
 
 
 def max_over_ranks(value: float, dist, device) -> float:
@@ -559,6 +590,45 @@ def main():
         m = re.search(r"^traffic per launch \(bytes\): ([0-9.e+]+)", open(tp).read(), re.M)
         traffic = float(m.group(1)) if m else None
 
+    # ---- the same for the plain FP64 path's level-0 smoothing step ----
+    c64 = ctx["fp64"]
+    pass64 = []
+    for r in range(reps):
+        e0.record(stream)
+        c64.smooth(0, SOLVER_KEYS["nSweepsPost"], precision=0)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        pass64.append(e0.elapsed_time(e1))
+    st64, chunk64 = c64.tuning(0, 0)
+    lps64 = -(-n_stages // max(st64, 1))
+    t64 = statistics.median(pass64) * 1e-3 / lps64
+    alg64 = (24.0 if st64 >= 2 else 12.0) * cells
+    ach64 = alg64 / t64 / 1e9
+    roof64 = {"bound": "hbm", "kernel": (f"k_sweep<double> level 0 ({lps64} launches of up to {st64} colour "
+                                         f"stages, {chunk64}-plane chunks)" if st64 else
+                                         f"colour pass<double> level 0 ({lps64} passes per 2-sweep step)"),
+              "achieved": round(ach64, 1), "peak": hbm, "unit": "GB/s", "frac": round(ach64 / hbm, 4),
+              "peak_kind": peak_kind, "algorithmic_bytes_per_launch": alg64,
+              "launch_us": round(t64 * 1e6, 2)}
+
+    # ---- the headline solution's error against an FP64 solution of the same
+    # system: the direct GPU FFT solve (Laplacian(x) = -f, b = -V f) ----
+    from briscola_b200 import fft as _fft
+
+    br0 = mesh.bricks[0]
+    Vd = torch.from_numpy(br0.cell_volumes().ravel()).to(f"cuda:{local}")
+    solve("mixed_fcg")
+    xf = torch.empty_like(b_d)
+    fs = _fft.FFTPoissonSolver(br0, device=local)
+    fs.solve(xf, -(b_d / Vd))
+    fs.close()
+
+    def _centred(t):
+        return t - (t * Vd).sum() / Vd.sum()
+
+    err_fp64 = float(torch.linalg.norm(_centred(x_d) - _centred(xf)) / torch.linalg.norm(_centred(xf)))
+    del xf, Vd
+
     # ---- end to end through the plugin call with host buffers ----
     d = bb.Dictionary(dict(SOLVER_KEYS, type="GPUMG", precision="mixed", krylov="fcg", device=local))
     s = bb.solver.New(d, mesh)
@@ -659,9 +729,20 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         times, cycles, threads = cpu_reference(args.size, steps=1)
+        times_ns, cycles_ns, _ = cpu_reference(args.size, steps=1, stale=0)
+        one_ms, one_cycle_ms, one_setup_ms = cpu_one_core(args.size, cycles)
         cpu = {"value": round(times[0], 1), "unit": "ms/solve", "cores": threads, "kind": "port",
+               "ranks": threads, "decomposition": [threads, 1, 1],
                "sample": f"one full solve of the same {args.size}^3 workload by the CPU restatement "
-                         f"of the reference MG ({cycles} V(2,2) cycles, {threads} threads)"}
+                         f"of the reference MG ({cycles} V(2,2) cycles) on {threads} threads emulating "
+                         f"{threads} ranks of a ({threads},1,1) slab decomposition (contiguous i-plane "
+                         "ranges, a barrier per pass for the halo exchange, coarse levels gathered to one "
+                         "thread); stale finest-level residual of MG.C:72 on, as in the reference",
+               "stale_residual_off": {"value": round(times_ns[0], 1), "cycles": cycles_ns},
+               "one_core": {"value": round(one_ms, 1), "ranks": 1, "decomposition": [1, 1, 1],
+                            "ms_per_cycle": round(one_cycle_ms, 1), "setup_ms": round(one_setup_ms, 1),
+                            "sample": "solves stopped after 1 and after 3 cycles on one thread; "
+                                      f"value = set-up + {cycles} cycles"}}
 
     # algorithmic bytes of one FP64 V(2,2) cycle: 164.6 B per finest cell
     hbm_gbs_fp64 = 164.6 * cells * statistics.mean(cyc_fp64) / (ms_fp64 / args.steps * 1e-3) / 1e9
@@ -683,6 +764,9 @@ def main():
             "arms_cycles": {"mixed_fcg": cyc_head[0], "fp64": cyc_fp64[0], "mixed": cyc_mixed[0],
                             "fp64_fcg": cyc_fp64_fcg[0]},
             "rel_residual": rep_head.rel_residual,
+            "error_vs_fp64": {"value": err_fp64, "against": "the direct FP64 GPU FFT solve of the same system",
+                              "norm": "relative L2 of the volume-weighted mean-free solutions"},
+            "roofline_fp64_smoother": roof64,
             "hbm_gbs_fp64_cycle_algorithmic": round(hbm_gbs_fp64, 1),
             "roofline": {"bound": "hbm",
                          "kernel": (f"k_sweep<float> level 0 ({launches_per_step} launches of up to "

@@ -23,6 +23,7 @@ CRITERION = {"initial": 0, "rhs": 1}
 COARSE_MODE = {"direct": 0, "smooth": 1}
 RESTRICT = {"linear": 0, "average": 1}
 PROLONG = {"linear": 0, "injection": 1}
+ROW_LAYOUT = {"split": 0, "natural": 1}
 DEVICE_PTRS, ZERO_GUESS, PER_VOLUME = 1, 2, 4
 
 # Every function the header declares; the loader checks they are exported.
@@ -77,6 +78,7 @@ class Options(ctypes.Structure):
         ("coarse_mode", ctypes.c_int),
         ("restrict_scheme", ctypes.c_int),
         ("prolong_scheme", ctypes.c_int),
+        ("row_layout", ctypes.c_int),
     ]
 
 

@@ -89,6 +89,7 @@ struct HostLevel {
     double* x64b = nullptr;  // second x buffers: fused smoothing writes here, then swaps
     float* x32b = nullptr;
     bool fusedOK = false;    // single brick large enough for the fused smoother
+    bool ks = false;         // parity-split rows (bmg_internal.h)
     // per precision (0: FP64, 1: FP32), picked by autotune():
     int fusedS[2] = {kFusedMaxStages, kFusedMaxStages};  // colour stages per fused launch
     int fusedTi[2] = {64, 64};                             // planes per CTA chunk
@@ -194,6 +195,21 @@ void finishAxis(Axis& a, int n, bool periodic, double glo, double ghi) {
     }
 }
 
+// storage position of k in a parity-split row (kpos_split of bmg_stencil.cuh)
+inline int kposSplit(int k) { return (k & ~15) | ((k & 1) << 3) | ((k >> 1) & 7); }
+
+// a slab field in natural row order -> parity-split order (interior k of
+// every row of the brick, ghost rows included; the k ghosts stay)
+void splitRows(const HostBrick& B, std::vector<double>& f) {
+    std::vector<double> tmp(B.n[2]);
+    for (int i = -1; i <= B.n[0]; ++i)
+        for (int j = -1; j <= B.n[1]; ++j) {
+            const long r = B.base + (long)i * B.si + (long)j * B.sj;
+            for (int k = 0; k < B.n[2]; ++k) tmp[kposSplit(k)] = f[r + k];
+            for (int k = 0; k < B.n[2]; ++k) f[r + k] = tmp[k];
+        }
+}
+
 // Rows of pitch p2 = round_up(n2 + 5, 4) with interior k = 0 at offset 4:
 // rows and interiors start on 16-byte (FP32) / 32-byte (FP64) boundaries so
 // pairs of k-neighbours load as one vector; the k ghosts sit at offsets 3
@@ -241,6 +257,13 @@ void buildTables(HostLevel& L, const int dirichlet[6]) {
             to.h[d] = off;
             off = next(off, B.n[d]);
         }
+        to.kwl = to.kwh = -1;
+        if (L.ks) {
+            to.kwl = off;
+            off = next(off, B.n[2]);
+            to.kwh = off;
+            off = next(off, B.n[2]);
+        }
         to.total = off;
         L.tab.resize(off, 0.0);
         for (int d = 0; d < 3; ++d) {
@@ -258,6 +281,11 @@ void buildTables(HostLevel& L, const int dirichlet[6]) {
                 L.tab[to.h[d] + i] = hi;
             }
         }
+        if (L.ks)  // the k couplings once more, in the rows' storage order
+            for (int k = 0; k < B.n[2]; ++k) {
+                L.tab[to.kwl + kposSplit(k)] = L.tab[to.wl[2] + k];
+                L.tab[to.kwh + kposSplit(k)] = L.tab[to.wh[2] + k];
+            }
     }
 }
 
@@ -308,6 +336,7 @@ Bricks<T> bricks(const bmg_ctx* c, int l) {
         v.per1 = c->periodic[1];
         v.per2 = c->periodic[2];
         v.cpar = K.cpar;
+        v.ks = H.ks ? 1 : 0;
         // a smoothed coarse level of a singular system keeps global cell 0
         // (brick 0's first cell) at zero
         v.pin = l == c->lc && b == 0 && c->singular && c->opt.coarse_mode == BMG_COARSE_SMOOTH;
@@ -560,6 +589,7 @@ void validateOptions(const bmg_options* o) {
     if (o->coarse_mode < 0 || o->coarse_mode > 1) throw BadArg{BMG_BAD_ARG, "unknown coarseMode"};
     if (o->restrict_scheme < 0 || o->restrict_scheme > 1) throw BadArg{BMG_BAD_ARG, "unknown restriction scheme"};
     if (o->prolong_scheme < 0 || o->prolong_scheme > 1) throw BadArg{BMG_BAD_ARG, "unknown prolongation scheme"};
+    if (o->row_layout < 0 || o->row_layout > 1) throw BadArg{BMG_BAD_ARG, "unknown rowLayout"};
 }
 
 // Level-0 bricks from the mesh description; contacts between bricks.
@@ -878,8 +908,11 @@ void uploadLambda(bmg_ctx* c) {
                 }
             if (!L.lam64[d]) L.lam64[d] = dalloc<double>(L.cells);
             if (!L.lam32[d]) L.lam32[d] = dalloc<float>(L.cells);
-            upload(L.lam64[d], L.lam_host[d]);
-            upload(L.lam32[d], to_f32(L.lam_host[d]));
+            // lam_host keeps the natural order (the coarse matrix reads it)
+            std::vector<double> dev = L.lam_host[d];
+            if (L.ks) splitRows(L.br[0], dev);
+            upload(L.lam64[d], dev);
+            upload(L.lam32[d], to_f32(dev));
         }
     }
 }
@@ -992,6 +1025,11 @@ void build(bmg_ctx* c, HostLevel&& L0) {
     for (auto& L : c->lv) {
         layout(L);
         if (L.cells >= (1L << 31)) throw BadArg{BMG_UNSUPPORTED, "a level above 2^31 cells"};
+        // parity-split rows on the single-brick levels the per-pass kernels
+        // run (above the single-CTA coarse end's size) whose rows are whole
+        // 16-cell blocks
+        L.ks = c->opt.row_layout == BMG_ROWS_SPLIT && !c->multi && L.br[0].n[2] % 16 == 0 &&
+               L.ncell > kTailCells;
         buildTables(L, c->dirichlet);
         L.x64 = dalloc<double>(L.cells);
         L.b64 = dalloc<double>(L.cells);
@@ -1006,7 +1044,7 @@ void build(bmg_ctx* c, HostLevel&& L0) {
         // and it relies on periodic extents being even (a wrapped neighbour
         // then has the other colour, as an interior one does)
         const HostBrick& B = L.br[0];
-        L.fusedOK = !c->multi && B.n[0] >= 16 && B.n[1] >= 16 && B.n[2] >= 16 && B.n[2] % 4 == 0;
+        L.fusedOK = !c->multi && !L.ks && B.n[0] >= 16 && B.n[1] >= 16 && B.n[2] >= 16 && B.n[2] % 4 == 0;
         for (int d = 0; d < 3; ++d)
             if (c->periodic[d] && B.n[d] % 2) L.fusedOK = false;
         if (L.fusedOK) {
@@ -1840,6 +1878,7 @@ int bmg_default_options(bmg_options* o) {
     o->coarse_mode = BMG_COARSE_DIRECT;
     o->restrict_scheme = BMG_RESTRICT_LINEAR;
     o->prolong_scheme = BMG_PROLONG_LINEAR;
+    o->row_layout = BMG_ROWS_SPLIT;
     return BMG_OK;
 }
 
@@ -1897,6 +1936,8 @@ int bmg_set_options(bmg_ctx* c, const bmg_options* o) {
     return guarded(c, [&] {
         validateOptions(o);
         if (o->device != c->opt.device) throw BadArg{BMG_BAD_ARG, "the device of a context is fixed"};
+        if (o->row_layout != c->opt.row_layout)
+            throw BadArg{BMG_BAD_ARG, "the row layout of a context is fixed at creation"};
         const bool coarseChanged = o->coarse_level != c->opt.coarse_level || o->coarse_mode != c->opt.coarse_mode;
         const bool transfersChanged =
             o->restrict_scheme != c->opt.restrict_scheme || o->prolong_scheme != c->opt.prolong_scheme;

@@ -12,6 +12,17 @@
 //   Compact (interior-only) arrays list the bricks one after another, each
 //   k fastest, as the C ABI does.
 //
+// Parity-split rows (LevelView::ks, single-brick levels above kTailCells
+// cells with n2 % 16 == 0): the interior of every row is stored in blocks of
+// 16 cells, the 8 even k of a block first, then its 8 odd k, so cell (i,j,k)
+// sits at base + i*si + j*sj + kpos_split(k).  In a row the even k have one
+// red-black colour and the odd k the other, and the same-k cells of the
+// neighbouring rows have the other colour of the same k parity: a colour
+// pass reads and writes whole 32-byte sectors of one colour only, where the
+// natural order reads every sector of x and b to update half of them.  The
+// k ghosts keep their natural places (k = -1 and k = n2), and so do the
+// periodic images (a cell and its k image are n2 apart in both orders).
+//
 // Ghosts: on a single brick, periodic axes keep their ghost layers (faces,
 //   edges, corners) current by write-through -- every kernel that stores an
 //   interior value also stores its ghost images -- so stencils read ghosts
@@ -47,6 +58,8 @@ struct TabOff {
     int wl[3];   // coupling to the lower neighbour, per cell along the axis
     int wh[3];   // coupling to the upper neighbour
     int h[3];    // cell sizes (volume factors)
+    int kwl, kwh;  // parity-split levels: the k couplings in the row's storage
+                   // order (entry kpos_split(k) holds wl[2] / wh[2] of k); -1 otherwise
     int total;
 };
 
@@ -72,6 +85,7 @@ struct LevelView {
     int cpar;          // parity of the brick origin: colour = (i+j+k+cpar) & 1
     int pin;           // smoothers keep cell (0,0,0) at zero: the singularity pin
                        // of an iteratively smoothed coarse level (solver.C:201-231)
+    int ks;            // rows parity-split (see above); 0: natural k order
 };
 
 // Wall faces of a single-brick level 0: bit f of mask for a Dirichlet face

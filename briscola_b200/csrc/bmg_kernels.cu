@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(256) k_colour_pass(Bricks<T> B, int colour) {
     const long c = r + k;
     if (L.pin && (i | j | k) == 0) return;  // the pinned cell stays zero
     T w[6];
-    couplings<T, VAR>(L, i, j, k, c, w);
+    couplings<T, VAR>(L, i, j, k, c, c + 1, w);  // natural rows only (n2 % 4 != 0)
     const T xn[6] = {e ? xm.y : xm.x, e ? xp.y : xp.x, e ? ym.y : ym.x, e ? yp.y : yp.x,
                      e ? own.x : x[c0 - 1], e ? x[c0 + 2] : own.y};
     store_x(L, c, i, j, k, gs_value(w, xn, L.b[c]));
@@ -123,6 +123,50 @@ struct Row4<double> {
     }
 };
 
+// The logical k-quad k0 .. k0+3 (k0 % 4 == 0) of a row, at slab index c
+// = the quad's first cell: one vector in a natural row; in a parity-split
+// row the even pair (k0, k0+2) at c and the odd pair (k0+1, k0+3) at c + 8.
+template <typename T>
+__device__ __forceinline__ void ldq(const T* p, int ks, T v[4]) {
+    if (ks) {
+        Row4<T>::ld2(p, v[0], v[2]);
+        Row4<T>::ld2(p + 8, v[1], v[3]);
+    } else {
+        Row4<T>::ld(p, v);
+    }
+}
+template <typename T>
+__device__ __forceinline__ void ldgq(const T* p, int ks, T v[4]) {
+    if (ks) {
+        v[0] = ldg(p);
+        v[2] = ldg(p + 1);
+        v[1] = ldg(p + 8);
+        v[3] = ldg(p + 9);
+    } else {
+        Row4<T>::ldg4(p, v);
+    }
+}
+template <typename T>
+__device__ __forceinline__ void stq(T* p, int ks, const T v[4]);
+template <>
+__device__ __forceinline__ void stq<float>(float* p, int ks, const float v[4]) {
+    if (ks) {
+        *reinterpret_cast<float2*>(p) = make_float2(v[0], v[2]);
+        *reinterpret_cast<float2*>(p + 8) = make_float2(v[1], v[3]);
+    } else {
+        Row4<float>::st(p, v);
+    }
+}
+template <>
+__device__ __forceinline__ void stq<double>(double* p, int ks, const double v[4]) {
+    if (ks) {
+        *reinterpret_cast<double2*>(p) = make_double2(v[0], v[2]);
+        *reinterpret_cast<double2*>(p + 8) = make_double2(v[1], v[3]);
+    } else {
+        Row4<double>::st(p, v);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Red-black colour pass, four cells per thread: the thread owns the k-quad
 // (4p .. 4p+3) of one row and updates the two cells of the requested colour.
@@ -132,7 +176,8 @@ struct Row4<double> {
 // safe; a quad is never a ghost).  colour_quad_item is shared with the
 // single-CTA coarse cycle (k_tail_cycle).  The arithmetic is gs_value's, so results are
 // bit-identical to k_colour_pass and the fused smoother.  Needs every
-// brick's n2 % 4 == 0.
+// brick's n2 % 4 == 0 and natural rows (parity-split levels take
+// k_colour_split).
 // ---------------------------------------------------------------------------
 template <typename T, bool VAR>
 __device__ __forceinline__ void colour_quad_item(const LevelView<T>& L, int i, int j, int p, int colour) {
@@ -207,6 +252,115 @@ __global__ void __launch_bounds__(256) k_colour_quad(Bricks<T> B, int colour) {
     colour_quad_item<T, VAR>(L, i, j, p, colour);
 }
 
+// ---------------------------------------------------------------------------
+// Red-black colour pass on a parity-split level (bmg_internal.h): the
+// thread owns one 32-byte sector of the pass's colour, NC = 32 / sizeof(T)
+// consecutive slots (8 FP32 or 4 FP64 cells) of one half of a 16-cell block
+// of a row.  Every value it reads is one the update needs: the other
+// colour's slots of its own row (the same slots of the other half) and one
+// k neighbour beyond them, the same slots of the four neighbouring rows,
+// b of its own cells, the k couplings from tables stored in the same order,
+// all as whole 16-byte vectors; it writes its sector back.  Per cell the
+// arithmetic is gs_value's with colour_quad_item's couplings and neighbour
+// order, so the pass is bit-identical to the natural-order kernels.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct Sector;
+template <>
+struct Sector<float> {
+    static constexpr int N = 8;
+    static __device__ __forceinline__ void ld(const float* p, float v[8]) {
+        const float4 a = reinterpret_cast<const float4*>(p)[0], b = reinterpret_cast<const float4*>(p)[1];
+        v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+    }
+    static __device__ __forceinline__ void ldg(const float* p, float v[8]) {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(p)), b = __ldg(reinterpret_cast<const float4*>(p) + 1);
+        v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+    }
+    static __device__ __forceinline__ void st(float* p, const float v[8]) {
+        reinterpret_cast<float4*>(p)[0] = make_float4(v[0], v[1], v[2], v[3]);
+        reinterpret_cast<float4*>(p)[1] = make_float4(v[4], v[5], v[6], v[7]);
+    }
+};
+template <>
+struct Sector<double> {
+    static constexpr int N = 4;
+    static __device__ __forceinline__ void ld(const double* p, double v[4]) { Row4<double>::ld(p, v); }
+    static __device__ __forceinline__ void ldg(const double* p, double v[4]) { Row4<double>::ldg4(p, v); }
+    static __device__ __forceinline__ void st(double* p, const double v[4]) { Row4<double>::st(p, v); }
+};
+
+template <typename T, bool VAR>
+__global__ void __launch_bounds__(256) k_colour_split(LevelView<T> L, int colour) {
+    constexpr int NC = Sector<T>::N;  // cells per thread
+    constexpr int TH = 8 / NC;        // threads per half block
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i >= L.n0 || j >= L.n1 || t >= L.n2 / (2 * NC)) return;
+    const int g = t / TH, m0 = (t % TH) * NC;  // block of the row, first slot
+    // h = 0: the even k of this row have the pass's colour (k = 16g + 2m + h)
+    const int h = (colour ^ (i + j + L.cpar)) & 1;
+    const int si = (int)L.si, sj = (int)L.sj;
+    const int row = (int)L.base + i * si + j * sj;
+    const int own = row + 16 * g + 8 * h + m0;
+    const int oth = row + 16 * g + 8 * (1 - h) + m0;
+    // the k neighbour beyond the slots: below the first cell (h = 0; the
+    // previous block's last odd cell, or the ghost k = -1) or above the last
+    // one (h = 1; the next block's first even cell, or the ghost k = n2)
+    const int ext = h == 0 ? (m0 > 0 ? oth - 1 : row + 16 * g - 1) : (m0 + NC < 8 ? oth + NC : row + 16 * g + 16);
+    T xo[NC], xm[NC], xp[NC], ym[NC], yp[NC], bb[NC], wkl[NC], wkh[NC];
+    Sector<T>::ld(L.x + oth, xo);
+    Sector<T>::ld(L.x + own - si, xm);
+    Sector<T>::ld(L.x + own + si, xp);
+    Sector<T>::ld(L.x + own - sj, ym);
+    Sector<T>::ld(L.x + own + sj, yp);
+    Sector<T>::ld(L.b + own, bb);
+    const T e = L.x[ext];
+    Sector<T>::ldg(L.tab + L.to.kwl + (own - row), wkl);
+    Sector<T>::ldg(L.tab + L.to.kwh + (own - row), wkh);
+    const T wil = ldg(L.tab + L.to.wl[0] + i), wih = ldg(L.tab + L.to.wh[0] + i);
+    const T wjl = ldg(L.tab + L.to.wl[1] + j), wjh = ldg(L.tab + L.to.wh[1] + j);
+    T l0[NC], l0p[NC], l1[NC], l1p[NC], l2[NC], l2u[NC], l2e = T(1);
+    if (VAR) {
+        Sector<T>::ldg(L.lam0 + own, l0);
+        Sector<T>::ldg(L.lam0 + own + si, l0p);
+        Sector<T>::ldg(L.lam1 + own, l1);
+        Sector<T>::ldg(L.lam1 + own + sj, l1p);
+        Sector<T>::ldg(L.lam2 + own, l2);
+        Sector<T>::ldg(L.lam2 + oth, l2u);  // lower faces of the other colour's slots
+        l2e = ldg(L.lam2 + ext);
+    }
+    T v[NC];
+#pragma unroll
+    for (int m = 0; m < NC; ++m) {
+        // k neighbours: h = 0 reads (e, xo[0]), (xo[0], xo[1]), ...;
+        // h = 1 reads (xo[0], xo[1]), ..., (xo[NC-1], e)
+        const T klo = h == 0 ? (m == 0 ? e : xo[m - 1]) : xo[m];
+        const T khi = h == 0 ? xo[m] : (m == NC - 1 ? e : xo[m + 1]);
+        T w[6] = {wil, wih, wjl, wjh, wkl[m], wkh[m]};
+        if (VAR) {
+            w[0] *= l0[m];
+            w[1] *= l0p[m];
+            w[2] *= l1[m];
+            w[3] *= l1p[m];
+            w[4] *= l2[m];
+            w[5] *= h == 0 ? l2u[m] : (m == NC - 1 ? l2e : l2u[m + 1]);
+        }
+        const T xn[6] = {xm[m], xp[m], ym[m], yp[m], klo, khi};
+        v[m] = gs_value(w, xn, bb[m]);
+    }
+    // the pinned cell (0,0,0), when this pass updates it, keeps its value
+    if (L.pin && (i | j | g | h | m0) == 0) v[0] = L.x[own];
+    Sector<T>::st(L.x + own, v);
+    const int last = L.n2 / 16 - 1;
+    if ((L.per0 && (i == 0 || i == L.n0 - 1)) || (L.per1 && (j == 0 || j == L.n1 - 1)) ||
+        (L.per2 && (((g | h | m0) == 0) || (g == last && h == 1 && m0 + NC == 8)))) {
+#pragma unroll
+        for (int m = 0; m < NC; ++m) store_images(L, own + m, i, j, 16 * g + 2 * (m0 + m) + h, v[m]);
+    }
+}
+
 // Damped Jacobi (omega = 0.8, jacSmoother.C:15) into a temporary, then copy.
 template <typename T, bool VAR>
 __global__ void __launch_bounds__(256) k_jacobi(Bricks<T> B, T* tmp) {
@@ -215,10 +369,11 @@ __global__ void __launch_bounds__(256) k_jacobi(Bricks<T> B, T* tmp) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (j >= L.n1 || k >= L.n2) return;
-    const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
+    const long row = row_at(L, i, j), c = row + kpos(L, k);
     T w[6], s, d;
-    couplings<T, VAR>(L, i, j, k, c, w);
-    stencil(L.x, c, L.si, L.sj, w, s, d);
+    const long ckm = row + kpos(L, k - 1), ckp = row + kpos(L, k + 1);
+    couplings<T, VAR>(L, i, j, k, c, ckp, w);
+    stencil(L.x, c, ckm, ckp, L.si, L.sj, w, s, d);
     const T omega = T(0.8);
     tmp[c] = (L.pin && (i | j | k) == 0) ? T(0) : (T(1) - omega) * L.x[c] + omega * (s - L.b[c]) / d;
 }
@@ -230,7 +385,7 @@ __global__ void __launch_bounds__(256) k_copy_interior(Bricks<T> B, const T* src
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (j >= L.n1 || k >= L.n2) return;
-    const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
+    const long row = row_at(L, i, j), c = row + kpos(L, k);
     store_x(L, c, i, j, k, src[c]);
 }
 
@@ -265,16 +420,17 @@ __global__ void __launch_bounds__(256) k_residual_restrict(Bricks<T> FB, Bricks<
             const T rab = ra * ldg(ratio + F.n0 + j);
             for (int e = 0; e < t.R2; ++e) {
                 const int k = K * t.R2 + e;
-                const long c = F.base + (long)i * F.si + (long)j * F.sj + k;
+                const long row = row_at(F, i, j), c = row + kpos(F, k);
+                const long ckm = row + kpos(F, k - 1), ckp = row + kpos(F, k + 1);
                 T w[6], s, d;
-                couplings<T, VAR>(F, i, j, k, c, w);
-                stencil(F.x, c, F.si, F.sj, w, s, d);
+                couplings<T, VAR>(F, i, j, k, c, ckp, w);
+                stencil(F.x, c, ckm, ckp, F.si, F.sj, w, s, d);
                 const T r = F.b[c] + d * F.x[c] - s;
                 acc += rab * ldg(ratio + F.n0 + F.n1 + k) * r;
             }
         }
     }
-    C.b[C.base + (long)I * C.si + (long)J * C.sj + K] = acc;
+    C.b[row_at(C, I, J) + kpos(C, K)] = acc;
 }
 
 // ---------------------------------------------------------------------------
@@ -313,12 +469,13 @@ __global__ void __launch_bounds__(256) k_prolong_correct(Bricks<T> FB, Bricks<T>
     const long r10 = C.base + (long)I1 * C.si + (long)J0 * C.sj;
     const long r11 = C.base + (long)I1 * C.si + (long)J1 * C.sj;
     const T uk = T(1) - wk, uj = T(1) - wj, ui = T(1) - wi;
-    const T v00 = uk * X[r00 + K0] + wk * X[r00 + K1];
-    const T v01 = uk * X[r01 + K0] + wk * X[r01 + K1];
-    const T v10 = uk * X[r10 + K0] + wk * X[r10 + K1];
-    const T v11 = uk * X[r11 + K0] + wk * X[r11 + K1];
+    const int P0 = kpos(C, K0), P1 = kpos(C, K1);
+    const T v00 = uk * X[r00 + P0] + wk * X[r00 + P1];
+    const T v01 = uk * X[r01 + P0] + wk * X[r01 + P1];
+    const T v10 = uk * X[r10 + P0] + wk * X[r10 + P1];
+    const T v11 = uk * X[r11 + P0] + wk * X[r11 + P1];
     const T v = ui * (uj * v00 + wj * v01) + wi * (uj * v10 + wj * v11);
-    const long c = F.base + (long)i * F.si + (long)j * F.sj + k;
+    const long c = row_at(F, i, j) + kpos(F, k);
     store_x(F, c, i, j, k, F.x[c] + v);
 }
 
@@ -350,14 +507,15 @@ __device__ __forceinline__ void prolong_quad_item(const LevelView<T>& F, const L
     const int r10 = cell32(C, I1, J0, 0), r11 = cell32(C, I1, J1, 0);
     const int c0 = cell32(F, i, j, k0);
     T xf[4];
-    Row4<T>::ld(F.x + c0, xf);
+    ldq(F.x + c0, F.ks, xf);
     const int* pk = pidx + 2 * (F.n0 + F.n1);
     const T* wk = pw + F.n0 + F.n1;
     // Fine cells k0 .. k0+3 (k0 = 4p) have parents 2p, 2p, 2p+1, 2p+1 and
     // second coarse cells Ka, 2p+1, 2p, Kd: four coarse values per row,
     // the middle pair (2p, 2p+1) one aligned vector (interior k starts at an
     // offset of 4 in every row, so 2p sits at an even offset).
-    const int Ka = ldg(pk + 2 * k0 + 1), Kb = ldg(pk + 2 * k0), Kd = ldg(pk + 2 * (k0 + 3) + 1);
+    const int Ka = kpos(C, ldg(pk + 2 * k0 + 1)), Kb = ldg(pk + 2 * k0), Kd = kpos(C, ldg(pk + 2 * (k0 + 3) + 1));
+    const int Pb = kpos(C, Kb), Pc = kpos(C, Kb + 1);
     T w[4], u[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -369,7 +527,12 @@ __device__ __forceinline__ void prolong_quad_item(const LevelView<T>& F, const L
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
         T xb, xc;
-        Row4<T>::ld2(X + rows[r] + Kb, xb, xc);
+        if (C.ks) {
+            xb = X[rows[r] + Pb];
+            xc = X[rows[r] + Pc];
+        } else {
+            Row4<T>::ld2(X + rows[r] + Kb, xb, xc);
+        }
         const T xa = X[rows[r] + Ka], xd = X[rows[r] + Kd];
         v[r][0] = u[0] * xb + w[0] * xa;
         v[r][1] = u[1] * xb + w[1] * xc;
@@ -379,10 +542,10 @@ __device__ __forceinline__ void prolong_quad_item(const LevelView<T>& F, const L
 #pragma unroll
     for (int q = 0; q < 4; ++q)
         xf[q] += ui * (uj * v[0][q] + wj * v[1][q]) + wi * (uj * v[2][q] + wj * v[3][q]);
-    Row4<T>::st(F.x + c0, xf);
+    stq(F.x + c0, F.ks, xf);
     if (quad_has_images(F, i, j, k0)) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) store_images(F, c0 + q, i, j, k0 + q, xf[q]);
+        for (int q = 0; q < 4; ++q) store_images(F, c0 + quad_off(F.ks, q), i, j, k0 + q, xf[q]);
     }
 }
 
@@ -422,23 +585,25 @@ __device__ __forceinline__ void restrict_quad_item(const LevelView<T>& F, const 
             const int j = 2 * J + e;
             const T rab = ra * ldg(ratio + F.n0 + j);
             const T wjl = ldg(F.tab + F.to.wl[1] + j), wjh = ldg(F.tab + F.to.wh[1] + j);
-            const int c = cell32(F, i, j, k0), si = (int)F.si, sj = (int)F.sj;
+            const int row = (int)row_at(F, i, j), si = (int)F.si, sj = (int)F.sj;
+            const int c = row + kpos(F, k0), ks = F.ks;
             T own[4], xm[4], xp[4], ym[4], yp[4], bb[4];
-            Row4<T>::ld(F.x + c, own);
-            Row4<T>::ld(F.x + c - si, xm);
-            Row4<T>::ld(F.x + c + si, xp);
-            Row4<T>::ld(F.x + c - sj, ym);
-            Row4<T>::ld(F.x + c + sj, yp);
-            Row4<T>::ld(F.b + c, bb);
-            const T left = F.x[c - 1], right = F.x[c + 4];
+            ldq(F.x + c, ks, own);
+            ldq(F.x + c - si, ks, xm);
+            ldq(F.x + c + si, ks, xp);
+            ldq(F.x + c - sj, ks, ym);
+            ldq(F.x + c + sj, ks, yp);
+            ldq(F.b + c, ks, bb);
+            const int cl = row + kpos(F, k0 - 1), cr = row + kpos(F, k0 + 4);
+            const T left = F.x[cl], right = F.x[cr];
             T l0[4], l0p[4], l1[4], l1p[4], l2[4], l2r = T(1);
             if (VAR) {
-                Row4<T>::ldg4(F.lam0 + c, l0);
-                Row4<T>::ldg4(F.lam0 + c + si, l0p);
-                Row4<T>::ldg4(F.lam1 + c, l1);
-                Row4<T>::ldg4(F.lam1 + c + sj, l1p);
-                Row4<T>::ldg4(F.lam2 + c, l2);
-                l2r = ldg(F.lam2 + c + 4);
+                ldgq(F.lam0 + c, ks, l0);
+                ldgq(F.lam0 + c + si, ks, l0p);
+                ldgq(F.lam1 + c, ks, l1);
+                ldgq(F.lam1 + c + sj, ks, l1p);
+                ldgq(F.lam2 + c, ks, l2);
+                l2r = ldg(F.lam2 + cr);
             }
             T r[4];
 #pragma unroll
@@ -461,9 +626,8 @@ __device__ __forceinline__ void restrict_quad_item(const LevelView<T>& F, const 
             acc1 += rab * (rk[2] * r[2] + rk[3] * r[3]);
         }
     }
-    const int cc = cell32(C, I, J, K0);
-    C.b[cc] = acc0;
-    C.b[cc + 1] = acc1;
+    C.b[cell32(C, I, J, K0)] = acc0;
+    C.b[cell32(C, I, J, K0 + 1)] = acc1;
 }
 
 template <typename T, bool VAR>
@@ -501,7 +665,7 @@ __device__ __forceinline__ void coarse_solve_block(const Bricks<T>& CB, const do
                 const LevelView<T>& C = CB.v[0];
                 const int nn = C.n1 * C.n2;
                 const int i = r / nn, j = (r / C.n2) % C.n1, k = r % C.n2;
-                store_x(C, C.base + (long)i * C.si + (long)j * C.sj + k, i, j, k, (T)s);
+                store_x(C, row_at(C, i, j) + kpos(C, k), i, j, k, (T)s);
             } else {
                 CB.v[0].x[cidx[r]] = (T)s;
             }
@@ -588,10 +752,11 @@ __global__ void __launch_bounds__(256) k_residual_out(Bricks<T> B, double* out) 
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (j >= L.n1 || k >= L.n2) return;
-    const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
+    const long row = row_at(L, i, j), c = row + kpos(L, k);
     T w[6], s, d;
-    couplings<T, VAR>(L, i, j, k, c, w);
-    stencil(L.x, c, L.si, L.sj, w, s, d);
+    const long ckm = row + kpos(L, k - 1), ckp = row + kpos(L, k + 1);
+    couplings<T, VAR>(L, i, j, k, c, ckp, w);
+    stencil(L.x, c, ckm, ckp, L.si, L.sj, w, s, d);
     const double r = (double)(L.b[c] + d * L.x[c] - s);
     const double V = L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j] * L.tab64[L.to.h[2] + k];
     out[compact_index(L, i, j, k)] = r * V;
@@ -616,10 +781,11 @@ __global__ void __launch_bounds__(kReduceThreads) k_residual_norm(Bricks<double>
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     double a1 = 0.0, a2 = 0.0, a3 = 0.0;
     if (j < L.n1 && k < L.n2) {
-        const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
+        const long row = row_at(L, i, j), c = row + kpos(L, k);
         double w[6], s, d;
-        couplings<double, VAR>(L, i, j, k, c, w);
-        stencil(L.x, c, L.si, L.sj, w, s, d);
+        const long ckm = row + kpos(L, k - 1), ckp = row + kpos(L, k + 1);
+        couplings<double, VAR>(L, i, j, k, c, ckp, w);
+        stencil(L.x, c, ckm, ckp, L.si, L.sj, w, s, d);
         const double r = L.b[c] + d * L.x[c] - s;
         const double V = L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j] * L.tab64[L.to.h[2] + k];
         const double rr = V * r;
@@ -627,7 +793,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_residual_norm(Bricks<double>
         if (mode == 0) {
             const double bb = V * L.b[c];
             // A*mean(x): nonzero only in the rows of Dirichlet faces
-            const double ay = B.walls.mask ? -V * *B.walls.ybar * wall_sum(L, B.walls, i, j, k, c, false) : 0.0;
+            const double ay = B.walls.mask ? -V * *B.walls.ybar * wall_sum(L, B.walls, i, j, k, c, ckp, false) : 0.0;
             const double t = fabs(rr - bb + ay) + fabs(bb - ay);
             a2 = t * t;
             a3 = bb * bb;
@@ -700,7 +866,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_mean_partials(Bricks<double>
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     double a = 0.0;
     if (j < L.n1 && k < L.n2) {
-        const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
+        const long row = row_at(L, i, j), c = row + kpos(L, k);
         a = L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j] * L.tab64[L.to.h[2] + k] * L.x[c];
     }
     a = block_sum<kReduceThreads>(a, sh);
@@ -722,7 +888,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_plain_partials(Bricks<double
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     double a = 0.0;
-    if (j < L.n1 && k < L.n2) a = L.x[L.base + (long)i * L.si + (long)j * L.sj + k];
+    if (j < L.n1 && k < L.n2) a = L.x[row_at(L, i, j) + kpos(L, k)];
     a = block_sum<kReduceThreads>(a, sh);
     if (threadIdx.x == 0 && threadIdx.y == 0) partials[block_id()] = a;
 }
@@ -748,11 +914,11 @@ __global__ void __launch_bounds__(256) k_load_b(Bricks<double> B, const double* 
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (j >= L.n1 || k >= L.n2) return;
-    const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
+    const long row = row_at(L, i, j), c = row + kpos(L, k);
     const double V = L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j] * L.tab64[L.to.h[2] + k];
     double v = compact[compact_index(L, i, j, k)] / V;
     // face values: Dirichlet b -= 2 A_f g, Neumann b -= A_f g / delta
-    if (B.walls.mask | B.walls.nmask) v -= wall_sum(L, B.walls, i, j, k, c, true);
+    if (B.walls.mask | B.walls.nmask) v -= wall_sum(L, B.walls, i, j, k, c, row + kpos(L, k + 1), true);
     L.b[c] = v;
 }
 
@@ -762,7 +928,7 @@ __global__ void __launch_bounds__(256) k_load_x(Bricks<double> B, const double* 
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (j >= L.n1 || k >= L.n2) return;
-    const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
+    const long row = row_at(L, i, j), c = row + kpos(L, k);
     store_x(L, c, i, j, k, compact[compact_index(L, i, j, k)]);
 }
 
@@ -772,7 +938,7 @@ __global__ void __launch_bounds__(256) k_store_x(Bricks<double> B, double* compa
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (j >= L.n1 || k >= L.n2) return;
-    const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
+    const long row = row_at(L, i, j), c = row + kpos(L, k);
     compact[compact_index(L, i, j, k)] = L.x[c];
 }
 
@@ -783,7 +949,7 @@ __global__ void __launch_bounds__(256) k_load_field(Bricks<T> B, int field, cons
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (j >= L.n1 || k >= L.n2) return;
-    const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
+    const long row = row_at(L, i, j), c = row + kpos(L, k);
     double v = compact[compact_index(L, i, j, k)];
     if (field == 0) {
         store_x(L, c, i, j, k, (T)v);
@@ -800,7 +966,7 @@ __global__ void __launch_bounds__(256) k_store_field(Bricks<T> B, int field, dou
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (j >= L.n1 || k >= L.n2) return;
-    const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
+    const long row = row_at(L, i, j), c = row + kpos(L, k);
     double v = field == 0 ? (double)L.x[c] : (double)L.b[c];
     if (field == 1 && unscale)
         v *= L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j] * L.tab64[L.to.h[2] + k];
@@ -814,7 +980,7 @@ __global__ void __launch_bounds__(256) k_add_correction(Bricks<double> B, Bricks
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (j >= L.n1 || k >= L.n2) return;
-    const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
+    const long row = row_at(L, i, j), c = row + kpos(L, k);
     store_x(L, c, i, j, k, L.x[c] + (double)E.v[b].x[c]);
 }
 
@@ -830,6 +996,15 @@ long reduce_blocks(const Bricks<double>& B) {
 
 template <typename T, bool VAR>
 void launch_colour_pass(const Bricks<T>& B, int colour, cudaStream_t s) {
+    if (B.v[0].ks) {  // parity-split rows (single brick, n2 % 16 == 0)
+        const LevelView<T>& L = B.v[0];
+        const int tr = L.n2 / (64 / (int)sizeof(T));  // threads per row
+        const int bx = std::min(tr, 32), by = std::min(256 / bx, L.n1), bz = std::max(1, 256 / (bx * by));
+        const dim3 blk(bx, by, bz);
+        const dim3 grid((tr + bx - 1) / bx, (L.n1 + by - 1) / by, (L.n0 + bz - 1) / bz);
+        k_colour_split<T, VAR><<<grid, blk, 0, s>>>(L, colour);
+        return;
+    }
     bool quads = true;
     for (int b = 0; b < B.nb; ++b) quads = quads && B.v[b].n2 % 4 == 0;
     if (quads) {

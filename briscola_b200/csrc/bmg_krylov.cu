@@ -46,16 +46,17 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_residual(Bricks<double> 
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     double a1 = 0.0, a2 = 0.0, a3 = 0.0;
     if (j < L.n1 && k < L.n2) {
-        const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
+        const long row = row_at(L, i, j), c = row + kpos(L, k);
         double w[6], s, d;
-        couplings<double, VAR>(L, i, j, k, c, w);
-        stencil(L.x, c, L.si, L.sj, w, s, d);
+        const long ckm = row + kpos(L, k - 1), ckp = row + kpos(L, k + 1);
+        couplings<double, VAR>(L, i, j, k, c, ckp, w);
+        stencil(L.x, c, ckm, ckp, L.si, L.sj, w, s, d);
         const double r = L.b[c] + d * L.x[c] - s;
         const double V = cell_volume(L, i, j, k);
         a1 = (V * r) * (V * r);
         if (mode == 0) {
             const double bb = V * L.b[c];
-            const double ay = B.walls.mask ? -V * *B.walls.ybar * wall_sum(L, B.walls, i, j, k, c, false) : 0.0;
+            const double ay = B.walls.mask ? -V * *B.walls.ybar * wall_sum(L, B.walls, i, j, k, c, ckp, false) : 0.0;
             const double t = fabs(V * r - bb + ay) + fabs(bb - ay);
             a2 = t * t;
             a3 = bb * bb;
@@ -92,7 +93,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_dots(Bricks<double> B, c
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     double a1 = 0.0, a2 = 0.0;
     if (j < L.n1 && k < L.n2) {
-        const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
+        const long row = row_at(L, i, j), c = row + kpos(L, k);
         const double Vz = cell_volume(L, i, j, k) * (double)z[c];
         a1 = Vz * r[c];
         a2 = Vz * q[c];
@@ -131,12 +132,13 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_direction(Bricks<double>
     double a = 0.0;
     if (j < L.n1 && k < L.n2) {
         const double beta = st->beta;
-        const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
+        const long row = row_at(L, i, j), c = row + kpos(L, k);
         double w[6];
-        couplings<double, VAR>(L, i, j, k, c, w);
+        const long ckm = row + kpos(L, k - 1), ckp = row + kpos(L, k + 1);
+        couplings<double, VAR>(L, i, j, k, c, ckp, w);
         const double zc = (double)z[c];
         const double s = w[0] * (double)z[c - L.si] + w[1] * (double)z[c + L.si] + w[2] * (double)z[c - L.sj] +
-                         w[3] * (double)z[c + L.sj] + w[4] * (double)z[c - 1] + w[5] * (double)z[c + 1];
+                         w[3] * (double)z[c + L.sj] + w[4] * (double)z[ckm] + w[5] * (double)z[ckp];
         const double d = w[0] + w[1] + w[2] + w[3] + w[4] + w[5];
         // on the first step p and q hold whatever the last solve left
         const double pn = beta != 0.0 ? zc + beta * p[c] : zc;
@@ -171,7 +173,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_update(Bricks<double> B,
     double a = 0.0;
     if (j < L.n1 && k < L.n2) {
         const double alpha = st->alpha;
-        const long c = L.base + (long)i * L.si + (long)j * L.sj + k;
+        const long row = row_at(L, i, j), c = row + kpos(L, k);
         store_x(L, c, i, j, k, L.x[c] + alpha * p[c]);
         const double rn = r[c] - alpha * q[c];
         r[c] = rn;
@@ -198,33 +200,51 @@ __global__ void __launch_bounds__(kFinalThreads) k_fcg_true_norm(const double* p
 
 constexpr int kQuadPlanes = 64;  // grid z: plane groups
 
+// The logical k-quad k0 .. k0+3 at slab index p (its first cell): one
+// vector in a natural row (ks = 0); in a parity-split row (ks = 1) the even
+// pair (k0, k0+2) at p and the odd pair (k0+1, k0+3) at p + 8.
 template <typename T>
 struct Quad4;
 template <>
 struct Quad4<double> {
-    static __device__ __forceinline__ void ld(const double* p, double v[4]) {
-        const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+    static __device__ __forceinline__ void ld(const double* p, int ks, double v[4]) {
+        const double2 a = reinterpret_cast<const double2*>(p)[0];
+        const double2 b = *reinterpret_cast<const double2*>(p + (ks ? 8 : 2));
         v[0] = a.x;
-        v[1] = a.y;
-        v[2] = b.x;
+        v[1] = ks ? b.x : a.y;
+        v[2] = ks ? a.y : b.x;
         v[3] = b.y;
     }
-    static __device__ __forceinline__ void st(double* p, const double v[4]) {
-        reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
-        reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+    static __device__ __forceinline__ void st(double* p, int ks, const double v[4]) {
+        reinterpret_cast<double2*>(p)[0] = ks ? make_double2(v[0], v[2]) : make_double2(v[0], v[1]);
+        *reinterpret_cast<double2*>(p + (ks ? 8 : 2)) = ks ? make_double2(v[1], v[3]) : make_double2(v[2], v[3]);
     }
 };
 template <>
 struct Quad4<float> {
-    static __device__ __forceinline__ void ld(const float* p, float v[4]) {
-        const float4 a = *reinterpret_cast<const float4*>(p);
-        v[0] = a.x;
-        v[1] = a.y;
-        v[2] = a.z;
-        v[3] = a.w;
+    static __device__ __forceinline__ void ld(const float* p, int ks, float v[4]) {
+        if (ks) {
+            const float2 a = reinterpret_cast<const float2*>(p)[0];
+            const float2 b = *reinterpret_cast<const float2*>(p + 8);
+            v[0] = a.x;
+            v[1] = b.x;
+            v[2] = a.y;
+            v[3] = b.y;
+        } else {
+            const float4 a = *reinterpret_cast<const float4*>(p);
+            v[0] = a.x;
+            v[1] = a.y;
+            v[2] = a.z;
+            v[3] = a.w;
+        }
     }
-    static __device__ __forceinline__ void st(float* p, const float v[4]) {
-        *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    static __device__ __forceinline__ void st(float* p, int ks, const float v[4]) {
+        if (ks) {
+            reinterpret_cast<float2*>(p)[0] = make_float2(v[0], v[2]);
+            *reinterpret_cast<float2*>(p + 8) = make_float2(v[1], v[3]);
+        } else {
+            *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+        }
     }
 };
 
@@ -239,10 +259,11 @@ struct Quad4<float> {
             const LevelView<double>& L = (B).v[brick_of((B), zp, i)];                      \
             const int k0 = 4 * qx;                                                         \
             if (j < L.n1 && k0 < L.n2) {                                                   \
-                const long c = L.base + (long)i * L.si + (long)j * L.sj + k0;              \
+                const long row = row_at(L, i, j), c = row + kpos(L, k0);                   \
+                const int ks = L.ks;                                                       \
                 const double hij = L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j];        \
                 double hk[4];                                                              \
-                Quad4<double>::ld(L.tab64 + L.to.h[2] + k0, hk);                           \
+                Quad4<double>::ld(L.tab64 + L.to.h[2] + k0, 0, hk);                        \
                 __VA_ARGS__                                                                \
             }                                                                              \
         }                                                                                  \
@@ -256,9 +277,9 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_dots4(Bricks<double> B, 
     BMG_QUAD_LOOP(B, {
         T zq[4];
         double rq[4], qq[4];
-        Quad4<T>::ld(z + c, zq);
-        Quad4<double>::ld(r + c, rq);
-        Quad4<double>::ld(q + c, qq);
+        Quad4<T>::ld(z + c, ks, zq);
+        Quad4<double>::ld(r + c, ks, rq);
+        Quad4<double>::ld(q + c, ks, qq);
         for (int e = 0; e < 4; ++e) {
             const double Vz = (hij * hk[e]) * (double)zq[e];
             a1 += Vz * rq[e];
@@ -283,18 +304,19 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_direction4(Bricks<double
     double a = 0.0;
     BMG_QUAD_LOOP(B, {
         T zc[4], zim[4], zip[4], zjm[4], zjp[4];
-        Quad4<T>::ld(z + c, zc);
-        Quad4<T>::ld(z + c - L.si, zim);
-        Quad4<T>::ld(z + c + L.si, zip);
-        Quad4<T>::ld(z + c - L.sj, zjm);
-        Quad4<T>::ld(z + c + L.sj, zjp);
-        const T zl = z[c - 1], zr = z[c + 4];
+        Quad4<T>::ld(z + c, ks, zc);
+        Quad4<T>::ld(z + c - L.si, ks, zim);
+        Quad4<T>::ld(z + c + L.si, ks, zip);
+        Quad4<T>::ld(z + c - L.sj, ks, zjm);
+        Quad4<T>::ld(z + c + L.sj, ks, zjp);
+        const long cr = row + kpos(L, k0 + 4);
+        const T zl = z[row + kpos(L, k0 - 1)], zr = z[cr];
         double pq[4], qq[4], pn[4], qn[4];
-        Quad4<double>::ld(p + c, pq);
-        Quad4<double>::ld(q + c, qq);
+        Quad4<double>::ld(p + c, ks, pq);
+        Quad4<double>::ld(q + c, ks, qq);
         for (int e = 0; e < 4; ++e) {
             double w[6];
-            couplings<double, VAR>(L, i, j, k0 + e, c + e, w);
+            couplings<double, VAR>(L, i, j, k0 + e, c + quad_off(ks, e), e < 3 ? c + quad_off(ks, e + 1) : cr, w);
             const double km = e > 0 ? (double)zc[e - 1] : (double)zl;
             const double kp = e < 3 ? (double)zc[e + 1] : (double)zr;
             const double zz = (double)zc[e];
@@ -306,8 +328,8 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_direction4(Bricks<double
             qn[e] = beta != 0.0 ? (sv - d * zz) + beta * qq[e] : sv - d * zz;
             a += (hij * hk[e]) * pn[e] * qn[e];
         }
-        Quad4<double>::st(p + c, pn);
-        Quad4<double>::st(q + c, qn);
+        Quad4<double>::st(p + c, ks, pn);
+        Quad4<double>::st(q + c, ks, qn);
     })
     a = block_sum<kReduceThreads>(a, sh);
     if (threadIdx.x == 0 && threadIdx.y == 0) partials[block_id()] = a;
@@ -321,26 +343,26 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_update4(Bricks<double> B
     double a = 0.0;
     BMG_QUAD_LOOP(B, {
         double xq[4], pq[4], rq[4], qq[4], rn[4];
-        Quad4<double>::ld(L.x + c, xq);
-        Quad4<double>::ld(p + c, pq);
-        Quad4<double>::ld(r + c, rq);
-        Quad4<double>::ld(q + c, qq);
+        Quad4<double>::ld(L.x + c, ks, xq);
+        Quad4<double>::ld(p + c, ks, pq);
+        Quad4<double>::ld(r + c, ks, rq);
+        Quad4<double>::ld(q + c, ks, qq);
         for (int e = 0; e < 4; ++e) {
             xq[e] = xq[e] + alpha * pq[e];
             rn[e] = rq[e] - alpha * qq[e];
             const double Vr = (hij * hk[e]) * rn[e];
             a += Vr * Vr;
         }
-        Quad4<double>::st(L.x + c, xq);
+        Quad4<double>::st(L.x + c, ks, xq);
         if (quad_has_images(L, i, j, k0)) {
-            for (int e = 0; e < 4; ++e) store_images(L, c + e, i, j, k0 + e, xq[e]);
+            for (int e = 0; e < 4; ++e) store_images(L, c + quad_off(ks, e), i, j, k0 + e, xq[e]);
         }
-        Quad4<double>::st(r + c, rn);
+        Quad4<double>::st(r + c, ks, rn);
         if (pre32) {
             const float f[4] = {(float)rn[0], (float)rn[1], (float)rn[2], (float)rn[3]};
-            Quad4<float>::st(pre32 + c, f);
+            Quad4<float>::st(pre32 + c, ks, f);
         }
-        if (pre64) Quad4<double>::st(pre64 + c, rn);
+        if (pre64) Quad4<double>::st(pre64 + c, ks, rn);
     })
     a = block_sum<kReduceThreads>(a, sh);
     if (threadIdx.x == 0 && threadIdx.y == 0) partials[block_id()] = a;

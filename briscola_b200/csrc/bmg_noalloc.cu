@@ -21,19 +21,14 @@
 
 #include <cmath>
 #include <cstdio>
-#include <mutex>
 
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kMaxDevices = 64;
 
 // Scratch shared by every call on a device: one partial sum per (i, j) row.
 // 512 KB, held by every GPU that loads the library until the process exits.
 static __device__ __align__(256) double g_row_partials[BMG_NOALLOC_MAX_ROWS];
-
-double* g_scratch[kMaxDevices] = {nullptr};
-std::mutex g_scratch_mutex;
 
 // row-scaled coupling between cell i and its lower (up = 0) or upper (up = 1)
 // neighbour along an axis with vertices p[0..n]: 1 / (centre distance * h_i).
@@ -128,23 +123,22 @@ __global__ void __launch_bounds__(kThreads) k_sum_rows(const double* rows, int n
     if (threadIdx.x == 0) *out = sqrt(sh[0]);
 }
 
-// Device address of the static scratch on the current device, looked up
-// once per device (host code must not pass the symbol itself to a kernel).
+// Device address of the static scratch on the current device.  Host code
+// must not pass the symbol itself to a kernel (in host code it names a
+// host-side stand-in).  The address is looked up on every call rather than
+// cached: a cached address would go stale if the application reset the
+// device or recreated its primary context between calls.
 int scratchForCurrentDevice(double** out) {
     int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return BMG_NO_DEVICE;
-    std::lock_guard<std::mutex> g(g_scratch_mutex);
-    if (!g_scratch[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_row_partials);
-        if (e != cudaSuccess) {
-            fprintf(stderr, "bmg_residual_norm_noalloc: cudaGetSymbolAddress failed on device %d: %s\n", dev,
-                    cudaGetErrorString(e));
-            return BMG_CUDA_ERROR;
-        }
-        g_scratch[dev] = static_cast<double*>(p);
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return BMG_NO_DEVICE;
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_row_partials);
+    if (e != cudaSuccess) {
+        fprintf(stderr, "bmg_residual_norm_noalloc: cudaGetSymbolAddress failed on device %d: %s\n", dev,
+                cudaGetErrorString(e));
+        return BMG_CUDA_ERROR;
     }
-    *out = g_scratch[dev];
+    *out = static_cast<double*>(p);
     return BMG_OK;
 }
 
@@ -172,11 +166,19 @@ extern "C" int bmg_residual_norm_noalloc(const double* x, const double* b, const
                 nrows, BMG_NOALLOC_MAX_ROWS);
         return BMG_BAD_ARG;
     }
+    // an error left pending by the caller's earlier work is reported, not
+    // cleared, and nothing is launched: this call must not swallow it
+    if (cudaPeekAtLastError() != cudaSuccess) return BMG_CUDA_ERROR;
     double* rows = nullptr;
     const int rc = scratchForCurrentDevice(&rows);
     if (rc != BMG_OK) return rc;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+        return BMG_CUDA_ERROR;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const int blocks = (int)(nrows < 148L * 8 ? nrows : 148L * 8);
+    const long grid = 8L * sms;  // eight resident blocks of 256 threads per SM
+    const int blocks = (int)(nrows < grid ? nrows : grid);
     k_rows<<<blocks, kThreads, 0, s>>>(x, b, n[0], n[1], n[2], points_x, points_y, points_z,
                                        bc[0] == BMG_BC_PERIODIC, bc[2] == BMG_BC_PERIODIC,
                                        bc[4] == BMG_BC_PERIODIC, dir, rows);

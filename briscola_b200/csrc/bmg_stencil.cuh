@@ -12,11 +12,23 @@ __device__ __forceinline__ T ldg(const T* p) {
     return __ldg(p);
 }
 
+// Storage position of logical k (-1 .. n2) in a parity-split row: blocks of
+// 16 cells, even k first (k & 1 selects the half, k >> 1 the slot).  The
+// ghosts map to themselves: -1 -> -1 and n2 (a multiple of 16) -> n2.
+__device__ __forceinline__ int kpos_split(int k) { return (k & ~15) | ((k & 1) << 3) | ((k >> 1) & 7); }
+
+template <typename T>
+__device__ __forceinline__ int kpos(const LevelView<T>& L, int k) {
+    return L.ks ? kpos_split(k) : k;
+}
+
 // Row-scaled couplings of cell (i,j,k) to its six neighbours in the order
 // of the reference's row product: l, r, b, t, a, f (linearSystemFunctions.H
 // :96-102), i.e. axis 0 lower/upper, axis 1 lower/upper, axis 2 lower/upper.
+// c is the cell's slab index, ckp the slab index of cell (i,j,k+1), whose
+// lower face is the cell's upper k face.
 template <typename T, bool VAR>
-__device__ __forceinline__ void couplings(const LevelView<T>& L, int i, int j, int k, long c,
+__device__ __forceinline__ void couplings(const LevelView<T>& L, int i, int j, int k, long c, long ckp,
                                           T w[6]) {
     w[0] = ldg(L.tab + L.to.wl[0] + i);
     w[1] = ldg(L.tab + L.to.wh[0] + i);
@@ -30,7 +42,7 @@ __device__ __forceinline__ void couplings(const LevelView<T>& L, int i, int j, i
         w[2] *= ldg(L.lam1 + c);
         w[3] *= ldg(L.lam1 + c + L.sj);
         w[4] *= ldg(L.lam2 + c);
-        w[5] *= ldg(L.lam2 + c + 1);
+        w[5] *= ldg(L.lam2 + ckp);
     }
 }
 
@@ -67,12 +79,13 @@ __device__ __forceinline__ T gs_value(const T w[6], const T xn[6], T b) {
     return gs_div(rn_sub(s, b), d);
 }
 
-// sum of couplings times neighbour values, and the sum of couplings
+// sum of couplings times neighbour values, and the sum of couplings; ckm
+// and ckp are the slab indices of the k neighbours
 template <typename T>
-__device__ __forceinline__ void stencil(const T* x, long c, long si, long sj, const T w[6], T& s,
-                                        T& d) {
+__device__ __forceinline__ void stencil(const T* x, long c, long ckm, long ckp, long si, long sj, const T w[6],
+                                        T& s, T& d) {
     s = w[0] * x[c - si] + w[1] * x[c + si] + w[2] * x[c - sj] + w[3] * x[c + sj] +
-        w[4] * x[c - 1] + w[5] * x[c + 1];
+        w[4] * x[ckm] + w[5] * x[ckp];
     d = w[0] + w[1] + w[2] + w[3] + w[4] + w[5];
 }
 
@@ -84,7 +97,7 @@ __device__ __forceinline__ void stencil(const T* x, long c, long si, long sj, co
 // with a gradient g, A_f g / (delta V) = lambda g / h
 // (NeumannBoundaryCondition.C:44-50).
 __device__ __forceinline__ double wall_sum(const LevelView<double>& L, const Walls& W, int i, int j, int k,
-                                           long c, bool values) {
+                                           long c, long ckp, bool values) {
     double s = 0.0;
     const int at[6] = {i == 0, i == L.n0 - 1, j == 0, j == L.n1 - 1, k == 0, k == L.n2 - 1};
     const int q[3] = {i, j, k};
@@ -97,7 +110,7 @@ __device__ __forceinline__ double wall_sum(const LevelView<double>& L, const Wal
         const bool dir = (W.mask >> f) & 1;
         double w = dir ? L.tab64[(up ? L.to.wh[d] : L.to.wl[d]) + q[d]] : 1.0 / L.tab64[L.to.h[d] + q[d]];
         const double* lam = d == 0 ? L.lam0 : d == 1 ? L.lam1 : L.lam2;
-        if (lam) w *= lam[c + (up ? st[d] : 0)];
+        if (lam) w *= lam[!up ? c : d == 2 ? ckp : c + st[d]];
         s += values ? w * W.g[f] : w;
     }
     return s;
@@ -113,11 +126,23 @@ __device__ __forceinline__ bool quad_has_images(const LevelView<T>& L, int i, in
 }
 
 // slab index of cell (i,j,k) in 32-bit arithmetic (the host rejects levels
-// of 2^31 cells or more)
+// of 2^31 cells or more); k is logical, its storage position comes from kpos
 template <typename T>
 __device__ __forceinline__ int cell32(const LevelView<T>& L, int i, int j, int k) {
-    return (int)L.base + i * (int)L.si + j * (int)L.sj + k;
+    return (int)L.base + i * (int)L.si + j * (int)L.sj + kpos(L, k);
 }
+
+// slab index of the first (logical k = 0) position of row (i, j)
+template <typename T>
+__device__ __forceinline__ long row_at(const LevelView<T>& L, int i, int j) {
+    return L.base + (long)i * L.si + (long)j * L.sj;
+}
+
+// Position, relative to the quad's first cell, of cell e (0..3) of the
+// logical k-quad k0 .. k0+3 (k0 % 4 == 0): consecutive in natural rows; in a
+// parity-split row the even pair sits at kpos(k0), kpos(k0)+1 and the odd
+// pair 8 further on.
+__device__ __forceinline__ int quad_off(int ks, int e) { return ks ? ((e & 1) << 3) | (e >> 1) : e; }
 
 // index of cell (i,j,k) in the caller's (compact, brick-frame) arrays
 template <typename T>

@@ -425,6 +425,10 @@ def make_options(d: Dictionary | dict | None = None, **over) -> N.Options:
         if v not in table:
             raise FatalError(f"GPUMG {key} scheme must be one of {sorted(table)}, not {v}")
         setattr(o, field, table[v])
+    rl = str(d.get("rowLayout", "split"))
+    if rl not in N.ROW_LAYOUT:
+        raise FatalError(f"unknown rowLayout {rl}")
+    o.row_layout = N.ROW_LAYOUT[rl]
     return o
 
 

@@ -77,6 +77,15 @@ enum { BMG_PROLONG_LINEAR = 0, BMG_PROLONG_INJECTION = 1 };
  * ||b||_2 whatever the initial guess (used to compare solves that start from
  * different guesses).  The absolute tolerance applies in both. */
 enum { BMG_CRITERION_INITIAL = 0, BMG_CRITERION_RHS = 1 };
+/* Storage order of the rows of the device levels (rowLayout; no counterpart
+ * in the reference, whose arrays are k fastest, utils.H:569).  Split: on
+ * single-brick levels above 4096 cells with n2 % 16 == 0, each row's cells
+ * are kept in blocks of 16, the 8 even k before the 8 odd k, so a red-black
+ * colour pass reads and writes only sectors of the colours it needs; the
+ * caller's arrays keep the reference's order.  Natural: k fastest on every
+ * level.  Both give bit-identical results.  Fixed when the context is
+ * created. */
+enum { BMG_ROWS_SPLIT = 0, BMG_ROWS_NATURAL = 1 };
 
 /* bmg_solve flags */
 enum {
@@ -139,6 +148,7 @@ typedef struct bmg_options {
     int coarse_mode;    /* coarseMode (direct): BMG_COARSE_* (MG.C:110-126)     */
     int restrict_scheme;/* restrict (linear): BMG_RESTRICT_*                   */
     int prolong_scheme; /* prolong (linear): BMG_PROLONG_*                     */
+    int row_layout;     /* rowLayout (split): BMG_ROWS_*, fixed at creation    */
 } bmg_options;
 
 typedef struct bmg_report {
@@ -258,9 +268,12 @@ int bmg_project_correct(struct bmg_ctx* ctx, double* u0, double* u1, double* u2,
  * a message on stderr.  Every call overwrites the partials it reads, so no
  * state carries over, but all calls on a device share the array: calls that
  * overlap on the GPU (different streams, or threads without ordering) race.
- * The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture. */
+ * Every call looks up the array's device address (cudaGetSymbolAddress)
+ * with the current device; the first call on a device also loads the
+ * library's device code there, so make that first call before any stream
+ * capture.  An error that earlier work left pending (cudaPeekAtLastError)
+ * is returned as BMG_CUDA_ERROR before anything is launched, and left
+ * pending for its owner. */
 #define BMG_NOALLOC_MAX_ROWS 65536
 int bmg_residual_norm_noalloc(const double* x, const double* b, const int n[3],
                               const double* points_x, const double* points_y,

@@ -35,11 +35,26 @@ def _dirichlet_mesh(N):
 _BC = {"periodic": NA.BC_PERIODIC, "Neumann": NA.BC_NEUMANN, "Dirichlet": NA.BC_DIRICHLET}
 
 
-@pytest.mark.parametrize("name,N", [("channel", 32), ("cavity", 24), ("dirichlet", 16)])
+def _long_box():
+    # 2304 rows (more than one pass of the row grid) and rows of 384 cells
+    # (more than one pass of the 256 threads along k); walls all round, so
+    # that the reference context coarsens it (odd periodic extents would not)
+    from briscola_b200.mesh import Brick, Mesh, tanh_points, uniform_points
+
+    br = Brick([uniform_points(48), tanh_points(48, 2.0), uniform_points(384)])
+    return Mesh([br]), np.random.default_rng(6).standard_normal(48 * 48 * 384), None
+
+
+@pytest.mark.parametrize("name,N", [("channel", 32), ("cavity", 24), ("dirichlet", 16), ("long_box", 0)])
 def test_noalloc_norm_matches_context_residual(native, name, N):
     import torch
 
-    mesh, b, _ = _dirichlet_mesh(N) if name == "dirichlet" else workloads.CONFIGS[name](N)
+    if name == "dirichlet":
+        mesh, b, _ = _dirichlet_mesh(N)
+    elif name == "long_box":
+        mesh, b, _ = _long_box()
+    else:
+        mesh, b, _ = workloads.CONFIGS[name](N)
     br = mesh.bricks[0]
     rng = np.random.default_rng(17)
     x = rng.standard_normal(b.size)
@@ -60,12 +75,24 @@ def test_noalloc_norm_matches_context_residual(native, name, N):
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     for call in range(2):  # the static scratch is reused by the second call
         out.fill_(-1.0)
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info(dev)[0]
         rc = native.bmg_residual_norm_noalloc(_ptr(xd), _ptr(bd), n, *[_ptr(p) for p in pts], bc, _ptr(out),
                                               stream)
         torch.cuda.synchronize()
         assert rc == NA.OK, (call, rc)
+        if call == 1:  # the first call may load the module; the second allocates nothing
+            assert torch.cuda.mem_get_info(dev)[0] == free0
         got = float(out.item())
         assert abs(got - ref) <= 1e-12 * ref, (call, got, ref)
+    if name == "channel":
+        # independent check: the residual of the CPU oracle
+        from oracle.pyoracle import Oracle
+
+        o = Oracle(br.points, periodic=br.periodic, nthreads=2)
+        o.assemble(n_pre=2, n_post=2, cycle_type="V", coarse_level=1)
+        ro = float(np.linalg.norm(o.residual(0, x.reshape(br.N), b.reshape(br.N))))
+        assert abs(float(out.item()) - ro) <= 1e-12 * ro
 
 
 def test_noalloc_rejects_sizes_beyond_scratch(native):
