@@ -580,10 +580,15 @@ def main():
     alg_bytes = (12.0 if stages_per_launch >= 2 else 6.0) * cells
     hbm, peak_kind = peaks()
     achieved = alg_bytes / t_pass / 1e9
+    # level 0 is kept in parity-split rows (rowLayout split, n2 % 16 == 0):
+    # its colour passes run k_colour_split
+    n2_0 = c.shape(0)[2]
+    split0 = n2_0 % 16 == 0 and not stages_per_launch
+    pass_kernel = "k_colour_split" if split0 else "k_colour_quad"
     # DRAM bytes per launch from the committed ncu summary of this kernel
     traffic = None
     tp = os.path.join(ROOT, "profiles", "k_sweep_fp32_channel256.md" if stages_per_launch else
-                      "k_colour_quad_fp32_channel256.md")
+                      f"{pass_kernel}_fp32_channel256.md")
     if os.path.exists(tp):
         import re
 
@@ -604,9 +609,17 @@ def main():
     t64 = statistics.median(pass64) * 1e-3 / lps64
     alg64 = (24.0 if st64 >= 2 else 12.0) * cells
     ach64 = alg64 / t64 / 1e9
+    traffic64 = None
+    tp64 = os.path.join(ROOT, "profiles", f"{pass_kernel}_fp64_channel256.md")
+    if not st64 and os.path.exists(tp64):
+        import re
+
+        m = re.search(r"^traffic per launch \(bytes\): ([0-9.e+]+)", open(tp64).read(), re.M)
+        traffic64 = float(m.group(1)) if m else None
     roof64 = {"bound": "hbm", "kernel": (f"k_sweep<double> level 0 ({lps64} launches of up to {st64} colour "
                                          f"stages, {chunk64}-plane chunks)" if st64 else
-                                         f"colour pass<double> level 0 ({lps64} passes per 2-sweep step)"),
+                                         f"{pass_kernel}<double> level 0 ({lps64} passes per 2-sweep step)"),
+              "traffic": traffic64,
               "achieved": round(ach64, 1), "peak": hbm, "unit": "GB/s", "frac": round(ach64 / hbm, 4),
               "peak_kind": peak_kind, "algorithmic_bytes_per_launch": alg64,
               "launch_us": round(t64 * 1e6, 2)}
@@ -772,8 +785,8 @@ def main():
                          "kernel": (f"k_sweep<float> level 0 ({launches_per_step} launches of up to "
                                     f"{stages_per_launch} colour stages per 2-sweep step, {chunk}-plane chunks)"
                                     if stages_per_launch else
-                                    f"k_colour_quad<float> level 0 ({launches_per_step} passes per "
-                                    "2-sweep step; autotuner's choice)"),
+                                    f"{pass_kernel}<float> level 0 ({launches_per_step} passes per "
+                                    "2-sweep step)"),
                          "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                          "frac": round(achieved / hbm, 4), "peak_kind": peak_kind,
                          "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,

@@ -195,8 +195,9 @@ void finishAxis(Axis& a, int n, bool periodic, double glo, double ghi) {
     }
 }
 
-// storage position of k in a parity-split row (kpos_split of bmg_stencil.cuh)
-inline int kposSplit(int k) { return (k & ~15) | ((k & 1) << 3) | ((k >> 1) & 7); }
+// storage position of interior k in a parity-split row of n2 cells
+// (kpos_split of bmg_stencil.cuh): the even k first, then the odd k
+inline int kposSplit(int k, int n2) { return (k & 1) * (n2 / 2) + (k >> 1); }
 
 // a slab field in natural row order -> parity-split order (interior k of
 // every row of the brick, ghost rows included; the k ghosts stay)
@@ -205,7 +206,7 @@ void splitRows(const HostBrick& B, std::vector<double>& f) {
     for (int i = -1; i <= B.n[0]; ++i)
         for (int j = -1; j <= B.n[1]; ++j) {
             const long r = B.base + (long)i * B.si + (long)j * B.sj;
-            for (int k = 0; k < B.n[2]; ++k) tmp[kposSplit(k)] = f[r + k];
+            for (int k = 0; k < B.n[2]; ++k) tmp[kposSplit(k, B.n[2])] = f[r + k];
             for (int k = 0; k < B.n[2]; ++k) f[r + k] = tmp[k];
         }
 }
@@ -283,8 +284,8 @@ void buildTables(HostLevel& L, const int dirichlet[6]) {
         }
         if (L.ks)  // the k couplings once more, in the rows' storage order
             for (int k = 0; k < B.n[2]; ++k) {
-                L.tab[to.kwl + kposSplit(k)] = L.tab[to.wl[2] + k];
-                L.tab[to.kwh + kposSplit(k)] = L.tab[to.wh[2] + k];
+                L.tab[to.kwl + kposSplit(k, B.n[2])] = L.tab[to.wl[2] + k];
+                L.tab[to.kwh + kposSplit(k, B.n[2])] = L.tab[to.wh[2] + k];
             }
     }
 }
@@ -336,7 +337,7 @@ Bricks<T> bricks(const bmg_ctx* c, int l) {
         v.per1 = c->periodic[1];
         v.per2 = c->periodic[2];
         v.cpar = K.cpar;
-        v.ks = H.ks ? 1 : 0;
+        v.kh = H.ks ? K.n[2] / 2 : 0;
         // a smoothed coarse level of a singular system keeps global cell 0
         // (brick 0's first cell) at zero
         v.pin = l == c->lc && b == 0 && c->singular && c->opt.coarse_mode == BMG_COARSE_SMOOTH;

@@ -12,36 +12,18 @@
 //   Compact (interior-only) arrays list the bricks one after another, each
 //   k fastest, as the C ABI does.
 //
-// Parity-split rows (LevelView::ks, single-brick levels above kTailCells
-// cells with n2 % 16 == 0): the interior of every row is stored in blocks of
-// 16 cells, the 8 even k of a block first, then its 8 odd k, so cell (i,j,k)
-// sits at base + i*si + j*sj + kpos_split(k).  In a row the even k have one
-// red-black colour and the odd k the other, and the same-k cells of the
-// neighbouring rows have the other colour of the same k parity: a colour
-// pass reads and writes whole 32-byte sectors of one colour only, where the
-// natural order reads every sector of x and b to update half of them.  The
-// k ghosts keep their natural places (k = -1 and k = n2), and so do the
-// periodic images (a cell and its k image are n2 apart in both orders).
-//
-// Ghosts: on a single brick, periodic axes keep their ghost layers (faces,
-//   edges, corners) current by write-through -- every kernel that stores an
-//   interior value also stores its ghost images -- so stencils read ghosts
-//   without an exchange step (the reference exchanges them per sweep,
-//   rbgsSmoother.C:405-428).  Between bricks, a gather kernel refreshes the
-//   ghost frame from the neighbouring bricks (and zero-gradient copies at
-//   walls) before every stencil pass, the device-side counterpart of the
-//   reference's inter-processor exchange (parallelBoundaryCondition.C:84-174).
-//   Wall couplings are zero after the Neumann elimination
-//   (NeumannBoundaryCondition.C:19-56), so wall ghosts only matter to the
-//   prolongation.
-//
-// The operator is stored row-scaled by the inverse cell volume (A' = A/V,
-// b' = b/V), which leaves every Gauss-Seidel, Jacobi and coarse-solve update
-// unchanged and makes the constant-coefficient couplings 1-D tables: the
-// coupling to the lower x neighbour is delta_x(i)/h_x(i), times the face
-// lambda for a variable coefficient.  Multi-brick meshes always carry face
-// lambdas: 1 on faces inside a brick and on contact faces, 0 on the wall
-// parts of brick faces.  No 7-coefficient array exists on the device.
+// Parity-split rows (LevelView::kh > 0, single-brick levels above
+// kTailCells cells with n2 % 16 == 0): the interior of every row is stored
+// as its n2/2 even-k cells followed by its n2/2 odd-k cells, so cell
+// (i,j,k) sits at base + i*si + j*sj + kpos(k), kpos(k) = (k & 1) * kh +
+// (k >> 1) with kh = n2/2.  In a row the even k have one red-black colour
+// and the odd k the other, and the same-k cells of the neighbouring rows
+// have the other colour of the same k parity: a colour pass reads and
+// writes contiguous half-rows of one colour only (whole sectors, coalesced
+// warp loads), where the natural order reads every sector of x and b to
+// update half of them.  The k ghosts keep their natural places (k = -1 and
+// k = n2), and so do the periodic images (a cell and its k image are n2
+// apart in both orders).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -59,7 +41,7 @@ struct TabOff {
     int wh[3];   // coupling to the upper neighbour
     int h[3];    // cell sizes (volume factors)
     int kwl, kwh;  // parity-split levels: the k couplings in the row's storage
-                   // order (entry kpos_split(k) holds wl[2] / wh[2] of k); -1 otherwise
+                   // order (entry kpos(k) holds wl[2] / wh[2] of k); -1 otherwise
     int total;
 };
 
@@ -85,7 +67,8 @@ struct LevelView {
     int cpar;          // parity of the brick origin: colour = (i+j+k+cpar) & 1
     int pin;           // smoothers keep cell (0,0,0) at zero: the singularity pin
                        // of an iteratively smoothed coarse level (solver.C:201-231)
-    int ks;            // rows parity-split (see above); 0: natural k order
+    int kh;            // parity-split rows: offset n2/2 of the odd-k half (see
+                       // above); 0: natural k order
 };
 
 // Wall faces of a single-brick level 0: bit f of mask for a Dirichlet face

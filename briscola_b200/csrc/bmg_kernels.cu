@@ -124,44 +124,45 @@ struct Row4<double> {
 };
 
 // The logical k-quad k0 .. k0+3 (k0 % 4 == 0) of a row, at slab index c
-// = the quad's first cell: one vector in a natural row; in a parity-split
-// row the even pair (k0, k0+2) at c and the odd pair (k0+1, k0+3) at c + 8.
+// = the quad's first cell: one vector in a natural row (kh = 0); in a
+// parity-split row the even pair (k0, k0+2) at c and the odd pair
+// (k0+1, k0+3) at c + kh.
 template <typename T>
-__device__ __forceinline__ void ldq(const T* p, int ks, T v[4]) {
-    if (ks) {
+__device__ __forceinline__ void ldq(const T* p, int kh, T v[4]) {
+    if (kh) {
         Row4<T>::ld2(p, v[0], v[2]);
-        Row4<T>::ld2(p + 8, v[1], v[3]);
+        Row4<T>::ld2(p + kh, v[1], v[3]);
     } else {
         Row4<T>::ld(p, v);
     }
 }
 template <typename T>
-__device__ __forceinline__ void ldgq(const T* p, int ks, T v[4]) {
-    if (ks) {
+__device__ __forceinline__ void ldgq(const T* p, int kh, T v[4]) {
+    if (kh) {
         v[0] = ldg(p);
         v[2] = ldg(p + 1);
-        v[1] = ldg(p + 8);
-        v[3] = ldg(p + 9);
+        v[1] = ldg(p + kh);
+        v[3] = ldg(p + kh + 1);
     } else {
         Row4<T>::ldg4(p, v);
     }
 }
 template <typename T>
-__device__ __forceinline__ void stq(T* p, int ks, const T v[4]);
+__device__ __forceinline__ void stq(T* p, int kh, const T v[4]);
 template <>
-__device__ __forceinline__ void stq<float>(float* p, int ks, const float v[4]) {
-    if (ks) {
+__device__ __forceinline__ void stq<float>(float* p, int kh, const float v[4]) {
+    if (kh) {
         *reinterpret_cast<float2*>(p) = make_float2(v[0], v[2]);
-        *reinterpret_cast<float2*>(p + 8) = make_float2(v[1], v[3]);
+        *reinterpret_cast<float2*>(p + kh) = make_float2(v[1], v[3]);
     } else {
         Row4<float>::st(p, v);
     }
 }
 template <>
-__device__ __forceinline__ void stq<double>(double* p, int ks, const double v[4]) {
-    if (ks) {
+__device__ __forceinline__ void stq<double>(double* p, int kh, const double v[4]) {
+    if (kh) {
         *reinterpret_cast<double2*>(p) = make_double2(v[0], v[2]);
-        *reinterpret_cast<double2*>(p + 8) = make_double2(v[1], v[3]);
+        *reinterpret_cast<double2*>(p + kh) = make_double2(v[1], v[3]);
     } else {
         Row4<double>::st(p, v);
     }
@@ -254,81 +255,81 @@ __global__ void __launch_bounds__(256) k_colour_quad(Bricks<T> B, int colour) {
 
 // ---------------------------------------------------------------------------
 // Red-black colour pass on a parity-split level (bmg_internal.h): the
-// thread owns one 32-byte sector of the pass's colour, NC = 32 / sizeof(T)
-// consecutive slots (8 FP32 or 4 FP64 cells) of one half of a 16-cell block
-// of a row.  Every value it reads is one the update needs: the other
-// colour's slots of its own row (the same slots of the other half) and one
-// k neighbour beyond them, the same slots of the four neighbouring rows,
-// b of its own cells, the k couplings from tables stored in the same order,
-// all as whole 16-byte vectors; it writes its sector back.  Per cell the
-// arithmetic is gs_value's with colour_quad_item's couplings and neighbour
-// order, so the pass is bit-identical to the natural-order kernels.
+// thread owns one 16-byte vector of the pass's colour, NC = 16 / sizeof(T)
+// consecutive slots (4 FP32 or 2 FP64 cells) of its row's half of that
+// colour, so a warp's loads and stores are whole contiguous runs.  Every
+// value it reads is one the update needs: the other colour's same slots of
+// its own row and one k neighbour beyond them, the same slots of the four
+// neighbouring rows, b of its own cells, and the k couplings from tables
+// kept in the same order.  Per cell the arithmetic is gs_value's with
+// colour_quad_item's couplings and neighbour order, so the pass is
+// bit-identical to the natural-order kernels.
 // ---------------------------------------------------------------------------
 template <typename T>
-struct Sector;
+struct Vec16;
 template <>
-struct Sector<float> {
-    static constexpr int N = 8;
-    static __device__ __forceinline__ void ld(const float* p, float v[8]) {
-        const float4 a = reinterpret_cast<const float4*>(p)[0], b = reinterpret_cast<const float4*>(p)[1];
-        v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
-    }
-    static __device__ __forceinline__ void ldg(const float* p, float v[8]) {
-        const float4 a = __ldg(reinterpret_cast<const float4*>(p)), b = __ldg(reinterpret_cast<const float4*>(p) + 1);
-        v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
-    }
-    static __device__ __forceinline__ void st(float* p, const float v[8]) {
-        reinterpret_cast<float4*>(p)[0] = make_float4(v[0], v[1], v[2], v[3]);
-        reinterpret_cast<float4*>(p)[1] = make_float4(v[4], v[5], v[6], v[7]);
-    }
+struct Vec16<float> {
+    static constexpr int N = 4;
+    static __device__ __forceinline__ void ld(const float* p, float v[4]) { Row4<float>::ld(p, v); }
+    static __device__ __forceinline__ void ldg(const float* p, float v[4]) { Row4<float>::ldg4(p, v); }
+    static __device__ __forceinline__ void st(float* p, const float v[4]) { Row4<float>::st(p, v); }
 };
 template <>
-struct Sector<double> {
-    static constexpr int N = 4;
-    static __device__ __forceinline__ void ld(const double* p, double v[4]) { Row4<double>::ld(p, v); }
-    static __device__ __forceinline__ void ldg(const double* p, double v[4]) { Row4<double>::ldg4(p, v); }
-    static __device__ __forceinline__ void st(double* p, const double v[4]) { Row4<double>::st(p, v); }
+struct Vec16<double> {
+    static constexpr int N = 2;
+    static __device__ __forceinline__ void ld(const double* p, double v[2]) { Row4<double>::ld2(p, v[0], v[1]); }
+    static __device__ __forceinline__ void ldg(const double* p, double v[2]) {
+        const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+        v[0] = a.x;
+        v[1] = a.y;
+    }
+    static __device__ __forceinline__ void st(double* p, const double v[2]) {
+        *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+    }
 };
 
 template <typename T, bool VAR>
 __global__ void __launch_bounds__(256) k_colour_split(LevelView<T> L, int colour) {
-    constexpr int NC = Sector<T>::N;  // cells per thread
-    constexpr int TH = 8 / NC;        // threads per half block
+    constexpr int NC = Vec16<T>::N;  // cells per thread
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z * blockDim.z + threadIdx.z;
-    if (i >= L.n0 || j >= L.n1 || t >= L.n2 / (2 * NC)) return;
-    const int g = t / TH, m0 = (t % TH) * NC;  // block of the row, first slot
-    // h = 0: the even k of this row have the pass's colour (k = 16g + 2m + h)
+    const int i = blockIdx.z;
+    const int kh = L.kh;
+    if (j >= L.n1 || t * NC >= kh) return;
+    const int m0 = t * NC;  // first slot of the thread in its half row
+    // h = 0: the even k of this row have the pass's colour (k = 2m + h)
     const int h = (colour ^ (i + j + L.cpar)) & 1;
     const int si = (int)L.si, sj = (int)L.sj;
     const int row = (int)L.base + i * si + j * sj;
-    const int own = row + 16 * g + 8 * h + m0;
-    const int oth = row + 16 * g + 8 * (1 - h) + m0;
+    const int own = row + h * kh + m0;
+    const int oth = row + (1 - h) * kh + m0;
     // the k neighbour beyond the slots: below the first cell (h = 0; the
-    // previous block's last odd cell, or the ghost k = -1) or above the last
-    // one (h = 1; the next block's first even cell, or the ghost k = n2)
-    const int ext = h == 0 ? (m0 > 0 ? oth - 1 : row + 16 * g - 1) : (m0 + NC < 8 ? oth + NC : row + 16 * g + 16);
+    // previous slot of the odd half, or the ghost k = -1) or above the last
+    // one (h = 1; the next slot of the even half, or the ghost k = n2)
+    const int ext = h == 0 ? (m0 > 0 ? oth - 1 : row - 1) : (m0 + NC < kh ? oth + NC : row + 2 * kh);
+    // every load is issued before any is used, so one memory latency covers them
     T xo[NC], xm[NC], xp[NC], ym[NC], yp[NC], bb[NC], wkl[NC], wkh[NC];
-    Sector<T>::ld(L.x + oth, xo);
-    Sector<T>::ld(L.x + own - si, xm);
-    Sector<T>::ld(L.x + own + si, xp);
-    Sector<T>::ld(L.x + own - sj, ym);
-    Sector<T>::ld(L.x + own + sj, yp);
-    Sector<T>::ld(L.b + own, bb);
+    Vec16<T>::ld(L.x + oth, xo);
+    Vec16<T>::ld(L.x + own - si, xm);
+    Vec16<T>::ld(L.x + own + si, xp);
+    Vec16<T>::ld(L.x + own - sj, ym);
+    Vec16<T>::ld(L.x + own + sj, yp);
+    Vec16<T>::ld(L.b + own, bb);
     const T e = L.x[ext];
-    Sector<T>::ldg(L.tab + L.to.kwl + (own - row), wkl);
-    Sector<T>::ldg(L.tab + L.to.kwh + (own - row), wkh);
+    Vec16<T>::ldg(L.tab + L.to.kwl + (own - row), wkl);
+    Vec16<T>::ldg(L.tab + L.to.kwh + (own - row), wkh);
     const T wil = ldg(L.tab + L.to.wl[0] + i), wih = ldg(L.tab + L.to.wh[0] + i);
     const T wjl = ldg(L.tab + L.to.wl[1] + j), wjh = ldg(L.tab + L.to.wh[1] + j);
     T l0[NC], l0p[NC], l1[NC], l1p[NC], l2[NC], l2u[NC], l2e = T(1);
     if (VAR) {
-        Sector<T>::ldg(L.lam0 + own, l0);
-        Sector<T>::ldg(L.lam0 + own + si, l0p);
-        Sector<T>::ldg(L.lam1 + own, l1);
-        Sector<T>::ldg(L.lam1 + own + sj, l1p);
-        Sector<T>::ldg(L.lam2 + own, l2);
-        Sector<T>::ldg(L.lam2 + oth, l2u);  // lower faces of the other colour's slots
+        Vec16<T>::ldg(L.lam0 + own, l0);
+        Vec16<T>::ldg(L.lam0 + own + si, l0p);
+        Vec16<T>::ldg(L.lam1 + own, l1);
+        Vec16<T>::ldg(L.lam1 + own + sj, l1p);
+        Vec16<T>::ldg(L.lam2 + own, l2);
+        Vec16<T>::ldg(L.lam2 + oth, l2u);  // lower faces of the other colour's slots
+        // the upper k face of the last cell (h = 1) is the lower face of the
+        // next even slot, or the face at k = n2 (both at ext)
         l2e = ldg(L.lam2 + ext);
     }
     T v[NC];
@@ -351,13 +352,12 @@ __global__ void __launch_bounds__(256) k_colour_split(LevelView<T> L, int colour
         v[m] = gs_value(w, xn, bb[m]);
     }
     // the pinned cell (0,0,0), when this pass updates it, keeps its value
-    if (L.pin && (i | j | g | h | m0) == 0) v[0] = L.x[own];
-    Sector<T>::st(L.x + own, v);
-    const int last = L.n2 / 16 - 1;
+    if (L.pin && (i | j | h | m0) == 0) v[0] = L.x[own];
+    Vec16<T>::st(L.x + own, v);
     if ((L.per0 && (i == 0 || i == L.n0 - 1)) || (L.per1 && (j == 0 || j == L.n1 - 1)) ||
-        (L.per2 && (((g | h | m0) == 0) || (g == last && h == 1 && m0 + NC == 8)))) {
+        (L.per2 && (((h | m0) == 0) || (h == 1 && m0 + NC == kh)))) {
 #pragma unroll
-        for (int m = 0; m < NC; ++m) store_images(L, own + m, i, j, 16 * g + 2 * (m0 + m) + h, v[m]);
+        for (int m = 0; m < NC; ++m) store_images(L, own + m, i, j, 2 * (m0 + m) + h, v[m]);
     }
 }
 
@@ -507,7 +507,7 @@ __device__ __forceinline__ void prolong_quad_item(const LevelView<T>& F, const L
     const int r10 = cell32(C, I1, J0, 0), r11 = cell32(C, I1, J1, 0);
     const int c0 = cell32(F, i, j, k0);
     T xf[4];
-    ldq(F.x + c0, F.ks, xf);
+    ldq(F.x + c0, F.kh, xf);
     const int* pk = pidx + 2 * (F.n0 + F.n1);
     const T* wk = pw + F.n0 + F.n1;
     // Fine cells k0 .. k0+3 (k0 = 4p) have parents 2p, 2p, 2p+1, 2p+1 and
@@ -527,7 +527,7 @@ __device__ __forceinline__ void prolong_quad_item(const LevelView<T>& F, const L
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
         T xb, xc;
-        if (C.ks) {
+        if (C.kh) {
             xb = X[rows[r] + Pb];
             xc = X[rows[r] + Pc];
         } else {
@@ -542,10 +542,10 @@ __device__ __forceinline__ void prolong_quad_item(const LevelView<T>& F, const L
 #pragma unroll
     for (int q = 0; q < 4; ++q)
         xf[q] += ui * (uj * v[0][q] + wj * v[1][q]) + wi * (uj * v[2][q] + wj * v[3][q]);
-    stq(F.x + c0, F.ks, xf);
+    stq(F.x + c0, F.kh, xf);
     if (quad_has_images(F, i, j, k0)) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) store_images(F, c0 + quad_off(F.ks, q), i, j, k0 + q, xf[q]);
+        for (int q = 0; q < 4; ++q) store_images(F, c0 + quad_off(F.kh, q), i, j, k0 + q, xf[q]);
     }
 }
 
@@ -586,23 +586,23 @@ __device__ __forceinline__ void restrict_quad_item(const LevelView<T>& F, const 
             const T rab = ra * ldg(ratio + F.n0 + j);
             const T wjl = ldg(F.tab + F.to.wl[1] + j), wjh = ldg(F.tab + F.to.wh[1] + j);
             const int row = (int)row_at(F, i, j), si = (int)F.si, sj = (int)F.sj;
-            const int c = row + kpos(F, k0), ks = F.ks;
+            const int c = row + kpos(F, k0), kh = F.kh;
             T own[4], xm[4], xp[4], ym[4], yp[4], bb[4];
-            ldq(F.x + c, ks, own);
-            ldq(F.x + c - si, ks, xm);
-            ldq(F.x + c + si, ks, xp);
-            ldq(F.x + c - sj, ks, ym);
-            ldq(F.x + c + sj, ks, yp);
-            ldq(F.b + c, ks, bb);
+            ldq(F.x + c, kh, own);
+            ldq(F.x + c - si, kh, xm);
+            ldq(F.x + c + si, kh, xp);
+            ldq(F.x + c - sj, kh, ym);
+            ldq(F.x + c + sj, kh, yp);
+            ldq(F.b + c, kh, bb);
             const int cl = row + kpos(F, k0 - 1), cr = row + kpos(F, k0 + 4);
             const T left = F.x[cl], right = F.x[cr];
             T l0[4], l0p[4], l1[4], l1p[4], l2[4], l2r = T(1);
             if (VAR) {
-                ldgq(F.lam0 + c, ks, l0);
-                ldgq(F.lam0 + c + si, ks, l0p);
-                ldgq(F.lam1 + c, ks, l1);
-                ldgq(F.lam1 + c + sj, ks, l1p);
-                ldgq(F.lam2 + c, ks, l2);
+                ldgq(F.lam0 + c, kh, l0);
+                ldgq(F.lam0 + c + si, kh, l0p);
+                ldgq(F.lam1 + c, kh, l1);
+                ldgq(F.lam1 + c + sj, kh, l1p);
+                ldgq(F.lam2 + c, kh, l2);
                 l2r = ldg(F.lam2 + cr);
             }
             T r[4];
@@ -638,6 +638,199 @@ __global__ void __launch_bounds__(256) k_restrict_quad(Bricks<T> FB, Bricks<T> C
     const int J = blockIdx.y * blockDim.y + threadIdx.y;
     if (J >= CB.v[b].n1 || 2 * P >= CB.v[b].n2) return;
     restrict_quad_item<T, VAR>(FB.v[b], CB.v[b], ts.t[b], I, J, P);
+}
+
+// ---------------------------------------------------------------------------
+// The same two transfers for a parity-split fine level (single brick,
+// factor 2 along every axis): a thread owns the fine slots 4P .. 4P+3 of
+// both halves of a row -- the eight consecutive cells k = 8P .. 8P+7, four
+// even and four odd -- so every fine array moves as whole vectors.  The
+// restriction writes the coarse cells K = 4P .. 4P+3 (the parents of
+// those eight), the prolongation reads them and their two outer
+// neighbours.  Per cell the arithmetic and its order are those of
+// restrict_quad_item and prolong_quad_item, so the results are
+// bit-identical.
+// ---------------------------------------------------------------------------
+template <typename T, bool VAR>
+__global__ void __launch_bounds__(256) k_restrict_split(Bricks<T> FB, Bricks<T> CB, TransferSet ts) {
+    const LevelView<T>& F = FB.v[0];
+    const LevelView<T>& C = CB.v[0];
+    const TransferTabs& t = ts.t[0];
+    const int P = blockIdx.x * blockDim.x + threadIdx.x;
+    const int J = blockIdx.y * blockDim.y + threadIdx.y;
+    const int I = blockIdx.z;
+    const int kh = F.kh;
+    if (J >= C.n1 || 4 * P >= kh) return;
+    const T* ratio;
+    if constexpr (sizeof(T) == 8)
+        ratio = reinterpret_cast<const T*>(t.ratio64);
+    else
+        ratio = reinterpret_cast<const T*>(t.ratio32);
+    const int m0 = 4 * P;
+    // k couplings and k shares of the even (k = 2(m0+m)) and odd cells
+    T wke[4], whe[4], wko[4], who[4], rke[4], rko[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        const int k = 2 * (m0 + m);
+        wke[m] = ldg(F.tab + F.to.wl[2] + k);
+        whe[m] = ldg(F.tab + F.to.wh[2] + k);
+        wko[m] = ldg(F.tab + F.to.wl[2] + k + 1);
+        who[m] = ldg(F.tab + F.to.wh[2] + k + 1);
+        rke[m] = ldg(ratio + F.n0 + F.n1 + k);
+        rko[m] = ldg(ratio + F.n0 + F.n1 + k + 1);
+    }
+    T acc[4] = {T(0), T(0), T(0), T(0)};
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+        const int i = 2 * I + a;
+        const T ra = ldg(ratio + i);
+        const T wil = ldg(F.tab + F.to.wl[0] + i), wih = ldg(F.tab + F.to.wh[0] + i);
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int j = 2 * J + e;
+            const T rab = ra * ldg(ratio + F.n0 + j);
+            const T wjl = ldg(F.tab + F.to.wl[1] + j), wjh = ldg(F.tab + F.to.wh[1] + j);
+            const int si = (int)F.si, sj = (int)F.sj;
+            const int row = (int)row_at(F, i, j);
+            const int ce = row + m0, co = row + kh + m0;           // even and odd slots
+            const int clo = m0 > 0 ? co - 1 : row - 1;            // k = 8P - 1
+            const int chi = m0 + 4 < kh ? ce + 4 : row + 2 * kh;  // k = 8P + 8
+            T xe[4], xo[4], me[4], mo[4], pe[4], po[4], ne[4], no[4], qe[4], qo[4], be[4], bo[4];
+            Row4<T>::ld(F.x + ce, xe);
+            Row4<T>::ld(F.x + co, xo);
+            Row4<T>::ld(F.x + ce - si, me);
+            Row4<T>::ld(F.x + co - si, mo);
+            Row4<T>::ld(F.x + ce + si, pe);
+            Row4<T>::ld(F.x + co + si, po);
+            Row4<T>::ld(F.x + ce - sj, ne);
+            Row4<T>::ld(F.x + co - sj, no);
+            Row4<T>::ld(F.x + ce + sj, qe);
+            Row4<T>::ld(F.x + co + sj, qo);
+            Row4<T>::ld(F.b + ce, be);
+            Row4<T>::ld(F.b + co, bo);
+            const T left = F.x[clo], right = F.x[chi];
+            T l0e[4], l0o[4], l0pe[4], l0po[4], l1e[4], l1o[4], l1pe[4], l1po[4], l2e[4], l2o[4], l2r = T(1);
+            if (VAR) {
+                Row4<T>::ldg4(F.lam0 + ce, l0e);
+                Row4<T>::ldg4(F.lam0 + co, l0o);
+                Row4<T>::ldg4(F.lam0 + ce + si, l0pe);
+                Row4<T>::ldg4(F.lam0 + co + si, l0po);
+                Row4<T>::ldg4(F.lam1 + ce, l1e);
+                Row4<T>::ldg4(F.lam1 + co, l1o);
+                Row4<T>::ldg4(F.lam1 + ce + sj, l1pe);
+                Row4<T>::ldg4(F.lam1 + co + sj, l1po);
+                Row4<T>::ldg4(F.lam2 + ce, l2e);
+                Row4<T>::ldg4(F.lam2 + co, l2o);
+                l2r = ldg(F.lam2 + chi);
+            }
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                // the even cell k = 2(m0+m) and the odd cell k + 1, in that order
+                T r2[2];
+#pragma unroll
+                for (int sd = 0; sd < 2; ++sd) {
+                    T w[6] = {wil, wih, wjl, wjh, sd ? wko[m] : wke[m], sd ? who[m] : whe[m]};
+                    if (VAR) {
+                        w[0] *= sd ? l0o[m] : l0e[m];
+                        w[1] *= sd ? l0po[m] : l0pe[m];
+                        w[2] *= sd ? l1o[m] : l1e[m];
+                        w[3] *= sd ? l1po[m] : l1pe[m];
+                        w[4] *= sd ? l2o[m] : l2e[m];
+                        // upper k face: the lower face of the next cell
+                        w[5] *= sd ? (m < 3 ? l2e[m + 1] : l2r) : l2o[m];
+                    }
+                    const T own = sd ? xo[m] : xe[m];
+                    const T km = sd ? xe[m] : (m > 0 ? xo[m - 1] : left);
+                    const T kp = sd ? (m < 3 ? xe[m + 1] : right) : xo[m];
+                    const T xmv = sd ? mo[m] : me[m], xpv = sd ? po[m] : pe[m];
+                    const T ymv = sd ? no[m] : ne[m], ypv = sd ? qo[m] : qe[m];
+                    const T sv = w[0] * xmv + w[1] * xpv + w[2] * ymv + w[3] * ypv + w[4] * km + w[5] * kp;
+                    const T d = w[0] + w[1] + w[2] + w[3] + w[4] + w[5];
+                    r2[sd] = (sd ? bo[m] : be[m]) + d * own - sv;
+                }
+                acc[m] += rab * (rke[m] * r2[0] + rko[m] * r2[1]);
+            }
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < 4; ++m) C.b[cell32(C, I, J, m0 + m)] = acc[m];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_prolong_split(Bricks<T> FB, Bricks<T> CB, TransferSet ts) {
+    const LevelView<T>& F = FB.v[0];
+    const LevelView<T>& C = CB.v[0];
+    const TransferTabs& t = ts.t[0];
+    const int P = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = blockIdx.z;
+    const int kh = F.kh;
+    if (j >= F.n1 || 4 * P >= kh) return;
+    const int m0 = 4 * P;
+    const int* pidx = t.pidx;
+    const T* pw;
+    if constexpr (sizeof(T) == 8)
+        pw = reinterpret_cast<const T*>(t.pw64);
+    else
+        pw = reinterpret_cast<const T*>(t.pw32);
+    const int I0 = ldg(pidx + 2 * i), I1 = ldg(pidx + 2 * i + 1);
+    const int J0 = ldg(pidx + 2 * F.n0 + 2 * j), J1 = ldg(pidx + 2 * F.n0 + 2 * j + 1);
+    const T wi = ldg(pw + i), wj = ldg(pw + F.n0 + j);
+    const T ui = T(1) - wi, uj = T(1) - wj;
+    const int* pk = pidx + 2 * (F.n0 + F.n1);
+    const T* wk = pw + F.n0 + F.n1;
+    // parents of the eight cells: K = m0 .. m0+3; second coarse cells: K - 1
+    // for the even cells and K + 1 for the odd ones, the outer two from the
+    // tables (they may be a wrapped, a ghost or the parent's own index)
+    const int Klo = kpos(C, ldg(pk + 2 * (2 * m0) + 1));
+    const int Khi = kpos(C, ldg(pk + 2 * (2 * m0 + 7) + 1));
+    T we[4], ue[4], wo[4], uo[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        we[m] = ldg(wk + 2 * (m0 + m));
+        wo[m] = ldg(wk + 2 * (m0 + m) + 1);
+        ue[m] = T(1) - we[m];
+        uo[m] = T(1) - wo[m];
+    }
+    const int rows[4] = {cell32(C, I0, J0, 0), cell32(C, I0, J1, 0), cell32(C, I1, J0, 0), cell32(C, I1, J1, 0)};
+    T ve[4][4], vo[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const T* X = C.x + rows[r];
+        T xc[4];  // the parents K = m0 .. m0+3
+        if (C.kh) {
+            Row4<T>::ld2(X + m0 / 2, xc[0], xc[2]);
+            Row4<T>::ld2(X + C.kh + m0 / 2, xc[1], xc[3]);
+        } else {
+            Row4<T>::ld(X + m0, xc);
+        }
+        const T xlo = X[Klo], xhi = X[Khi];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            ve[r][m] = ue[m] * xc[m] + we[m] * (m > 0 ? xc[m - 1] : xlo);
+            vo[r][m] = uo[m] * xc[m] + wo[m] * (m < 3 ? xc[m + 1] : xhi);
+        }
+    }
+    const int row = (int)row_at(F, i, j);
+    const int ce = row + m0, co = row + kh + m0;
+    T xe[4], xo[4];
+    Row4<T>::ld(F.x + ce, xe);
+    Row4<T>::ld(F.x + co, xo);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        xe[m] += ui * (uj * ve[0][m] + wj * ve[1][m]) + wi * (uj * ve[2][m] + wj * ve[3][m]);
+        xo[m] += ui * (uj * vo[0][m] + wj * vo[1][m]) + wi * (uj * vo[2][m] + wj * vo[3][m]);
+    }
+    Row4<T>::st(F.x + ce, xe);
+    Row4<T>::st(F.x + co, xo);
+    if ((F.per0 && (i == 0 || i == F.n0 - 1)) || (F.per1 && (j == 0 || j == F.n1 - 1)) ||
+        (F.per2 && (m0 == 0 || m0 + 4 == kh))) {
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            store_images(F, ce + m, i, j, 2 * (m0 + m), xe[m]);
+            store_images(F, co + m, i, j, 2 * (m0 + m) + 1, xo[m]);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -996,12 +1189,13 @@ long reduce_blocks(const Bricks<double>& B) {
 
 template <typename T, bool VAR>
 void launch_colour_pass(const Bricks<T>& B, int colour, cudaStream_t s) {
-    if (B.v[0].ks) {  // parity-split rows (single brick, n2 % 16 == 0)
+    if (B.v[0].kh) {  // parity-split rows (single brick, n2 % 16 == 0)
         const LevelView<T>& L = B.v[0];
-        const int tr = L.n2 / (64 / (int)sizeof(T));  // threads per row
-        const int bx = std::min(tr, 32), by = std::min(256 / bx, L.n1), bz = std::max(1, 256 / (bx * by));
-        const dim3 blk(bx, by, bz);
-        const dim3 grid((tr + bx - 1) / bx, (L.n1 + by - 1) / by, (L.n0 + bz - 1) / bz);
+        const int tr = L.kh / (16 / (int)sizeof(T));  // threads per half row
+        int bx = 1;
+        while (bx < tr && bx < 32) bx *= 2;
+        const dim3 blk(bx, 256 / bx, 1);
+        const dim3 grid((tr + bx - 1) / bx, (L.n1 + blk.y - 1) / blk.y, L.n0);
         k_colour_split<T, VAR><<<grid, blk, 0, s>>>(L, colour);
         return;
     }
@@ -1035,8 +1229,22 @@ bool quad_transfers(const Bricks<T>& F, const TransferSet& t) {
     return true;
 }
 
+// the split-level transfers: blocks of 256 threads over (slot groups, rows), one plane per grid z
+inline dim3 split_block(int groups) {
+    int bx = 1;
+    while (bx < groups && bx < 32) bx *= 2;
+    return dim3(bx, 256 / bx, 1);
+}
+
 template <typename T, bool VAR>
 void launch_residual_restrict(const Bricks<T>& F, const Bricks<T>& C, const TransferSet& t, cudaStream_t s) {
+    if (F.v[0].kh && quad_transfers(F, t)) {
+        const int groups = F.v[0].kh / 4;
+        const dim3 blk = split_block(groups);
+        const dim3 grid((groups + blk.x - 1) / blk.x, (C.v[0].n1 + blk.y - 1) / blk.y, C.v[0].n0);
+        k_restrict_split<T, VAR><<<grid, blk, 0, s>>>(F, C, t);
+        return;
+    }
     if (quad_transfers(F, t)) {
         const int np = C.max2 / 2;
         const dim3 blk = np >= 32 ? dim3(32, 8, 1) : np >= 8 ? dim3(8, 32, 1) : dim3(2, 128, 1);
@@ -1049,6 +1257,13 @@ void launch_residual_restrict(const Bricks<T>& F, const Bricks<T>& C, const Tran
 
 template <typename T>
 void launch_prolong_correct(const Bricks<T>& F, const Bricks<T>& C, const TransferSet& t, cudaStream_t s) {
+    if (F.v[0].kh && quad_transfers(F, t)) {
+        const int groups = F.v[0].kh / 4;
+        const dim3 blk = split_block(groups);
+        const dim3 grid((groups + blk.x - 1) / blk.x, (F.v[0].n1 + blk.y - 1) / blk.y, F.v[0].n0);
+        k_prolong_split<T><<<grid, blk, 0, s>>>(F, C, t);
+        return;
+    }
     if (quad_transfers(F, t)) {
         const int nq = F.max2 / 4;
         const dim3 blk = nq >= 32 ? dim3(32, 8, 1) : nq >= 8 ? dim3(8, 32, 1) : dim3(2, 128, 1);

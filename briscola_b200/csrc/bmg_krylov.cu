@@ -201,31 +201,31 @@ __global__ void __launch_bounds__(kFinalThreads) k_fcg_true_norm(const double* p
 constexpr int kQuadPlanes = 64;  // grid z: plane groups
 
 // The logical k-quad k0 .. k0+3 at slab index p (its first cell): one
-// vector in a natural row (ks = 0); in a parity-split row (ks = 1) the even
-// pair (k0, k0+2) at p and the odd pair (k0+1, k0+3) at p + 8.
+// vector in a natural row (kh = 0); in a parity-split row the even pair
+// (k0, k0+2) at p and the odd pair (k0+1, k0+3) at p + kh.
 template <typename T>
 struct Quad4;
 template <>
 struct Quad4<double> {
-    static __device__ __forceinline__ void ld(const double* p, int ks, double v[4]) {
+    static __device__ __forceinline__ void ld(const double* p, int kh, double v[4]) {
         const double2 a = reinterpret_cast<const double2*>(p)[0];
-        const double2 b = *reinterpret_cast<const double2*>(p + (ks ? 8 : 2));
+        const double2 b = *reinterpret_cast<const double2*>(p + (kh ? kh : 2));
         v[0] = a.x;
-        v[1] = ks ? b.x : a.y;
-        v[2] = ks ? a.y : b.x;
+        v[1] = kh ? b.x : a.y;
+        v[2] = kh ? a.y : b.x;
         v[3] = b.y;
     }
-    static __device__ __forceinline__ void st(double* p, int ks, const double v[4]) {
-        reinterpret_cast<double2*>(p)[0] = ks ? make_double2(v[0], v[2]) : make_double2(v[0], v[1]);
-        *reinterpret_cast<double2*>(p + (ks ? 8 : 2)) = ks ? make_double2(v[1], v[3]) : make_double2(v[2], v[3]);
+    static __device__ __forceinline__ void st(double* p, int kh, const double v[4]) {
+        reinterpret_cast<double2*>(p)[0] = kh ? make_double2(v[0], v[2]) : make_double2(v[0], v[1]);
+        *reinterpret_cast<double2*>(p + (kh ? kh : 2)) = kh ? make_double2(v[1], v[3]) : make_double2(v[2], v[3]);
     }
 };
 template <>
 struct Quad4<float> {
-    static __device__ __forceinline__ void ld(const float* p, int ks, float v[4]) {
-        if (ks) {
+    static __device__ __forceinline__ void ld(const float* p, int kh, float v[4]) {
+        if (kh) {
             const float2 a = reinterpret_cast<const float2*>(p)[0];
-            const float2 b = *reinterpret_cast<const float2*>(p + 8);
+            const float2 b = *reinterpret_cast<const float2*>(p + kh);
             v[0] = a.x;
             v[1] = b.x;
             v[2] = a.y;
@@ -238,10 +238,10 @@ struct Quad4<float> {
             v[3] = a.w;
         }
     }
-    static __device__ __forceinline__ void st(float* p, int ks, const float v[4]) {
-        if (ks) {
+    static __device__ __forceinline__ void st(float* p, int kh, const float v[4]) {
+        if (kh) {
             reinterpret_cast<float2*>(p)[0] = make_float2(v[0], v[2]);
-            *reinterpret_cast<float2*>(p + 8) = make_float2(v[1], v[3]);
+            *reinterpret_cast<float2*>(p + kh) = make_float2(v[1], v[3]);
         } else {
             *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
         }
@@ -260,7 +260,7 @@ struct Quad4<float> {
             const int k0 = 4 * qx;                                                         \
             if (j < L.n1 && k0 < L.n2) {                                                   \
                 const long row = row_at(L, i, j), c = row + kpos(L, k0);                   \
-                const int ks = L.ks;                                                       \
+                const int ks = L.kh;                                                       \
                 const double hij = L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j];        \
                 double hk[4];                                                              \
                 Quad4<double>::ld(L.tab64 + L.to.h[2] + k0, 0, hk);                        \
@@ -331,6 +331,65 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_direction4(Bricks<double
         Quad4<double>::st(p + c, ks, pn);
         Quad4<double>::st(q + c, ks, qn);
     })
+    a = block_sum<kReduceThreads>(a, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0) partials[block_id()] = a;
+}
+
+// The same direction step on a parity-split level 0 (one brick): the
+// thread owns four consecutive positions of one half of a row, the cells
+// k = 2 (m0 + e) + h of one parity, so z, its neighbours and p and q load as
+// whole vectors; the k neighbours are the other half's same slots and one
+// beyond them (as in k_colour_split).  Per cell the arithmetic is
+// k_fcg_direction4's; the partial sums group the cells differently.
+template <typename T, bool VAR>
+__global__ void __launch_bounds__(kReduceThreads) k_fcg_direction_split(Bricks<double> B, const T* z, double* p,
+                                                                        double* q, double* partials,
+                                                                        const SolveState* st) {
+    __shared__ double sh[kReduceThreads / 32];
+    const double beta = st->beta;
+    double a = 0.0;
+    const LevelView<double>& L = B.v[0];
+    const int qx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int kh = L.kh;
+    if (j < L.n1 && 4 * qx < L.n2) {
+        const int h = 4 * qx >= kh ? 1 : 0;
+        const int m0 = 4 * qx - h * kh;
+        for (int i = blockIdx.z; i < L.n0; i += gridDim.z) {
+            const long row = row_at(L, i, j), c = row + 4 * qx;
+            const long co = row + (1 - h) * kh + m0;  // the other half, same slots
+            const long ce = h == 0 ? (m0 > 0 ? co - 1 : row - 1) : (m0 + 4 < kh ? co + 4 : row + 2 * kh);
+            T zc[4], zo[4], zim[4], zip[4], zjm[4], zjp[4];
+            Quad4<T>::ld(z + c, 0, zc);
+            Quad4<T>::ld(z + co, 0, zo);
+            Quad4<T>::ld(z + c - L.si, 0, zim);
+            Quad4<T>::ld(z + c + L.si, 0, zip);
+            Quad4<T>::ld(z + c - L.sj, 0, zjm);
+            Quad4<T>::ld(z + c + L.sj, 0, zjp);
+            const T ze = z[ce];
+            double pq[4], qq[4], pn[4], qn[4];
+            Quad4<double>::ld(p + c, 0, pq);
+            Quad4<double>::ld(q + c, 0, qq);
+            const double hij = L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j];
+            for (int e = 0; e < 4; ++e) {
+                const int k = 2 * (m0 + e) + h;
+                double w[6];
+                const long ckp = h == 0 ? co + e : (e < 3 ? co + e + 1 : ce);
+                couplings<double, VAR>(L, i, j, k, c + e, ckp, w);
+                const double km = h == 0 ? (double)(e == 0 ? ze : zo[e - 1]) : (double)zo[e];
+                const double kp = h == 0 ? (double)zo[e] : (double)(e == 3 ? ze : zo[e + 1]);
+                const double zz = (double)zc[e];
+                const double sv = w[0] * (double)zim[e] + w[1] * (double)zip[e] + w[2] * (double)zjm[e] +
+                                  w[3] * (double)zjp[e] + w[4] * km + w[5] * kp;
+                const double d = w[0] + w[1] + w[2] + w[3] + w[4] + w[5];
+                pn[e] = beta != 0.0 ? zz + beta * pq[e] : zz;
+                qn[e] = beta != 0.0 ? (sv - d * zz) + beta * qq[e] : sv - d * zz;
+                a += (hij * L.tab64[L.to.h[2] + k]) * pn[e] * qn[e];
+            }
+            Quad4<double>::st(p + c, 0, pn);
+            Quad4<double>::st(q + c, 0, qn);
+        }
+    }
     a = block_sum<kReduceThreads>(a, sh);
     if (threadIdx.x == 0 && threadIdx.y == 0) partials[block_id()] = a;
 }
@@ -413,7 +472,9 @@ void launch_fcg_beta(const Bricks<double>& B, const T* z, const double* r, const
 template <typename T, bool VAR>
 void launch_fcg_direction(const Bricks<double>& B, const T* z, double* p, double* q, double* partials,
                           SolveState* st, cudaStream_t s) {
-    if (fcg_quads(B)) {
+    if (B.v[0].kh) {
+        k_fcg_direction_split<T, VAR><<<quad_grid(B), dim3(16, 16, 1), 0, s>>>(B, z, p, q, partials, st);
+    } else if (fcg_quads(B)) {
         k_fcg_direction4<T, VAR><<<quad_grid(B), dim3(16, 16, 1), 0, s>>>(B, z, p, q, partials, st);
     } else {
         const dim3 blk = block_for(B.max2);

@@ -12,14 +12,16 @@ __device__ __forceinline__ T ldg(const T* p) {
     return __ldg(p);
 }
 
-// Storage position of logical k (-1 .. n2) in a parity-split row: blocks of
-// 16 cells, even k first (k & 1 selects the half, k >> 1 the slot).  The
-// ghosts map to themselves: -1 -> -1 and n2 (a multiple of 16) -> n2.
-__device__ __forceinline__ int kpos_split(int k) { return (k & ~15) | ((k & 1) << 3) | ((k >> 1) & 7); }
+// Storage position of logical k (-1 .. n2) in a row: k itself in natural
+// rows (kh = 0); in a parity-split row (kh = n2/2) the even k first, then
+// the odd k, with the ghosts k = -1 and k = n2 at their natural places.
+__device__ __forceinline__ int kpos_split(int k, int kh) {
+    return (k >= 0 && k < 2 * kh) ? (k & 1) * kh + (k >> 1) : k;
+}
 
 template <typename T>
 __device__ __forceinline__ int kpos(const LevelView<T>& L, int k) {
-    return L.ks ? kpos_split(k) : k;
+    return L.kh ? kpos_split(k, L.kh) : k;
 }
 
 // Row-scaled couplings of cell (i,j,k) to its six neighbours in the order
@@ -139,10 +141,10 @@ __device__ __forceinline__ long row_at(const LevelView<T>& L, int i, int j) {
 }
 
 // Position, relative to the quad's first cell, of cell e (0..3) of the
-// logical k-quad k0 .. k0+3 (k0 % 4 == 0): consecutive in natural rows; in a
-// parity-split row the even pair sits at kpos(k0), kpos(k0)+1 and the odd
-// pair 8 further on.
-__device__ __forceinline__ int quad_off(int ks, int e) { return ks ? ((e & 1) << 3) | (e >> 1) : e; }
+// logical k-quad k0 .. k0+3 (k0 % 4 == 0): consecutive in natural rows
+// (kh = 0); in a parity-split row the even pair sits at kpos(k0),
+// kpos(k0)+1 and the odd pair kh further on.
+__device__ __forceinline__ int quad_off(int kh, int e) { return kh ? (e & 1) * kh + (e >> 1) : e; }
 
 // index of cell (i,j,k) in the caller's (compact, brick-frame) arrays
 template <typename T>

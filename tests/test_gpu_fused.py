@@ -2,7 +2,9 @@
 against the same passes launched one by one.  Both use the same stencil
 arithmetic (bmg_stencil.cuh), so the results must be bit-identical, in FP64
 and FP32, with constant and variable coefficients, walls and periodic axes,
-and for sequences longer than one fused launch."""
+and for sequences longer than one fused launch.  The fused smoother works on
+natural rows, so these contexts keep rowLayout natural (parity-split levels
+take the per-colour split kernel instead, tests/test_gpu_layout.py)."""
 import numpy as np
 import pytest
 
@@ -42,7 +44,7 @@ def _lam(br, seed):
 def test_fused_smoothing_bit_identical(native, name, precision, variable, stages):
     br = BRICKS[name]()
     mesh = Mesh([br])
-    ctx = {f: bb.Context(mesh, bb.make_options({"fused": f, "autotune": "off", "coarseLevel": 1}))
+    ctx = {f: bb.Context(mesh, bb.make_options({"fused": f, "autotune": "off", "coarseLevel": 1, "rowLayout": "natural"}))
            for f in (str(stages), "off")}
     ctx["on"] = ctx.pop(str(stages))
     assert ctx["on"].tuning(0, precision)[0] == stages and ctx["off"].tuning(0, precision)[0] == 0
@@ -75,7 +77,7 @@ def test_fused_solve_bit_identical(native, precision):
     mesh, b, _ = workloads.channel(64, seed=8)
     xs, reps = {}, {}
     for f in ("on", "off"):
-        c = bb.Context(mesh, bb.make_options({"fused": f, "autotune": "off", "relTol": 1e-10,
+        c = bb.Context(mesh, bb.make_options({"fused": f, "autotune": "off", "relTol": 1e-10, "rowLayout": "natural",
                                               "nSweepsPre": 2, "nSweepsPost": 2,
                                               "cycleType": "V", "coarseLevel": 1, "precision": precision}))
         x = np.zeros_like(b)
@@ -88,7 +90,8 @@ def test_fused_solve_bit_identical(native, precision):
 
 def test_autotuner_picks_valid_shapes(native):
     mesh, b, _ = workloads.channel(64, seed=9)
-    c = bb.Context(mesh, bb.make_options({"nSweepsPre": 2, "nSweepsPost": 2, "coarseLevel": 1}))
+    c = bb.Context(mesh, bb.make_options({"nSweepsPre": 2, "nSweepsPost": 2, "coarseLevel": 1,
+                                          "rowLayout": "natural"}))
     for l in range(c.num_levels):
         for p in (0, 1):
             s, t = c.tuning(l, p)
@@ -103,7 +106,8 @@ def test_autotuner_picks_valid_shapes(native):
 
 def test_pinned_launch_shapes(native):
     mesh, b, _ = workloads.channel(64, seed=10)
-    c = bb.Context(mesh, bb.make_options({"coarseLevel": 1, "autotune": "off", "precision": "mixed"}))
+    c = bb.Context(mesh, bb.make_options({"coarseLevel": 1, "autotune": "off", "precision": "mixed",
+                                          "rowLayout": "natural"}))
     c.set_tuning(0, 1, 2, 24)
     c.set_tuning(0, 0, 0, 64)
     assert c.tuning(0, 1) == (2, 24) and c.tuning(0, 0) == (0, 0)
@@ -116,7 +120,8 @@ def test_pinned_launch_shapes(native):
         c.set_tuning(coarsest, 1, 3, 16)  # a level the fused smoother does not handle
     x = np.zeros_like(b)
     rep = c.solve(b, x, zero_guess=True)
-    ref = bb.Context(mesh, bb.make_options({"coarseLevel": 1, "fused": "off", "precision": "mixed"}))
+    ref = bb.Context(mesh, bb.make_options({"coarseLevel": 1, "fused": "off", "precision": "mixed",
+                                            "rowLayout": "natural"}))
     x2 = np.zeros_like(b)
     rep2 = ref.solve(b, x2, zero_guess=True)
     assert rep.status == 0 and rep.cycles == rep2.cycles and np.array_equal(x, x2)

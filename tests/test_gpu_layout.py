@@ -1,11 +1,16 @@
 """Parity-split rows (rowLayout split, the default) against natural rows.
 
 On single-brick levels above 4096 cells with n2 % 16 == 0 the device keeps
-each row's cells in blocks of 16, even k first; the arithmetic of every
-kernel is unchanged, so solves with either layout must agree bit for bit,
-whatever the precision, outer loop, cycle, smoother, coefficient or wall
-condition.  The building blocks on split levels are also checked against
-the CPU oracle, as the natural ones are in test_gpu_parity.py.
+each row's even-k cells first, then its odd-k cells; the per-cell
+arithmetic of every kernel is unchanged, so solves with either layout must
+agree bit for bit, whatever the precision, cycle, smoother, coefficient or
+wall condition.  The one exception is the flexible-CG outer loop: on a
+split level 0 its direction kernel adds its per-block partial sums over
+cells of one parity, so the inner products round differently and the
+solutions agree to the solve's accuracy (relative 1e-9 at relTol 1e-10)
+with the same cycle count.  The building blocks on split levels are also
+checked against the CPU oracle, as the natural ones are in
+test_gpu_parity.py.
 """
 import numpy as np
 import pytest
@@ -85,7 +90,10 @@ def test_split_rows_are_bit_identical_to_natural(native, name):
     xn, rn = _solve(mesh, b, "natural", lam, **kw)
     assert rs.status == rn.status and rs.cycles == rn.cycles
     assert rs.status == 0 or name == "coarse_smooth", rs.status
-    assert np.array_equal(xs, xn), float(np.abs(xs - xn).max())
+    if kw.get("krylov") == "fcg":
+        assert rel(xs - xs.mean(), xn - xn.mean()) <= 1e-9
+    else:
+        assert np.array_equal(xs, xn), float(np.abs(xs - xn).max())
 
 
 def test_split_levels_are_in_use(native):
@@ -112,7 +120,7 @@ def _oracle(br, lam=None):
 
 SPLIT_MESHES = {
     "walls_graded_k": lambda: Brick([uniform_points(16), geometric_points(16, 2.0), geometric_points(32, 0.5)]),
-    "channel": lambda: Brick([uniform_points(32), tanh_points(16, 2.0), uniform_points(48)],
+    "channel": lambda: Brick([uniform_points(32), tanh_points(16, 2.0), uniform_points(64)],
                              (PERIODIC, PERIODIC, NEUMANN, NEUMANN, PERIODIC, PERIODIC)),
     "all_periodic": lambda: Brick([uniform_points(16), uniform_points(16), uniform_points(32)], (PERIODIC,) * 6),
 }
