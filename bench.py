@@ -461,6 +461,7 @@ def main():
     ap.add_argument("--learned-pairs", type=int, default=2000)
     ap.add_argument("--learned-steps", type=int, default=2000)
     ap.add_argument("--learned-held", type=int, default=200)
+    ap.add_argument("--no-learned-coarse", action="store_true")
     ap.add_argument("--profile-region", choices=["mixed_fcg", "mixed_fcg_fused", "fp64", "unet_fwd", "fft"],
                     default=None,
                     help="set up, warm up, then run one solve (or one U-Net forward) between "
@@ -739,6 +740,21 @@ def main():
                                       args.learned_held)
         torch.cuda.empty_cache()
 
+    # ---- learned coarse-level correction (config 5): the network on the 64^3
+    # level of the 128^3 and of the 256^3 cube in place of the recursion below ----
+    learned_coarse = None
+    if not args.no_learned_coarse:
+        from briscola_b200 import learned
+
+        learned_coarse = []
+        for N in sorted({128, args.size}):
+            level = {128: 1, 256: 2, 512: 3}.get(N)
+            if level is None:
+                continue
+            learned_coarse.append(learned.benchmark_coarse(N, level, args.learned_pairs, args.learned_steps,
+                                                           args.learned_held))
+            torch.cuda.empty_cache()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         times, cycles, threads = cpu_reference(args.size, steps=1)
@@ -802,6 +818,7 @@ def main():
             "fft": fft_t,
             "split": split_t,
             "learned": learned_t,
+            "learned_coarse": learned_coarse,
         }
         print(json.dumps(line), flush=True)
     for cc in ctx.values():

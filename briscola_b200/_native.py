@@ -34,8 +34,12 @@ EXPORTED = (
     "bmg_op_colour_pass", "bmg_op_smooth", "bmg_op_residual", "bmg_op_residual_restrict",
     "bmg_op_prolong_correct", "bmg_op_coarse_solve", "bmg_coarse_level_index",
     "bmg_residual_norm_noalloc", "bmg_level_tuning", "bmg_set_level_tuning", "bmg_project_rhs",
-    "bmg_project_correct",
+    "bmg_project_correct", "bmg_set_level_solver",
 )
+
+# int (*bmg_level_solver)(void* user, void* stream, const float* rhs, float* x, const int n[3])
+LEVEL_SOLVER = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                ctypes.POINTER(ctypes.c_int))
 
 
 class Brick(ctypes.Structure):
@@ -146,6 +150,7 @@ def load(path: str = LIB_PATH):
     L.bmg_set_level_tuning.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.bmg_project_rhs.argtypes = [vp, vp, vp, vp, ctypes.c_double, vp, ctypes.c_int]
     L.bmg_project_correct.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_double]
+    L.bmg_set_level_solver.argtypes = [vp, ctypes.c_int, LEVEL_SOLVER, vp]
     _lib = L
     return L
 

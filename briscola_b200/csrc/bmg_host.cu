@@ -165,6 +165,13 @@ struct bmg_ctx {
     cudaGraphExec_t gexec = nullptr;
     cudaGraphConditionalHandle cond = 0;
     cudaStream_t capStream = nullptr;  // private stream used only for capture
+    // a level solver in place of the FP32 cycle's recursion below hookLevel
+    // (bmg_set_level_solver), with its right-hand side and result arrays
+    int hookLevel = -1;
+    bmg_level_solver hook = nullptr;
+    void* hookUser = nullptr;
+    float* hookRhs = nullptr;
+    float* hookX = nullptr;
     bool graphZero = false;
     long launchesInitPost = 0, launchesBody = 0;
 };
@@ -573,6 +580,8 @@ void freeAll(bmg_ctx* c) {
     destroyGraph(c);
     if (c->capStream) cudaStreamDestroy(c->capStream);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    if (c->hookRhs) cudaFree(c->hookRhs);
+    if (c->hookX) cudaFree(c->hookX);
 }
 
 void validateOptions(const bmg_options* o) {
@@ -1381,6 +1390,8 @@ int tailFirst(const bmg_ctx* c) {
     int first = lc;
     while (first > 0 && c->lv[first - 1].ncell <= kTailCells) --first;
     if (first == lc || lc - first + 1 > kMaxTail) return -1;
+    // a level solver inside the tail's levels would be skipped by it
+    if (c->hook && c->hookLevel >= first) return -1;
     for (int q = first; q < lc; ++q) {
         const HostBrick& F = c->lv[q].br[0];
         const HostBrick& C = c->lv[q + 1].br[0];
@@ -1421,8 +1432,27 @@ void tailCycle(bmg_ctx* c, int first) {
         launch_tail_cycle<T, false>(P, c->stream);
 }
 
+// The level solver's turn (bmg_set_level_solver): the level's right-hand
+// side out to the solver, its result back as the level's correction, then
+// the level's post-smoothing; nothing below the level runs.
+void hookCycle(bmg_ctx* c, int l) {
+    const Bricks<float> B = bricks<float>(c, l);
+    const HostBrick& K = c->lv[l].br[0];
+    c->launches += 2;
+    launch_b_to_plain32(B, c->hookRhs, c->stream);
+    const int n[3] = {K.n[0], K.n[1], K.n[2]};
+    if (c->hook(c->hookUser, c->stream, c->hookRhs, c->hookX, n) != 0)
+        throw CudaError{"the level solver returned an error"};
+    launch_plain32_to_x(B, c->hookX, c->stream);
+    if (c->opt.n_post > 0) smooth<float>(c, l, c->opt.n_post);
+    c->visits[l]++;
+}
+
 template <typename T>
 void cycle(bmg_ctx* c, int l) {
+    if constexpr (sizeof(T) == 4) {
+        if (c->hook && l == c->hookLevel) return hookCycle(c, l);
+    }
     if (l == c->tail) return tailCycle<T>(c, l);
     if (c->opt.n_pre > 0) smooth<T>(c, l, c->opt.n_pre);
     if (l < c->lc) {
@@ -1945,6 +1975,8 @@ int bmg_set_options(bmg_ctx* c, const bmg_options* o) {
         const bool retune = o->autotune && (!c->opt.autotune || o->fused != c->opt.fused ||
                                             o->n_pre != c->opt.n_pre || o->n_post != c->opt.n_post);
         // options the hierarchy cannot take are refused before anything changes
+        if (coarseChanged && c->hook && c->hookLevel > coarseLevelFor(c, *o))
+            throw BadArg{BMG_BAD_ARG, "the level solver's level would lie below the coarse solve level"};
         if (coarseChanged) coarseLevelFor(c, *o);
         c->opt = *o;
         destroyGraph(c);
@@ -1954,6 +1986,30 @@ int bmg_set_options(bmg_ctx* c, const bmg_options* o) {
         c->tail = tailFirst(c);
         if (!o->autotune) applyChunk(c);
         if (retune) autotune(c);
+        return BMG_OK;
+    });
+}
+
+int bmg_set_level_solver(bmg_ctx* c, int level, bmg_level_solver fn, void* user) {
+    if (!c) return BMG_BAD_ARG;
+    return guarded(c, [&] {
+        if (fn && (level < 1 || level > c->lc))
+            throw BadArg{BMG_BAD_ARG, "level solver: level outside 1 .. the coarse solve level"};
+        if (fn && c->multi) throw BadArg{BMG_UNSUPPORTED, "level solver on a multi-brick mesh"};
+        BMG_CUDA(cudaSetDevice(c->opt.device));
+        BMG_CUDA(cudaStreamSynchronize(c->stream));
+        destroyGraph(c);
+        if (c->hookRhs) cudaFree(c->hookRhs);
+        if (c->hookX) cudaFree(c->hookX);
+        c->hookRhs = c->hookX = nullptr;
+        c->hook = fn;
+        c->hookUser = fn ? user : nullptr;
+        c->hookLevel = fn ? level : -1;
+        if (fn) {
+            c->hookRhs = dalloc<float>(c->lv[level].ncell);
+            c->hookX = dalloc<float>(c->lv[level].ncell);
+        }
+        c->tail = tailFirst(c);
         return BMG_OK;
     });
 }

@@ -272,5 +272,8 @@ template <typename T>
 void launch_store_field(const Bricks<T>& B, int field, double* compact, int unscale, cudaStream_t s);
 // x64 += x32 on the interior (write-through)
 void launch_add_correction(const Bricks<double>& B, const Bricks<float>& E, cudaStream_t s);
+// single-brick FP32 level b -> plain interior array, and plain array -> x
+void launch_b_to_plain32(const Bricks<float>& B, float* out, cudaStream_t s);
+void launch_plain32_to_x(const Bricks<float>& B, const float* in, cudaStream_t s);
 
 }  // namespace bmg

@@ -1166,6 +1166,27 @@ __global__ void __launch_bounds__(256) k_store_field(Bricks<T> B, int field, dou
     compact[compact_index(L, i, j, k)] = v;
 }
 
+// A single-brick FP32 level and a plain interior array (index (i n1 + j) n2
+// + k, the level's own frame): b to the array, the array to x (with its
+// periodic images) -- the two ends of a level solver (bmg_set_level_solver).
+__global__ void __launch_bounds__(256) k_b_to_plain32(Bricks<float> B, float* out) {
+    int i;
+    const LevelView<float>& L = B.v[brick_of(B, blockIdx.z, i)];
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (j >= L.n1 || k >= L.n2) return;
+    out[((long)i * L.n1 + j) * L.n2 + k] = L.b[row_at(L, i, j) + kpos(L, k)];
+}
+
+__global__ void __launch_bounds__(256) k_plain32_to_x(Bricks<float> B, const float* in) {
+    int i;
+    const LevelView<float>& L = B.v[brick_of(B, blockIdx.z, i)];
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (j >= L.n1 || k >= L.n2) return;
+    store_x(L, row_at(L, i, j) + kpos(L, k), i, j, k, in[((long)i * L.n1 + j) * L.n2 + k]);
+}
+
 __global__ void __launch_bounds__(256) k_add_correction(Bricks<double> B, Bricks<float> E) {
     int i;
     const int b = brick_of(B, blockIdx.z, i);
@@ -1352,6 +1373,16 @@ template <typename T>
 void launch_store_field(const Bricks<T>& B, int field, double* compact, int unscale, cudaStream_t s) {
     const dim3 blk = block_for(B.max2);
     k_store_field<T><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, field, compact, unscale);
+}
+
+void launch_b_to_plain32(const Bricks<float>& B, float* out, cudaStream_t s) {
+    const dim3 blk = block_for(B.max2);
+    k_b_to_plain32<<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, out);
+}
+
+void launch_plain32_to_x(const Bricks<float>& B, const float* in, cudaStream_t s) {
+    const dim3 blk = block_for(B.max2);
+    k_plain32_to_x<<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, in);
 }
 
 void launch_add_correction(const Bricks<double>& B, const Bricks<float>& E, cudaStream_t s) {

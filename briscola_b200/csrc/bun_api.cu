@@ -190,4 +190,15 @@ int bun_sumsq(long n, const double* x, int nblocks, double* part, double* out, v
     return status(sumsq_launch(n, x, part, nblocks, out, S(stream)));
 }
 
+int bun_rms_normalise(long n, const float* x, float sign, int nblocks, double* part, double* rms, float* y,
+                      void* stream) {
+    if (n < 1 || !x || nblocks < 1 || !part || !rms || !y) return BUN_BAD_ARG;
+    return status(rms_normalise_launch(n, x, sign, part, nblocks, rms, y, S(stream)));
+}
+
+int bun_rms_restore(long n, const float* y, double scale, const double* rms, float* x, void* stream) {
+    if (n < 1 || !y || !rms || !x) return BUN_BAD_ARG;
+    return status(rms_restore_launch(n, y, scale, rms, x, S(stream)));
+}
+
 }  // extern "C"

@@ -30,5 +30,8 @@ cudaError_t lap_residual_launch(int n0, int n1, int n2, const float* y, const fl
                                 cudaStream_t s);
 cudaError_t lap_add_launch(int n0, int n1, int n2, const float* g, float w, float* dy, cudaStream_t s);
 cudaError_t sumsq_launch(long n, const double* x, double* part, int nblocks, double* out, cudaStream_t s);
+cudaError_t rms_normalise_launch(long n, const float* x, float sign, double* part, int nblocks, double* rms,
+                                 float* y, cudaStream_t s);
+cudaError_t rms_restore_launch(long n, const float* y, double scale, const double* rms, float* x, cudaStream_t s);
 
 }  // namespace bun

@@ -448,6 +448,62 @@ cudaError_t lap_add_launch(int n0, int n1, int n2, const float* g, float w, floa
     return cudaGetLastError();
 }
 
+// ---- RMS normalisation with the scale kept on the device ---------------------
+// (for a network queued inside a captured graph: no host round trip)
+__global__ void __launch_bounds__(kBlock) k_sumsq32(long n, const float* __restrict__ x, double* __restrict__ part) {
+    __shared__ double sh[kBlock / 32];
+    double a = 0.0;
+    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
+        a += (double)x[q] * (double)x[q];
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) sh[warp] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int q = 0; q < kBlock / 32; ++q) t += sh[q];
+        part[blockIdx.x] = t;
+    }
+}
+
+// *rms = sqrt(sum of the parts / n), parts added in a fixed order
+__global__ void k_rms_final(const double* __restrict__ part, int nparts, long n, double* rms) {
+    double a = 0.0;
+    for (int q = threadIdx.x; q < nparts; q += 32) a += part[q];
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (threadIdx.x == 0) *rms = sqrt(a / (double)n);
+}
+
+// y = sign * x / rms (zero when rms is zero)
+__global__ void k_div_rms(long n, const float* __restrict__ x, float sign, const double* __restrict__ rms,
+                          float* __restrict__ y) {
+    const double r = *rms;
+    const float f = r > 0.0 ? (float)(sign / r) : 0.f;
+    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
+        y[q] = f * x[q];
+}
+
+// x = y * scale * rms
+__global__ void k_mul_rms(long n, const float* __restrict__ y, double scale, const double* __restrict__ rms,
+                          float* __restrict__ x) {
+    const float f = (float)(scale * *rms);
+    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
+        x[q] = f * y[q];
+}
+
+cudaError_t rms_normalise_launch(long n, const float* x, float sign, double* part, int nblocks, double* rms,
+                                 float* y, cudaStream_t s) {
+    k_sumsq32<<<(unsigned)nblocks, kBlock, 0, s>>>(n, x, part);
+    k_rms_final<<<1, 32, 0, s>>>(part, nblocks, n, rms);
+    k_div_rms<<<blocks_for(n), kBlock, 0, s>>>(n, x, sign, rms, y);
+    return cudaGetLastError();
+}
+
+cudaError_t rms_restore_launch(long n, const float* y, double scale, const double* rms, float* x, cudaStream_t s) {
+    k_mul_rms<<<blocks_for(n), kBlock, 0, s>>>(n, y, scale, rms, x);
+    return cudaGetLastError();
+}
+
 cudaError_t sumsq_launch(long n, const double* x, double* part, int nblocks, double* out, cudaStream_t s) {
     k_sumsq<<<(unsigned)nblocks, kBlock, 0, s>>>(n, x, part);
     k_sum_double<<<1, 32, 0, s>>>(part, nblocks, out);

@@ -11,6 +11,15 @@ output scaled back.  The U-Net (``unet.UNet``) trains on its own kernels.
 with the convergence test relative to ||b|| (``criterion rhs``), so the
 guess can only help by leaving less residual for the cycles to remove; the
 solver always finishes to tolerance.
+
+``CoarseCorrection`` puts a network trained on one level of the hierarchy
+in place of the multigrid recursion below that level (the restricted
+residual in, the level's correction out, then the level's post-smoothing;
+MG.C:77-99 is the recursion it replaces) in the FP32 cycles of a
+mixed-precision solve.  Its training pairs are the right-hand sides that
+level actually receives during solves of the sequence, with the level's
+exact solutions as targets (``CoarsePairSet``).  The outer FP64 loop still
+decides convergence, so the solve always finishes to tolerance.
 """
 from __future__ import annotations
 
@@ -186,3 +195,202 @@ def benchmark(N: int, n_pairs: int, steps: int, n_held: int, seed: int = 1, lr: 
             "learned_guess": {"ms_per_solve": round(e[1].elapsed_time(e[2]) / n_held, 3),
                               "cycles_mean": float(np.mean(cyc1)),
                               "guess_ms": round(e[2].elapsed_time(e[3]) / n_held, 3)}}
+
+
+def _copy_from_ptr(dst, ptr: int):
+    """dst (contiguous CUDA tensor) <- the device memory at ptr (same size)"""
+    import ctypes
+
+    import torch
+
+    n = dst.numel() * dst.element_size()
+    rc = torch.cuda.cudart().cudaMemcpy(ctypes.c_void_p(dst.data_ptr()), ctypes.c_void_p(ptr), n, 3)
+    if int(rc) != 0:
+        raise RuntimeError(f"cudaMemcpy failed: {rc}")
+
+
+def _copy_to_ptr(ptr: int, src):
+    """the device memory at ptr <- src (contiguous CUDA tensor)"""
+    import ctypes
+
+    import torch
+
+    n = src.numel() * src.element_size()
+    rc = torch.cuda.cudart().cudaMemcpy(ctypes.c_void_p(ptr), ctypes.c_void_p(src.data_ptr()), n, 3)
+    if int(rc) != 0:
+        raise RuntimeError(f"cudaMemcpy failed: {rc}")
+
+
+class CoarsePairSet:
+    """Normalised (input, target) pairs of one level of the N^3 cube's
+    hierarchy: the right-hand sides the level receives in the cycles of
+    mixed-precision flexible-CG solves of a Taylor-Green sequence (recorded
+    through the level-solver hook, without a graph), with the level's own
+    solutions (an exact solve on the level's grid) as targets.  While
+    recording, the hook answers with that exact solution, so the recorded
+    inputs are those of a cycle whose recursion below the level is exact --
+    the cycle the network imitates.  Same normalisation as PairSet: input
+    f / rms(f), target x / rms(f) / scale."""
+
+    def __init__(self, N: int, level: int, count: int, seed: int, device=None, skip: int = 0, every: int = 1):
+        import torch
+
+        dev = device or torch.device("cuda", torch.cuda.current_device())
+        self.N = N >> level  # the level's grid (training and residual loss)
+        n = self.N ** 3
+        V = (1.0 / self.N) ** 3
+        self.inputs = torch.zeros(count, n, dtype=torch.float32, device=dev)
+        self.targets = torch.zeros(count, n, dtype=torch.float32, device=dev)
+        exact = Context(cube_mesh(self.N), make_options(dict(TARGET_KEYS, device=dev.index or 0)))
+        xe = torch.zeros(n, dtype=torch.float64, device=dev)
+        self.count = 0
+
+        def record(stream, rhs, x, shape):
+            if shape != (self.N,) * 3:
+                raise ValueError(f"level shape {shape}, expected {(self.N,) * 3}")
+            torch.cuda.synchronize()  # the recording solve runs without a graph: the rhs is ready
+            r = torch.empty(n, dtype=torch.float32, device=dev)
+            _copy_from_ptr(r, rhs)
+            rep = exact.solve(r.double() * V, xe, zero_guess=True)  # the level's system form V b'
+            if rep.status != 0:
+                raise RuntimeError(f"level solve failed: status {rep.status}")
+            torch.cuda.synchronize()
+            _copy_to_ptr(x, xe.float().contiguous())
+            if self.count < count:
+                rms = float(torch.sqrt(torch.mean(r.double() ** 2)))
+                if rms > 0.0:
+                    self.inputs[self.count] = -r / rms
+                    self.targets[self.count] = (xe / rms).float()
+                    self.count += 1
+            torch.cuda.synchronize()
+
+        fine = Context(cube_mesh(N), make_options(dict(TARGET_KEYS, graph="off", device=dev.index or 0)))
+        fine.set_level_solver(level, record)
+        seq = workloads.TaylorGreenSequence(N, seed, dev)
+        for _ in range(skip):
+            seq.step()
+        xf = torch.zeros(N ** 3, dtype=torch.float64, device=dev)
+        while self.count < count:
+            rep = fine.solve(seq.rhs(), xf, zero_guess=True)
+            if fine._hook_error is not None:
+                raise fine._hook_error
+            if rep.status != 0:
+                raise RuntimeError(f"recording solve failed: status {rep.status}")
+            for _ in range(every):
+                seq.step()
+        fine.close()
+        exact.close()
+        self.scale = float(torch.sqrt(torch.mean(self.targets.double() ** 2)))
+        self.targets /= self.scale
+
+    def __len__(self):
+        return self.count
+
+
+class CoarseCorrection:
+    """A trained network as the solver of one level of a context's FP32
+    cycles (bmg_set_level_solver): the level's right-hand side in, the
+    network's solution (scaled back) out, then the level's post-smoothing."""
+
+    def __init__(self, net: U.UNet, ctx: Context, level: int, scale: float):
+        import torch
+
+        self.net = net
+        self.ctx = ctx
+        self.level = level
+        self.scale = scale
+        shape = tuple(ctx.shape(level))
+        if shape != net.shape:
+            raise ValueError(f"network grid {net.shape} is not level {level}'s {shape}")
+        # one eager call first: every kernel it queues is loaded before the
+        # solver's graph capture calls it
+        probe = torch.zeros(net.nvox[0], dtype=torch.float32, device=net.dev)
+        net.solve_level(torch.cuda.current_stream().cuda_stream, probe.data_ptr(), probe.data_ptr(), scale)
+        torch.cuda.synchronize()
+        ctx.set_level_solver(level, self._solve)
+
+    def _solve(self, stream, rhs, x, shape):
+        self.net.solve_level(stream, rhs, x, self.scale)
+
+    def remove(self):
+        self.ctx.set_level_solver(self.level, None)
+
+
+def benchmark_coarse(N: int, level: int, n_pairs: int, steps: int, n_held: int, seed: int = 1,
+                     lr: float = 1e-3):
+    """The learned coarse-level correction as one measurement: record and
+    train on n_pairs level-`level` pairs of one Taylor-Green sequence, then
+    time n_held held-out solves of another sequence (mixed precision,
+    flexible CG, ||b||-relative 1e-8) with the multigrid recursion below the
+    level and with the network in its place.  Returns timings (CUDA events)
+    and cycle counts."""
+    import time
+
+    import torch
+
+    t0 = time.perf_counter()
+    pairs = CoarsePairSet(N, level, n_pairs, seed=seed)
+    t_data = time.perf_counter() - t0
+    net = U.UNet((pairs.N,) * 3, seed=seed)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    losses = train(net, pairs, steps, lr=lr)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    scale = pairs.scale
+    del pairs
+    torch.cuda.empty_cache()
+    keys = dict(TARGET_KEYS, relTol=1e-8)
+    plain = Context(cube_mesh(N), make_options(keys))
+    learned_ctx = Context(cube_mesh(N), make_options(keys))
+    stream = torch.cuda.current_stream()
+    plain.set_stream(stream.cuda_stream)
+    learned_ctx.set_stream(stream.cuda_stream)
+    cc = CoarseCorrection(net, learned_ctx, level, scale)
+    seq = workloads.TaylorGreenSequence(N, seed + 1000, torch.device("cuda", torch.cuda.current_device()))
+    for _ in range(17):
+        seq.step()
+    held = []
+    for _ in range(n_held):
+        held.append(seq.rhs().clone())
+        for _ in range(3):
+            seq.step()
+    x = torch.zeros(N ** 3, dtype=torch.float64, device=net.dev)
+    for q in range(min(3, n_held)):  # warm-up (graph capture)
+        plain.solve(held[q], x, zero_guess=True)
+        learned_ctx.solve(held[q], x, zero_guess=True)
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    cyc0, cyc1, res1 = [], [], []
+    torch.cuda.synchronize()
+    e[0].record(stream)
+    for q in range(n_held):
+        cyc0.append(plain.solve(held[q], x, zero_guess=True).cycles)
+    e[1].record(stream)
+    for q in range(n_held):
+        rep = learned_ctx.solve(held[q], x, zero_guess=True)
+        cyc1.append(rep.cycles)
+        res1.append(rep.rhs_rel_residual)
+    e[2].record(stream)
+    torch.cuda.synchronize()
+    net.check_errors()
+    # the network alone, once per cycle of the learned solves
+    e2 = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    rhs = torch.randn(net.nvox[0], device=net.dev)
+    out = torch.empty_like(rhs)
+    e2[0].record(stream)
+    for _ in range(20):
+        net.solve_level(stream.cuda_stream, rhs.data_ptr(), out.data_ptr(), scale)
+    e2[1].record(stream)
+    torch.cuda.synchronize()
+    cc.remove()
+    plain.close()
+    learned_ctx.close()
+    return {"grid": [N] * 3, "level": level, "level_grid": [N >> level] * 3, "training_pairs": n_pairs,
+            "training_steps": steps, "held_out": n_held, "data_s": round(t_data, 1), "train_s": round(t_train, 1),
+            "final_loss": float(np.mean(losses[-50:])),
+            "multigrid_below_level": {"ms_per_solve": round(e[0].elapsed_time(e[1]) / n_held, 3),
+                                      "cycles_mean": float(np.mean(cyc0))},
+            "learned_coarse_correction": {"ms_per_solve": round(e[1].elapsed_time(e[2]) / n_held, 3),
+                                          "cycles_mean": float(np.mean(cyc1)),
+                                          "max_rhs_rel_residual": float(np.max(res1)),
+                                          "network_ms": round(e2[0].elapsed_time(e2[1]) / 20, 3)}}

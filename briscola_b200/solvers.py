@@ -261,6 +261,29 @@ class Context:
         if getattr(self, "_stream", None) != cur:
             self.set_stream(cur)
 
+    def set_level_solver(self, level: int, fn=None):
+        """fn(stream, rhs_ptr, x_ptr, n) -> None in place of the FP32 cycle's
+        recursion below `level` (bmg_set_level_solver); None removes it.  fn
+        queues its work on `stream` (an int cudaStream_t) and must neither
+        synchronise nor allocate inside a graphed solve."""
+        if fn is None:
+            self.check(self._lib.bmg_set_level_solver(self.h, level, N.LEVEL_SOLVER(), None), "bmg_set_level_solver")
+            self._hook = None
+            return
+
+        def call(user, stream, rhs, x, n):
+            try:
+                fn(stream or 0, rhs, x, (n[0], n[1], n[2]))
+                return 0
+            except Exception as e:  # reported through the solve's status
+                self._hook_error = e
+                return 1
+
+        hook = N.LEVEL_SOLVER(call)
+        self._hook_error = None
+        self.check(self._lib.bmg_set_level_solver(self.h, level, hook, None), "bmg_set_level_solver")
+        self._hook = hook  # kept alive with the context
+
     def set_stream(self, stream_ptr: int):
         self.check(self._lib.bmg_set_stream(self.h, ctypes.c_void_p(stream_ptr)), "bmg_set_stream")
         self._stream = stream_ptr

@@ -80,6 +80,8 @@ def load(path: str = LIB_PATH):
         "bun_scale_to_float": [l, vp, d, vp, vp],
         "bun_scale_to_double": [l, vp, d, vp, vp],
         "bun_sumsq": [l, vp, i, vp, vp, vp],
+        "bun_rms_normalise": [l, vp, f, i, vp, vp, vp, vp],
+        "bun_rms_restore": [l, vp, d, vp, vp, vp],
         "bun_laplace_residual": [i, i, i, vp, vp, f, vp, vp],
         "bun_laplace_add": [i, i, i, vp, f, vp, vp],
         "bun_conv3_stage_width": [i, i, i, i],
@@ -97,6 +99,7 @@ def load(path: str = LIB_PATH):
 EXPORTED = ("bun_conv3", "bun_conv3_wgrad", "bun_wgrad_part_floats", "bun_pack_weights", "bun_conv_in",
             "bun_conv_in_wgrad", "bun_head", "bun_head_grad", "bun_pool", "bun_unpool_grad", "bun_skip_grad",
             "bun_mse", "bun_adam", "bun_scale_to_float", "bun_scale_to_double", "bun_sumsq",
+            "bun_rms_normalise", "bun_rms_restore",
             "bun_laplace_residual", "bun_laplace_add", "bun_conv3_stage_width")
 
 
@@ -274,10 +277,14 @@ class UNet:
         self.part = torch.zeros(part, dtype=f32, device=dev)
         self.dpart = torch.zeros(self.red_blocks, dtype=torch.float64, device=dev)
         self.dsum = torch.zeros(1, dtype=torch.float64, device=dev)
+        self.rms = torch.zeros(1, dtype=torch.float64, device=dev)  # input scale kept on the device
+        self.stream = None  # a cudaStream_t (int) to queue on instead of torch's current stream
         self.pack()
 
     # -- helpers -------------------------------------------------------------
     def _s(self):
+        if self.stream is not None:
+            return ctypes.c_void_p(self.stream)
         return ctypes.c_void_p(self.torch.cuda.current_stream().cuda_stream)
 
     def _w(self, name, buf=None):
@@ -461,6 +468,25 @@ class UNet:
         return net, meta
 
     # -- the solver's view ---------------------------------------------------
+    def solve_level(self, stream: int, rhs: int, x: int, scale: float) -> None:
+        """The network as a level's solver (bmg_set_level_solver): rhs and x
+        are device pointers to the level's FP32 interior cells, rhs the
+        row-scaled right-hand side b/V = -f.  The input is f / rms(f) and
+        x = scale * rms(f) * output, with rms(f) kept on the device, so every
+        kernel is queued on `stream` and nothing returns to the host (the
+        calls may be captured into the solver's graph)."""
+        L = self.L
+        n = self.nvox[0]
+        self.stream = stream
+        try:
+            _check(L.bun_rms_normalise(n, ctypes.c_void_p(rhs), -1.0, self.red_blocks, self.dpart.data_ptr(),
+                                       self.rms.data_ptr(), self.x.data_ptr(), self._s()), "rms_normalise")
+            self.forward()
+            _check(L.bun_rms_restore(n, self.y.data_ptr(), scale, self.rms.data_ptr(), ctypes.c_void_p(x),
+                                     self._s()), "rms_restore")
+        finally:
+            self.stream = None
+
     def guess(self, b, V: float, x0, scale: float = 1.0):
         """Initial guess x0 (FP64 device) for the system right-hand side b
         (FP64 device, b = -V f on a uniform grid of cell volume V); scale:

@@ -247,6 +247,30 @@ int bmg_project_rhs(struct bmg_ctx* ctx, const double* u0, const double* u1, con
 int bmg_project_correct(struct bmg_ctx* ctx, double* u0, double* u1, double* u2, const double* p,
                         const double* lam0, const double* lam1, const double* lam2, double c_dt);
 
+/* ---- A level solver in place of the cycle's coarse recursion ---------------
+ * No counterpart in the reference: the learned coarse-level correction.  In
+ * the cycle MG.C:19-130 a level l > 0 receives the restricted residual as
+ * its right-hand side and returns the correction its sub-cycle computes
+ * (MG.C:77-99).  With a level solver set at level l, the FP32 cycles of a
+ * mixed-precision solve (precision mixed) instead hand that level's
+ * right-hand side to fn and take fn's result as the level's correction,
+ * then post-smooth it (nSweepsPost sweeps); the levels below l are not
+ * visited.  FP64 cycles keep the multigrid recursion.
+ *
+ * fn(user, stream, rhs, x, n) is called on the host while the cycle is
+ * being launched: rhs and x are device arrays of the level's interior
+ * cells (n[0]*n[1]*n[2] floats, k fastest), rhs the row-scaled right-hand
+ * side b/V of the level (equal to -f for a Poisson source f), x to be
+ * filled with the correction.  fn must queue all its work on `stream` (a
+ * cudaStream_t) and neither synchronise nor allocate: inside a graphed
+ * solve it runs while the solve graph is being captured, and its kernels
+ * become part of the graph.  A nonzero return aborts the solve with
+ * BMG_CUDA_ERROR.  Single-brick meshes, 1 <= level <= the coarse solve
+ * level; fn NULL removes the solver.  The context keeps two level-sized
+ * FP32 arrays for rhs and x. */
+typedef int (*bmg_level_solver)(void* user, void* stream, const float* rhs, float* x, const int n[3]);
+int bmg_set_level_solver(struct bmg_ctx* ctx, int level, bmg_level_solver fn, void* user);
+
 /* ---- Residual norm without any device allocation ---------------------------
  * No counterpart in the reference: an addition for callers that must not
  * call cudaMalloc when they want a residual -- an application whose device

@@ -113,6 +113,14 @@ int bun_scale_to_float(long n, const double* x, double scale, float* y, void* st
 int bun_scale_to_double(long n, const float* x, double scale, double* y, void* stream);
 /* *out = sum x^2 (FP64, fixed order); part: nblocks doubles of scratch */
 int bun_sumsq(long n, const double* x, int nblocks, double* part, double* out, void* stream);
+/* The network's input from a field of any size, with the scale kept on the
+ * device (nothing returns to the host, so the calls can be captured into a
+ * CUDA graph): *rms = sqrt(sum x^2 / n) (FP64, fixed order; part: nblocks
+ * doubles of scratch) and y = sign * x / *rms (zero when *rms is zero);
+ * then, for the output, x = scale * *rms * y. */
+int bun_rms_normalise(long n, const float* x, float sign, int nblocks, double* part, double* rms, float* y,
+                      void* stream);
+int bun_rms_restore(long n, const float* y, double scale, const double* rms, float* x, void* stream);
 
 #ifdef __cplusplus
 }

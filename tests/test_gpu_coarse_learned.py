@@ -1,0 +1,127 @@
+"""The level solver (bmg_set_level_solver) and the learned coarse-level
+correction built on it (learned.CoarseCorrection): a network trained on the
+right-hand sides one level of the hierarchy receives takes the place of the
+multigrid recursion below that level in the FP32 cycles of a mixed-precision
+solve.  The outer FP64 flexible-CG loop still decides convergence."""
+import numpy as np
+import pytest
+
+import briscola_b200 as bb
+from briscola_b200 import learned, unet, workloads
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+KEYS = dict(learned.TARGET_KEYS, relTol=1e-8)
+
+
+@pytest.fixture(scope="module")
+def built():
+    from briscola_b200.build import build_unet
+
+    build_unet()
+    unet.load()
+
+
+def test_level_solver_contract(native):
+    """The hook sees the level's shape and a compatible right-hand side (the
+    all-wall system's level sums vanish), its result becomes the level's
+    correction, and an exact level solve as the hook converges at least as
+    fast as the multigrid recursion it replaces."""
+    N, level = 64, 1
+    mesh = learned.cube_mesh(N)
+    plain = bb.Context(mesh, bb.make_options(dict(KEYS, graph="off")))
+    hooked = bb.Context(mesh, bb.make_options(dict(KEYS, graph="off")))
+    exact = bb.Context(learned.cube_mesh(N >> level), bb.make_options(dict(learned.TARGET_KEYS, relTol=1e-12)))
+    n = (N >> level) ** 3
+    V = (1.0 / (N >> level)) ** 3
+    seen = []
+
+    def exact_level(stream, rhs, x, shape):
+        torch.cuda.synchronize()
+        r = torch.empty(n, dtype=torch.float32, device="cuda")
+        learned._copy_from_ptr(r, rhs)
+        seen.append((shape, float(r.double().sum() / r.double().abs().sum())))
+        xe = torch.zeros(n, dtype=torch.float64, device="cuda")
+        rep = exact.solve(r.double() * V, xe, zero_guess=True)
+        assert rep.status == 0
+        torch.cuda.synchronize()
+        learned._copy_to_ptr(x, xe.float().contiguous())
+
+    hooked.set_level_solver(level, exact_level)
+    b = workloads.TaylorGreenSequence(N, 3, torch.device("cuda", 0)).rhs()
+    x0, x1 = torch.zeros_like(b), torch.zeros_like(b)
+    r0 = plain.solve(b, x0, zero_guess=True)
+    r1 = hooked.solve(b, x1, zero_guess=True)
+    assert hooked._hook_error is None
+    assert r0.status == 0 and r1.status == 0 and r1.rhs_rel_residual <= 1e-8
+    assert seen and all(s == (N >> level,) * 3 for s, _ in seen)
+    assert all(abs(q) <= 1e-5 for _, q in seen)  # compatible: the level's sum vanishes
+    assert r1.cycles <= r0.cycles
+    d = (x0 - x0.mean()) - (x1 - x1.mean())
+    assert float(d.norm() / (x0 - x0.mean()).norm()) <= 1e-5
+    # removing the hook restores the plain cycle exactly
+    hooked.set_level_solver(level, None)
+    x2 = torch.zeros_like(b)
+    r2 = hooked.solve(b, x2, zero_guess=True)
+    assert r2.cycles == r0.cycles and torch.equal(x2, x0)
+
+
+def test_level_solver_rejects_bad_levels(native):
+    c = bb.Context(learned.cube_mesh(32), bb.make_options(dict(KEYS)))
+    with pytest.raises(bb.FatalError):
+        c.set_level_solver(0, lambda *a: None)
+    with pytest.raises(bb.FatalError):
+        c.set_level_solver(c.num_levels, lambda *a: None)
+
+
+@pytest.fixture(scope="module")
+def coarse_net(built):
+    """a network for level 1 (64^3) of the 128^3 cube, trained on 160
+    recorded level pairs of one Taylor-Green sequence"""
+    pairs = learned.CoarsePairSet(128, 1, 160, seed=1)
+    net = unet.UNet((64,) * 3, seed=0)
+    losses = learned.train(net, pairs, steps=600, lr=2e-3)
+    return net, pairs.scale, losses
+
+
+def test_learned_coarse_correction(native, coarse_net):
+    """The network in place of the recursion below level 1: graphed and
+    eager solves agree bit for bit (the network's kernels are captured into
+    the solve graph), the solve always reaches 1e-8 of ||b||, and the
+    network's level solutions are closer to the exact ones than zero."""
+    net, scale, losses = coarse_net
+    assert np.mean(losses[-50:]) < np.mean(losses[:50])
+    N, level = 128, 1
+    mesh = learned.cube_mesh(N)
+    seq = workloads.TaylorGreenSequence(N, 1001, torch.device("cuda", 0))
+    for _ in range(7):
+        seq.step()
+    b = seq.rhs().clone()
+    out = {}
+    for graph in ("on", "off"):
+        c = bb.Context(mesh, bb.make_options(dict(KEYS, graph=graph, maxIter=100)))
+        cc = learned.CoarseCorrection(net, c, level, scale)
+        x = torch.zeros_like(b)
+        rep = c.solve(b, x, zero_guess=True)
+        rep2 = c.solve(b, torch.zeros_like(b), zero_guess=True)  # replayed graph
+        assert c._hook_error is None
+        assert rep.status == 0 and rep.rhs_rel_residual <= 1e-8, (graph, rep.status, rep.rhs_rel_residual)
+        assert rep2.cycles == rep.cycles
+        out[graph] = (x, rep.cycles)
+        cc.remove()
+        c.close()
+    assert out["on"][1] == out["off"][1] and torch.equal(out["on"][0], out["off"][0])
+    # the network as a level solver on held-out level pairs: relative error < 1
+    held = learned.CoarsePairSet(N, level, 8, seed=77)
+    errs = []
+    for q in range(len(held)):
+        rhs = (-held.inputs[q]).contiguous()  # the level's b/V for a unit-rms f
+        y = torch.empty_like(rhs)
+        net.solve_level(torch.cuda.current_stream().cuda_stream, rhs.data_ptr(), y.data_ptr(), scale)
+        t = held.targets[q] * held.scale
+        errs.append(float((y - y.mean() - (t - t.mean())).norm() / (t - t.mean()).norm()))
+    torch.cuda.synchronize()
+    print("held-out level errors", errs)
+    assert max(errs) < 1.0, errs
