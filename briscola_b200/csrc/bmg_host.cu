@@ -265,11 +265,13 @@ void buildTables(HostLevel& L, const int dirichlet[6]) {
             to.h[d] = off;
             off = next(off, B.n[d]);
         }
-        to.kwl = to.kwh = -1;
+        to.kwl = to.kwh = to.ksz = -1;
         if (L.ks) {
             to.kwl = off;
             off = next(off, B.n[2]);
             to.kwh = off;
+            off = next(off, B.n[2]);
+            to.ksz = off;
             off = next(off, B.n[2]);
         }
         to.total = off;
@@ -293,6 +295,7 @@ void buildTables(HostLevel& L, const int dirichlet[6]) {
             for (int k = 0; k < B.n[2]; ++k) {
                 L.tab[to.kwl + kposSplit(k, B.n[2])] = L.tab[to.wl[2] + k];
                 L.tab[to.kwh + kposSplit(k, B.n[2])] = L.tab[to.wh[2] + k];
+                L.tab[to.ksz + kposSplit(k, B.n[2])] = L.tab[to.h[2] + k];
             }
     }
 }

@@ -42,6 +42,7 @@ struct TabOff {
     int h[3];    // cell sizes (volume factors)
     int kwl, kwh;  // parity-split levels: the k couplings in the row's storage
                    // order (entry kpos(k) holds wl[2] / wh[2] of k); -1 otherwise
+    int ksz;       // ... and the cell sizes along k (h[2]) in the same order
     int total;
 };
 

@@ -652,7 +652,8 @@ __global__ void __launch_bounds__(256) k_restrict_quad(Bricks<T> FB, Bricks<T> C
 // bit-identical.
 // ---------------------------------------------------------------------------
 template <typename T, bool VAR>
-__global__ void __launch_bounds__(256) k_restrict_split(Bricks<T> FB, Bricks<T> CB, TransferSet ts) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 && !VAR ? 3 : 2) k_restrict_split(Bricks<T> FB, Bricks<T> CB,
+                                                                                   TransferSet ts) {
     const LevelView<T>& F = FB.v[0];
     const LevelView<T>& C = CB.v[0];
     const TransferTabs& t = ts.t[0];
@@ -667,20 +668,37 @@ __global__ void __launch_bounds__(256) k_restrict_split(Bricks<T> FB, Bricks<T> 
     else
         ratio = reinterpret_cast<const T*>(t.ratio32);
     const int m0 = 4 * P;
-    // k couplings and k shares of the even (k = 2(m0+m)) and odd cells
+    // k couplings and k shares of the even (k = 2(m0+m)) and odd cells: the
+    // eight consecutive k = 8P .. 8P+7 of the natural tables, as vectors
     T wke[4], whe[4], wko[4], who[4], rke[4], rko[4];
+    {
+        T a[8], b[8], r[8];
+        Row4<T>::ldg4(F.tab + F.to.wl[2] + 2 * m0, a);
+        Row4<T>::ldg4(F.tab + F.to.wl[2] + 2 * m0 + 4, a + 4);
+        Row4<T>::ldg4(F.tab + F.to.wh[2] + 2 * m0, b);
+        Row4<T>::ldg4(F.tab + F.to.wh[2] + 2 * m0 + 4, b + 4);
+        const T* rp = ratio + F.n0 + F.n1 + 2 * m0;
+        if (((F.n0 + F.n1) & 3) == 0) {  // 16-byte aligned: two vectors
+            Row4<T>::ldg4(rp, r);
+            Row4<T>::ldg4(rp + 4, r + 4);
+        } else {
 #pragma unroll
-    for (int m = 0; m < 4; ++m) {
-        const int k = 2 * (m0 + m);
-        wke[m] = ldg(F.tab + F.to.wl[2] + k);
-        whe[m] = ldg(F.tab + F.to.wh[2] + k);
-        wko[m] = ldg(F.tab + F.to.wl[2] + k + 1);
-        who[m] = ldg(F.tab + F.to.wh[2] + k + 1);
-        rke[m] = ldg(ratio + F.n0 + F.n1 + k);
-        rko[m] = ldg(ratio + F.n0 + F.n1 + k + 1);
+            for (int q = 0; q < 8; ++q) r[q] = ldg(rp + q);
+        }
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            wke[m] = a[2 * m];
+            wko[m] = a[2 * m + 1];
+            whe[m] = b[2 * m];
+            who[m] = b[2 * m + 1];
+            rke[m] = r[2 * m];
+            rko[m] = r[2 * m + 1];
+        }
     }
     T acc[4] = {T(0), T(0), T(0), T(0)};
-#pragma unroll
+    // FP64 and variable-coefficient rows hold twice the registers: one fine
+    // plane at a time there
+#pragma unroll(sizeof(T) == 4 && !VAR ? 2 : 1)
     for (int a = 0; a < 2; ++a) {
         const int i = 2 * I + a;
         const T ra = ldg(ratio + i);
@@ -785,12 +803,22 @@ __global__ void __launch_bounds__(256) k_prolong_split(Bricks<T> FB, Bricks<T> C
     const int Klo = kpos(C, ldg(pk + 2 * (2 * m0) + 1));
     const int Khi = kpos(C, ldg(pk + 2 * (2 * m0 + 7) + 1));
     T we[4], ue[4], wo[4], uo[4];
+    {
+        T a[8];  // the weights of k = 8P .. 8P+7 (natural order, contiguous)
+        if (((F.n0 + F.n1) & 3) == 0) {  // 16-byte aligned: two vectors
+            Row4<T>::ldg4(wk + 2 * m0, a);
+            Row4<T>::ldg4(wk + 2 * m0 + 4, a + 4);
+        } else {
 #pragma unroll
-    for (int m = 0; m < 4; ++m) {
-        we[m] = ldg(wk + 2 * (m0 + m));
-        wo[m] = ldg(wk + 2 * (m0 + m) + 1);
-        ue[m] = T(1) - we[m];
-        uo[m] = T(1) - wo[m];
+            for (int q = 0; q < 8; ++q) a[q] = ldg(wk + 2 * m0 + q);
+        }
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            we[m] = a[2 * m];
+            wo[m] = a[2 * m + 1];
+            ue[m] = T(1) - we[m];
+            uo[m] = T(1) - wo[m];
+        }
     }
     const int rows[4] = {cell32(C, I0, J0, 0), cell32(C, I0, J1, 0), cell32(C, I1, J0, 0), cell32(C, I1, J1, 0)};
     T ve[4][4], vo[4][4];

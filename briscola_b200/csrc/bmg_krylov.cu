@@ -342,7 +342,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_direction4(Bricks<double
 // beyond them (as in k_colour_split).  Per cell the arithmetic is
 // k_fcg_direction4's; the partial sums group the cells differently.
 template <typename T, bool VAR>
-__global__ void __launch_bounds__(kReduceThreads) k_fcg_direction_split(Bricks<double> B, const T* z, double* p,
+__global__ void __launch_bounds__(kReduceThreads, VAR ? 2 : 3) k_fcg_direction_split(Bricks<double> B, const T* z, double* p,
                                                                         double* q, double* partials,
                                                                         const SolveState* st) {
     __shared__ double sh[kReduceThreads / 32];
@@ -355,6 +355,8 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_direction_split(Bricks<d
     if (j < L.n1 && 4 * qx < L.n2) {
         const int h = 4 * qx >= kh ? 1 : 0;
         const int m0 = 4 * qx - h * kh;
+        const double wjl = L.tab64[L.to.wl[1] + j], wjh = L.tab64[L.to.wh[1] + j];
+        const double hj = L.tab64[L.to.h[1] + j];
         for (int i = blockIdx.z; i < L.n0; i += gridDim.z) {
             const long row = row_at(L, i, j), c = row + 4 * qx;
             const long co = row + (1 - h) * kh + m0;  // the other half, same slots
@@ -370,12 +372,35 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_direction_split(Bricks<d
             double pq[4], qq[4], pn[4], qn[4];
             Quad4<double>::ld(p + c, 0, pq);
             Quad4<double>::ld(q + c, 0, qq);
-            const double hij = L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j];
+            const double wil = L.tab64[L.to.wl[0] + i], wih = L.tab64[L.to.wh[0] + i];
+            const double hij = L.tab64[L.to.h[0] + i] * hj;
+            // k couplings and cell sizes of the four cells, from the tables
+            // kept in the rows' storage order (contiguous)
+            double wkl[4], wkh[4], hk[4];
+            Quad4<double>::ld(L.tab64 + L.to.kwl + 4 * qx, 0, wkl);
+            Quad4<double>::ld(L.tab64 + L.to.kwh + 4 * qx, 0, wkh);
+            Quad4<double>::ld(L.tab64 + L.to.ksz + 4 * qx, 0, hk);
+            double l0[4], l0p[4], l1[4], l1p[4], l2[4], l2o[4], l2e = 1.0;
+            if (VAR) {
+                Quad4<double>::ld(L.lam0 + c, 0, l0);
+                Quad4<double>::ld(L.lam0 + c + L.si, 0, l0p);
+                Quad4<double>::ld(L.lam1 + c, 0, l1);
+                Quad4<double>::ld(L.lam1 + c + L.sj, 0, l1p);
+                Quad4<double>::ld(L.lam2 + c, 0, l2);
+                Quad4<double>::ld(L.lam2 + co, 0, l2o);  // lower faces of the other half's slots
+                l2e = L.lam2[ce];
+            }
             for (int e = 0; e < 4; ++e) {
-                const int k = 2 * (m0 + e) + h;
-                double w[6];
-                const long ckp = h == 0 ? co + e : (e < 3 ? co + e + 1 : ce);
-                couplings<double, VAR>(L, i, j, k, c + e, ckp, w);
+                // the couplings of couplings(): l, r, b, t, a, f
+                double w[6] = {wil, wih, wjl, wjh, wkl[e], wkh[e]};
+                if (VAR) {
+                    w[0] *= l0[e];
+                    w[1] *= l0p[e];
+                    w[2] *= l1[e];
+                    w[3] *= l1p[e];
+                    w[4] *= l2[e];
+                    w[5] *= h == 0 ? l2o[e] : (e < 3 ? l2o[e + 1] : l2e);
+                }
                 const double km = h == 0 ? (double)(e == 0 ? ze : zo[e - 1]) : (double)zo[e];
                 const double kp = h == 0 ? (double)zo[e] : (double)(e == 3 ? ze : zo[e + 1]);
                 const double zz = (double)zc[e];
@@ -384,7 +409,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_direction_split(Bricks<d
                 const double d = w[0] + w[1] + w[2] + w[3] + w[4] + w[5];
                 pn[e] = beta != 0.0 ? zz + beta * pq[e] : zz;
                 qn[e] = beta != 0.0 ? (sv - d * zz) + beta * qq[e] : sv - d * zz;
-                a += (hij * L.tab64[L.to.h[2] + k]) * pn[e] * qn[e];
+                a += (hij * hk[e]) * pn[e] * qn[e];
             }
             Quad4<double>::st(p + c, 0, pn);
             Quad4<double>::st(q + c, 0, qn);

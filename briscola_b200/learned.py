@@ -241,7 +241,7 @@ class CoarsePairSet:
         V = (1.0 / self.N) ** 3
         self.inputs = torch.zeros(count, n, dtype=torch.float32, device=dev)
         self.targets = torch.zeros(count, n, dtype=torch.float32, device=dev)
-        exact = Context(cube_mesh(self.N), make_options(dict(TARGET_KEYS, device=dev.index or 0)))
+        exact = Context(cube_mesh(self.N), make_options(dict(TARGET_KEYS, precision="fp64", device=dev.index or 0)))
         xe = torch.zeros(n, dtype=torch.float64, device=dev)
         self.count = 0
 
@@ -272,8 +272,6 @@ class CoarsePairSet:
         xf = torch.zeros(N ** 3, dtype=torch.float64, device=dev)
         while self.count < count:
             rep = fine.solve(seq.rhs(), xf, zero_guess=True)
-            if fine._hook_error is not None:
-                raise fine._hook_error
             if rep.status != 0:
                 raise RuntimeError(f"recording solve failed: status {rep.status}")
             for _ in range(every):

@@ -292,6 +292,10 @@ class Context:
         rep = N.Report()
         rc = self._lib.bmg_solve(self.h, ctypes.c_void_p(b_ptr), ctypes.c_void_p(x_ptr), flags,
                                  ctypes.byref(rep))
+        err = getattr(self, "_hook_error", None)
+        if err is not None:  # the level solver raised: report its own exception
+            self._hook_error = None
+            raise FatalError(f"bmg_solve: the level solver raised {err!r}") from err
         if rc in (N.BAD_ARG, N.CUDA_ERROR, N.UNSUPPORTED, N.NO_DEVICE):
             self.check(rc, "bmg_solve")
         rep.status = rc
