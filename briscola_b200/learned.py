@@ -197,28 +197,32 @@ def benchmark(N: int, n_pairs: int, steps: int, n_held: int, seed: int = 1, lr: 
                               "guess_ms": round(e[2].elapsed_time(e[3]) / n_held, 3)}}
 
 
-def _copy_from_ptr(dst, ptr: int):
-    """dst (contiguous CUDA tensor) <- the device memory at ptr (same size)"""
-    import ctypes
+class _DeviceArray:
+    """A raw device pointer as an object torch can view without a copy."""
 
+    def __init__(self, ptr: int, n: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (int(ptr), False),
+                                         "version": 3, "strides": None}
+
+
+def device_view(ptr: int, n: int, dtype=None):
+    """A torch CUDA tensor aliasing n elements at the device pointer ptr
+    (FP32 unless dtype says otherwise)."""
     import torch
 
-    n = dst.numel() * dst.element_size()
-    rc = torch.cuda.cudart().cudaMemcpy(ctypes.c_void_p(dst.data_ptr()), ctypes.c_void_p(ptr), n, 3)
-    if int(rc) != 0:
-        raise RuntimeError(f"cudaMemcpy failed: {rc}")
+    dtype = dtype or torch.float32
+    typestr = {torch.float32: "<f4", torch.float64: "<f8"}[dtype]
+    return torch.as_tensor(_DeviceArray(ptr, n, typestr), device="cuda")
+
+
+def _copy_from_ptr(dst, ptr: int):
+    """dst (contiguous CUDA tensor) <- the device memory at ptr (same size and type)"""
+    dst.copy_(device_view(ptr, dst.numel(), dst.dtype))
 
 
 def _copy_to_ptr(ptr: int, src):
     """the device memory at ptr <- src (contiguous CUDA tensor)"""
-    import ctypes
-
-    import torch
-
-    n = src.numel() * src.element_size()
-    rc = torch.cuda.cudart().cudaMemcpy(ctypes.c_void_p(ptr), ctypes.c_void_p(src.data_ptr()), n, 3)
-    if int(rc) != 0:
-        raise RuntimeError(f"cudaMemcpy failed: {rc}")
+    device_view(ptr, src.numel(), src.dtype).copy_(src)
 
 
 class CoarsePairSet:
@@ -288,15 +292,23 @@ class CoarsePairSet:
 class CoarseCorrection:
     """A trained network as the solver of one level of a context's FP32
     cycles (bmg_set_level_solver): the level's right-hand side in, the
-    network's solution (scaled back) out, then the level's post-smoothing."""
+    network's solution (scaled back) out, then the level's post-smoothing.
 
-    def __init__(self, net: U.UNet, ctx: Context, level: int, scale: float):
+    The network makes the preconditioner nonlinear, and flexible CG can
+    stall with it short of the tolerance; ``solve`` therefore gives the
+    learned solve ctx's maxIter and, if it has not converged, finishes from
+    its x with ``fallback`` -- a context of the same mesh and keys with the
+    plain multigrid recursion -- so every solve reaches the tolerance."""
+
+    def __init__(self, net: U.UNet, ctx: Context, level: int, scale: float, fallback: Context | None = None):
         import torch
 
         self.net = net
         self.ctx = ctx
         self.level = level
         self.scale = scale
+        self.fallback = fallback
+        self.fallbacks = 0
         shape = tuple(ctx.shape(level))
         if shape != net.shape:
             raise ValueError(f"network grid {net.shape} is not level {level}'s {shape}")
@@ -309,6 +321,19 @@ class CoarseCorrection:
 
     def _solve(self, stream, rhs, x, shape):
         self.net.solve_level(stream, rhs, x, self.scale)
+
+    def solve(self, b, x, zero_guess: bool = True):
+        """the learned solve, then (when it stopped short) the plain one from
+        its x; returns (report of the last solve, total cycles)"""
+        from . import _native as N
+
+        rep = self.ctx.solve(b, x, zero_guess=zero_guess)
+        cycles = rep.cycles
+        if rep.status == N.NOT_CONVERGED and self.fallback is not None:
+            self.fallbacks += 1
+            rep = self.fallback.solve(b, x, zero_guess=False)
+            cycles += rep.cycles
+        return rep, cycles
 
     def remove(self):
         self.ctx.set_level_solver(self.level, None)
@@ -340,11 +365,8 @@ def benchmark_coarse(N: int, level: int, n_pairs: int, steps: int, n_held: int, 
     torch.cuda.empty_cache()
     keys = dict(TARGET_KEYS, relTol=1e-8)
     plain = Context(cube_mesh(N), make_options(keys))
-    learned_ctx = Context(cube_mesh(N), make_options(keys))
     stream = torch.cuda.current_stream()
     plain.set_stream(stream.cuda_stream)
-    learned_ctx.set_stream(stream.cuda_stream)
-    cc = CoarseCorrection(net, learned_ctx, level, scale)
     seq = workloads.TaylorGreenSequence(N, seed + 1000, torch.device("cuda", torch.cuda.current_device()))
     for _ in range(17):
         seq.step()
@@ -356,7 +378,14 @@ def benchmark_coarse(N: int, level: int, n_pairs: int, steps: int, n_held: int, 
     x = torch.zeros(N ** 3, dtype=torch.float64, device=net.dev)
     for q in range(min(3, n_held)):  # warm-up (graph capture)
         plain.solve(held[q], x, zero_guess=True)
-        learned_ctx.solve(held[q], x, zero_guess=True)
+    cyc_plain = plain.solve(held[0], x, zero_guess=True).cycles
+    # the learned solve gets twice the plain solve's cycles before the fallback
+    learned_ctx = Context(cube_mesh(N), make_options(dict(keys, maxIter=2 * cyc_plain)))
+    learned_ctx.set_stream(stream.cuda_stream)
+    cc = CoarseCorrection(net, learned_ctx, level, scale, fallback=plain)
+    for q in range(min(3, n_held)):
+        cc.solve(held[q], x)
+    cc.fallbacks = 0
     e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
     cyc0, cyc1, res1 = [], [], []
     torch.cuda.synchronize()
@@ -365,8 +394,8 @@ def benchmark_coarse(N: int, level: int, n_pairs: int, steps: int, n_held: int, 
         cyc0.append(plain.solve(held[q], x, zero_guess=True).cycles)
     e[1].record(stream)
     for q in range(n_held):
-        rep = learned_ctx.solve(held[q], x, zero_guess=True)
-        cyc1.append(rep.cycles)
+        rep, cyc = cc.solve(held[q], x)
+        cyc1.append(cyc)
         res1.append(rep.rhs_rel_residual)
     e[2].record(stream)
     torch.cuda.synchronize()
@@ -381,6 +410,27 @@ def benchmark_coarse(N: int, level: int, n_pairs: int, steps: int, n_held: int, 
     e2[1].record(stream)
     torch.cuda.synchronize()
     cc.remove()
+    # the bound for any network: the level solved exactly (eager, cycles only)
+    exact_cycles = []
+    n_l = (N >> level) ** 3
+    V_l = (N >> level) ** -3.0
+    exact = Context(cube_mesh(N >> level), make_options(dict(TARGET_KEYS, relTol=1e-10, precision="fp64")))
+    bound = Context(cube_mesh(N), make_options(dict(keys, graph="off")))
+
+    def exact_level(stream_, rhs_, x_, shape):
+        torch.cuda.synchronize()
+        r = device_view(rhs_, n_l).double()
+        xe = torch.zeros(n_l, dtype=torch.float64, device=net.dev)
+        exact.solve(r * V_l, xe, zero_guess=True)
+        torch.cuda.synchronize()
+        device_view(x_, n_l).copy_(xe.float())
+        torch.cuda.synchronize()
+
+    bound.set_level_solver(level, exact_level)
+    for q in range(min(5, n_held)):
+        exact_cycles.append(bound.solve(held[q], x, zero_guess=True).cycles)
+    bound.close()
+    exact.close()
     plain.close()
     learned_ctx.close()
     return {"grid": [N] * 3, "level": level, "level_grid": [N >> level] * 3, "training_pairs": n_pairs,
@@ -390,5 +440,7 @@ def benchmark_coarse(N: int, level: int, n_pairs: int, steps: int, n_held: int, 
                                       "cycles_mean": float(np.mean(cyc0))},
             "learned_coarse_correction": {"ms_per_solve": round(e[1].elapsed_time(e[2]) / n_held, 3),
                                           "cycles_mean": float(np.mean(cyc1)),
+                                          "fallbacks": cc.fallbacks,
                                           "max_rhs_rel_residual": float(np.max(res1)),
-                                          "network_ms": round(e2[0].elapsed_time(e2[1]) / 20, 3)}}
+                                          "network_ms": round(e2[0].elapsed_time(e2[1]) / 20, 3)},
+            "exact_level_solve_cycles_mean": float(np.mean(exact_cycles))}
