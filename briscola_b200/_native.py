@@ -24,6 +24,7 @@ COARSE_MODE = {"direct": 0, "smooth": 1}
 RESTRICT = {"linear": 0, "average": 1}
 PROLONG = {"linear": 0, "injection": 1}
 ROW_LAYOUT = {"split": 0, "natural": 1}
+LEVEL_MODE = {"replace": 0, "guess": 1}
 DEVICE_PTRS, ZERO_GUESS, PER_VOLUME = 1, 2, 4
 
 # Every function the header declares; the loader checks they are exported.
@@ -83,6 +84,7 @@ class Options(ctypes.Structure):
         ("restrict_scheme", ctypes.c_int),
         ("prolong_scheme", ctypes.c_int),
         ("row_layout", ctypes.c_int),
+        ("fuse_first", ctypes.c_int),
     ]
 
 
@@ -150,7 +152,7 @@ def load(path: str = LIB_PATH):
     L.bmg_set_level_tuning.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.bmg_project_rhs.argtypes = [vp, vp, vp, vp, ctypes.c_double, vp, ctypes.c_int]
     L.bmg_project_correct.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_double]
-    L.bmg_set_level_solver.argtypes = [vp, ctypes.c_int, LEVEL_SOLVER, vp]
+    L.bmg_set_level_solver.argtypes = [vp, ctypes.c_int, LEVEL_SOLVER, vp, ctypes.c_int]
     _lib = L
     return L
 

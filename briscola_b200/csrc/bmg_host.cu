@@ -167,7 +167,11 @@ struct bmg_ctx {
     cudaStream_t capStream = nullptr;  // private stream used only for capture
     // a level solver in place of the FP32 cycle's recursion below hookLevel
     // (bmg_set_level_solver), with its right-hand side and result arrays
+    // level 0's first FP32 colour pass of the next cycle was written by the
+    // flexible-CG kernel that made its right-hand side (FirstPass)
+    bool skipFirst0 = false;
     int hookLevel = -1;
+    int hookMode = BMG_LEVEL_REPLACE;
     bmg_level_solver hook = nullptr;
     void* hookUser = nullptr;
     float* hookRhs = nullptr;
@@ -1186,13 +1190,17 @@ void smooth(bmg_ctx* c, int l, int sweeps) {
     cudaStream_t s = c->stream;
     HostLevel& H = c->lv[l];
     const int prec = sizeof(T) == 8 ? 0 : 1;
+    std::vector<int> seq = colourSequence(H, sweeps);
+    if (sizeof(T) == 4 && l == 0 && c->skipFirst0) {  // the first pass is done (FirstPass)
+        seq.erase(seq.begin());
+        c->skipFirst0 = false;
+    }
     // (the fused smoother does not keep a pinned cell: a pinned level runs
     // pass by pass)
     const bool pinned = l == c->lc && c->singular && c->opt.coarse_mode == BMG_COARSE_SMOOTH;
     if (c->opt.smoother == BMG_SMOOTHER_RBGS && c->opt.fused > 0 && H.fusedOK && H.fusedS[prec] > 0 && !pinned) {
         // the colour sequence alternates; run it in launches of up to
         // maxS stages, each writing the other x buffer
-        const std::vector<int> seq = colourSequence(H, sweeps);
         const FusedGeom g = fusedGeom(c, H, prec);
         const size_t maxS = (size_t)std::min({c->opt.fused, H.fusedS[prec], kFusedMaxStages});
         for (size_t p = 0; p < seq.size(); p += maxS) {
@@ -1229,7 +1237,7 @@ void smooth(bmg_ctx* c, int l, int sweeps) {
         }
         return;
     }
-    for (int col : colourSequence(H, sweeps)) {
+    for (int col : seq) {
         exchange<T>(c, l);
         c->launches += 1;
         if (c->variable)
@@ -1436,9 +1444,8 @@ void tailCycle(bmg_ctx* c, int first) {
 }
 
 // The level solver's turn (bmg_set_level_solver): the level's right-hand
-// side out to the solver, its result back as the level's correction, then
-// the level's post-smoothing; nothing below the level runs.
-void hookCycle(bmg_ctx* c, int l) {
+// side out to the solver, its result back as the level's x.
+void hookSolve(bmg_ctx* c, int l) {
     const Bricks<float> B = bricks<float>(c, l);
     const HostBrick& K = c->lv[l].br[0];
     c->launches += 2;
@@ -1447,14 +1454,22 @@ void hookCycle(bmg_ctx* c, int l) {
     if (c->hook(c->hookUser, c->stream, c->hookRhs, c->hookX, n) != 0)
         throw CudaError{"the level solver returned an error"};
     launch_plain32_to_x(B, c->hookX, c->stream);
-    if (c->opt.n_post > 0) smooth<float>(c, l, c->opt.n_post);
-    c->visits[l]++;
 }
 
 template <typename T>
 void cycle(bmg_ctx* c, int l) {
     if constexpr (sizeof(T) == 4) {
-        if (c->hook && l == c->hookLevel) return hookCycle(c, l);
+        if (c->hook && l == c->hookLevel) {
+            hookSolve(c, l);
+            if (c->hookMode == BMG_LEVEL_REPLACE) {
+                // the solver's result is the level's correction: post-smooth
+                // it; nothing below the level runs
+                if (c->opt.n_post > 0) smooth<float>(c, l, c->opt.n_post);
+                c->visits[l]++;
+                return;
+            }
+            // BMG_LEVEL_GUESS: the usual cycle below, from the solver's x
+        }
     }
     if (l == c->tail) return tailCycle<T>(c, l);
     if (c->opt.n_pre > 0) smooth<T>(c, l, c->opt.n_pre);
@@ -1517,6 +1532,7 @@ SolveState initialState(const bmg_ctx* c) {
 // first convergence test.  The state is copied from the pinned host copy,
 // which the caller fills before every solve (also when replayed as a graph).
 void segInitFcg(bmg_ctx* c, const double* bsrc, const double* xsrc, bool zero, bool setCondition);
+FirstPass firstPass(const bmg_ctx* c);
 void segBodyFcg(bmg_ctx* c, bool setCondition);
 void segPostFcg(bmg_ctx* c, double* xdst);
 
@@ -1581,8 +1597,28 @@ Bricks<double> fcgView(const bmg_ctx* c) {
     return V;
 }
 
+// Whether the flexible-CG kernels that write the FP32 cycle's right-hand
+// side also write its first level-0 colour pass (FirstPass): a mixed
+// flexible-CG solve of one brick with constant coefficients whose level 0 is
+// smoothed by red-black passes before anything else reads its x.
+FirstPass firstPass(const bmg_ctx* c) {
+    FirstPass fp{nullptr, nullptr, 0};
+    const HostLevel& L0 = c->lv[0];
+    if (!c->opt.fuse_first || c->opt.precision != BMG_PRECISION_MIXED || c->opt.krylov != BMG_KRYLOV_FCG ||
+        c->variable || c->multi ||
+        c->opt.smoother != BMG_SMOOTHER_RBGS || c->opt.n_pre < 1 || c->tail == 0 || L0.br[0].n[2] % 4)
+        return fp;
+    fp.z = L0.x32;
+    fp.tab = L0.tab32;
+    fp.colour = colourSequence(L0, c->opt.n_pre)[0];
+    return fp;
+}
+
 void segInitFcg(bmg_ctx* c, const double* bsrc, const double* xsrc, bool zero, bool setCondition) {
     cudaStream_t s = c->stream;
+    const FirstPass fp = firstPass(c);
+    // ghosts and cells the first pass leaves alone start at zero
+    if (fp.z) BMG_CUDA(cudaMemsetAsync(c->lv[0].x32, 0, c->lv[0].cells * sizeof(float), s));
     const Bricks<double> V = fcgView(c);
     const bool mixed = c->opt.precision == BMG_PRECISION_MIXED;
     launch_load_b(V, bsrc, s);
@@ -1601,9 +1637,9 @@ void segInitFcg(bmg_ctx* c, const double* bsrc, const double* xsrc, bool zero, b
     float* pre32 = mixed ? c->lv[0].b32 : nullptr;
     double* pre64 = mixed ? nullptr : c->lv[0].b64;
     if (c->variable)
-        launch_fcg_residual<true>(V, 0, c->fr, pre32, pre64, c->partials, s);
+        launch_fcg_residual<true>(V, 0, c->fr, pre32, pre64, c->partials, fp, s);
     else
-        launch_fcg_residual<false>(V, 0, c->fr, pre32, pre64, c->partials, s);
+        launch_fcg_residual<false>(V, 0, c->fr, pre32, pre64, c->partials, fp, s);
     launch_finalize(V, c->partials, c->st, 0, c->cond, setCondition ? 1 : 0, s);
     c->launches += 2;
 }
@@ -1617,7 +1653,7 @@ void fcgStep(bmg_ctx* c, const T* z, float* pre32, double* pre64, bool setCondit
         launch_fcg_direction<T, true>(V, z, c->fp, c->fq, c->partials, c->st, s);
     else
         launch_fcg_direction<T, false>(V, z, c->fp, c->fq, c->partials, c->st, s);
-    launch_fcg_update(V, c->fp, c->fr, c->fq, pre32, pre64, c->partials, c->st, s);
+    launch_fcg_update(V, c->fp, c->fr, c->fq, pre32, pre64, c->partials, c->st, firstPass(c), s);
     launch_finalize_n(c->partials, fcg_partials(V), c->st, 1, c->cond, setCondition ? 1 : 0, s);
     c->launches += 6;
 }
@@ -1628,8 +1664,14 @@ void segBodyFcg(bmg_ctx* c, bool setCondition) {
     HostLevel& L0 = c->lv[0];
     std::fill(c->visits.begin(), c->visits.end(), 0);
     if (c->opt.precision == BMG_PRECISION_MIXED) {
-        BMG_CUDA(cudaMemsetAsync(L0.x32, 0, L0.cells * sizeof(float), s));
+        // z = 0 and its first colour pass were written with the right-hand
+        // side (FirstPass), or z starts from zero here
+        if (firstPass(c).z)
+            c->skipFirst0 = true;
+        else
+            BMG_CUDA(cudaMemsetAsync(L0.x32, 0, L0.cells * sizeof(float), s));
         cycle<float>(c, 0);
+        c->skipFirst0 = false;
         exchange<float>(c, 0);
         fcgStep<float>(c, L0.x32, L0.b32, nullptr, setCondition);
     } else {
@@ -1646,9 +1688,9 @@ void segPostFcg(bmg_ctx* c, double* xdst) {
     const Bricks<double> V = fcgView(c);
     exchangeField<double>(c, 0, c->fx);
     if (c->variable)
-        launch_fcg_residual<true>(V, 2, nullptr, nullptr, nullptr, c->partials, s);
+        launch_fcg_residual<true>(V, 2, nullptr, nullptr, nullptr, c->partials, FirstPass{}, s);
     else
-        launch_fcg_residual<false>(V, 2, nullptr, nullptr, nullptr, c->partials, s);
+        launch_fcg_residual<false>(V, 2, nullptr, nullptr, nullptr, c->partials, FirstPass{}, s);
     launch_fcg_true_norm(V, c->partials, c->st, s);
     c->launches += 2;
     if (c->opt.remove_mean && c->singular) {
@@ -1913,6 +1955,7 @@ int bmg_default_options(bmg_options* o) {
     o->restrict_scheme = BMG_RESTRICT_LINEAR;
     o->prolong_scheme = BMG_PROLONG_LINEAR;
     o->row_layout = BMG_ROWS_SPLIT;
+    o->fuse_first = 1;
     return BMG_OK;
 }
 
@@ -1993,9 +2036,11 @@ int bmg_set_options(bmg_ctx* c, const bmg_options* o) {
     });
 }
 
-int bmg_set_level_solver(bmg_ctx* c, int level, bmg_level_solver fn, void* user) {
+int bmg_set_level_solver(bmg_ctx* c, int level, bmg_level_solver fn, void* user, int mode) {
     if (!c) return BMG_BAD_ARG;
     return guarded(c, [&] {
+        if (mode != BMG_LEVEL_REPLACE && mode != BMG_LEVEL_GUESS)
+            throw BadArg{BMG_BAD_ARG, "level solver: unknown mode"};
         if (fn && (level < 1 || level > c->lc))
             throw BadArg{BMG_BAD_ARG, "level solver: level outside 1 .. the coarse solve level"};
         if (fn && c->multi) throw BadArg{BMG_UNSUPPORTED, "level solver on a multi-brick mesh"};
@@ -2008,6 +2053,7 @@ int bmg_set_level_solver(bmg_ctx* c, int level, bmg_level_solver fn, void* user)
         c->hook = fn;
         c->hookUser = fn ? user : nullptr;
         c->hookLevel = fn ? level : -1;
+        c->hookMode = mode;
         if (fn) {
             c->hookRhs = dalloc<float>(c->lv[level].ncell);
             c->hookX = dalloc<float>(c->lv[level].ncell);

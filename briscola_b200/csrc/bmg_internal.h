@@ -224,12 +224,23 @@ long reduce_blocks(const Bricks<double>& B);
 // sets the dynamic shared memory limits of the fused smoother instances
 void configure_fused_kernels();
 
+// The first colour pass of the next FP32 preconditioning cycle, written by
+// the kernel that produces the cycle's right-hand side: the cycle starts
+// from z = 0, so its first pass sets the cells of `colour` to gs_value with
+// zero neighbours and leaves the others at 0.  z == nullptr: not written
+// (constant coefficients only; the tables are level 0's FP32 ones).
+struct FirstPass {
+    float* z;
+    const float* tab;
+    int colour;
+};
+
 // ---- flexible CG outer loop (bmg_krylov.cu), level 0, FP64 ------------------
 // r = b - A'x into r (and the cycle's right-hand side pre32 or pre64);
 // partials as launch_residual_norm.  mode 2: only ||V r||^2, nothing written.
 template <bool VAR>
 void launch_fcg_residual(const Bricks<double>& B, int mode, double* r, float* pre32, double* pre64,
-                         double* partials, cudaStream_t s);
+                         double* partials, FirstPass fp, cudaStream_t s);
 // partials of (z, V r) and (z, V q), then beta and gamma (kernel pair)
 template <typename T>
 void launch_fcg_beta(const Bricks<double>& B, const T* z, const double* r, const double* q, double* partials,
@@ -241,7 +252,7 @@ void launch_fcg_direction(const Bricks<double>& B, const T* z, double* p, double
 // x += alpha p (B.x, periodic write-through), r -= alpha q, pre = r,
 // partials of ||V r||^2
 void launch_fcg_update(const Bricks<double>& B, const double* p, double* r, const double* q, float* pre32,
-                       double* pre64, double* partials, const SolveState* st, cudaStream_t s);
+                       double* pre64, double* partials, const SolveState* st, FirstPass fp, cudaStream_t s);
 // number of per-block partials the FCG dots / direction / update kernels write
 long fcg_partials(const Bricks<double>& B);
 // the convergence decision from n partials (as launch_finalize)

@@ -33,12 +33,24 @@ __device__ __forceinline__ double cell_volume(const LevelView<double>& L, int i,
     return L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j] * L.tab64[L.to.h[2] + k];
 }
 
+// The next cycle's first colour pass for cell (i,j,k) of right-hand side f
+// (FirstPass): gs_value with zero neighbours on the cells of fp.colour, the
+// arithmetic of the colour-pass kernels on x = 0, and 0 elsewhere.
+__device__ __forceinline__ float first_pass_value(const LevelView<double>& L, const FirstPass& fp, int i, int j,
+                                                  int k, float f) {
+    if (((i + j + k + L.cpar) & 1) != fp.colour) return 0.f;
+    const float w[6] = {ldg(fp.tab + L.to.wl[0] + i), ldg(fp.tab + L.to.wh[0] + i), ldg(fp.tab + L.to.wl[1] + j),
+                        ldg(fp.tab + L.to.wh[1] + j), ldg(fp.tab + L.to.wl[2] + k), ldg(fp.tab + L.to.wh[2] + k)};
+    const float zero[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    return gs_value(w, zero, f);
+}
+
 // r = b - A'x (FP64), written to r and to the cycle's right-hand side;
 // partials: ||V r||^2 and, for mode 0, the normFactor sum (as k_residual_norm)
 template <bool VAR>
 __global__ void __launch_bounds__(kReduceThreads) k_fcg_residual(Bricks<double> B, int mode, double* r_out,
                                                                  float* pre32, double* pre64, double* partials,
-                                                                 long nblocks) {
+                                                                 long nblocks, FirstPass fp) {
     __shared__ double sh[kReduceThreads / 32];
     int i;
     const LevelView<double>& L = B.v[brick_of(B, blockIdx.z, i)];
@@ -65,6 +77,11 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_residual(Bricks<double> 
             r_out[c] = r;
             if (pre32) pre32[c] = (float)r;
             if (pre64) pre64[c] = r;
+            if (fp.z) {
+                const float z = first_pass_value(L, fp, i, j, k, (float)r);
+                fp.z[c] = z;
+                store_images_to(L, fp.z, c, i, j, k, z);
+            }
         }
     }
     const long bid = block_id();
@@ -421,7 +438,8 @@ __global__ void __launch_bounds__(kReduceThreads, VAR ? 2 : 3) k_fcg_direction_s
 
 __global__ void __launch_bounds__(kReduceThreads) k_fcg_update4(Bricks<double> B, const double* p, double* r,
                                                                 const double* q, float* pre32, double* pre64,
-                                                                double* partials, const SolveState* st) {
+                                                                double* partials, const SolveState* st,
+                                                                FirstPass fp) {
     __shared__ double sh[kReduceThreads / 32];
     const double alpha = st->alpha;
     double a = 0.0;
@@ -445,6 +463,14 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_update4(Bricks<double> B
         if (pre32) {
             const float f[4] = {(float)rn[0], (float)rn[1], (float)rn[2], (float)rn[3]};
             Quad4<float>::st(pre32 + c, ks, f);
+            if (fp.z) {
+                float zq[4];
+                for (int e = 0; e < 4; ++e) zq[e] = first_pass_value(L, fp, i, j, k0 + e, f[e]);
+                Quad4<float>::st(fp.z + c, ks, zq);
+                if (quad_has_images(L, i, j, k0)) {
+                    for (int e = 0; e < 4; ++e) store_images_to(L, fp.z, c + quad_off(ks, e), i, j, k0 + e, zq[e]);
+                }
+            }
         }
         if (pre64) Quad4<double>::st(pre64 + c, ks, rn);
     })
@@ -475,10 +501,10 @@ long fcg_partials(const Bricks<double>& B) {
 
 template <bool VAR>
 void launch_fcg_residual(const Bricks<double>& B, int mode, double* r, float* pre32, double* pre64,
-                         double* partials, cudaStream_t s) {
+                         double* partials, FirstPass fp, cudaStream_t s) {
     const dim3 blk = block_for(B.max2);
     k_fcg_residual<VAR><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, mode, r, pre32, pre64, partials,
-                                                                   reduce_blocks(B));
+                                                                   reduce_blocks(B), fp);
 }
 
 template <typename T>
@@ -509,9 +535,9 @@ void launch_fcg_direction(const Bricks<double>& B, const T* z, double* p, double
 }
 
 void launch_fcg_update(const Bricks<double>& B, const double* p, double* r, const double* q, float* pre32,
-                       double* pre64, double* partials, const SolveState* st, cudaStream_t s) {
+                       double* pre64, double* partials, const SolveState* st, FirstPass fp, cudaStream_t s) {
     if (fcg_quads(B)) {
-        k_fcg_update4<<<quad_grid(B), dim3(16, 16, 1), 0, s>>>(B, p, r, q, pre32, pre64, partials, st);
+        k_fcg_update4<<<quad_grid(B), dim3(16, 16, 1), 0, s>>>(B, p, r, q, pre32, pre64, partials, st, fp);
         return;
     }
     const dim3 blk = block_for(B.max2);
@@ -523,9 +549,9 @@ void launch_fcg_true_norm(const Bricks<double>& B, const double* partials, Solve
 }
 
 template void launch_fcg_residual<false>(const Bricks<double>&, int, double*, float*, double*, double*,
-                                         cudaStream_t);
+                                         FirstPass, cudaStream_t);
 template void launch_fcg_residual<true>(const Bricks<double>&, int, double*, float*, double*, double*,
-                                        cudaStream_t);
+                                        FirstPass, cudaStream_t);
 template void launch_fcg_beta<float>(const Bricks<double>&, const float*, const double*, const double*, double*,
                                      SolveState*, cudaStream_t);
 template void launch_fcg_beta<double>(const Bricks<double>&, const double*, const double*, const double*,

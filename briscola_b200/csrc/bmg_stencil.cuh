@@ -160,6 +160,8 @@ __device__ __forceinline__ long compact_index(const LevelView<T>& L, int i, int 
 // stores, so nothing lives in local memory.
 template <typename T>
 __device__ __forceinline__ void store_images(const LevelView<T>& L, long c, int i, int j, int k, T v);
+template <typename T, typename U>
+__device__ __forceinline__ void store_images_to(const LevelView<T>& L, U* x, long c, int i, int j, int k, U v);
 
 template <typename T>
 __device__ __forceinline__ void store_x(const LevelView<T>& L, long c, int i, int j, int k, T v) {
@@ -171,6 +173,12 @@ __device__ __forceinline__ void store_x(const LevelView<T>& L, long c, int i, in
 // value themselves (as part of a vector store)
 template <typename T>
 __device__ __forceinline__ void store_images(const LevelView<T>& L, long c, int i, int j, int k, T v) {
+    store_images_to(L, L.x, c, i, j, k, v);
+}
+
+// the same images of a value of another array with L's geometry
+template <typename T, typename U>
+__device__ __forceinline__ void store_images_to(const LevelView<T>& L, U* x, long c, int i, int j, int k, U v) {
     const long up0 = (L.per0 && i == 0) ? (long)L.n0 * L.si : 0;
     const long dn0 = (L.per0 && i == L.n0 - 1) ? -(long)L.n0 * L.si : 0;
     const long up1 = (L.per1 && j == 0) ? (long)L.n1 * L.sj : 0;
@@ -190,7 +198,7 @@ __device__ __forceinline__ void store_images(const LevelView<T>& L, long c, int 
             for (int f = 0; f < 3; ++f) {
                 const long o2 = f == 0 ? 0 : f == 1 ? up2 : dn2;
                 if (f && !o2) continue;
-                if (a | e | f) L.x[c + o0 + o1 + o2] = v;
+                if (a | e | f) x[c + o0 + o1 + o2] = v;
             }
         }
     }

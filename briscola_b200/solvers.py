@@ -261,13 +261,15 @@ class Context:
         if getattr(self, "_stream", None) != cur:
             self.set_stream(cur)
 
-    def set_level_solver(self, level: int, fn=None):
+    def set_level_solver(self, level: int, fn=None, mode: str = "replace"):
         """fn(stream, rhs_ptr, x_ptr, n) -> None in place of the FP32 cycle's
-        recursion below `level` (bmg_set_level_solver); None removes it.  fn
-        queues its work on `stream` (an int cudaStream_t) and must neither
-        synchronise nor allocate inside a graphed solve."""
+        recursion below `level` (mode "replace"), or as the start of the
+        level's usual cycle (mode "guess"); bmg_set_level_solver.  None
+        removes it.  fn queues its work on `stream` (an int cudaStream_t)
+        and must neither synchronise nor allocate inside a graphed solve."""
         if fn is None:
-            self.check(self._lib.bmg_set_level_solver(self.h, level, N.LEVEL_SOLVER(), None), "bmg_set_level_solver")
+            self.check(self._lib.bmg_set_level_solver(self.h, level, N.LEVEL_SOLVER(), None, 0),
+                       "bmg_set_level_solver")
             self._hook = None
             return
 
@@ -281,7 +283,8 @@ class Context:
 
         hook = N.LEVEL_SOLVER(call)
         self._hook_error = None
-        self.check(self._lib.bmg_set_level_solver(self.h, level, hook, None), "bmg_set_level_solver")
+        self.check(self._lib.bmg_set_level_solver(self.h, level, hook, None, N.LEVEL_MODE[mode]),
+                   "bmg_set_level_solver")
         self._hook = hook  # kept alive with the context
 
     def set_stream(self, stream_ptr: int):
@@ -456,6 +459,7 @@ def make_options(d: Dictionary | dict | None = None, **over) -> N.Options:
     if rl not in N.ROW_LAYOUT:
         raise FatalError(f"unknown rowLayout {rl}")
     o.row_layout = N.ROW_LAYOUT[rl]
+    o.fuse_first = int(_switch(d.get("fuseFirstPass", "on")))
     return o
 
 

@@ -149,6 +149,10 @@ typedef struct bmg_options {
     int restrict_scheme;/* restrict (linear): BMG_RESTRICT_*                   */
     int prolong_scheme; /* prolong (linear): BMG_PROLONG_*                     */
     int row_layout;     /* rowLayout (split): BMG_ROWS_*, fixed at creation    */
+    int fuse_first;     /* fuseFirstPass (1): a mixed flexible-CG solve writes
+                           the first level-0 colour pass of each FP32 cycle
+                           with the cycle's right-hand side (constant
+                           coefficient, one brick); results bit-identical   */
 } bmg_options;
 
 typedef struct bmg_report {
@@ -257,6 +261,11 @@ int bmg_project_correct(struct bmg_ctx* ctx, double* u0, double* u1, double* u2,
  * then post-smooth it (nSweepsPost sweeps); the levels below l are not
  * visited.  FP64 cycles keep the multigrid recursion.
  *
+ * With mode BMG_LEVEL_GUESS the solver's result instead starts the level's
+ * usual cycle (pre-smoothing, the recursion below, post-smoothing) in place
+ * of zero: the levels below keep their work, and the network only has to
+ * improve the level's starting point.
+ *
  * fn(user, stream, rhs, x, n) is called on the host while the cycle is
  * being launched: rhs and x are device arrays of the level's interior
  * cells (n[0]*n[1]*n[2] floats, k fastest), rhs the row-scaled right-hand
@@ -269,7 +278,8 @@ int bmg_project_correct(struct bmg_ctx* ctx, double* u0, double* u1, double* u2,
  * level; fn NULL removes the solver.  The context keeps two level-sized
  * FP32 arrays for rhs and x. */
 typedef int (*bmg_level_solver)(void* user, void* stream, const float* rhs, float* x, const int n[3]);
-int bmg_set_level_solver(struct bmg_ctx* ctx, int level, bmg_level_solver fn, void* user);
+enum { BMG_LEVEL_REPLACE = 0, BMG_LEVEL_GUESS = 1 };
+int bmg_set_level_solver(struct bmg_ctx* ctx, int level, bmg_level_solver fn, void* user, int mode);
 
 /* ---- Residual norm without any device allocation ---------------------------
  * No counterpart in the reference: an addition for callers that must not

@@ -174,3 +174,24 @@ def test_split_level_kernels_match_oracle(native, name, variable, precision):
     c.prolong_correct(0, precision=precision)
     assert rel(c.download(0, "x", precision=precision), o.prolong(0, xc, x, op="+=")) <= tol
     c.close()
+
+
+@pytest.mark.parametrize("case", ["channel", "cavity"])
+def test_first_pass_fusion_is_bit_identical(native, case):
+    """With fuseFirstPass on (the default) the flexible-CG kernels that write
+    each FP32 cycle's right-hand side also write that cycle's first level-0
+    colour pass (the cycle starts from z = 0); the solve is bit-identical to
+    the one that zeroes z and runs the pass."""
+    mesh, b, _ = workloads.CONFIGS[case](64)
+    kw = dict(relTol=1e-10, precision="mixed", krylov="fcg")
+    out = {}
+    for f in ("on", "off"):
+        d = dict(V22, fuseFirstPass=f, **kw)
+        c = bb.Context(mesh, bb.make_options(d))
+        x = np.zeros_like(b)
+        rep = c.solve(b, x, zero_guess=True)
+        assert rep.status == 0
+        out[f] = (x, rep.cycles, rep.kernel_launches)
+        c.close()
+    assert out["on"][1] == out["off"][1] and np.array_equal(out["on"][0], out["off"][0])
+    assert out["on"][2] < out["off"][2]  # one colour pass fewer per cycle
