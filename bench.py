@@ -225,10 +225,10 @@ def profile_region(args, local):
     from briscola_b200 import workloads
 
     stream = torch.cuda.current_stream()
-    if args.profile_region == "fft":
+    if args.profile_region in ("fft", "fft_box"):
         from briscola_b200 import fft
 
-        mesh, _, _ = workloads.channel(args.size)
+        mesh, _, _ = (workloads.channel if args.profile_region == "fft" else workloads.cavity)(args.size)
         solver = fft.FFTPoissonSolver(mesh.bricks[0], device=local)
         f = torch.randn(mesh.bricks[0].N, dtype=torch.float64, device=f"cuda:{local}")
         x = torch.empty_like(f)
@@ -284,15 +284,13 @@ def profile_region(args, local):
         raise RuntimeError(f"solve failed: status {rep.status}")
 
 
-def fft_timing(args, local, stream, mesh, barrier):
-    """The FFT Poisson solver (briscola_b200.fft) on the bench's channel:
-    Laplacian(x) = -f for a seeded zero-mean f, device-resident, CUDA events;
-    the discrete Laplacian residual is checked on the device."""
+def _fft_one(args, local, stream, br, barrier):
+    """Solves of one brick (device-resident, CUDA events) and the max of the
+    discrete Laplacian residual over max |f|."""
     import torch
 
     from briscola_b200 import fft
 
-    br = mesh.bricks[0]
     solver = fft.FFTPoissonSolver(br, device=local)
     n = br.N
     g = torch.Generator(device=f"cuda:{local}").manual_seed(11)
@@ -313,8 +311,8 @@ def fft_timing(args, local, stream, mesh, barrier):
     e1.record(stream)
     barrier()
     ms = e0.elapsed_time(e1) / reps
-    # residual of the cell-centred Laplacian (periodic x and z, zero-gradient
-    # walls in y: mirrored ghost cells)
+    # residual of the cell-centred Laplacian (periodic axes wrap, zero-gradient
+    # walls: mirrored ghost cells)
     h = [torch.from_numpy(br.cell_sizes(d)).to(f.device) for d in range(3)]
     r = f.clone()
     for d in range(3):
@@ -338,12 +336,27 @@ def fft_timing(args, local, stream, mesh, barrier):
     cells = n[0] * n[1] * n[2]
     sdir = solver.solve_direction
     solver.close()
-    return {"workload": "the bench channel, Laplacian(x) = -f, seeded N(0,1) f with zero volume-weighted mean",
-            "ms_per_solve": round(ms, 4), "solve_direction": sdir,
-            "max_residual_over_max_rhs": res,
-            "algorithmic_gb_per_s": round(cells * 8 * 10 / (ms * 1e-3) / 1e9, 1),
-            "algorithmic_bytes_note": "10 passes of 8 B/cell: read+write per transform (4) and "
-                                      "tridiagonal (read+write each way)"}
+    return {"ms_per_solve": round(ms, 4), "solve_direction": sdir, "max_residual_over_max_rhs": res,
+            "algorithmic_gb_per_s": round(cells * 8 * 10 / (ms * 1e-3) / 1e9, 1)}
+
+
+def fft_timing(args, local, stream, mesh, barrier):
+    """The FFT Poisson solver (briscola_b200.fft) on the bench's channel (real
+    FFTs along x and z) and on the closed box of the same size (all walls
+    zero-gradient: cosine transforms along both transform axes):
+    Laplacian(x) = -f for a seeded zero-mean f, device-resident, CUDA events;
+    the discrete Laplacian residual is checked on the device."""
+    from briscola_b200 import workloads
+
+    out = {"workload": "the bench channel, Laplacian(x) = -f, seeded N(0,1) f with zero volume-weighted mean"}
+    out.update(_fft_one(args, local, stream, mesh.bricks[0], barrier))
+    out["algorithmic_bytes_note"] = ("10 passes of 8 B/cell: read+write per transform (4) and "
+                                     "tridiagonal (read+write each way)")
+    box, _, _ = workloads.cavity(args.size)
+    out["closed_box"] = dict({"workload": f"uniform {args.size}^3 box, all walls zero-gradient (REDFT10/01 "
+                                          "along both transform axes)"},
+                             **_fft_one(args, local, stream, box.bricks[0], barrier))
+    return out
 
 
 def split_timing(args, local, stream, barrier):
@@ -462,7 +475,7 @@ def main():
     ap.add_argument("--learned-steps", type=int, default=2000)
     ap.add_argument("--learned-held", type=int, default=200)
     ap.add_argument("--no-learned-coarse", action="store_true")
-    ap.add_argument("--profile-region", choices=["mixed_fcg", "mixed_fcg_fused", "fp64", "unet_fwd", "fft"],
+    ap.add_argument("--profile-region", choices=["mixed_fcg", "mixed_fcg_fused", "fp64", "unet_fwd", "fft", "fft_box"],
                     default=None,
                     help="set up, warm up, then run one solve (or one U-Net forward) between "
                          "cudaProfilerStart/Stop for ncu --profile-from-start off; prints no bench line")

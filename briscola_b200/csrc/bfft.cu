@@ -59,6 +59,8 @@ struct Lines {
 
 struct Transform {
     int M, logM, mode;
+    int kind;             // Kind
+    int odd;              // K_DCT2 / K_DCT3: the sine kinds RODFT10 / RODFT01
     int logN;             // log2 of the line length (transformed extents are powers of two)
     int logLB;            // log2 of the lines per CTA
     const double2* pre;   // n entries, nullptr: 1
@@ -192,17 +194,27 @@ constexpr int kPerThread = kTileComplex / kTransformThreads;    // 16 values per
 constexpr int kMaxLines = 256;  // lines of a tile (short lines fill less than the tile)
 
 // tile index -> shared-memory slot: one pad slot after every 16, so the
-// first Stockham pass's writes (stride R) do not pile onto one bank group
-__device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
+// first Stockham pass's writes (stride R) do not pile onto one bank group,
+// and for lines of 16 points or more one more after every line, so that
+// the same point of consecutive lines (the strided axes' staging and
+// output, thread by thread) falls in consecutive 16-byte bank groups
+// instead of one (a line of M points and its pads is 17 M / 16 slots, a
+// multiple of the eight groups)
+template <int LOGM>
+__device__ __forceinline__ int pad(int i) {
+    return i + (i >> 4) + (LOGM >= 4 ? (i >> LOGM) : 0);
+}
 
-// pad(base + r 2^S) for r = 0..R-1 as pad(base) + r * stride: exact when
-// S >= 4, or when base is a multiple of 16 and R 2^S <= 16
+// pad(base + r 2^S) for r = 0..R-1 as pad(base) + r * stride (all inside
+// one line): exact when S >= 4, or when base is a multiple of 16 and
+// R 2^S <= 16
 template <int S>
 __device__ __forceinline__ constexpr int padded_step() {
     return S >= 4 ? 17 << (S - 4) : 1 << S;
 }
-constexpr int kTileSlots = kTileComplex + kTileComplex / 16;
-constexpr int kTransformSmem = kTileSlots * 16 + kTileComplex * 8;  // tile and staging buffer
+constexpr int kTileSlots = kTileComplex + kTileComplex / 16 + kTileComplex / 16;
+constexpr int kStage = 2 * kTileComplex;  // real values of a staged tile (two real lines per complex one)
+constexpr int kTransformSmem = kTileSlots * 16 + kStage * 8;  // tile and staging buffer
 
 // One Stockham radix-R pass (Govindaraju et al., SC 2008) in place over the
 // tile: group j of a line reads points j + r M/R, twiddles them by
@@ -231,12 +243,12 @@ __device__ __forceinline__ void stockham_pass(double2* __restrict__ buf, const d
         const int t = g >> LOGG, j = g & ((1 << LOGG) - 1);
         const int row = (t << LOGM) + j;
         if constexpr (affineRead) {
-            const double2* src = buf + pad(row);
+            const double2* src = buf + pad<LOGM>(row);
 #pragma unroll
             for (int r = 0; r < R; ++r) v[gi][r] = src[r * padded_step<LOGG>()];
         } else {
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[gi][r] = buf[pad(row + (r << LOGG))];
+            for (int r = 0; r < R; ++r) v[gi][r] = buf[pad<LOGM>(row + (r << LOGG))];
         }
     }
     __syncthreads();
@@ -255,14 +267,14 @@ __device__ __forceinline__ void stockham_pass(double2* __restrict__ buf, const d
         dft_regs<R, LOGR>(v[gi]);
         const int idxD = (t << LOGM) + ((j >> LOGNS) << (LOGNS + LOGR)) + jm;
         if constexpr (affineWrite) {
-            double2* dst = buf + pad(idxD);
+            double2* dst = buf + pad<LOGM>(idxD);
 #pragma unroll
             for (int r = 0; r < R; ++r)
                 if (ok) dst[r * padded_step<LOGNS>()] = v[gi][r];
         } else {
 #pragma unroll
             for (int r = 0; r < R; ++r)
-                if (ok) buf[pad(idxD + (r << LOGNS))] = v[gi][r];
+                if (ok) buf[pad<LOGM>(idxD + (r << LOGNS))] = v[gi][r];
         }
     }
     __syncthreads();
@@ -308,14 +320,40 @@ __device__ __forceinline__ void cp16(void* smem, const void* gmem, int bytes) {
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-enum Kind { K_R2HC = 0, K_HC2R = 1, K_TRIG = 2 };
+// Transform kinds.  K_TRIG: one zero-padded M = 2N point complex FFT per
+// line with a pre-twiddle of the input and a post-twiddle of the output
+// (the quarter-wave kinds REDFT11 / RODFT11).  The others put two real lines
+// into one N-point complex FFT (line 2u as the real part, line 2u + 1 as the
+// imaginary part) and separate the two spectra afterwards from
+// Z(k) and conj Z(N - k):
+//   K_R2HC  forward real FFT, halfcomplex output
+//   K_HC2R  inverse real FFT of halfcomplex input (unnormalised)
+//   K_DCT2  REDFT10 by Makhoul's reordering (J. Makhoul, "A fast cosine
+//           transform in one and two dimensions", IEEE TASSP 28 (1980)):
+//           v = (x0, x2, x4, ..., x5, x3, x1), X_k = 2 Re(e^{-i pi k/2N} V_k);
+//           with `odd`, RODFT10 as REDFT10 of (-1)^n x_n, read backwards
+//   K_DCT3  REDFT01, the inverse of that reordering: V_k = e^{i pi k/2N}
+//           (X_k - i X_{N-k}) (X_N = 0), v = IDFT(V), x_2n = v_n,
+//           x_2n+1 = v_{N-1-n}; with `odd`, RODFT01 as (-1)^n REDFT01 of
+//           the reversed input
+// so every kind the solver meets on a periodic, Dirichlet-Dirichlet or
+// Neumann-Neumann axis costs half an N-point complex FFT per line.
+enum Kind { K_R2HC = 0, K_HC2R = 1, K_TRIG = 2, K_DCT2 = 3, K_DCT3 = 4 };
 
-// out(line) = transform of in(line), tile by tile (LB = min(2048 / M, 256)
-// lines of n points, M-point FFTs), persistent: while a tile's FFT runs, the
-// next tile's lines are already on their way into a staging buffer by
-// cp.async, so the loads of HBM overlap the arithmetic.  in == out is
-// allowed: every element belongs to one tile, which the same CTA loads
-// before it writes.
+// the slot of point p in Makhoul's reordering (even points first, then the
+// odd ones backwards)
+template <int N>
+__device__ __forceinline__ int makhoul(int p) {
+    return (p & 1) ? N - 1 - (p >> 1) : p >> 1;
+}
+
+// out(line) = transform of in(line), tile by tile, persistent: while a
+// tile's FFT runs, the next tile's lines are already on their way into a
+// staging buffer by cp.async, so the loads of HBM overlap the arithmetic.
+// in == out is allowed: every element belongs to one tile, which the same
+// CTA loads before it writes.  A tile holds LB lines of N points:
+// LB = min(4096 / N, 256) for the paired kinds (LB / 2 complex lines of M =
+// N points), min(2048 / M, 256) for K_TRIG.
 //
 // Element q of a tile is point p of tile line t, with t fastest along the
 // strided axes (LF: a run of lines is a run of consecutive k) and p fastest
@@ -328,17 +366,21 @@ __global__ void __launch_bounds__(kTransformThreads, 3) k_transform(const double
                                                                     Transform T, LoadPrep LP, long tiles, int pair) {
     extern __shared__ double2 dsm[];
     double2* buf = dsm;                                          // [kTileSlots]
-    double* stage = reinterpret_cast<double*>(dsm + kTileSlots);  // [kTileComplex]
+    double* stage = reinterpret_cast<double*>(dsm + kTileSlots);  // [kStage]
     constexpr int NT = kTransformThreads;
+    constexpr bool PK = KIND != K_TRIG;  // two real lines per complex FFT
     constexpr int M = 1 << LOGM;
-    constexpr int LOGN = KIND == K_TRIG ? LOGM - 1 : LOGM;
+    constexpr int LOGN = PK ? LOGM : LOGM - 1;
     constexpr int N = 1 << LOGN;
-    constexpr int LOGLB = 11 - LOGM < 8 ? 11 - LOGM : 8;
+    constexpr int LOGLB0 = PK ? 12 - LOGM : 11 - LOGM;
+    constexpr int LOGLB = LOGLB0 < 8 ? LOGLB0 : 8;
     constexpr int LB = 1 << LOGLB;
+    constexpr int LBC = PK ? LB / 2 : LB;            // complex lines of a tile
     constexpr int TOTAL = LB << LOGN;             // elements of a tile
     constexpr int PAIRS = (TOTAL / 2 + NT - 1) / NT;  // element pairs per thread
-    static_assert(LB >= 2 && TOTAL >= 2, "tiles hold pairs");
+    static_assert(LB >= 2 && TOTAL >= 2 && TOTAL <= kStage, "tiles hold pairs");
     const int tid = threadIdx.x;
+    double* bufd = reinterpret_cast<double*>(buf);
 
     // element q -> (line t, point p)
     auto tp = [&](int q, int& t, int& p) {
@@ -426,38 +468,63 @@ __global__ void __launch_bounds__(kTransformThreads, 3) k_transform(const double
         // the staged tile is complete, and the previous tile's output phase
         // has finished reading buf
         __syncthreads();
-        if constexpr (KIND == K_HC2R) {
-            // conj(Y_k) of the halfcomplex spectra: element (t, k) of buf
-            // from points k and N - k of the staged line
+        if constexpr (KIND == K_HC2R || KIND == K_DCT3) {
+            // spectral input: point p of staged line t (the first
+            // transform's prep applied)
             auto h = [&](int t, int p) {
                 const int q = LF ? (p << LOGLB) + t : (t << LOGN) + p;
                 const double x = stage[q];
                 return LP.on ? prep(x, tile, t, p, fixed_terms(tile * LB + t)) : x;
             };
-            double2 y[2 * PAIRS];
-#pragma unroll
-            for (int u = 0; u < 2 * PAIRS; ++u) {
-                const int q = tid + u * NT;
-                double re = 0.0, im = 0.0;
-                if (q < TOTAL) {
-                    const int t = q >> LOGM, k = q & (M - 1);
-                    if (k == 0) {
-                        re = h(t, 0);
-                    } else if (2 * k < N) {
-                        re = h(t, k);
-                        im = -h(t, N - k);
-                    } else if (2 * k == N) {
-                        re = h(t, k);
-                    } else {
-                        re = h(t, N - k);
-                        im = h(t, k);
-                    }
+            // slot (u, k) of the complex tile from lines 2u and 2u + 1:
+            // conj of the combined spectrum, so the forward FFT below gives
+            // the conjugate of the inverse transform
+            constexpr int SLOTS = TOTAL / 2;
+#pragma unroll 4
+            for (int s = tid; s < SLOTS; s += NT) {
+                const int u = s >> LOGN, k = s & (N - 1);
+                const int ta = 2 * u, tb = 2 * u + 1;
+                double ar, ai, br, bi;
+                if constexpr (KIND == K_HC2R) {
+                    // A_k of a halfcomplex line: (r_k, i_k), i_k stored at N - k
+                    auto hc = [&](int t, double& re, double& im) {
+                        if (k == 0) {
+                            re = h(t, 0);
+                            im = 0.0;
+                        } else if (2 * k < N) {
+                            re = h(t, k);
+                            im = h(t, N - k);
+                        } else if (2 * k == N) {
+                            re = h(t, k);
+                            im = 0.0;
+                        } else {
+                            re = h(t, N - k);
+                            im = -h(t, k);
+                        }
+                    };
+                    hc(ta, ar, ai);
+                    hc(tb, br, bi);
+                } else {
+                    // V_k = c_k (X_k - i X_{N-k}), c_k = e^{i pi k / 2N}
+                    const double2 c = __ldg(T.pre + k);
+                    auto v = [&](int t, double& re, double& im) {
+                        double xk, xn;
+                        if (T.odd) {  // the reversed line
+                            xk = h(t, N - 1 - k);
+                            xn = k ? h(t, k - 1) : 0.0;
+                        } else {
+                            xk = h(t, k);
+                            xn = k ? h(t, N - k) : 0.0;
+                        }
+                        re = c.x * xk + c.y * xn;
+                        im = c.y * xk - c.x * xn;
+                    };
+                    v(ta, ar, ai);
+                    v(tb, br, bi);
                 }
-                y[u] = make_double2(re, im);
+                // conj(A + i B)
+                buf[pad<LOGM>((u << LOGM) + k)] = make_double2(ar - bi, -(ai + br));
             }
-#pragma unroll
-            for (int u = 0; u < 2 * PAIRS; ++u)
-                if (tid + u * NT < TOTAL) buf[pad(tid + u * NT)] = y[u];
         } else {
             // along LF axes the thread's line pair is fixed for the tile
             double fx[2] = {0.0, 0.0};
@@ -471,25 +538,46 @@ __global__ void __launch_bounds__(kTransformThreads, 3) k_transform(const double
                 if (q >= TOTAL) break;
                 const double2 x2 = *reinterpret_cast<const double2*>(stage + q);
                 double xs[2] = {x2.x, x2.y};
+                int tq[2], pq[2];
 #pragma unroll
                 for (int e = 0; e < 2; ++e) {
-                    int t, p;
-                    tp(q + e, t, p);
+                    tp(q + e, tq[e], pq[e]);
                     double x = xs[e];
-                    if (LP.on) x = prep(x, tile, t, p, LF ? fx[e] : fixed_terms(tile * LB + t));
-                    double2 c = make_double2(x, 0.0);
-                    if (KIND == K_TRIG && T.pre) {
-                        const double2 w = __ldg(T.pre + p);
-                        c = make_double2(w.x * x, w.y * x);
+                    if (LP.on) x = prep(x, tile, tq[e], pq[e], LF ? fx[e] : fixed_terms(tile * LB + tq[e]));
+                    if constexpr (KIND == K_DCT2) {
+                        if (T.odd && (pq[e] & 1)) x = -x;
                     }
-                    buf[pad((t << LOGM) + p)] = c;
+                    xs[e] = x;
+                }
+                if constexpr (KIND == K_TRIG) {
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        double2 c = make_double2(xs[e], 0.0);
+                        if (T.pre) {
+                            const double2 w = __ldg(T.pre + pq[e]);
+                            c = make_double2(w.x * xs[e], w.y * xs[e]);
+                        }
+                        buf[pad<LOGM>((tq[e] << LOGM) + pq[e])] = c;
+                    }
+                } else {
+                    // real part from the even line of a pair, imaginary part
+                    // from the odd one; DCT2 reorders the points
+                    const int p0 = KIND == K_DCT2 ? makhoul<N>(pq[0]) : pq[0];
+                    if constexpr (LF) {  // the two elements are lines t, t + 1 at one point
+                        buf[pad<LOGM>(((tq[0] >> 1) << LOGM) + p0)] = make_double2(xs[0], xs[1]);
+                    } else {  // points p, p + 1 of one line
+                        const int p1 = KIND == K_DCT2 ? makhoul<N>(pq[1]) : pq[1];
+                        const int base = (tq[0] >> 1) << LOGM, part = tq[0] & 1;
+                        bufd[2 * pad<LOGM>(base + p0) + part] = xs[0];
+                        bufd[2 * pad<LOGM>(base + p1) + part] = xs[1];
+                    }
                 }
             }
             if constexpr (KIND == K_TRIG) {  // zero padding: points N..2N-1 of every line
 #pragma unroll
                 for (int u = 0; u < 2 * PAIRS; ++u) {
                     const int q = tid + u * NT;
-                    if (q < TOTAL) buf[pad(((q >> LOGN) << LOGM) + N + (q & (N - 1)))] = make_double2(0.0, 0.0);
+                    if (q < TOTAL) buf[pad<LOGM>(((q >> LOGN) << LOGM) + N + (q & (N - 1)))] = make_double2(0.0, 0.0);
                 }
             }
         }
@@ -497,7 +585,7 @@ __global__ void __launch_bounds__(kTransformThreads, 3) k_transform(const double
         // stage is free: the next tile's loads run under this tile's FFT
         if (tile + gridDim.x < tiles) issue(tile + gridDim.x);
 
-        stockham_all<LOGM, 0, LB>(buf, T.tw);
+        stockham_all<LOGM, 0, LBC>(buf, T.tw);
 
         // output: element q of the tile from spectrum entry (t, k)
         const long l = pair_line(tile);
@@ -511,15 +599,36 @@ __global__ void __launch_bounds__(kTransformThreads, 3) k_transform(const double
             for (int e = 0; e < 2; ++e) {
                 int t, k;
                 tp(q + e, t, k);
-                const int row = t << LOGM;
-                if constexpr (KIND == K_R2HC) {
-                    y[e] = 2 * k <= N ? buf[pad(row + k)].x : buf[pad(row + N - k)].y;
-                } else if constexpr (KIND == K_HC2R) {
-                    y[e] = buf[pad(row + k)].x;
-                } else {
-                    const double2 z = buf[pad(row + k)];
+                if constexpr (KIND == K_TRIG) {
+                    const double2 z = buf[pad<LOGM>((t << LOGM) + k)];
                     const double2 c = T.post ? cmul(__ldg(T.post + k), z) : z;
                     y[e] = T.mode == M_RE ? c.x : -c.y;
+                } else {
+                    const int row = (t >> 1) << LOGM, part = t & 1;
+                    if constexpr (KIND == K_R2HC) {
+                        // A = (Z_k + conj Z_{N-k}) / 2, B = (Z_k - conj Z_{N-k}) / 2i;
+                        // halfcomplex: Re at k <= N/2, Im of N - k above
+                        const int kk = 2 * k <= N ? k : N - k;
+                        const double2 zk = buf[pad<LOGM>(row + kk)], zn = buf[pad<LOGM>(row + ((N - kk) & (N - 1)))];
+                        if (2 * k <= N)
+                            y[e] = part == 0 ? 0.5 * (zk.x + zn.x) : 0.5 * (zk.y + zn.y);
+                        else
+                            y[e] = part == 0 ? 0.5 * (zk.y - zn.y) : -0.5 * (zk.x - zn.x);
+                    } else if constexpr (KIND == K_DCT2) {
+                        // 2 Re(w_k A_k) or 2 Re(w_k B_k), w_k = e^{-i pi k / 2N}
+                        const int kk = T.odd ? N - 1 - k : k;
+                        const double2 zk = buf[pad<LOGM>(row + kk)], zn = buf[pad<LOGM>(row + ((N - kk) & (N - 1)))];
+                        const double2 w = __ldg(T.post + kk);
+                        y[e] = part == 0 ? w.x * (zk.x + zn.x) - w.y * (zk.y - zn.y)
+                                         : w.x * (zk.y + zn.y) + w.y * (zk.x - zn.x);
+                    } else {
+                        // the forward FFT of conj(A + i B) is conj(a + i b)
+                        const int slot = KIND == K_DCT3 ? makhoul<N>(k) : k;
+                        const double2 z = buf[pad<LOGM>(row + slot)];
+                        double v = part == 0 ? z.x : -z.y;
+                        if (KIND == K_DCT3 && T.odd && (k & 1)) v = -v;
+                        y[e] = v;
+                    }
                 }
             }
             int t, p;
@@ -874,60 +983,48 @@ __global__ void k_prep(double* __restrict__ w, const double* __restrict__ b, con
     }
 }
 
-template <int LOGM, int KIND, bool LF>
-void launch_one(unsigned grid, cudaStream_t st, const double* in, double* out, const Lines& L, const Transform& T,
-                const LoadPrep& lp, long tiles, int pair) {
-    k_transform<LOGM, KIND, LF><<<grid, kTransformThreads, kTransformSmem, st>>>(in, out, L, T, lp, tiles, pair);
-}
+// the line lengths of a kind: M = N = 1 .. kMaxN for the paired kinds,
+// M = 2N = 2 .. 2 kMaxN for K_TRIG
+constexpr int kMinLogM(int kind) { return kind == K_TRIG ? 1 : 0; }
 
-template <int KIND, bool LF>
+template <int KIND, bool LF, int LOGM = kMinLogM(KIND)>
 void launch_kind(int logM, unsigned grid, cudaStream_t st, const double* in, double* out, const Lines& L,
                  const Transform& T, const LoadPrep& lp, long tiles, int pair) {
-    switch (logM) {
-        case 1: launch_one<1, KIND, LF>(grid, st, in, out, L, T, lp, tiles, pair); break;
-        case 2: launch_one<2, KIND, LF>(grid, st, in, out, L, T, lp, tiles, pair); break;
-        case 3: launch_one<3, KIND, LF>(grid, st, in, out, L, T, lp, tiles, pair); break;
-        case 4: launch_one<4, KIND, LF>(grid, st, in, out, L, T, lp, tiles, pair); break;
-        case 5: launch_one<5, KIND, LF>(grid, st, in, out, L, T, lp, tiles, pair); break;
-        case 6: launch_one<6, KIND, LF>(grid, st, in, out, L, T, lp, tiles, pair); break;
-        case 7: launch_one<7, KIND, LF>(grid, st, in, out, L, T, lp, tiles, pair); break;
-        case 8: launch_one<8, KIND, LF>(grid, st, in, out, L, T, lp, tiles, pair); break;
-        case 9: launch_one<9, KIND, LF>(grid, st, in, out, L, T, lp, tiles, pair); break;
-        default: launch_one<10, KIND, LF>(grid, st, in, out, L, T, lp, tiles, pair); break;
+    if constexpr (LOGM <= kMinLogM(KIND) + 9) {
+        if (logM == LOGM)
+            k_transform<LOGM, KIND, LF><<<grid, kTransformThreads, kTransformSmem, st>>>(in, out, L, T, lp, tiles, pair);
+        else
+            launch_kind<KIND, LF, LOGM + 1>(logM, grid, st, in, out, L, T, lp, tiles, pair);
+    }
+}
+
+template <bool LF>
+void launch_lf(int kind, int logM, unsigned grid, cudaStream_t st, const double* in, double* out, const Lines& L,
+               const Transform& T, const LoadPrep& lp, long tiles, int pair) {
+    switch (kind) {
+        case K_R2HC: launch_kind<K_R2HC, LF>(logM, grid, st, in, out, L, T, lp, tiles, pair); break;
+        case K_HC2R: launch_kind<K_HC2R, LF>(logM, grid, st, in, out, L, T, lp, tiles, pair); break;
+        case K_DCT2: launch_kind<K_DCT2, LF>(logM, grid, st, in, out, L, T, lp, tiles, pair); break;
+        case K_DCT3: launch_kind<K_DCT3, LF>(logM, grid, st, in, out, L, T, lp, tiles, pair); break;
+        default: launch_kind<K_TRIG, LF>(logM, grid, st, in, out, L, T, lp, tiles, pair); break;
     }
 }
 
 void launch_transform(int kind, int logM, unsigned grid, cudaStream_t st, const double* in, double* out,
                       const Lines& L, const Transform& T, const LoadPrep& lp, long tiles, int pair) {
-    const bool lf = L.line_fast != 0;
-    if (kind == K_R2HC)
-        lf ? launch_kind<K_R2HC, true>(logM, grid, st, in, out, L, T, lp, tiles, pair)
-           : launch_kind<K_R2HC, false>(logM, grid, st, in, out, L, T, lp, tiles, pair);
-    else if (kind == K_HC2R)
-        lf ? launch_kind<K_HC2R, true>(logM, grid, st, in, out, L, T, lp, tiles, pair)
-           : launch_kind<K_HC2R, false>(logM, grid, st, in, out, L, T, lp, tiles, pair);
+    if (L.line_fast)
+        launch_lf<true>(kind, logM, grid, st, in, out, L, T, lp, tiles, pair);
     else
-        lf ? launch_kind<K_TRIG, true>(logM, grid, st, in, out, L, T, lp, tiles, pair)
-           : launch_kind<K_TRIG, false>(logM, grid, st, in, out, L, T, lp, tiles, pair);
+        launch_lf<false>(kind, logM, grid, st, in, out, L, T, lp, tiles, pair);
 }
 
-template <int LOGM, int KIND, bool LF>
-void allow_one() {
-    cudaFuncSetAttribute(k_transform<LOGM, KIND, LF>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTransformSmem);
-}
-
-template <int KIND, bool LF>
+template <int KIND, bool LF, int LOGM = kMinLogM(KIND)>
 void allow_kind() {
-    allow_one<1, KIND, LF>();
-    allow_one<2, KIND, LF>();
-    allow_one<3, KIND, LF>();
-    allow_one<4, KIND, LF>();
-    allow_one<5, KIND, LF>();
-    allow_one<6, KIND, LF>();
-    allow_one<7, KIND, LF>();
-    allow_one<8, KIND, LF>();
-    allow_one<9, KIND, LF>();
-    allow_one<10, KIND, LF>();
+    if constexpr (LOGM <= kMinLogM(KIND) + 9) {
+        cudaFuncSetAttribute(k_transform<LOGM, KIND, LF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kTransformSmem);
+        allow_kind<KIND, LF, LOGM + 1>();
+    }
 }
 
 void allow_smem_all() {
@@ -935,6 +1032,10 @@ void allow_smem_all() {
     allow_kind<K_R2HC, false>();
     allow_kind<K_HC2R, true>();
     allow_kind<K_HC2R, false>();
+    allow_kind<K_DCT2, true>();
+    allow_kind<K_DCT2, false>();
+    allow_kind<K_DCT3, true>();
+    allow_kind<K_DCT3, false>();
     allow_kind<K_TRIG, true>();
     allow_kind<K_TRIG, false>();
 }
@@ -1019,8 +1120,10 @@ void planTransforms(bfft_ctx* c, int d) {
     const int N = c->n[d];
     if (A.pair == P_EMPTY) return;
     const long double pi = 3.141592653589793238462643383279502884L;
-    const bool cc = A.pair == P_CC;
-    const int M = cc ? N : 2 * N;
+    // periodic, D-D and N-N axes: two real lines per N-point complex FFT;
+    // the quarter-wave kinds (D-N, N-D): a zero-padded 2N-point FFT per line
+    const bool paired = A.pair == P_CC || A.pair == P_NN || A.pair == P_DD;
+    const int M = paired ? N : 2 * N;
     std::vector<double2> tw(M);
     for (int j = 0; j < M; ++j) tw[j] = expi(-2.0L * pi * j / M);
     const double2* twd = upload(c, tw);
@@ -1029,24 +1132,23 @@ void planTransforms(bfft_ctx* c, int d) {
         for (int q = 0; q < N; ++q) t[q] = f(q);
         return upload(c, t);
     };
-    const int LB = std::min(kTileComplex / M, kMaxLines);
-    Transform f{M, log2i(M), M_RE, log2i(N), log2i(LB), nullptr, nullptr, twd};
+    const int LB = paired ? std::min(kStage / N, kMaxLines) : std::min(kTileComplex / M, kMaxLines);
+    Transform f{M, log2i(M), M_RE, K_TRIG, 0, log2i(N), log2i(LB), nullptr, nullptr, twd};
     Transform b = f;
     switch (A.pair) {
         case P_CC:
             f.mode = M_R2HC;
             b.mode = M_HC2R;
+            f.kind = K_R2HC;
+            b.kind = K_HC2R;
             break;
         case P_NN:  // REDFT10 / REDFT01
-            f.post = table([&](int k) { return expi(-pi * k / (2.0L * N), 2.0L); });
-            b.pre = table([&](int q) { return expi(-pi * q / (2.0L * N), q == 0 ? 1.0L : 2.0L); });
-            break;
         case P_DD:  // RODFT10 / RODFT01
-            f.mode = b.mode = M_NEG_IM;
-            f.pre = table([&](int q) { return expi(-pi * q / N); });
-            f.post = table([&](int k) { return expi(-pi * (k + 1) / (2.0L * N), 2.0L); });
-            b.pre = table([&](int q) { return expi(-pi * q / (2.0L * N), q == N - 1 ? 1.0L : 2.0L); });
-            b.post = table([&](int k) { return expi(-pi * (2 * k + 1) / (2.0L * N)); });
+            f.kind = K_DCT2;
+            b.kind = K_DCT3;
+            f.odd = b.odd = A.pair == P_DD;
+            f.post = table([&](int k) { return expi(-pi * k / (2.0L * N)); });
+            b.pre = table([&](int k) { return expi(pi * k / (2.0L * N)); });
             break;
         case P_DN:  // RODFT11 both ways
         case P_ND:  // REDFT11 both ways
@@ -1058,7 +1160,7 @@ void planTransforms(bfft_ctx* c, int d) {
     A.fwd = f;
     A.bwd = b;
     A.LB = LB;
-    A.identity = cc && N == 1;
+    A.identity = A.pair == P_CC && N == 1;
     // pairs: consecutive lines along the strided axes (adjacent when the k
     // rows hold an even number of cells), consecutive points along k
     const long n1 = c->n[1], n2 = c->n[2];
@@ -1344,8 +1446,7 @@ void transform(bfft_ctx* c, int a, bool forward, const double* in, double* out, 
     const long tiles = (A.lines.count + A.LB - 1) / A.LB;
     // persistent: as many CTAs as fit at once (three per SM)
     const long grid = std::min<long>(tiles, 3L * c->sms);
-    const int kind = T.mode == M_R2HC ? K_R2HC : T.mode == M_HC2R ? K_HC2R : K_TRIG;
-    launch_transform(kind, T.logM, (unsigned)grid, c->stream, in, out, A.lines, T, lp, tiles, A.adjacent);
+    launch_transform(T.kind, T.logM, (unsigned)grid, c->stream, in, out, A.lines, T, lp, tiles, A.adjacent);
     check(cudaGetLastError(), "k_transform");
 }
 
