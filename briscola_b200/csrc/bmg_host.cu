@@ -44,6 +44,10 @@ struct HostBrick {
     int origin[3] = {0, 0, 0};  // cell offset in the level's global lattice
     Axis ax[3];
     bool open[6] = {false, false, false, false, false, false};  // periodic or touching another brick
+    // Dirichlet wall faces, and the Dirichlet value or Neumann gradient of
+    // each wall face (level 0; coarse levels keep the Dirichlet flags)
+    int dirichlet[6] = {0, 0, 0, 0, 0, 0};
+    double dval[6] = {0, 0, 0, 0, 0, 0};
     int nbr[6] = {-1, -1, -1, -1, -1, -1};  // a brick touching the face (its ghost points come from it)
     // orientation of the caller's arrays: local axis d runs along axis
     // tax[d] of this (global) frame, reversed when tfl[d]
@@ -129,8 +133,6 @@ struct BadArg {
 struct bmg_ctx {
     bmg_options opt{};
     int periodic[3] = {0, 0, 0};  // single brick only
-    int dirichlet[6] = {0, 0, 0, 0, 0, 0};  // Dirichlet faces (single brick only)
-    double dval[6] = {0, 0, 0, 0, 0, 0};    // their values
     bool singular = true;         // no Dirichlet face (linearSystem.H:227-230)
     bool multi = false;           // more than one brick
     cudaStream_t stream = nullptr;
@@ -253,7 +255,7 @@ void layout(HostLevel& L) {
 // cells stay zero: A_c -= A_f after A_c = -(sum of all faces)
 // (DirichletBoundaryCondition.C:19-51).  Faces touching another brick keep
 // their coupling and get their wall parts zeroed through the face lambdas.
-void buildTables(HostLevel& L, const int dirichlet[6]) {
+void buildTables(HostLevel& L) {
     int off = 0;
     L.tab.clear();
     // every sub-table starts on a multiple of 4 entries, so the colour pass
@@ -288,8 +290,8 @@ void buildTables(HostLevel& L, const int dirichlet[6]) {
                 const double dlo = 1.0 / std::fabs(a.cc[i + 1] - a.cc[i]);
                 const double dhi = 1.0 / std::fabs(a.cc[i + 2] - a.cc[i + 1]);
                 double wl = dlo / hi, wh = dhi / hi;
-                if (!B.open[2 * d] && i == 0) wl = dirichlet[2 * d] ? 2.0 * wl : 0.0;
-                if (!B.open[2 * d + 1] && i == n - 1) wh = dirichlet[2 * d + 1] ? 2.0 * wh : 0.0;
+                if (!B.open[2 * d] && i == 0) wl = B.dirichlet[2 * d] ? 2.0 * wl : 0.0;
+                if (!B.open[2 * d + 1] && i == n - 1) wh = B.dirichlet[2 * d + 1] ? 2.0 * wh : 0.0;
                 L.tab[to.wl[d] + i] = wl;
                 L.tab[to.wh[d] + i] = wh;
                 L.tab[to.h[d] + i] = hi;
@@ -361,17 +363,23 @@ Bricks<T> bricks(const bmg_ctx* c, int l) {
         B.max2 = std::max(B.max2, K.n[2]);
     }
     B.z0[B.nb] = z;
-    B.walls.mask = 0;
-    B.walls.nmask = 0;
-    if (l == 0 && !c->multi) {
-        for (int f = 0; f < 6; ++f) {
-            B.walls.mask |= c->dirichlet[f] << f;
-            B.walls.nmask |= (!c->dirichlet[f] && c->dval[f] != 0.0) << f;
-            B.walls.g[f] = c->dval[f];
-        }
-        B.walls.ybar = c->st ? &c->st->ybar : nullptr;
-    }
     return B;
+}
+
+// the face values of the level-0 bricks (Dirichlet values, Neumann gradients)
+Walls walls(const bmg_ctx* c) {
+    Walls W{};
+    const HostLevel& L0 = c->lv[0];
+    for (size_t b = 0; b < L0.br.size(); ++b) {
+        const HostBrick& K = L0.br[b];
+        for (int f = 0; f < 6; ++f) {
+            W.mask[b] |= K.dirichlet[f] << f;
+            W.nmask[b] |= (!K.dirichlet[f] && K.dval[f] != 0.0) << f;
+            W.g[b][f] = K.dval[f];
+        }
+    }
+    W.ybar = c->st ? &c->st->ybar : nullptr;
+    return W;
 }
 
 TransferSet ttabs(const bmg_ctx* c, int l) {
@@ -665,14 +673,8 @@ void readBricks(bmg_ctx* c, const bmg_mesh_desc* mesh, HostLevel& L0) {
                     throw BadArg{BMG_BAD_ARG, "unknown boundary condition type"};
                 if (t == BMG_BC_PERIODIC) continue;
                 if (!std::isfinite(v)) throw BadArg{BMG_BAD_ARG, "a face value is not finite"};
-                if ((t == BMG_BC_DIRICHLET || v != 0.0) && nb > 1)
-                    throw BadArg{BMG_UNSUPPORTED,
-                                 "Dirichlet faces and Neumann gradients on multi-brick meshes are not supported"};
-                c->dval[2 * d + side] = v;
-                if (t == BMG_BC_DIRICHLET) {
-                    c->dirichlet[2 * d + side] = 1;
-                    c->singular = false;
-                }
+                K.dval[2 * d + side] = v;
+                K.dirichlet[2 * d + side] = t == BMG_BC_DIRICHLET;
             }
             if (lo == BMG_BC_PERIODIC && c->multi) L0.wrap[d] |= 1 << b;  // resolved below
             if (!c->multi) c->periodic[d] = lo == BMG_BC_PERIODIC;
@@ -750,6 +752,42 @@ void readBricks(bmg_ctx* c, const bmg_mesh_desc* mesh, HostLevel& L0) {
                 if (L0.br[b].nbr[2 * d] < 0) L0.br[b].nbr[2 * d] = a;
             }
         }
+    // A face wholly in contact with other bricks is an interface and carries
+    // no boundary condition (the reference links whole faces of bricks,
+    // brickFaceLink.C); a face partly in contact keeps zero-gradient walls on
+    // the rest, which cannot take a Dirichlet value or a gradient.
+    for (auto& B : L0.br)
+        for (int d = 0; d < 3; ++d)
+            for (int side = 0; side < 2; ++side) {
+                const int f = 2 * d + side;
+                if (!B.open[f]) continue;
+                const int t1 = (d + 1) % 3, t2 = (d + 2) % 3;
+                long touching = 0;
+                for (int u = 0; u < B.n[t1]; ++u)
+                    for (int v = 0; v < B.n[t2]; ++v) {
+                        int g[3], loc[3];
+                        g[d] = side ? B.origin[d] + B.n[d] : B.origin[d] - 1;
+                        g[t1] = B.origin[t1] + u;
+                        g[t2] = B.origin[t2] + v;
+                        touching += findBrick(L0, g, loc) >= 0;
+                    }
+                if (touching == (long)B.n[t1] * B.n[t2]) {
+                    B.dirichlet[f] = 0;
+                    B.dval[f] = 0.0;
+                } else if (B.dirichlet[f] || B.dval[f] != 0.0) {
+                    throw BadArg{BMG_UNSUPPORTED,
+                                 "a Dirichlet value or a Neumann gradient on a brick face partly in contact with "
+                                 "another brick"};
+                }
+            }
+}
+
+// a system with no Dirichlet face anywhere is singular (linearSystem.H:227-230)
+bool singularSystem(const HostLevel& L0) {
+    for (const auto& B : L0.br)
+        for (int f = 0; f < 6; ++f)
+            if (B.dirichlet[f]) return false;
+    return true;
 }
 
 // Coarse level: halve every extent (single brick: the reference's rule,
@@ -775,6 +813,8 @@ bool coarsenLevel(const bmg_ctx* c, const HostLevel& F, HostLevel& C) {
             K.ax[d].pts.assign(K.n[d] + 3, 0.0);
             for (int q = 0; q <= K.n[d]; ++q) K.ax[d].pts[q + 1] = B.ax[d].pts[q * K.R[d] + 1];
             K.open[2 * d] = K.open[2 * d + 1] = c->periodic[d];
+            K.dirichlet[2 * d] = B.dirichlet[2 * d];
+            K.dirichlet[2 * d + 1] = B.dirichlet[2 * d + 1];
         }
         C.br.push_back(std::move(K));
         return true;
@@ -800,6 +840,7 @@ bool coarsenLevel(const bmg_ctx* c, const HostLevel& F, HostLevel& C) {
         for (int f = 0; f < 6; ++f) {
             K.open[f] = B.open[f];
             K.nbr[f] = B.nbr[f];
+            K.dirichlet[f] = B.dirichlet[f];
         }
         for (int d = 0; d < 3; ++d) {
             K.tax[d] = B.tax[d];
@@ -880,7 +921,8 @@ void contactMask(const HostLevel& L, std::vector<double> mask[3]) {
 
 // Ghost frame of every brick: from the brick that owns the position, else a
 // zero-gradient copy of the brick's own nearest cell (what the reference's
-// unset-boundary copies give at walls, meshLevel.C:301-328).
+// unset-boundary copies give at walls, meshLevel.C:301-328), except beyond a
+// Dirichlet face, where the ghost is left at zero as on a single brick.
 void ghostList(const HostLevel& L, std::vector<int>& dst, std::vector<int>& src) {
     dst.clear();
     src.clear();
@@ -899,6 +941,13 @@ void ghostList(const HostLevel& L, std::vector<int>& dst, std::vector<int>& src)
                     if (nb >= 0) {
                         s = L.br[nb].at(loc[0], loc[1], loc[2]);
                     } else {
+                        // beyond a Dirichlet wall the ghost stays zero: the
+                        // eliminated coupling (twice the face's) reads it
+                        bool dir = false;
+                        for (int d = 0; d < 3; ++d)
+                            dir = dir || (l3[d] < 0 && B.dirichlet[2 * d]) || (l3[d] >= B.n[d] && B.dirichlet[2 * d + 1]);
+                        if (dir) continue;
+                        // elsewhere a zero-gradient copy of the nearest cell
                         const int ci = std::min(std::max(i, 0), B.n[0] - 1);
                         const int cj = std::min(std::max(j, 0), B.n[1] - 1);
                         const int ck = std::min(std::max(k, 0), B.n[2] - 1);
@@ -984,7 +1033,7 @@ void buildTransfers(bmg_ctx* c) {
                                 I1 = (In + C.n[d]) % C.n[d];
                             } else if (C.open[2 * d + (In >= C.n[d])]) {
                                 I1 = In;  // ghost cell, refreshed from the neighbouring brick
-                            } else if (c->dirichlet[2 * d + (In >= C.n[d])]) {
+                            } else if (C.dirichlet[2 * d + (In >= C.n[d])]) {
                                 // the coarse ghost is -x (DirichletBoundaryCondition.C
                                 // :59-80 above level 0): (1 - w) x + w (-x) = (1 - 2w) x,
                                 // read as weight 2w on the ghost cell, which holds zero
@@ -1047,7 +1096,7 @@ void build(bmg_ctx* c, HostLevel&& L0) {
         // 16-cell blocks
         L.ks = c->opt.row_layout == BMG_ROWS_SPLIT && !c->multi && L.br[0].n[2] % 16 == 0 &&
                L.ncell > kTailCells;
-        buildTables(L, c->dirichlet);
+        buildTables(L);
         L.x64 = dalloc<double>(L.cells);
         L.b64 = dalloc<double>(L.cells);
         L.x32 = dalloc<float>(L.cells);
@@ -1502,9 +1551,9 @@ void residualNorm(bmg_ctx* c, int mode, bool setCondition) {
     float* b32 = c->opt.precision == BMG_PRECISION_MIXED ? c->lv[0].b32 : nullptr;
     c->launches += 2;
     if (c->variable)
-        launch_residual_norm<true>(L, mode, c->partials, b32, c->stream);
+        launch_residual_norm<true>(L, walls(c), mode, c->partials, b32, c->stream);
     else
-        launch_residual_norm<false>(L, mode, c->partials, b32, c->stream);
+        launch_residual_norm<false>(L, walls(c), mode, c->partials, b32, c->stream);
     launch_finalize(L, c->partials, c->st, mode, c->cond, setCondition ? 1 : 0, c->stream);
 }
 
@@ -1541,7 +1590,7 @@ void segInit(bmg_ctx* c, const double* bsrc, const double* xsrc, bool zero, bool
     cudaStream_t s = c->stream;
     HostLevel& L0 = c->lv[0];
     const Bricks<double> V0 = bricks<double>(c, 0);
-    launch_load_b(V0, bsrc, s);
+    launch_load_b(V0, walls(c), bsrc, s);
     BMG_CUDA(cudaMemsetAsync(L0.x64, 0, L0.cells * sizeof(double), s));
     c->launches += 1;
     if (!zero) {
@@ -1621,7 +1670,7 @@ void segInitFcg(bmg_ctx* c, const double* bsrc, const double* xsrc, bool zero, b
     if (fp.z) BMG_CUDA(cudaMemsetAsync(c->lv[0].x32, 0, c->lv[0].cells * sizeof(float), s));
     const Bricks<double> V = fcgView(c);
     const bool mixed = c->opt.precision == BMG_PRECISION_MIXED;
-    launch_load_b(V, bsrc, s);
+    launch_load_b(V, walls(c), bsrc, s);
     BMG_CUDA(cudaMemsetAsync(c->fx, 0, c->lv[0].cells * sizeof(double), s));
     c->launches += 1;
     if (!zero) {
@@ -1637,9 +1686,9 @@ void segInitFcg(bmg_ctx* c, const double* bsrc, const double* xsrc, bool zero, b
     float* pre32 = mixed ? c->lv[0].b32 : nullptr;
     double* pre64 = mixed ? nullptr : c->lv[0].b64;
     if (c->variable)
-        launch_fcg_residual<true>(V, 0, c->fr, pre32, pre64, c->partials, fp, s);
+        launch_fcg_residual<true>(V, walls(c), 0, c->fr, pre32, pre64, c->partials, fp, s);
     else
-        launch_fcg_residual<false>(V, 0, c->fr, pre32, pre64, c->partials, fp, s);
+        launch_fcg_residual<false>(V, walls(c), 0, c->fr, pre32, pre64, c->partials, fp, s);
     launch_finalize(V, c->partials, c->st, 0, c->cond, setCondition ? 1 : 0, s);
     c->launches += 2;
 }
@@ -1688,9 +1737,9 @@ void segPostFcg(bmg_ctx* c, double* xdst) {
     const Bricks<double> V = fcgView(c);
     exchangeField<double>(c, 0, c->fx);
     if (c->variable)
-        launch_fcg_residual<true>(V, 2, nullptr, nullptr, nullptr, c->partials, FirstPass{}, s);
+        launch_fcg_residual<true>(V, walls(c), 2, nullptr, nullptr, nullptr, c->partials, FirstPass{}, s);
     else
-        launch_fcg_residual<false>(V, 2, nullptr, nullptr, nullptr, c->partials, FirstPass{}, s);
+        launch_fcg_residual<false>(V, walls(c), 2, nullptr, nullptr, nullptr, c->partials, FirstPass{}, s);
     launch_fcg_true_norm(V, c->partials, c->st, s);
     c->launches += 2;
     if (c->opt.remove_mean && c->singular) {
@@ -1972,6 +2021,7 @@ int bmg_create(bmg_ctx** out, const bmg_mesh_desc* mesh, const bmg_options* opts
         // the mesh is checked on the host before any device work
         HostLevel L0;
         readBricks(c, mesh, L0);
+        c->singular = singularSystem(L0);
         int ndev = 0;
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= c->opt.device || c->opt.device < 0)
             throw BadArg{BMG_NO_DEVICE, "no CUDA device with the requested ordinal"};

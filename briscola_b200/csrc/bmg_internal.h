@@ -82,10 +82,13 @@ struct LevelView {
 // delta) and the normFactor's A*mean(x) term (solver.C:28-45) need the faces
 // themselves.  ybar: the plain mean of the initial x (SolveState::ybar).
 // Both masks are 0 on coarse levels.
+// Face values of the level-0 bricks: per brick, bit f of mask marks a
+// Dirichlet face, bit f of nmask a Neumann face with a nonzero gradient,
+// g[b][f] the value or gradient
 struct Walls {
-    int mask;
-    int nmask;
-    double g[6];
+    int mask[kMaxBricks];
+    int nmask[kMaxBricks];
+    double g[kMaxBricks][6];
     const double* ybar;
 };
 
@@ -97,7 +100,6 @@ struct Bricks {
     int z0[kMaxBricks + 1];  // first plane of each brick; z0[nb] = total planes
     int nb;
     int max1, max2;          // largest n1 and n2 (grid extents)
-    Walls walls;
 };
 
 // Transfer tables between level l (fine) and l+1 (coarse), fine-indexed.
@@ -213,7 +215,8 @@ void launch_fill_ghosts(T* x, const int* dst, const int* src, long n, cudaStream
 // sum and ||b||^2: three partial arrays), 1: current.  When b32 is given the scaled residual is also written
 // there in FP32 (the right-hand side of the next mixed-precision cycle).
 template <bool VAR>
-void launch_residual_norm(const Bricks<double>& B, int mode, double* partials, float* b32, cudaStream_t s);
+void launch_residual_norm(const Bricks<double>& B, const Walls& W, int mode, double* partials, float* b32,
+                          cudaStream_t s);
 void launch_finalize(const Bricks<double>& B, const double* partials, SolveState* st, int mode,
                      cudaGraphConditionalHandle cond, int setCondition, cudaStream_t s);
 void launch_mean(const Bricks<double>& B, double* partials, SolveState* st, cudaStream_t s);
@@ -239,7 +242,7 @@ struct FirstPass {
 // r = b - A'x into r (and the cycle's right-hand side pre32 or pre64);
 // partials as launch_residual_norm.  mode 2: only ||V r||^2, nothing written.
 template <bool VAR>
-void launch_fcg_residual(const Bricks<double>& B, int mode, double* r, float* pre32, double* pre64,
+void launch_fcg_residual(const Bricks<double>& B, const Walls& W, int mode, double* r, float* pre32, double* pre64,
                          double* partials, FirstPass fp, cudaStream_t s);
 // partials of (z, V r) and (z, V q), then beta and gamma (kernel pair)
 template <typename T>
@@ -275,7 +278,7 @@ void launch_project_correct(double* u0, double* u1, double* u2, const double* p,
                             const double* lam1, const double* lam2, const ProjGeom& G, cudaStream_t s);
 
 // compact interior <-> ghost-framed conversions
-void launch_load_b(const Bricks<double>& B, const double* compact, cudaStream_t s);
+void launch_load_b(const Bricks<double>& B, const Walls& W, const double* compact, cudaStream_t s);
 void launch_load_x(const Bricks<double>& B, const double* compact, cudaStream_t s);
 void launch_store_x(const Bricks<double>& B, double* compact, cudaStream_t s);
 template <typename T>

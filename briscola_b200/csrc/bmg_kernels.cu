@@ -995,11 +995,12 @@ __global__ void __launch_bounds__(256) k_residual_out(Bricks<T> B, double* out) 
 // except in the rows of Dirichlet faces.
 // ---------------------------------------------------------------------------
 template <bool VAR>
-__global__ void __launch_bounds__(kReduceThreads) k_residual_norm(Bricks<double> B, int mode, double* partials,
-                                                                  long nblocks, float* b32) {
+__global__ void __launch_bounds__(kReduceThreads) k_residual_norm(Bricks<double> B, Walls W, int mode,
+                                                                  double* partials, long nblocks, float* b32) {
     __shared__ double sh[kReduceThreads / 32];
     int i;
-    const LevelView<double>& L = B.v[brick_of(B, blockIdx.z, i)];
+    const int bk = brick_of(B, blockIdx.z, i);
+    const LevelView<double>& L = B.v[bk];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     double a1 = 0.0, a2 = 0.0, a3 = 0.0;
@@ -1016,7 +1017,8 @@ __global__ void __launch_bounds__(kReduceThreads) k_residual_norm(Bricks<double>
         if (mode == 0) {
             const double bb = V * L.b[c];
             // A*mean(x): nonzero only in the rows of Dirichlet faces
-            const double ay = B.walls.mask ? -V * *B.walls.ybar * wall_sum(L, B.walls, i, j, k, c, ckp, false) : 0.0;
+            const double ay =
+                W.mask[bk] ? -V * *W.ybar * wall_sum(L, W, bk, i, j, k, c, ckp, false) : 0.0;
             const double t = fabs(rr - bb + ay) + fabs(bb - ay);
             a2 = t * t;
             a3 = bb * bb;
@@ -1131,9 +1133,10 @@ __global__ void k_sub_mean(double* x, long n, const SolveState* st) {
         x[q] -= m;
 }
 
-__global__ void __launch_bounds__(256) k_load_b(Bricks<double> B, const double* compact) {
+__global__ void __launch_bounds__(256) k_load_b(Bricks<double> B, Walls W, const double* compact) {
     int i;
-    const LevelView<double>& L = B.v[brick_of(B, blockIdx.z, i)];
+    const int bk = brick_of(B, blockIdx.z, i);
+    const LevelView<double>& L = B.v[bk];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (j >= L.n1 || k >= L.n2) return;
@@ -1141,7 +1144,7 @@ __global__ void __launch_bounds__(256) k_load_b(Bricks<double> B, const double* 
     const double V = L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j] * L.tab64[L.to.h[2] + k];
     double v = compact[compact_index(L, i, j, k)] / V;
     // face values: Dirichlet b -= 2 A_f g, Neumann b -= A_f g / delta
-    if (B.walls.mask | B.walls.nmask) v -= wall_sum(L, B.walls, i, j, k, c, row + kpos(L, k + 1), true);
+    if (W.mask[bk] | W.nmask[bk]) v -= wall_sum(L, W, bk, i, j, k, c, row + kpos(L, k + 1), true);
     L.b[c] = v;
 }
 
@@ -1348,9 +1351,10 @@ void launch_residual_out(const Bricks<T>& B, double* out, cudaStream_t s) {
 }
 
 template <bool VAR>
-void launch_residual_norm(const Bricks<double>& B, int mode, double* partials, float* b32, cudaStream_t s) {
+void launch_residual_norm(const Bricks<double>& B, const Walls& W, int mode, double* partials, float* b32,
+                          cudaStream_t s) {
     const dim3 blk = block_for(B.max2);
-    k_residual_norm<VAR><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, mode, partials, reduce_blocks(B), b32);
+    k_residual_norm<VAR><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, W, mode, partials, reduce_blocks(B), b32);
 }
 
 void launch_finalize(const Bricks<double>& B, const double* partials, SolveState* st, int mode,
@@ -1378,9 +1382,9 @@ void launch_plain_mean(const Bricks<double>& B, double* partials, SolveState* st
     k_plain_finalize<<<1, kFinalThreads, 0, s>>>(partials, reduce_blocks(B), st);
 }
 
-void launch_load_b(const Bricks<double>& B, const double* compact, cudaStream_t s) {
+void launch_load_b(const Bricks<double>& B, const Walls& W, const double* compact, cudaStream_t s) {
     const dim3 blk = block_for(B.max2);
-    k_load_b<<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, compact);
+    k_load_b<<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, W, compact);
 }
 
 void launch_load_x(const Bricks<double>& B, const double* compact, cudaStream_t s) {
@@ -1444,8 +1448,8 @@ template void launch_tail_cycle<float, false>(const TailPlan<float>&, cudaStream
 template void launch_tail_cycle<float, true>(const TailPlan<float>&, cudaStream_t);
 template void launch_fill_ghosts<double>(double*, const int*, const int*, long, cudaStream_t);
 template void launch_fill_ghosts<float>(float*, const int*, const int*, long, cudaStream_t);
-template void launch_residual_norm<false>(const Bricks<double>&, int, double*, float*, cudaStream_t);
-template void launch_residual_norm<true>(const Bricks<double>&, int, double*, float*, cudaStream_t);
+template void launch_residual_norm<false>(const Bricks<double>&, const Walls&, int, double*, float*, cudaStream_t);
+template void launch_residual_norm<true>(const Bricks<double>&, const Walls&, int, double*, float*, cudaStream_t);
 template void launch_load_field<double>(const Bricks<double>&, int, const double*, int, cudaStream_t);
 template void launch_load_field<float>(const Bricks<float>&, int, const double*, int, cudaStream_t);
 template void launch_store_field<double>(const Bricks<double>&, int, double*, int, cudaStream_t);

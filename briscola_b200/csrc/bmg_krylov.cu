@@ -48,12 +48,13 @@ __device__ __forceinline__ float first_pass_value(const LevelView<double>& L, co
 // r = b - A'x (FP64), written to r and to the cycle's right-hand side;
 // partials: ||V r||^2 and, for mode 0, the normFactor sum (as k_residual_norm)
 template <bool VAR>
-__global__ void __launch_bounds__(kReduceThreads) k_fcg_residual(Bricks<double> B, int mode, double* r_out,
+__global__ void __launch_bounds__(kReduceThreads) k_fcg_residual(Bricks<double> B, Walls W, int mode, double* r_out,
                                                                  float* pre32, double* pre64, double* partials,
                                                                  long nblocks, FirstPass fp) {
     __shared__ double sh[kReduceThreads / 32];
     int i;
-    const LevelView<double>& L = B.v[brick_of(B, blockIdx.z, i)];
+    const int bk = brick_of(B, blockIdx.z, i);
+    const LevelView<double>& L = B.v[bk];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     double a1 = 0.0, a2 = 0.0, a3 = 0.0;
@@ -68,7 +69,8 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_residual(Bricks<double> 
         a1 = (V * r) * (V * r);
         if (mode == 0) {
             const double bb = V * L.b[c];
-            const double ay = B.walls.mask ? -V * *B.walls.ybar * wall_sum(L, B.walls, i, j, k, c, ckp, false) : 0.0;
+            const double ay =
+                W.mask[bk] ? -V * *W.ybar * wall_sum(L, W, bk, i, j, k, c, ckp, false) : 0.0;
             const double t = fabs(V * r - bb + ay) + fabs(bb - ay);
             a2 = t * t;
             a3 = bb * bb;
@@ -500,10 +502,10 @@ long fcg_partials(const Bricks<double>& B) {
 }
 
 template <bool VAR>
-void launch_fcg_residual(const Bricks<double>& B, int mode, double* r, float* pre32, double* pre64,
+void launch_fcg_residual(const Bricks<double>& B, const Walls& W, int mode, double* r, float* pre32, double* pre64,
                          double* partials, FirstPass fp, cudaStream_t s) {
     const dim3 blk = block_for(B.max2);
-    k_fcg_residual<VAR><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, mode, r, pre32, pre64, partials,
+    k_fcg_residual<VAR><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, W, mode, r, pre32, pre64, partials,
                                                                    reduce_blocks(B), fp);
 }
 
@@ -548,9 +550,9 @@ void launch_fcg_true_norm(const Bricks<double>& B, const double* partials, Solve
     k_fcg_true_norm<<<1, kFinalThreads, 0, s>>>(partials, reduce_blocks(B), st);
 }
 
-template void launch_fcg_residual<false>(const Bricks<double>&, int, double*, float*, double*, double*,
+template void launch_fcg_residual<false>(const Bricks<double>&, const Walls&, int, double*, float*, double*, double*,
                                          FirstPass, cudaStream_t);
-template void launch_fcg_residual<true>(const Bricks<double>&, int, double*, float*, double*, double*,
+template void launch_fcg_residual<true>(const Bricks<double>&, const Walls&, int, double*, float*, double*, double*,
                                         FirstPass, cudaStream_t);
 template void launch_fcg_beta<float>(const Bricks<double>&, const float*, const double*, const double*, double*,
                                      SolveState*, cudaStream_t);

@@ -98,22 +98,22 @@ __device__ __forceinline__ void stencil(const T* x, long c, long ckm, long ckp, 
 // 2 A_f g / V (DirichletBoundaryCondition.C:47-48) plus, over Neumann faces
 // with a gradient g, A_f g / (delta V) = lambda g / h
 // (NeumannBoundaryCondition.C:44-50).
-__device__ __forceinline__ double wall_sum(const LevelView<double>& L, const Walls& W, int i, int j, int k,
+__device__ __forceinline__ double wall_sum(const LevelView<double>& L, const Walls& W, int b, int i, int j, int k,
                                            long c, long ckp, bool values) {
     double s = 0.0;
     const int at[6] = {i == 0, i == L.n0 - 1, j == 0, j == L.n1 - 1, k == 0, k == L.n2 - 1};
     const int q[3] = {i, j, k};
     const long st[3] = {L.si, L.sj, 1};
-    const int faces = values ? (W.mask | W.nmask) : W.mask;
+    const int faces = values ? (W.mask[b] | W.nmask[b]) : W.mask[b];
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
         if (!((faces >> f) & 1) || !at[f]) continue;
         const int d = f >> 1, up = f & 1;
-        const bool dir = (W.mask >> f) & 1;
+        const bool dir = (W.mask[b] >> f) & 1;
         double w = dir ? L.tab64[(up ? L.to.wh[d] : L.to.wl[d]) + q[d]] : 1.0 / L.tab64[L.to.h[d] + q[d]];
         const double* lam = d == 0 ? L.lam0 : d == 1 ? L.lam1 : L.lam2;
         if (lam) w *= lam[!up ? c : d == 2 ? ckp : c + st[d]];
-        s += values ? w * W.g[f] : w;
+        s += values ? w * W.g[b][f] : w;
     }
     return s;
 }

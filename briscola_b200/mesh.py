@@ -14,7 +14,8 @@ import numpy as np
 
 NEUMANN = "Neumann"
 PERIODIC = "periodic"
-# Dirichlet faces: both solvers (the multigrid on single-brick meshes);
+# Dirichlet faces: both solvers (on a multi-brick mesh, the multigrid takes
+# them on brick faces that touch no other brick);
 # empty axes: the FFT Poisson solver only (briscola_b200.fft)
 DIRICHLET = "Dirichlet"
 EMPTY = "empty"

@@ -42,13 +42,16 @@ typedef enum bmg_status {
     BMG_UNSUPPORTED = 7    /* a valid option this build does not implement                           */
 } bmg_status;
 
-/* Boundary condition of one outer brick face.  Dirichlet faces (single-brick
- * meshes) follow DirichletBoundaryCondition.C:19-80: the ghost coefficient
- * is eliminated into the centre (A_c -= A_f), the face value g enters the
- * right-hand side as b -= 2 A_f g at every solve, and the system is not
- * singular (no pin, no mean removal; linearSystem.H:227-230).  A Neumann
- * face's value is its gradient g (single-brick meshes): b -= A_f g / delta
- * (NeumannBoundaryCondition.C:19-56). */
+/* Boundary condition of one outer brick face.  Dirichlet faces follow
+ * DirichletBoundaryCondition.C:19-80: the ghost coefficient is eliminated
+ * into the centre (A_c -= A_f), the face value g enters the right-hand side
+ * as b -= 2 A_f g at every solve, and the system is not singular (no pin, no
+ * mean removal; linearSystem.H:227-230).  A Neumann face's value is its
+ * gradient g: b -= A_f g / delta (NeumannBoundaryCondition.C:19-56).  On a
+ * multi-brick mesh a face wholly in contact with other bricks is an
+ * interface and its condition is ignored; a face partly in contact keeps
+ * zero-gradient walls on the rest and takes neither a Dirichlet condition
+ * nor a gradient there (BMG_UNSUPPORTED). */
 enum { BMG_BC_NEUMANN = 0, BMG_BC_PERIODIC = 1, BMG_BC_DIRICHLET = 2 };
 
 /* Cycle types (MG.H:106-124) and smoothers (MG.C:313-373). */

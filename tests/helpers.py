@@ -106,7 +106,7 @@ def split_brick(brick, cuts):
                 lo = (edges[0][a], edges[1][b], edges[2][c])
                 hi = (edges[0][a + 1], edges[1][b + 1], edges[2][c + 1])
                 pts = [brick.points[d][lo[d]:hi[d] + 1] for d in range(3)]
-                bricks.append(Brick(pts, brick.bc, lo))
+                bricks.append(Brick(pts, brick.bc, lo, brick.values))
     return Mesh(bricks)
 
 
@@ -168,6 +168,61 @@ def union_operator(mesh):
     A = A - sp.diags(np.asarray(A.sum(axis=1)).ravel())
     V = hh[0] * hh[1] * hh[2]
     return A.tocsr(), V
+
+
+def union_operator_bc(mesh):
+    """union_operator with each brick's own conditions on its wall faces
+    (faces, or the cells of a face, with no brick beyond them; the mesh has
+    no periodic axis): a Dirichlet wall adds its coefficient area / h once
+    more to the centre and moves -2 (area / h) g to the right-hand side, a
+    Neumann wall with gradient g moves -area g there (the rules of
+    brick_operator, DirichletBoundaryCondition.C:19-51,
+    NeumannBoundaryCondition.C:19-56).  Returns (A, V, bdir)."""
+    import scipy.sparse as sp
+
+    A, V = union_operator(mesh)
+    lo = np.min([br.origin for br in mesh.bricks], axis=0)
+    hi = np.max([np.add(br.origin, br.N) for br in mesh.bricks], axis=0)
+    occupied = np.zeros(tuple(hi - lo), dtype=bool)
+    for br in mesh.bricks:
+        o = np.subtract(br.origin, lo)
+        occupied[o[0]:o[0] + br.N[0], o[1]:o[1] + br.N[1], o[2]:o[2] + br.N[2]] = True
+    ntot = A.shape[0]
+    diag = np.zeros(ntot)
+    bdir = np.zeros(ntot)
+    row0 = 0
+    for br in mesh.bricks:
+        n = br.N
+        idx = row0 + np.arange(int(np.prod(n))).reshape(n)
+        h = [br.cell_sizes(d) for d in range(3)]
+        o = np.subtract(br.origin, lo)
+        for d in range(3):
+            t1, t2 = (d + 1) % 3, (d + 2) % 3
+            for side in range(2):
+                kind, g = br.bc[2 * d + side], br.values[2 * d + side]
+                cell = 0 if side == 0 else n[d] - 1
+                outside = o[d] - 1 if side == 0 else o[d] + n[d]
+                sl = [slice(None)] * 3
+                sl[d] = slice(cell, cell + 1)
+                C = np.squeeze(idx[tuple(sl)], axis=d)  # (n[a], n[b]), a < b the two tangential axes
+                ta, tb = sorted((t1, t2))
+                area = h[ta][:, None] * h[tb][None, :]
+                if 0 <= outside < occupied.shape[d]:
+                    osl = [slice(None)] * 3
+                    osl[d] = outside
+                    osl[ta] = slice(o[ta], o[ta] + n[ta])
+                    osl[tb] = slice(o[tb], o[tb] + n[tb])
+                    wall = ~occupied[tuple(osl)]
+                else:
+                    wall = np.ones((n[ta], n[tb]), dtype=bool)
+                if kind == "Dirichlet":
+                    a = area / h[d][cell]
+                    diag[C[wall]] -= 2.0 * a[wall]
+                    bdir[C[wall]] -= 2.0 * a[wall] * g
+                elif kind == "Neumann" and g != 0.0:
+                    bdir[C[wall]] -= area[wall] * g
+        row0 += int(np.prod(n))
+    return (A + sp.diags(diag)).tocsr(), V, bdir
 
 
 def union_solve(mesh, b):

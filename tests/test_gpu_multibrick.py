@@ -9,14 +9,20 @@ lambdas.
   of the union-domain operator to 1e-10.
 * At full size (2.55 M cells) the FP64 and mixed solves reach 1e-8, checked
   with the union-domain operator on the host.
+* Dirichlet faces and Neumann gradients on the bricks' wall faces
+  (DirichletBoundaryCondition.C:19-80, NeumannBoundaryCondition.C:19-56,
+  per brick face): split bricks are bit-identical to the whole brick, and an
+  L-shaped three-brick domain matches the union-domain direct solve with the
+  same wall conditions to 1e-10.
 """
 import numpy as np
 import pytest
 
 import briscola_b200 as bb
 from briscola_b200 import workloads
-from briscola_b200.mesh import NEUMANN, PERIODIC, Brick, Mesh, geometric_points, uniform_points
-from tests.helpers import brick_to_compact, rel, split_brick, union_operator, union_solve, vmean
+from briscola_b200.mesh import DIRICHLET, NEUMANN, PERIODIC, Brick, Mesh, geometric_points, uniform_points
+from tests.helpers import (brick_to_compact, rel, split_brick, union_operator, union_operator_bc, union_solve,
+                           vmean)
 
 pytestmark = pytest.mark.gpu
 
@@ -33,6 +39,17 @@ SPLITS = {
                                  (PERIODIC, PERIODIC, NEUMANN, NEUMANN, PERIODIC, PERIODIC)), ([16], [], [8, 24])),
     "periodic_spanning": (lambda: Brick([uniform_points(16), uniform_points(32), uniform_points(16)],
                                         (NEUMANN, NEUMANN, NEUMANN, NEUMANN, PERIODIC, PERIODIC)), ([8], [16], [])),
+    # Dirichlet values and Neumann gradients on the wall faces (the pieces'
+    # faces in contact are interfaces and drop the brick's conditions)
+    "dirichlet_x2": (lambda: Brick([uniform_points(32)] * 3,
+                                   (DIRICHLET, NEUMANN, NEUMANN, DIRICHLET, NEUMANN, NEUMANN),
+                                   values=(1.0, 0.5, -0.25, 2.0, 0.0, 0.75)), ([16], [], [])),
+    "dirichlet_xyz8_graded": (lambda: Brick([uniform_points(32), geometric_points(32, 2.0), uniform_points(32)],
+                                            (DIRICHLET,) * 6, values=(1.0, -1.0, 0.5, 0.25, 2.0, -2.0)),
+                              ([16], [16], [16])),
+    "dirichlet_channel_xz": (lambda: Brick([uniform_points(32), geometric_points(16, 2.0), uniform_points(32)],
+                                           (PERIODIC, PERIODIC, DIRICHLET, DIRICHLET, PERIODIC, PERIODIC),
+                                           values=(0.0, 0.0, 1.0, -1.0, 0.0, 0.0)), ([16], [], [8, 24])),
 }
 
 
@@ -59,7 +76,8 @@ def _to_parts(parts, level, full, whole_shape):
     return np.concatenate(out)
 
 
-@pytest.mark.parametrize("name", ["x2", "y3", "xyz8", "periodic_x2", "channel_xz", "periodic_spanning"])
+@pytest.mark.parametrize("name", ["x2", "y3", "xyz8", "periodic_x2", "channel_xz", "periodic_spanning",
+                                  "dirichlet_x2", "dirichlet_xyz8_graded", "dirichlet_channel_xz"])
 @pytest.mark.parametrize("precision", [0, 1])
 def test_split_building_blocks_bit_identical(native, name, precision):
     br, whole, parts = _whole_and_parts(name)
@@ -200,3 +218,43 @@ def test_multibrick_full_size(native, precision):
     assert abs(r - rep.rel_residual) <= 1e-6 * r + 1e-15
     assert rep.final_residual <= 1e-8 * rep.initial_residual
     assert abs((V * x).sum()) <= 1e-12 * np.abs(V * x).sum()
+
+
+def _l_shape():
+    """Three 32 x 32 x 16 bricks in an L (cells of 1/64): A at the corner, B
+    beyond A along x, C beyond A along y; A-B and A-C share whole faces.
+    Dirichlet values on A's and C's x-lo, B's x-hi and y-lo and C's y-hi,
+    Neumann gradients on C's x-hi and A's z-lo, zero-gradient walls
+    elsewhere."""
+    h = 1 / 64
+
+    def pts(n, o):
+        return (o + np.arange(n + 1)) * h
+
+    D, N = DIRICHLET, NEUMANN
+    A = Brick([pts(32, 0), pts(32, 0), pts(16, 0)], (D, N, N, N, N, N), (0, 0, 0), (1.0, 0, 0, 0, 0.1, 0))
+    B = Brick([pts(32, 32), pts(32, 0), pts(16, 0)], (N, D, D, N, N, N), (32, 0, 0), (0, -0.5, 0.25, 0, 0, 0))
+    C = Brick([pts(32, 0), pts(32, 32), pts(16, 0)], (D, N, N, D, N, N), (0, 32, 0), (1.0, 0.3, 0, -1.0, 0, 0))
+    return Mesh([A, B, C])
+
+
+def test_multibrick_dirichlet_matches_union_direct_solve(native):
+    import scipy.sparse.linalg as spl
+
+    mesh = _l_shape()
+    A, V, bdir = union_operator_bc(mesh)
+    rng = np.random.default_rng(31)
+    b = -V * rng.standard_normal(V.size)
+    xref = spl.spsolve(A.tocsc(), b + bdir)
+    c = _ctx(mesh, relTol=1e-13, maxIter=200)
+    x = np.zeros_like(b)
+    rep = c.solve(b, x, zero_guess=True)
+    assert rep.status == 0
+    assert rel(x, xref) <= 1e-10
+    # the mixed solve with flexible CG, on the true residual of the union operator
+    c = _ctx(mesh, relTol=1e-10, precision="mixed", krylov="fcg", maxIter=100)
+    x = np.zeros_like(b)
+    rep = c.solve(b, x, zero_guess=True)
+    assert rep.status == 0
+    beff = b + bdir
+    assert np.linalg.norm(A @ x - beff) <= 2e-10 * np.linalg.norm(beff)

@@ -112,15 +112,55 @@ def test_valid_multibrick_passes_the_host_checks():
     assert "no usable" in _create_error(mesh)
 
 
-def test_dirichlet_and_gradients_on_multibrick_are_unsupported():
+@pytest.mark.skipif(not _no_gpu(), reason="a GPU is present")
+def test_dirichlet_and_gradients_on_multibrick_walls_pass_the_host_checks():
     bc = ("Dirichlet",) + ("Neumann",) * 5
     m = Mesh([Brick([_pts(8, 0), _pts(8, 0), _pts(8, 0)], bc, (0, 0, 0)),
               Brick([_pts(8, 0), _pts(8, 8), _pts(8, 0)], bc, (0, 8, 0))])
-    assert "unsupported" in _create_error(m)
+    assert "no usable" in _create_error(m)
     vals = (0.0, 0.5, 0.0, 0.0, 0.0, 0.0)
     m = Mesh([Brick([_pts(8, 0), _pts(8, 0), _pts(8, 0)], ("Neumann",) * 6, (0, 0, 0), vals),
               Brick([_pts(8, 0), _pts(8, 8), _pts(8, 0)], ("Neumann",) * 6, (0, 8, 0))])
-    assert "unsupported" in _create_error(m)
+    assert "no usable" in _create_error(m)
+    # faces wholly in contact are interfaces: their own conditions are ignored
+    m = Mesh([Brick([_pts(8, 0), _pts(8, 0), _pts(8, 0)], ("Dirichlet",) * 6, (0, 0, 0), (1.0,) * 6),
+              Brick([_pts(8, 0), _pts(8, 8), _pts(8, 0)], ("Dirichlet",) * 6, (0, 8, 0), (2.0,) * 6)])
+    assert "no usable" in _create_error(m)
+
+
+def test_conditions_on_faces_partly_in_contact_are_unsupported():
+    """brick 0's upper y face touches brick 1 over half its width; the other
+    half is a zero-gradient wall, which cannot take a Dirichlet value or a
+    gradient (the reference links whole faces only)"""
+    lower, upper = (0, 0, 0), (0, 8, 0)
+    for bc, vals in ((("Neumann",) * 3 + ("Dirichlet",) + ("Neumann",) * 2, (0.0,) * 6),
+                     (("Neumann",) * 6, (0.0, 0.0, 0.0, 0.25, 0.0, 0.0))):
+        m = Mesh([Brick([_pts(8, 0), _pts(8, 0), _pts(8, 0)], bc, lower, vals),
+                  Brick([_pts(4, 0), _pts(8, 8), _pts(8, 0)], ("Neumann",) * 6, upper)])
+        assert "unsupported" in _create_error(m)
+
+
+@pytest.mark.skipif(not _no_gpu(), reason="a GPU is present")
+def test_partial_contact_with_zero_gradient_walls_passes_the_host_checks():
+    m = Mesh([Brick([_pts(8, 0), _pts(8, 0), _pts(8, 0)], ("Neumann",) * 6, (0, 0, 0)),
+              Brick([_pts(4, 0), _pts(8, 8), _pts(8, 0)], ("Dirichlet",) + ("Neumann",) * 5, (0, 8, 0), (1.0,) * 6)])
+    assert "no usable" in _create_error(m)
+
+
+def test_union_operator_with_walls_of_split_brick_is_the_brick_operator():
+    from tests.helpers import brick_operator, union_operator_bc
+
+    pts = [uniform_points(8), geometric_points(6, 2.0), uniform_points(4)]
+    bc = ("Dirichlet", "Neumann", "Neumann", "Dirichlet", "Neumann", "Neumann")
+    vals = (1.0, 0.5, -0.25, 2.0, 0.0, 0.75)
+    br = Brick(pts, bc, values=vals)
+    A0, V0, b0 = brick_operator(pts, bc, vals)
+    A1, V1, b1 = union_operator_bc(Mesh([br]))
+    assert abs(A1 - A0).max() < 1e-15 and np.abs(b1 - b0).max() < 1e-15
+    parts = split_brick(br, ([4], [3], [2]))
+    A2, V2, b2 = union_operator_bc(parts)
+    perm = brick_to_compact(parts, np.arange(8 * 6 * 4).reshape(8, 6, 4))
+    assert abs(A0[perm][:, perm] - A2).max() < 1e-15 and np.abs(b0[perm] - b2).max() < 1e-15
 
 
 def test_unknown_face_type_and_bad_values_are_rejected():
