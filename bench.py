@@ -261,6 +261,10 @@ def profile_region(args, local):
     if args.profile_region == "mixed_fcg_fused":
         kw.update(autotune="off")  # the fused smoother on every level it fits (3 stages, 64-plane chunks)
     mesh, b, _ = workloads.channel(args.size)
+    if args.profile_region == "multibrick":
+        # the seven-brick mesh's mixed flexible-CG solve
+        kw = dict(precision="mixed", krylov="fcg", coarseLevel=0)
+        mesh, b, _ = workloads.multibrick(1)
     # the same kernels launched one by one (the profiler cannot see into a
     # graph with a conditional loop)
     if args.tuning:
@@ -475,7 +479,8 @@ def main():
     ap.add_argument("--learned-steps", type=int, default=2000)
     ap.add_argument("--learned-held", type=int, default=200)
     ap.add_argument("--no-learned-coarse", action="store_true")
-    ap.add_argument("--profile-region", choices=["mixed_fcg", "mixed_fcg_fused", "fp64", "unet_fwd", "fft", "fft_box"],
+    ap.add_argument("--profile-region", choices=["mixed_fcg", "mixed_fcg_fused", "fp64", "unet_fwd", "fft", "fft_box",
+                                                         "multibrick"],
                     default=None,
                     help="set up, warm up, then run one solve (or one U-Net forward) between "
                          "cudaProfilerStart/Stop for ncu --profile-from-start off; prints no bench line")

@@ -146,6 +146,7 @@ struct bmg_ctx {
     int ncoarse = 0;
     bool userLambda = false;  // a variable coefficient was given
     bool variable = false;    // kernels read face lambdas (user lambda or brick contacts)
+    bool conforming = true;   // every brick face in contact is wholly in contact (no contact mask)
     double* partials = nullptr;
     SolveState* st = nullptr;
     SolveState* st_host = nullptr;
@@ -774,7 +775,10 @@ void readBricks(bmg_ctx* c, const bmg_mesh_desc* mesh, HostLevel& L0) {
                 if (touching == (long)B.n[t1] * B.n[t2]) {
                     B.dirichlet[f] = 0;
                     B.dval[f] = 0.0;
-                } else if (B.dirichlet[f] || B.dval[f] != 0.0) {
+                    continue;
+                }
+                c->conforming = false;  // walls beside a contact: the contact mask
+                if (B.dirichlet[f] || B.dval[f] != 0.0) {
                     throw BadArg{BMG_UNSUPPORTED,
                                  "a Dirichlet value or a Neumann gradient on a brick face partly in contact with "
                                  "another brick"};
@@ -1127,8 +1131,10 @@ void build(bmg_ctx* c, HostLevel&& L0) {
             upload(L.gsrc, src);
         }
     }
-    // multi-brick meshes carry face lambdas for their contacts
-    c->variable = c->multi;
+    // multi-brick meshes whose faces are partly in contact carry face
+    // lambdas (the contact mask); where every contact covers whole faces
+    // the tables alone describe the operator
+    c->variable = c->multi && !c->conforming;
     if (c->multi) uploadLambda(c);
     buildTransfers(c);
     c->partials = dalloc<double>(3 * reduce_blocks(bricks<double>(c, 0)));
@@ -2137,7 +2143,7 @@ int bmg_set_coefficients(bmg_ctx* c, const double* lx, const double* ly, const d
             restrictLambda(c, src);
             c->userLambda = true;
         }
-        c->variable = c->userLambda || c->multi;
+        c->variable = c->userLambda || (c->multi && !c->conforming);
         if (c->variable) uploadLambda(c);
         refreshCoarseInverse(c);
         destroyGraph(c);  // kernels differ between constant and variable coefficients

@@ -7,10 +7,11 @@
 // over all bricks of a level in one launch: the grid's z index walks the
 // planes of brick 0, then brick 1, and so on.
 
+#include <algorithm>
+#include <cmath>
+
 #include "bmg_grid.cuh"
 #include "bmg_stencil.cuh"
-
-#include <cmath>
 
 namespace bmg {
 
@@ -870,15 +871,19 @@ __global__ void __launch_bounds__(256) k_prolong_split(Bricks<T> FB, Bricks<T> C
 // factored once per matrix on the host in FP64.  cidx gives the slab index of every
 // unknown (bricks one after another, k fastest).
 // ---------------------------------------------------------------------------
-// one CTA (any multiple of 32 threads); sb: n doubles of shared memory
+// rows r0, r0 + rstep, ... of x = A^-1 b, one warp per row (the CTA's
+// warps take consecutive rows); sb: n doubles of shared memory.  A row's
+// sum is formed the same way whichever CTA forms it.
 template <typename T>
 __device__ __forceinline__ void coarse_solve_block(const Bricks<T>& CB, const double* __restrict__ ainv,
-                                                   const int* __restrict__ cidx, int n, double* sb) {
+                                                   const int* __restrict__ cidx, int n, double* sb, int r0 = 0,
+                                                   int rstep = 0) {
     const T* bsrc = CB.v[0].b;
     for (int q = threadIdx.x; q < n; q += blockDim.x) sb[q] = (double)bsrc[cidx[q]];
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int r = warp; r < n; r += nw) {
+    if (rstep == 0) rstep = nw;
+    for (int r = r0 + warp; r < n; r += rstep) {
         double s = 0.0;
         for (int l = lane; l < n; l += 32) s += ainv[(long)r * n + l] * sb[l];
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
@@ -896,11 +901,14 @@ __device__ __forceinline__ void coarse_solve_block(const Bricks<T>& CB, const do
     }
 }
 
+// the dense coarse solve over many CTAs: CTA c takes rows 8c .. 8c + 7,
+// then 8 (c + gridDim.x) .., so the inverse streams through all SMs
 template <typename T>
 __global__ void __launch_bounds__(256) k_coarse_solve(Bricks<T> CB, const double* __restrict__ ainv,
                                                       const int* __restrict__ cidx, int n) {
     extern __shared__ double sb[];
-    coarse_solve_block<T>(CB, ainv, cidx, n, sb);
+    const int nw = blockDim.x >> 5;
+    coarse_solve_block<T>(CB, ainv, cidx, n, sb, blockIdx.x * nw, gridDim.x * nw);
 }
 
 // ---------------------------------------------------------------------------
@@ -1330,7 +1338,8 @@ void launch_prolong_correct(const Bricks<T>& F, const Bricks<T>& C, const Transf
 
 template <typename T>
 void launch_coarse_solve(const Bricks<T>& C, const double* ainv, const int* cidx, int n, cudaStream_t s) {
-    k_coarse_solve<T><<<1, 256, n * sizeof(double), s>>>(C, ainv, cidx, n);
+    const int grid = std::min((n + 7) / 8, 1184);  // 8 rows (warps) per CTA
+    k_coarse_solve<T><<<grid, 256, n * sizeof(double), s>>>(C, ainv, cidx, n);
 }
 
 template <typename T, bool VAR>
