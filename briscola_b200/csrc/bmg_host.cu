@@ -170,9 +170,9 @@ struct bmg_ctx {
     cudaStream_t capStream = nullptr;  // private stream used only for capture
     // a level solver in place of the FP32 cycle's recursion below hookLevel
     // (bmg_set_level_solver), with its right-hand side and result arrays
-    // level 0's first FP32 colour pass of the next cycle was written by the
-    // flexible-CG kernel that made its right-hand side (FirstPass)
-    bool skipFirst0 = false;
+    // the next FP32 cycle starts from z = 0 on a parity-split level 0: its
+    // first colour pass writes the whole level (no memset before it)
+    bool zeroFirst0 = false;
     int hookLevel = -1;
     int hookMode = BMG_LEVEL_REPLACE;
     bmg_level_solver hook = nullptr;
@@ -1245,10 +1245,11 @@ void smooth(bmg_ctx* c, int l, int sweeps) {
     cudaStream_t s = c->stream;
     HostLevel& H = c->lv[l];
     const int prec = sizeof(T) == 8 ? 0 : 1;
-    std::vector<int> seq = colourSequence(H, sweeps);
-    if (sizeof(T) == 4 && l == 0 && c->skipFirst0) {  // the first pass is done (FirstPass)
-        seq.erase(seq.begin());
-        c->skipFirst0 = false;
+    const std::vector<int> seq = colourSequence(H, sweeps);
+    bool zeroFirst = false;  // the first pass starts from x = 0 (zeroFirst0)
+    if (sizeof(T) == 4 && l == 0 && c->zeroFirst0) {
+        zeroFirst = true;
+        c->zeroFirst0 = false;
     }
     // (the fused smoother does not keep a pinned cell: a pinned level runs
     // pass by pass)
@@ -1296,9 +1297,10 @@ void smooth(bmg_ctx* c, int l, int sweeps) {
         exchange<T>(c, l);
         c->launches += 1;
         if (c->variable)
-            launch_colour_pass<T, true>(B, col, s);
+            launch_colour_pass<T, true>(B, col, s, zeroFirst);
         else
-            launch_colour_pass<T, false>(B, col, s);
+            launch_colour_pass<T, false>(B, col, s, zeroFirst);
+        zeroFirst = false;
     }
 }
 
@@ -1587,7 +1589,7 @@ SolveState initialState(const bmg_ctx* c) {
 // first convergence test.  The state is copied from the pinned host copy,
 // which the caller fills before every solve (also when replayed as a graph).
 void segInitFcg(bmg_ctx* c, const double* bsrc, const double* xsrc, bool zero, bool setCondition);
-FirstPass firstPass(const bmg_ctx* c);
+bool zeroFirst(const bmg_ctx* c);
 void segBodyFcg(bmg_ctx* c, bool setCondition);
 void segPostFcg(bmg_ctx* c, double* xdst);
 
@@ -1652,28 +1654,18 @@ Bricks<double> fcgView(const bmg_ctx* c) {
     return V;
 }
 
-// Whether the flexible-CG kernels that write the FP32 cycle's right-hand
-// side also write its first level-0 colour pass (FirstPass): a mixed
-// flexible-CG solve of one brick with constant coefficients whose level 0 is
-// smoothed by red-black passes before anything else reads its x.
-FirstPass firstPass(const bmg_ctx* c) {
-    FirstPass fp{nullptr, nullptr, 0};
-    const HostLevel& L0 = c->lv[0];
-    if (!c->opt.fuse_first || c->opt.precision != BMG_PRECISION_MIXED || c->opt.krylov != BMG_KRYLOV_FCG ||
-        c->variable || c->multi ||
-        c->opt.smoother != BMG_SMOOTHER_RBGS || c->opt.n_pre < 1 || c->tail == 0 || L0.br[0].n[2] % 4)
-        return fp;
-    fp.z = L0.x32;
-    fp.tab = L0.tab32;
-    fp.colour = colourSequence(L0, c->opt.n_pre)[0];
-    return fp;
+// Whether each FP32 cycle of a mixed flexible-CG solve starts with a
+// zero-start first colour pass on level 0 (fuseFirstPass) instead of a
+// memset and a pass: a parity-split level 0 smoothed by red-black passes
+// before anything else reads its x.
+bool zeroFirst(const bmg_ctx* c) {
+    return c->opt.fuse_first && c->opt.precision == BMG_PRECISION_MIXED && c->opt.krylov == BMG_KRYLOV_FCG &&
+           c->lv[0].ks && c->opt.smoother == BMG_SMOOTHER_RBGS && c->opt.n_pre >= 1 && c->tail != 0 &&
+           c->hookLevel != 0;
 }
 
 void segInitFcg(bmg_ctx* c, const double* bsrc, const double* xsrc, bool zero, bool setCondition) {
     cudaStream_t s = c->stream;
-    const FirstPass fp = firstPass(c);
-    // ghosts and cells the first pass leaves alone start at zero
-    if (fp.z) BMG_CUDA(cudaMemsetAsync(c->lv[0].x32, 0, c->lv[0].cells * sizeof(float), s));
     const Bricks<double> V = fcgView(c);
     const bool mixed = c->opt.precision == BMG_PRECISION_MIXED;
     launch_load_b(V, walls(c), bsrc, s);
@@ -1692,9 +1684,9 @@ void segInitFcg(bmg_ctx* c, const double* bsrc, const double* xsrc, bool zero, b
     float* pre32 = mixed ? c->lv[0].b32 : nullptr;
     double* pre64 = mixed ? nullptr : c->lv[0].b64;
     if (c->variable)
-        launch_fcg_residual<true>(V, walls(c), 0, c->fr, pre32, pre64, c->partials, fp, s);
+        launch_fcg_residual<true>(V, walls(c), 0, c->fr, pre32, pre64, c->partials, s);
     else
-        launch_fcg_residual<false>(V, walls(c), 0, c->fr, pre32, pre64, c->partials, fp, s);
+        launch_fcg_residual<false>(V, walls(c), 0, c->fr, pre32, pre64, c->partials, s);
     launch_finalize(V, c->partials, c->st, 0, c->cond, setCondition ? 1 : 0, s);
     c->launches += 2;
 }
@@ -1703,14 +1695,12 @@ template <typename T>
 void fcgStep(bmg_ctx* c, const T* z, float* pre32, double* pre64, bool setCondition) {
     cudaStream_t s = c->stream;
     const Bricks<double> V = fcgView(c);
-    launch_fcg_beta<T>(V, z, c->fr, c->fq, c->partials, c->st, s);
     if (c->variable)
-        launch_fcg_direction<T, true>(V, z, c->fp, c->fq, c->partials, c->st, s);
+        launch_fcg_step<T, true>(V, z, c->fp, c->fq, c->fr, pre32, pre64, c->partials, c->st, s);
     else
-        launch_fcg_direction<T, false>(V, z, c->fp, c->fq, c->partials, c->st, s);
-    launch_fcg_update(V, c->fp, c->fr, c->fq, pre32, pre64, c->partials, c->st, firstPass(c), s);
+        launch_fcg_step<T, false>(V, z, c->fp, c->fq, c->fr, pre32, pre64, c->partials, c->st, s);
     launch_finalize_n(c->partials, fcg_partials(V), c->st, 1, c->cond, setCondition ? 1 : 0, s);
-    c->launches += 6;
+    c->launches += fcg_step_launches(V) + 1;
 }
 
 // one preconditioning cycle z = cycle(r) from a zero guess, then one FCG step
@@ -1719,14 +1709,14 @@ void segBodyFcg(bmg_ctx* c, bool setCondition) {
     HostLevel& L0 = c->lv[0];
     std::fill(c->visits.begin(), c->visits.end(), 0);
     if (c->opt.precision == BMG_PRECISION_MIXED) {
-        // z = 0 and its first colour pass were written with the right-hand
-        // side (FirstPass), or z starts from zero here
-        if (firstPass(c).z)
-            c->skipFirst0 = true;
+        // z starts from zero: the cycle's first level-0 pass writes all of
+        // it (zeroFirst), or a memset does
+        if (zeroFirst(c))
+            c->zeroFirst0 = true;
         else
             BMG_CUDA(cudaMemsetAsync(L0.x32, 0, L0.cells * sizeof(float), s));
         cycle<float>(c, 0);
-        c->skipFirst0 = false;
+        c->zeroFirst0 = false;
         exchange<float>(c, 0);
         fcgStep<float>(c, L0.x32, L0.b32, nullptr, setCondition);
     } else {
@@ -1743,9 +1733,9 @@ void segPostFcg(bmg_ctx* c, double* xdst) {
     const Bricks<double> V = fcgView(c);
     exchangeField<double>(c, 0, c->fx);
     if (c->variable)
-        launch_fcg_residual<true>(V, walls(c), 2, nullptr, nullptr, nullptr, c->partials, FirstPass{}, s);
+        launch_fcg_residual<true>(V, walls(c), 2, nullptr, nullptr, nullptr, c->partials, s);
     else
-        launch_fcg_residual<false>(V, walls(c), 2, nullptr, nullptr, nullptr, c->partials, FirstPass{}, s);
+        launch_fcg_residual<false>(V, walls(c), 2, nullptr, nullptr, nullptr, c->partials, s);
     launch_fcg_true_norm(V, c->partials, c->st, s);
     c->launches += 2;
     if (c->opt.remove_mean && c->singular) {

@@ -192,8 +192,10 @@ struct TailPlan {
 };
 
 // ---- launchers (bmg_kernels.cu) -------------------------------------------
+// zero (parity-split levels only): the pass starts from x = 0 -- x is not
+// read, and the whole level (both colours, periodic images) is written
 template <typename T, bool VAR>
-void launch_colour_pass(const Bricks<T>& B, int colour, cudaStream_t s);
+void launch_colour_pass(const Bricks<T>& B, int colour, cudaStream_t s, bool zero = false);
 template <typename T, bool VAR>
 void launch_jacobi(const Bricks<T>& B, T* tmp, cudaStream_t s);
 template <typename T, bool VAR>
@@ -227,36 +229,22 @@ long reduce_blocks(const Bricks<double>& B);
 // sets the dynamic shared memory limits of the fused smoother instances
 void configure_fused_kernels();
 
-// The first colour pass of the next FP32 preconditioning cycle, written by
-// the kernel that produces the cycle's right-hand side: the cycle starts
-// from z = 0, so its first pass sets the cells of `colour` to gs_value with
-// zero neighbours and leaves the others at 0.  z == nullptr: not written
-// (constant coefficients only; the tables are level 0's FP32 ones).
-struct FirstPass {
-    float* z;
-    const float* tab;
-    int colour;
-};
-
 // ---- flexible CG outer loop (bmg_krylov.cu), level 0, FP64 ------------------
 // r = b - A'x into r (and the cycle's right-hand side pre32 or pre64);
 // partials as launch_residual_norm.  mode 2: only ||V r||^2, nothing written.
 template <bool VAR>
 void launch_fcg_residual(const Bricks<double>& B, const Walls& W, int mode, double* r, float* pre32, double* pre64,
-                         double* partials, FirstPass fp, cudaStream_t s);
-// partials of (z, V r) and (z, V q), then beta and gamma (kernel pair)
-template <typename T>
-void launch_fcg_beta(const Bricks<double>& B, const T* z, const double* r, const double* q, double* partials,
-                     SolveState* st, cudaStream_t s);
-// p = z + beta p, q = A'z + beta q, partials of (p, V q), then alpha
+                         double* partials, cudaStream_t s);
+// one FCG(1) step after the cycle z = M(r): beta, p = z + beta p,
+// q = A'z + beta q, alpha, x += alpha p (B.x, periodic write-through),
+// r -= alpha q, pre = r, and the partials of ||V r||^2 -- two passes and
+// one reduction on rows of whole quads, three passes otherwise
 template <typename T, bool VAR>
-void launch_fcg_direction(const Bricks<double>& B, const T* z, double* p, double* q, double* partials,
-                          SolveState* st, cudaStream_t s);
-// x += alpha p (B.x, periodic write-through), r -= alpha q, pre = r,
-// partials of ||V r||^2
-void launch_fcg_update(const Bricks<double>& B, const double* p, double* r, const double* q, float* pre32,
-                       double* pre64, double* partials, const SolveState* st, FirstPass fp, cudaStream_t s);
-// number of per-block partials the FCG dots / direction / update kernels write
+void launch_fcg_step(const Bricks<double>& B, const T* z, double* p, double* q, double* r, float* pre32,
+                     double* pre64, double* partials, SolveState* st, cudaStream_t s);
+// kernels launch_fcg_step launches
+int fcg_step_launches(const Bricks<double>& B);
+// number of per-block partials the FCG step kernels write
 long fcg_partials(const Bricks<double>& B);
 // the convergence decision from n partials (as launch_finalize)
 void launch_finalize_n(const double* partials, long n, SolveState* st, int mode, cudaGraphConditionalHandle cond,

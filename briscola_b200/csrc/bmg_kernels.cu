@@ -291,7 +291,11 @@ struct Vec16<double> {
     }
 };
 
-template <typename T, bool VAR>
+// ZERO: the first pass of a cycle that starts from x = 0 -- no x is read
+// (every neighbour is zero), and the thread also writes zero to the other
+// half's same slots, so the pass leaves the whole level written (the
+// arithmetic of a pass over a zeroed x).
+template <typename T, bool VAR, bool ZERO>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 && !VAR ? 5 : 1) k_colour_split(LevelView<T> L, int colour) {
     constexpr int NC = Vec16<T>::N;  // cells per thread
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -312,13 +316,19 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 && !VAR ? 5 : 1) k_colour_
     const int ext = h == 0 ? (m0 > 0 ? oth - 1 : row - 1) : (m0 + NC < kh ? oth + NC : row + 2 * kh);
     // every load is issued before any is used, so one memory latency covers them
     T xo[NC], xm[NC], xp[NC], ym[NC], yp[NC], bb[NC], wkl[NC], wkh[NC];
-    Vec16<T>::ld(L.x + oth, xo);
-    Vec16<T>::ld(L.x + own - si, xm);
-    Vec16<T>::ld(L.x + own + si, xp);
-    Vec16<T>::ld(L.x + own - sj, ym);
-    Vec16<T>::ld(L.x + own + sj, yp);
+    T e = T(0);
+    if constexpr (ZERO) {
+#pragma unroll
+        for (int m = 0; m < NC; ++m) xo[m] = xm[m] = xp[m] = ym[m] = yp[m] = T(0);
+    } else {
+        Vec16<T>::ld(L.x + oth, xo);
+        Vec16<T>::ld(L.x + own - si, xm);
+        Vec16<T>::ld(L.x + own + si, xp);
+        Vec16<T>::ld(L.x + own - sj, ym);
+        Vec16<T>::ld(L.x + own + sj, yp);
+        e = L.x[ext];
+    }
     Vec16<T>::ld(L.b + own, bb);
-    const T e = L.x[ext];
     Vec16<T>::ldg(L.tab + L.to.kwl + (own - row), wkl);
     Vec16<T>::ldg(L.tab + L.to.kwh + (own - row), wkh);
     const T wil = ldg(L.tab + L.to.wl[0] + i), wih = ldg(L.tab + L.to.wh[0] + i);
@@ -355,12 +365,23 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 && !VAR ? 5 : 1) k_colour_
         v[m] = gs_value(w, xn, bb[m]);
     }
     // the pinned cell (0,0,0), when this pass updates it, keeps its value
-    if (L.pin && (i | j | h | m0) == 0) v[0] = L.x[own];
+    if (L.pin && (i | j | h | m0) == 0) v[0] = ZERO ? T(0) : L.x[own];
     Vec16<T>::st(L.x + own, v);
-    if ((L.per0 && (i == 0 || i == L.n0 - 1)) || (L.per1 && (j == 0 || j == L.n1 - 1)) ||
-        (L.per2 && (((h | m0) == 0) || (h == 1 && m0 + NC == kh)))) {
+    const bool edge_ij = (L.per0 && (i == 0 || i == L.n0 - 1)) || (L.per1 && (j == 0 || j == L.n1 - 1));
+    if (edge_ij || (L.per2 && (((h | m0) == 0) || (h == 1 && m0 + NC == kh)))) {
 #pragma unroll
         for (int m = 0; m < NC; ++m) store_images(L, own + m, i, j, 2 * (m0 + m) + h, v[m]);
+    }
+    if constexpr (ZERO) {
+        T zero[NC];
+#pragma unroll
+        for (int m = 0; m < NC; ++m) zero[m] = T(0);
+        Vec16<T>::st(L.x + oth, zero);
+        const int ho = 1 - h;
+        if (edge_ij || (L.per2 && (((ho | m0) == 0) || (ho == 1 && m0 + NC == kh)))) {
+#pragma unroll
+            for (int m = 0; m < NC; ++m) store_images(L, oth + m, i, j, 2 * (m0 + m) + ho, T(0));
+        }
     }
 }
 
@@ -1250,7 +1271,7 @@ long reduce_blocks(const Bricks<double>& B) {
 }
 
 template <typename T, bool VAR>
-void launch_colour_pass(const Bricks<T>& B, int colour, cudaStream_t s) {
+void launch_colour_pass(const Bricks<T>& B, int colour, cudaStream_t s, bool zero) {
     if (B.v[0].kh) {  // parity-split rows (single brick, n2 % 16 == 0)
         const LevelView<T>& L = B.v[0];
         const int tr = L.kh / (16 / (int)sizeof(T));  // threads per half row
@@ -1258,7 +1279,10 @@ void launch_colour_pass(const Bricks<T>& B, int colour, cudaStream_t s) {
         while (bx < tr && bx < 32) bx *= 2;
         const dim3 blk(bx, 256 / bx, 1);
         const dim3 grid((tr + bx - 1) / bx, (L.n1 + blk.y - 1) / blk.y, L.n0);
-        k_colour_split<T, VAR><<<grid, blk, 0, s>>>(L, colour);
+        if (zero)
+            k_colour_split<T, VAR, true><<<grid, blk, 0, s>>>(L, colour);
+        else
+            k_colour_split<T, VAR, false><<<grid, blk, 0, s>>>(L, colour);
         return;
     }
     bool quads = true;
@@ -1435,7 +1459,7 @@ void launch_add_correction(const Bricks<double>& B, const Bricks<float>& E, cuda
 
 // explicit instantiations
 #define BMG_INST(T, V)                                                                                   \
-    template void launch_colour_pass<T, V>(const Bricks<T>&, int, cudaStream_t);                         \
+    template void launch_colour_pass<T, V>(const Bricks<T>&, int, cudaStream_t, bool);                   \
     template void launch_jacobi<T, V>(const Bricks<T>&, T*, cudaStream_t);                               \
     template void launch_residual_restrict<T, V>(const Bricks<T>&, const Bricks<T>&, const TransferSet&, \
                                                  cudaStream_t);                                          \

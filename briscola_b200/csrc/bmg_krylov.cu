@@ -33,24 +33,12 @@ __device__ __forceinline__ double cell_volume(const LevelView<double>& L, int i,
     return L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j] * L.tab64[L.to.h[2] + k];
 }
 
-// The next cycle's first colour pass for cell (i,j,k) of right-hand side f
-// (FirstPass): gs_value with zero neighbours on the cells of fp.colour, the
-// arithmetic of the colour-pass kernels on x = 0, and 0 elsewhere.
-__device__ __forceinline__ float first_pass_value(const LevelView<double>& L, const FirstPass& fp, int i, int j,
-                                                  int k, float f) {
-    if (((i + j + k + L.cpar) & 1) != fp.colour) return 0.f;
-    const float w[6] = {ldg(fp.tab + L.to.wl[0] + i), ldg(fp.tab + L.to.wh[0] + i), ldg(fp.tab + L.to.wl[1] + j),
-                        ldg(fp.tab + L.to.wh[1] + j), ldg(fp.tab + L.to.wl[2] + k), ldg(fp.tab + L.to.wh[2] + k)};
-    const float zero[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    return gs_value(w, zero, f);
-}
-
 // r = b - A'x (FP64), written to r and to the cycle's right-hand side;
 // partials: ||V r||^2 and, for mode 0, the normFactor sum (as k_residual_norm)
 template <bool VAR>
 __global__ void __launch_bounds__(kReduceThreads) k_fcg_residual(Bricks<double> B, Walls W, int mode, double* r_out,
                                                                  float* pre32, double* pre64, double* partials,
-                                                                 long nblocks, FirstPass fp) {
+                                                                 long nblocks) {
     __shared__ double sh[kReduceThreads / 32];
     int i;
     const int bk = brick_of(B, blockIdx.z, i);
@@ -79,11 +67,6 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_residual(Bricks<double> 
             r_out[c] = r;
             if (pre32) pre32[c] = (float)r;
             if (pre64) pre64[c] = r;
-            if (fp.z) {
-                const float z = first_pass_value(L, fp, i, j, k, (float)r);
-                fp.z[c] = z;
-                store_images_to(L, fp.z, c, i, j, k, z);
-            }
         }
     }
     const long bid = block_id();
@@ -288,175 +271,96 @@ struct Quad4<float> {
         }                                                                                  \
     }
 
-template <typename T>
-__global__ void __launch_bounds__(kReduceThreads) k_fcg_dots4(Bricks<double> B, const T* z, const double* r,
-                                                              const double* q, double* partials, long nblocks) {
+// ---- two passes per flexible-CG step (the FCG(1) recurrences above with
+// one reduction): pass 1 forms (z, V r), (z, V q_prev) and (z, V A'z), A'z
+// by the stencil on z; k_fcg_coeffs derives beta = -(z, V q_prev) /
+// (p_prev, V q_prev) and, since V A' is symmetric (so (p_prev, V A'z) =
+// (z, V q_prev)),
+//   (p, V q) = (z, V A'z) + 2 beta (z, V q_prev) + beta^2 (p_prev, V q_prev)
+//            = (z, V A'z) + beta (z, V q_prev),
+// and alpha = (z, V r) / (p, V q); pass 2 forms A'z again and updates p, q,
+// x and r in one sweep, writes the cycle's right-hand side and the partials
+// of ||V r||^2.  Per cell the streams are z, r, q (pass 1) and z, p, q, x,
+// r in, p, q, x, r and the FP32 right-hand side out (pass 2).
+
+// A'z of the quad at c (natural or split rows), the k couplings of the four
+// cells, and their volumes: the stencil of k_fcg_direction4
+#define BMG_QUAD_AZ(z, Az, zc)                                                                         \
+    T zc[4], zim_[4], zip_[4], zjm_[4], zjp_[4];                                                        \
+    Quad4<T>::ld(z + c, ks, zc);                                                                        \
+    Quad4<T>::ld(z + c - L.si, ks, zim_);                                                               \
+    Quad4<T>::ld(z + c + L.si, ks, zip_);                                                               \
+    Quad4<T>::ld(z + c - L.sj, ks, zjm_);                                                               \
+    Quad4<T>::ld(z + c + L.sj, ks, zjp_);                                                               \
+    const long cr_ = row + kpos(L, k0 + 4);                                                             \
+    const T zl_ = z[row + kpos(L, k0 - 1)], zr_ = z[cr_];                                               \
+    double Az[4];                                                                                      \
+    for (int e = 0; e < 4; ++e) {                                                                       \
+        double w[6];                                                                                    \
+        couplings<double, VAR>(L, i, j, k0 + e, c + quad_off(ks, e), e < 3 ? c + quad_off(ks, e + 1) : cr_, w); \
+        const double km = e > 0 ? (double)zc[e - 1] : (double)zl_;                                      \
+        const double kp = e < 3 ? (double)zc[e + 1] : (double)zr_;                                      \
+        const double sv = w[0] * (double)zim_[e] + w[1] * (double)zip_[e] + w[2] * (double)zjm_[e] +     \
+                          w[3] * (double)zjp_[e] + w[4] * km + w[5] * kp;                               \
+        const double d = w[0] + w[1] + w[2] + w[3] + w[4] + w[5];                                       \
+        Az[e] = sv - d * (double)zc[e];                                                                 \
+    }
+
+template <typename T, bool VAR>
+__global__ void __launch_bounds__(kReduceThreads) k_fcg_dots3_4(Bricks<double> B, const T* z, const double* r,
+                                                                const double* q, double* partials, long nblocks) {
     __shared__ double sh[kReduceThreads / 32];
-    double a1 = 0.0, a2 = 0.0;
+    double a1 = 0.0, a2 = 0.0, a3 = 0.0;
     BMG_QUAD_LOOP(B, {
-        T zq[4];
+        BMG_QUAD_AZ(z, Az, zc)
         double rq[4], qq[4];
-        Quad4<T>::ld(z + c, ks, zq);
         Quad4<double>::ld(r + c, ks, rq);
         Quad4<double>::ld(q + c, ks, qq);
         for (int e = 0; e < 4; ++e) {
-            const double Vz = (hij * hk[e]) * (double)zq[e];
+            const double Vz = (hij * hk[e]) * (double)zc[e];
             a1 += Vz * rq[e];
             a2 += Vz * qq[e];
+            a3 += Vz * Az[e];
         }
     })
     a1 = block_sum<kReduceThreads>(a1, sh);
     a2 = block_sum<kReduceThreads>(a2, sh);
+    a3 = block_sum<kReduceThreads>(a3, sh);
     if (threadIdx.x == 0 && threadIdx.y == 0) {
         const long bid = block_id();
         partials[bid] = a1;
         partials[nblocks + bid] = a2;
+        partials[2 * nblocks + bid] = a3;
     }
 }
 
 template <typename T, bool VAR>
-__global__ void __launch_bounds__(kReduceThreads) k_fcg_direction4(Bricks<double> B, const T* z, double* p,
-                                                                   double* q, double* partials,
-                                                                   const SolveState* st) {
+__global__ void __launch_bounds__(kReduceThreads) k_fcg_step4(Bricks<double> B, const T* z, double* p, double* q,
+                                                              double* r, float* pre32, double* pre64,
+                                                              double* partials, const SolveState* st) {
     __shared__ double sh[kReduceThreads / 32];
-    const double beta = st->beta;
+    const double beta = st->beta, alpha = st->alpha;
     double a = 0.0;
     BMG_QUAD_LOOP(B, {
-        T zc[4], zim[4], zip[4], zjm[4], zjp[4];
-        Quad4<T>::ld(z + c, ks, zc);
-        Quad4<T>::ld(z + c - L.si, ks, zim);
-        Quad4<T>::ld(z + c + L.si, ks, zip);
-        Quad4<T>::ld(z + c - L.sj, ks, zjm);
-        Quad4<T>::ld(z + c + L.sj, ks, zjp);
-        const long cr = row + kpos(L, k0 + 4);
-        const T zl = z[row + kpos(L, k0 - 1)], zr = z[cr];
-        double pq[4], qq[4], pn[4], qn[4];
+        BMG_QUAD_AZ(z, Az, zc)
+        double pq[4], qq[4], xq[4], rq[4], rn[4];
         Quad4<double>::ld(p + c, ks, pq);
         Quad4<double>::ld(q + c, ks, qq);
-        for (int e = 0; e < 4; ++e) {
-            double w[6];
-            couplings<double, VAR>(L, i, j, k0 + e, c + quad_off(ks, e), e < 3 ? c + quad_off(ks, e + 1) : cr, w);
-            const double km = e > 0 ? (double)zc[e - 1] : (double)zl;
-            const double kp = e < 3 ? (double)zc[e + 1] : (double)zr;
-            const double zz = (double)zc[e];
-            const double sv = w[0] * (double)zim[e] + w[1] * (double)zip[e] + w[2] * (double)zjm[e] +
-                              w[3] * (double)zjp[e] + w[4] * km + w[5] * kp;
-            const double d = w[0] + w[1] + w[2] + w[3] + w[4] + w[5];
-            // on the first step p and q hold whatever the last solve left
-            pn[e] = beta != 0.0 ? zz + beta * pq[e] : zz;
-            qn[e] = beta != 0.0 ? (sv - d * zz) + beta * qq[e] : sv - d * zz;
-            a += (hij * hk[e]) * pn[e] * qn[e];
-        }
-        Quad4<double>::st(p + c, ks, pn);
-        Quad4<double>::st(q + c, ks, qn);
-    })
-    a = block_sum<kReduceThreads>(a, sh);
-    if (threadIdx.x == 0 && threadIdx.y == 0) partials[block_id()] = a;
-}
-
-// The same direction step on a parity-split level 0 (one brick): the
-// thread owns four consecutive positions of one half of a row, the cells
-// k = 2 (m0 + e) + h of one parity, so z, its neighbours and p and q load as
-// whole vectors; the k neighbours are the other half's same slots and one
-// beyond them (as in k_colour_split).  Per cell the arithmetic is
-// k_fcg_direction4's; the partial sums group the cells differently.
-template <typename T, bool VAR>
-__global__ void __launch_bounds__(kReduceThreads, VAR ? 2 : 3) k_fcg_direction_split(Bricks<double> B, const T* z, double* p,
-                                                                        double* q, double* partials,
-                                                                        const SolveState* st) {
-    __shared__ double sh[kReduceThreads / 32];
-    const double beta = st->beta;
-    double a = 0.0;
-    const LevelView<double>& L = B.v[0];
-    const int qx = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int kh = L.kh;
-    if (j < L.n1 && 4 * qx < L.n2) {
-        const int h = 4 * qx >= kh ? 1 : 0;
-        const int m0 = 4 * qx - h * kh;
-        const double wjl = L.tab64[L.to.wl[1] + j], wjh = L.tab64[L.to.wh[1] + j];
-        const double hj = L.tab64[L.to.h[1] + j];
-        for (int i = blockIdx.z; i < L.n0; i += gridDim.z) {
-            const long row = row_at(L, i, j), c = row + 4 * qx;
-            const long co = row + (1 - h) * kh + m0;  // the other half, same slots
-            const long ce = h == 0 ? (m0 > 0 ? co - 1 : row - 1) : (m0 + 4 < kh ? co + 4 : row + 2 * kh);
-            T zc[4], zo[4], zim[4], zip[4], zjm[4], zjp[4];
-            Quad4<T>::ld(z + c, 0, zc);
-            Quad4<T>::ld(z + co, 0, zo);
-            Quad4<T>::ld(z + c - L.si, 0, zim);
-            Quad4<T>::ld(z + c + L.si, 0, zip);
-            Quad4<T>::ld(z + c - L.sj, 0, zjm);
-            Quad4<T>::ld(z + c + L.sj, 0, zjp);
-            const T ze = z[ce];
-            double pq[4], qq[4], pn[4], qn[4];
-            Quad4<double>::ld(p + c, 0, pq);
-            Quad4<double>::ld(q + c, 0, qq);
-            const double wil = L.tab64[L.to.wl[0] + i], wih = L.tab64[L.to.wh[0] + i];
-            const double hij = L.tab64[L.to.h[0] + i] * hj;
-            // k couplings and cell sizes of the four cells, from the tables
-            // kept in the rows' storage order (contiguous)
-            double wkl[4], wkh[4], hk[4];
-            Quad4<double>::ld(L.tab64 + L.to.kwl + 4 * qx, 0, wkl);
-            Quad4<double>::ld(L.tab64 + L.to.kwh + 4 * qx, 0, wkh);
-            Quad4<double>::ld(L.tab64 + L.to.ksz + 4 * qx, 0, hk);
-            double l0[4], l0p[4], l1[4], l1p[4], l2[4], l2o[4], l2e = 1.0;
-            if (VAR) {
-                Quad4<double>::ld(L.lam0 + c, 0, l0);
-                Quad4<double>::ld(L.lam0 + c + L.si, 0, l0p);
-                Quad4<double>::ld(L.lam1 + c, 0, l1);
-                Quad4<double>::ld(L.lam1 + c + L.sj, 0, l1p);
-                Quad4<double>::ld(L.lam2 + c, 0, l2);
-                Quad4<double>::ld(L.lam2 + co, 0, l2o);  // lower faces of the other half's slots
-                l2e = L.lam2[ce];
-            }
-            for (int e = 0; e < 4; ++e) {
-                // the couplings of couplings(): l, r, b, t, a, f
-                double w[6] = {wil, wih, wjl, wjh, wkl[e], wkh[e]};
-                if (VAR) {
-                    w[0] *= l0[e];
-                    w[1] *= l0p[e];
-                    w[2] *= l1[e];
-                    w[3] *= l1p[e];
-                    w[4] *= l2[e];
-                    w[5] *= h == 0 ? l2o[e] : (e < 3 ? l2o[e + 1] : l2e);
-                }
-                const double km = h == 0 ? (double)(e == 0 ? ze : zo[e - 1]) : (double)zo[e];
-                const double kp = h == 0 ? (double)zo[e] : (double)(e == 3 ? ze : zo[e + 1]);
-                const double zz = (double)zc[e];
-                const double sv = w[0] * (double)zim[e] + w[1] * (double)zip[e] + w[2] * (double)zjm[e] +
-                                  w[3] * (double)zjp[e] + w[4] * km + w[5] * kp;
-                const double d = w[0] + w[1] + w[2] + w[3] + w[4] + w[5];
-                pn[e] = beta != 0.0 ? zz + beta * pq[e] : zz;
-                qn[e] = beta != 0.0 ? (sv - d * zz) + beta * qq[e] : sv - d * zz;
-                a += (hij * hk[e]) * pn[e] * qn[e];
-            }
-            Quad4<double>::st(p + c, 0, pn);
-            Quad4<double>::st(q + c, 0, qn);
-        }
-    }
-    a = block_sum<kReduceThreads>(a, sh);
-    if (threadIdx.x == 0 && threadIdx.y == 0) partials[block_id()] = a;
-}
-
-__global__ void __launch_bounds__(kReduceThreads) k_fcg_update4(Bricks<double> B, const double* p, double* r,
-                                                                const double* q, float* pre32, double* pre64,
-                                                                double* partials, const SolveState* st,
-                                                                FirstPass fp) {
-    __shared__ double sh[kReduceThreads / 32];
-    const double alpha = st->alpha;
-    double a = 0.0;
-    BMG_QUAD_LOOP(B, {
-        double xq[4], pq[4], rq[4], qq[4], rn[4];
         Quad4<double>::ld(L.x + c, ks, xq);
-        Quad4<double>::ld(p + c, ks, pq);
         Quad4<double>::ld(r + c, ks, rq);
-        Quad4<double>::ld(q + c, ks, qq);
         for (int e = 0; e < 4; ++e) {
-            xq[e] = xq[e] + alpha * pq[e];
-            rn[e] = rq[e] - alpha * qq[e];
+            // on the first step p and q hold whatever the last solve left
+            const double pn = beta != 0.0 ? (double)zc[e] + beta * pq[e] : (double)zc[e];
+            const double qn = beta != 0.0 ? Az[e] + beta * qq[e] : Az[e];
+            pq[e] = pn;
+            qq[e] = qn;
+            xq[e] = xq[e] + alpha * pn;
+            rn[e] = rq[e] - alpha * qn;
             const double Vr = (hij * hk[e]) * rn[e];
             a += Vr * Vr;
         }
+        Quad4<double>::st(p + c, ks, pq);
+        Quad4<double>::st(q + c, ks, qq);
         Quad4<double>::st(L.x + c, ks, xq);
         if (quad_has_images(L, i, j, k0)) {
             for (int e = 0; e < 4; ++e) store_images(L, c + quad_off(ks, e), i, j, k0 + e, xq[e]);
@@ -465,19 +369,173 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_update4(Bricks<double> B
         if (pre32) {
             const float f[4] = {(float)rn[0], (float)rn[1], (float)rn[2], (float)rn[3]};
             Quad4<float>::st(pre32 + c, ks, f);
-            if (fp.z) {
-                float zq[4];
-                for (int e = 0; e < 4; ++e) zq[e] = first_pass_value(L, fp, i, j, k0 + e, f[e]);
-                Quad4<float>::st(fp.z + c, ks, zq);
-                if (quad_has_images(L, i, j, k0)) {
-                    for (int e = 0; e < 4; ++e) store_images_to(L, fp.z, c + quad_off(ks, e), i, j, k0 + e, zq[e]);
-                }
-            }
         }
         if (pre64) Quad4<double>::st(pre64 + c, ks, rn);
     })
     a = block_sum<kReduceThreads>(a, sh);
     if (threadIdx.x == 0 && threadIdx.y == 0) partials[block_id()] = a;
+}
+
+#undef BMG_QUAD_AZ
+
+// The two passes on a parity-split level 0 (one brick): the thread owns four
+// consecutive positions of one half of a row, the cells k = 2 (m0 + e) + h of
+// one parity (as k_fcg_direction_split), so z, its neighbours and the FP64
+// vectors load as whole vectors.
+#define BMG_SPLIT_AZ                                                                                   \
+    const int h = 4 * qx >= kh ? 1 : 0;                                                                 \
+    const int m0 = 4 * qx - h * kh;                                                                     \
+    const long row = row_at(L, i, j), c = row + 4 * qx;                                                 \
+    const long co = row + (1 - h) * kh + m0; /* the other half, same slots */                          \
+    const long ce = h == 0 ? (m0 > 0 ? co - 1 : row - 1) : (m0 + 4 < kh ? co + 4 : row + 2 * kh);       \
+    T zc[4], zo[4], zim[4], zip[4], zjm[4], zjp[4];                                                     \
+    Quad4<T>::ld(z + c, 0, zc);                                                                         \
+    Quad4<T>::ld(z + co, 0, zo);                                                                        \
+    Quad4<T>::ld(z + c - L.si, 0, zim);                                                                 \
+    Quad4<T>::ld(z + c + L.si, 0, zip);                                                                 \
+    Quad4<T>::ld(z + c - L.sj, 0, zjm);                                                                 \
+    Quad4<T>::ld(z + c + L.sj, 0, zjp);                                                                 \
+    const T ze = z[ce];                                                                                 \
+    const double wil = L.tab64[L.to.wl[0] + i], wih = L.tab64[L.to.wh[0] + i];                          \
+    const double hij = L.tab64[L.to.h[0] + i] * hj;                                                     \
+    double wkl[4], wkh[4], hk[4];                                                                      \
+    Quad4<double>::ld(L.tab64 + L.to.kwl + 4 * qx, 0, wkl);                                            \
+    Quad4<double>::ld(L.tab64 + L.to.kwh + 4 * qx, 0, wkh);                                            \
+    Quad4<double>::ld(L.tab64 + L.to.ksz + 4 * qx, 0, hk);                                             \
+    double l0[4], l0p[4], l1[4], l1p[4], l2[4], l2o[4], l2e = 1.0;                                      \
+    if (VAR) {                                                                                          \
+        Quad4<double>::ld(L.lam0 + c, 0, l0);                                                           \
+        Quad4<double>::ld(L.lam0 + c + L.si, 0, l0p);                                                   \
+        Quad4<double>::ld(L.lam1 + c, 0, l1);                                                           \
+        Quad4<double>::ld(L.lam1 + c + L.sj, 0, l1p);                                                   \
+        Quad4<double>::ld(L.lam2 + c, 0, l2);                                                           \
+        Quad4<double>::ld(L.lam2 + co, 0, l2o);                                                         \
+        l2e = L.lam2[ce];                                                                               \
+    }                                                                                                   \
+    double Az[4];                                                                                      \
+    for (int e = 0; e < 4; ++e) {                                                                       \
+        double w[6] = {wil, wih, wjl, wjh, wkl[e], wkh[e]};                                             \
+        if (VAR) {                                                                                      \
+            w[0] *= l0[e];                                                                              \
+            w[1] *= l0p[e];                                                                             \
+            w[2] *= l1[e];                                                                              \
+            w[3] *= l1p[e];                                                                             \
+            w[4] *= l2[e];                                                                              \
+            w[5] *= h == 0 ? l2o[e] : (e < 3 ? l2o[e + 1] : l2e);                                       \
+        }                                                                                               \
+        const double km = h == 0 ? (double)(e == 0 ? ze : zo[e - 1]) : (double)zo[e];                   \
+        const double kp = h == 0 ? (double)zo[e] : (double)(e == 3 ? ze : zo[e + 1]);                   \
+        const double sv = w[0] * (double)zim[e] + w[1] * (double)zip[e] + w[2] * (double)zjm[e] +        \
+                          w[3] * (double)zjp[e] + w[4] * km + w[5] * kp;                                \
+        const double d = w[0] + w[1] + w[2] + w[3] + w[4] + w[5];                                       \
+        Az[e] = sv - d * (double)zc[e];                                                                 \
+    }
+
+#define BMG_SPLIT_LOOP(...)                                                                            \
+    {                                                                                                   \
+        const LevelView<double>& L = B.v[0];                                                            \
+        const int qx = blockIdx.x * blockDim.x + threadIdx.x;                                           \
+        const int j = blockIdx.y * blockDim.y + threadIdx.y;                                            \
+        const int kh = L.kh;                                                                            \
+        if (j < L.n1 && 4 * qx < L.n2) {                                                                \
+            const double wjl = L.tab64[L.to.wl[1] + j], wjh = L.tab64[L.to.wh[1] + j];                  \
+            const double hj = L.tab64[L.to.h[1] + j];                                                   \
+            for (int i = blockIdx.z; i < L.n0; i += gridDim.z) {                                        \
+                BMG_SPLIT_AZ                                                                            \
+                __VA_ARGS__                                                                             \
+            }                                                                                           \
+        }                                                                                               \
+    }
+
+template <typename T, bool VAR>
+__global__ void __launch_bounds__(kReduceThreads, VAR ? 2 : 3) k_fcg_dots3_split(Bricks<double> B, const T* z,
+                                                                                  const double* r, const double* q,
+                                                                                  double* partials, long nblocks) {
+    __shared__ double sh[kReduceThreads / 32];
+    double a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    BMG_SPLIT_LOOP({
+        double rq[4], qq[4];
+        Quad4<double>::ld(r + c, 0, rq);
+        Quad4<double>::ld(q + c, 0, qq);
+        for (int e = 0; e < 4; ++e) {
+            const double Vz = (hij * hk[e]) * (double)zc[e];
+            a1 += Vz * rq[e];
+            a2 += Vz * qq[e];
+            a3 += Vz * Az[e];
+        }
+    })
+    a1 = block_sum<kReduceThreads>(a1, sh);
+    a2 = block_sum<kReduceThreads>(a2, sh);
+    a3 = block_sum<kReduceThreads>(a3, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        const long bid = block_id();
+        partials[bid] = a1;
+        partials[nblocks + bid] = a2;
+        partials[2 * nblocks + bid] = a3;
+    }
+}
+
+template <typename T, bool VAR>
+__global__ void __launch_bounds__(kReduceThreads, VAR ? 2 : 3) k_fcg_step_split(Bricks<double> B, const T* z,
+                                                                                 double* p, double* q, double* r,
+                                                                                 float* pre32, double* pre64,
+                                                                                 double* partials,
+                                                                                 const SolveState* st) {
+    __shared__ double sh[kReduceThreads / 32];
+    const double beta = st->beta, alpha = st->alpha;
+    double a = 0.0;
+    BMG_SPLIT_LOOP({
+        double pq[4], qq[4], xq[4], rq[4], rn[4];
+        Quad4<double>::ld(p + c, 0, pq);
+        Quad4<double>::ld(q + c, 0, qq);
+        Quad4<double>::ld(L.x + c, 0, xq);
+        Quad4<double>::ld(r + c, 0, rq);
+        for (int e = 0; e < 4; ++e) {
+            const double pn = beta != 0.0 ? (double)zc[e] + beta * pq[e] : (double)zc[e];
+            const double qn = beta != 0.0 ? Az[e] + beta * qq[e] : Az[e];
+            pq[e] = pn;
+            qq[e] = qn;
+            xq[e] = xq[e] + alpha * pn;
+            rn[e] = rq[e] - alpha * qn;
+            const double Vr = (hij * hk[e]) * rn[e];
+            a += Vr * Vr;
+        }
+        Quad4<double>::st(p + c, 0, pq);
+        Quad4<double>::st(q + c, 0, qq);
+        Quad4<double>::st(L.x + c, 0, xq);
+        if ((L.per0 && (i == 0 || i == L.n0 - 1)) || (L.per1 && (j == 0 || j == L.n1 - 1)) ||
+            (L.per2 && ((h == 0 && m0 == 0) || (h == 1 && m0 + 4 == kh)))) {
+            for (int e = 0; e < 4; ++e) store_images(L, c + e, i, j, 2 * (m0 + e) + h, xq[e]);
+        }
+        Quad4<double>::st(r + c, 0, rn);
+        if (pre32) {
+            const float f[4] = {(float)rn[0], (float)rn[1], (float)rn[2], (float)rn[3]};
+            Quad4<float>::st(pre32 + c, 0, f);
+        }
+        if (pre64) Quad4<double>::st(pre64 + c, 0, rn);
+    })
+    a = block_sum<kReduceThreads>(a, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0) partials[block_id()] = a;
+}
+
+#undef BMG_SPLIT_LOOP
+#undef BMG_SPLIT_AZ
+
+// beta, (p, V q) and alpha from the one reduction of pass 1
+__global__ void __launch_bounds__(kFinalThreads) k_fcg_coeffs(const double* partials, long nblocks, SolveState* st) {
+    __shared__ double sh[kFinalThreads / 32];
+    const double zr = sum_partials<kFinalThreads>(partials, nblocks, sh);
+    const double zq = sum_partials<kFinalThreads>(partials + nblocks, nblocks, sh);
+    const double zaz = sum_partials<kFinalThreads>(partials + 2 * nblocks, nblocks, sh);
+    if (threadIdx.x == 0) {
+        const double beta = st->first ? 0.0 : -zq / st->pq;
+        const double pq = st->first ? zaz : zaz + beta * zq;
+        st->gamma = zr;
+        st->beta = beta;
+        st->pq = pq;
+        st->alpha = zr / pq;
+        st->first = 0;
+    }
 }
 
 #undef BMG_QUAD_LOOP
@@ -503,68 +561,57 @@ long fcg_partials(const Bricks<double>& B) {
 
 template <bool VAR>
 void launch_fcg_residual(const Bricks<double>& B, const Walls& W, int mode, double* r, float* pre32, double* pre64,
-                         double* partials, FirstPass fp, cudaStream_t s) {
+                         double* partials, cudaStream_t s) {
     const dim3 blk = block_for(B.max2);
     k_fcg_residual<VAR><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, W, mode, r, pre32, pre64, partials,
-                                                                   reduce_blocks(B), fp);
-}
-
-template <typename T>
-void launch_fcg_beta(const Bricks<double>& B, const T* z, const double* r, const double* q, double* partials,
-                     SolveState* st, cudaStream_t s) {
-    const long nb = fcg_partials(B);
-    if (fcg_quads(B)) {
-        k_fcg_dots4<T><<<quad_grid(B), dim3(16, 16, 1), 0, s>>>(B, z, r, q, partials, nb);
-    } else {
-        const dim3 blk = block_for(B.max2);
-        k_fcg_dots<T><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, z, r, q, partials, nb);
-    }
-    k_fcg_beta<<<1, kFinalThreads, 0, s>>>(partials, nb, st);
+                                                                   reduce_blocks(B));
 }
 
 template <typename T, bool VAR>
-void launch_fcg_direction(const Bricks<double>& B, const T* z, double* p, double* q, double* partials,
-                          SolveState* st, cudaStream_t s) {
-    if (B.v[0].kh) {
-        k_fcg_direction_split<T, VAR><<<quad_grid(B), dim3(16, 16, 1), 0, s>>>(B, z, p, q, partials, st);
-    } else if (fcg_quads(B)) {
-        k_fcg_direction4<T, VAR><<<quad_grid(B), dim3(16, 16, 1), 0, s>>>(B, z, p, q, partials, st);
-    } else {
-        const dim3 blk = block_for(B.max2);
-        k_fcg_direction<T, VAR><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, z, p, q, partials, st);
-    }
-    k_fcg_alpha<<<1, kFinalThreads, 0, s>>>(partials, fcg_partials(B), st);
-}
-
-void launch_fcg_update(const Bricks<double>& B, const double* p, double* r, const double* q, float* pre32,
-                       double* pre64, double* partials, const SolveState* st, FirstPass fp, cudaStream_t s) {
+void launch_fcg_step(const Bricks<double>& B, const T* z, double* p, double* q, double* r, float* pre32,
+                     double* pre64, double* partials, SolveState* st, cudaStream_t s) {
+    const long nb = fcg_partials(B);
     if (fcg_quads(B)) {
-        k_fcg_update4<<<quad_grid(B), dim3(16, 16, 1), 0, s>>>(B, p, r, q, pre32, pre64, partials, st, fp);
+        // two passes and one reduction (k_fcg_coeffs)
+        const dim3 g = quad_grid(B), blk(16, 16, 1);
+        if (B.v[0].kh)
+            k_fcg_dots3_split<T, VAR><<<g, blk, 0, s>>>(B, z, r, q, partials, nb);
+        else
+            k_fcg_dots3_4<T, VAR><<<g, blk, 0, s>>>(B, z, r, q, partials, nb);
+        k_fcg_coeffs<<<1, kFinalThreads, 0, s>>>(partials, nb, st);
+        if (B.v[0].kh)
+            k_fcg_step_split<T, VAR><<<g, blk, 0, s>>>(B, z, p, q, r, pre32, pre64, partials, st);
+        else
+            k_fcg_step4<T, VAR><<<g, blk, 0, s>>>(B, z, p, q, r, pre32, pre64, partials, st);
         return;
     }
+    // rows of n2 % 4 != 0: one cell per thread, three passes
     const dim3 blk = block_for(B.max2);
-    k_fcg_update<<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, p, r, q, pre32, pre64, partials, st);
+    const dim3 g = grid_for(B, B.max2, blk);
+    k_fcg_dots<T><<<g, blk, 0, s>>>(B, z, r, q, partials, nb);
+    k_fcg_beta<<<1, kFinalThreads, 0, s>>>(partials, nb, st);
+    k_fcg_direction<T, VAR><<<g, blk, 0, s>>>(B, z, p, q, partials, st);
+    k_fcg_alpha<<<1, kFinalThreads, 0, s>>>(partials, nb, st);
+    k_fcg_update<<<g, blk, 0, s>>>(B, p, r, q, pre32, pre64, partials, st);
 }
+
+int fcg_step_launches(const Bricks<double>& B) { return fcg_quads(B) ? 3 : 5; }
 
 void launch_fcg_true_norm(const Bricks<double>& B, const double* partials, SolveState* st, cudaStream_t s) {
     k_fcg_true_norm<<<1, kFinalThreads, 0, s>>>(partials, reduce_blocks(B), st);
 }
 
-template void launch_fcg_residual<false>(const Bricks<double>&, const Walls&, int, double*, float*, double*, double*,
-                                         FirstPass, cudaStream_t);
-template void launch_fcg_residual<true>(const Bricks<double>&, const Walls&, int, double*, float*, double*, double*,
-                                        FirstPass, cudaStream_t);
-template void launch_fcg_beta<float>(const Bricks<double>&, const float*, const double*, const double*, double*,
-                                     SolveState*, cudaStream_t);
-template void launch_fcg_beta<double>(const Bricks<double>&, const double*, const double*, const double*,
-                                      double*, SolveState*, cudaStream_t);
-template void launch_fcg_direction<float, false>(const Bricks<double>&, const float*, double*, double*, double*,
-                                                 SolveState*, cudaStream_t);
-template void launch_fcg_direction<float, true>(const Bricks<double>&, const float*, double*, double*, double*,
-                                                SolveState*, cudaStream_t);
-template void launch_fcg_direction<double, false>(const Bricks<double>&, const double*, double*, double*,
-                                                  double*, SolveState*, cudaStream_t);
-template void launch_fcg_direction<double, true>(const Bricks<double>&, const double*, double*, double*,
-                                                 double*, SolveState*, cudaStream_t);
+template void launch_fcg_residual<false>(const Bricks<double>&, const Walls&, int, double*, float*, double*,
+                                         double*, cudaStream_t);
+template void launch_fcg_residual<true>(const Bricks<double>&, const Walls&, int, double*, float*, double*,
+                                        double*, cudaStream_t);
+#define BMG_INST(T, V)                                                                                         \
+    template void launch_fcg_step<T, V>(const Bricks<double>&, const T*, double*, double*, double*, float*, \
+                                        double*, double*, SolveState*, cudaStream_t);
+BMG_INST(float, false)
+BMG_INST(float, true)
+BMG_INST(double, false)
+BMG_INST(double, true)
+#undef BMG_INST
 
 }  // namespace bmg

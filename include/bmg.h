@@ -152,10 +152,10 @@ typedef struct bmg_options {
     int restrict_scheme;/* restrict (linear): BMG_RESTRICT_*                   */
     int prolong_scheme; /* prolong (linear): BMG_PROLONG_*                     */
     int row_layout;     /* rowLayout (split): BMG_ROWS_*, fixed at creation    */
-    int fuse_first;     /* fuseFirstPass (1): a mixed flexible-CG solve writes
-                           the first level-0 colour pass of each FP32 cycle
-                           with the cycle's right-hand side (constant
-                           coefficient, one brick); results bit-identical   */
+    int fuse_first;     /* fuseFirstPass (1): a mixed flexible-CG solve starts
+                           each FP32 cycle with a zero-start colour pass on
+                           a parity-split level 0 (no memset of z, no read
+                           of z); results bit-identical                      */
 } bmg_options;
 
 typedef struct bmg_report {

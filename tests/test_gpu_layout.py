@@ -178,10 +178,10 @@ def test_split_level_kernels_match_oracle(native, name, variable, precision):
 
 @pytest.mark.parametrize("case", ["channel", "cavity"])
 def test_first_pass_fusion_is_bit_identical(native, case):
-    """With fuseFirstPass on (the default) the flexible-CG kernels that write
-    each FP32 cycle's right-hand side also write that cycle's first level-0
-    colour pass (the cycle starts from z = 0); the solve is bit-identical to
-    the one that zeroes z and runs the pass."""
+    """With fuseFirstPass on (the default) each FP32 cycle of the flexible-CG
+    loop starts with a zero-start colour pass on the split level 0, which
+    reads no z and writes the whole level; the solve is bit-identical to the
+    one that zeroes z with a memset and runs the ordinary pass."""
     mesh, b, _ = workloads.CONFIGS[case](64)
     kw = dict(relTol=1e-10, precision="mixed", krylov="fcg")
     out = {}
@@ -194,4 +194,4 @@ def test_first_pass_fusion_is_bit_identical(native, case):
         out[f] = (x, rep.cycles, rep.kernel_launches)
         c.close()
     assert out["on"][1] == out["off"][1] and np.array_equal(out["on"][0], out["off"][0])
-    assert out["on"][2] < out["off"][2]  # one colour pass fewer per cycle
+    assert out["on"][2] == out["off"][2]  # the same kernels; the memset is gone
