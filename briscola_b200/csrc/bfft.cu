@@ -482,7 +482,11 @@ __global__ void __launch_bounds__(kTransformThreads, 3) k_transform(const double
             constexpr int SLOTS = TOTAL / 2;
 #pragma unroll 4
             for (int s = tid; s < SLOTS; s += NT) {
-                const int u = s >> LOGN, k = s & (N - 1);
+                // consecutive threads take consecutive points along k, or
+                // along the strided axes consecutive lines (adjacent in the
+                // staged tile there)
+                const int u = LF ? s & (LBC - 1) : s >> LOGN;
+                const int k = LF ? s >> (LOGLB - 1) : s & (N - 1);
                 const int ta = 2 * u, tb = 2 * u + 1;
                 double ar, ai, br, bi;
                 if constexpr (KIND == K_HC2R) {
