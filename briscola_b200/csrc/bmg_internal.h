@@ -35,6 +35,40 @@ namespace bmg {
 
 constexpr int kMaxBricks = 8;
 
+// ---- programmatic dependent launch (sm_90 and later) -------------------------
+// The solve's kernels follow one another on one stream, each reading what the
+// previous one wrote.  They are launched with programmatic stream
+// serialization, and every one of them begins with grid_dep_sync(): it waits
+// until the preceding grid has completed and its writes are visible
+// (griddepcontrol.wait), then lets the next grid be scheduled
+// (griddepcontrol.launch_dependents).  The next kernel's launch then
+// overlaps this one's execution instead of following its completion; its
+// CTAs take only the slots this grid leaves free and wait at their own
+// grid_dep_sync.  After a kernel launched without the attribute, or after a
+// memset or a copy, the wait returns at once.
+__device__ __forceinline__ void grid_dep_sync() {
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
+constexpr bool kProgrammaticLaunch = true;
+
+template <typename... KArgs, typename... Args>
+inline void launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                     Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = kProgrammaticLaunch ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kernel, static_cast<Args&&>(args)...);
+}
+
 // 1-D table offsets inside one level's coefficient table
 struct TabOff {
     int wl[3];   // coupling to the lower neighbour, per cell along the axis

@@ -39,6 +39,7 @@ struct Pair<double> {
 // ---------------------------------------------------------------------------
 template <typename T, bool VAR>
 __global__ void __launch_bounds__(256) k_colour_pass(Bricks<T> B, int colour) {
+    grid_dep_sync();
     using V2 = typename Pair<T>::type;
     int i;
     const LevelView<T>& L = B.v[brick_of(B, blockIdx.z, i)];
@@ -246,6 +247,7 @@ __device__ __forceinline__ void colour_quad_item(const LevelView<T>& L, int i, i
 
 template <typename T, bool VAR>
 __global__ void __launch_bounds__(256) k_colour_quad(Bricks<T> B, int colour) {
+    grid_dep_sync();
     int i;
     const LevelView<T>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -297,6 +299,7 @@ struct Vec16<double> {
 // arithmetic of a pass over a zeroed x).
 template <typename T, bool VAR, bool ZERO>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 && !VAR ? 5 : 1) k_colour_split(LevelView<T> L, int colour) {
+    grid_dep_sync();
     constexpr int NC = Vec16<T>::N;  // cells per thread
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -388,6 +391,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 && !VAR ? 5 : 1) k_colour_
 // Damped Jacobi (omega = 0.8, jacSmoother.C:15) into a temporary, then copy.
 template <typename T, bool VAR>
 __global__ void __launch_bounds__(256) k_jacobi(Bricks<T> B, T* tmp) {
+    grid_dep_sync();
     int i;
     const LevelView<T>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -404,6 +408,7 @@ __global__ void __launch_bounds__(256) k_jacobi(Bricks<T> B, T* tmp) {
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_copy_interior(Bricks<T> B, const T* src) {
+    grid_dep_sync();
     int i;
     const LevelView<T>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -422,6 +427,7 @@ __global__ void __launch_bounds__(256) k_copy_interior(Bricks<T> B, const T* src
 // ---------------------------------------------------------------------------
 template <typename T, bool VAR>
 __global__ void __launch_bounds__(256) k_residual_restrict(Bricks<T> FB, Bricks<T> CB, TransferSet ts) {
+    grid_dep_sync();
     int I;
     const int b = brick_of(CB, blockIdx.z, I);
     const LevelView<T>& C = CB.v[b];
@@ -468,6 +474,7 @@ __global__ void __launch_bounds__(256) k_residual_restrict(Bricks<T> FB, Bricks<
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(256) k_prolong_correct(Bricks<T> FB, Bricks<T> CB, TransferSet ts) {
+    grid_dep_sync();
     int i;
     const int b = brick_of(FB, blockIdx.z, i);
     const LevelView<T>& F = FB.v[b];
@@ -575,6 +582,7 @@ __device__ __forceinline__ void prolong_quad_item(const LevelView<T>& F, const L
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_prolong_quad(Bricks<T> FB, Bricks<T> CB, TransferSet ts) {
+    grid_dep_sync();
     int i;
     const int b = brick_of(FB, blockIdx.z, i);
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -656,6 +664,7 @@ __device__ __forceinline__ void restrict_quad_item(const LevelView<T>& F, const 
 
 template <typename T, bool VAR>
 __global__ void __launch_bounds__(256) k_restrict_quad(Bricks<T> FB, Bricks<T> CB, TransferSet ts) {
+    grid_dep_sync();
     int I;
     const int b = brick_of(CB, blockIdx.z, I);
     const int P = blockIdx.x * blockDim.x + threadIdx.x;
@@ -678,6 +687,7 @@ __global__ void __launch_bounds__(256) k_restrict_quad(Bricks<T> FB, Bricks<T> C
 template <typename T, bool VAR>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 && !VAR ? 3 : 2) k_restrict_split(Bricks<T> FB, Bricks<T> CB,
                                                                                    TransferSet ts) {
+    grid_dep_sync();
     const LevelView<T>& F = FB.v[0];
     const LevelView<T>& C = CB.v[0];
     const TransferTabs& t = ts.t[0];
@@ -800,6 +810,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 && !VAR ? 3 : 2) k_restric
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_prolong_split(Bricks<T> FB, Bricks<T> CB, TransferSet ts) {
+    grid_dep_sync();
     const LevelView<T>& F = FB.v[0];
     const LevelView<T>& C = CB.v[0];
     const TransferTabs& t = ts.t[0];
@@ -927,6 +938,7 @@ __device__ __forceinline__ void coarse_solve_block(const Bricks<T>& CB, const do
 template <typename T>
 __global__ void __launch_bounds__(256) k_coarse_solve(Bricks<T> CB, const double* __restrict__ ainv,
                                                       const int* __restrict__ cidx, int n) {
+    grid_dep_sync();
     extern __shared__ double sb[];
     const int nw = blockDim.x >> 5;
     coarse_solve_block<T>(CB, ainv, cidx, n, sb, blockIdx.x * nw, gridDim.x * nw);
@@ -943,6 +955,7 @@ __global__ void __launch_bounds__(256) k_coarse_solve(Bricks<T> CB, const double
 // ---------------------------------------------------------------------------
 template <typename T, bool VAR>
 __global__ void __launch_bounds__(kTailThreads) k_tail_cycle(TailPlan<T> P) {
+    grid_dep_sync();
     extern __shared__ double sb[];
     const int nt = blockDim.x;
     const int nl = P.nlev;
@@ -992,6 +1005,7 @@ __global__ void __launch_bounds__(kTailThreads) k_tail_cycle(TailPlan<T> P) {
 
 template <typename T>
 __global__ void k_fill_ghosts(T* x, const int* __restrict__ dst, const int* __restrict__ src, long n) {
+    grid_dep_sync();
     for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
         x[dst[q]] = x[src[q]];
 }
@@ -999,6 +1013,7 @@ __global__ void k_fill_ghosts(T* x, const int* __restrict__ dst, const int* __re
 // residual r = b - A x of any level, unscaled, into a compact array
 template <typename T, bool VAR>
 __global__ void __launch_bounds__(256) k_residual_out(Bricks<T> B, double* out) {
+    grid_dep_sync();
     int i;
     const LevelView<T>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1026,6 +1041,7 @@ __global__ void __launch_bounds__(256) k_residual_out(Bricks<T> B, double* out) 
 template <bool VAR>
 __global__ void __launch_bounds__(kReduceThreads) k_residual_norm(Bricks<double> B, Walls W, int mode,
                                                                   double* partials, long nblocks, float* b32) {
+    grid_dep_sync();
     __shared__ double sh[kReduceThreads / 32];
     int i;
     const int bk = brick_of(B, blockIdx.z, i);
@@ -1076,6 +1092,7 @@ __global__ void __launch_bounds__(kFinalThreads) k_finalize(const double* partia
                                                              SolveState* st, int mode,
                                                              cudaGraphConditionalHandle cond,
                                                              int setCondition) {
+    grid_dep_sync();
     __shared__ double sh[kFinalThreads / 32];
     const double a1 = sum_partials<kFinalThreads>(partials, nblocks, sh);
     double a2 = 0.0, a3 = 0.0;
@@ -1113,6 +1130,7 @@ __global__ void __launch_bounds__(kFinalThreads) k_finalize(const double* partia
 }
 
 __global__ void __launch_bounds__(kReduceThreads) k_mean_partials(Bricks<double> B, double* partials) {
+    grid_dep_sync();
     __shared__ double sh[kReduceThreads / 32];
     int i;
     const LevelView<double>& L = B.v[brick_of(B, blockIdx.z, i)];
@@ -1129,6 +1147,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_mean_partials(Bricks<double>
 
 __global__ void __launch_bounds__(kFinalThreads) k_mean_finalize(const double* partials, long nblocks,
                                                                  SolveState* st) {
+    grid_dep_sync();
     __shared__ double sh[kFinalThreads / 32];
     const double a = sum_partials<kFinalThreads>(partials, nblocks, sh);
     if (threadIdx.x == 0) st->mean = a / st->vol_total;
@@ -1136,6 +1155,7 @@ __global__ void __launch_bounds__(kFinalThreads) k_mean_finalize(const double* p
 
 // plain (unweighted) sum of the interior x per block, then the mean
 __global__ void __launch_bounds__(kReduceThreads) k_plain_partials(Bricks<double> B, double* partials) {
+    grid_dep_sync();
     __shared__ double sh[kReduceThreads / 32];
     int i;
     const LevelView<double>& L = B.v[brick_of(B, blockIdx.z, i)];
@@ -1149,6 +1169,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_plain_partials(Bricks<double
 
 __global__ void __launch_bounds__(kFinalThreads) k_plain_finalize(const double* partials, long nblocks,
                                                                   SolveState* st) {
+    grid_dep_sync();
     __shared__ double sh[kFinalThreads / 32];
     const double a = sum_partials<kFinalThreads>(partials, nblocks, sh);
     if (threadIdx.x == 0) st->ybar = a / st->ncells;
@@ -1157,12 +1178,14 @@ __global__ void __launch_bounds__(kFinalThreads) k_plain_finalize(const double* 
 // subtract the mean everywhere, ghosts included (a constant shift keeps the
 // periodic images consistent)
 __global__ void k_sub_mean(double* x, long n, const SolveState* st) {
+    grid_dep_sync();
     const double m = st->mean;
     for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
         x[q] -= m;
 }
 
 __global__ void __launch_bounds__(256) k_load_b(Bricks<double> B, Walls W, const double* compact) {
+    grid_dep_sync();
     int i;
     const int bk = brick_of(B, blockIdx.z, i);
     const LevelView<double>& L = B.v[bk];
@@ -1178,6 +1201,7 @@ __global__ void __launch_bounds__(256) k_load_b(Bricks<double> B, Walls W, const
 }
 
 __global__ void __launch_bounds__(256) k_load_x(Bricks<double> B, const double* compact) {
+    grid_dep_sync();
     int i;
     const LevelView<double>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1188,6 +1212,7 @@ __global__ void __launch_bounds__(256) k_load_x(Bricks<double> B, const double* 
 }
 
 __global__ void __launch_bounds__(256) k_store_x(Bricks<double> B, double* compact) {
+    grid_dep_sync();
     int i;
     const LevelView<double>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1199,6 +1224,7 @@ __global__ void __launch_bounds__(256) k_store_x(Bricks<double> B, double* compa
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_load_field(Bricks<T> B, int field, const double* compact, int unscale) {
+    grid_dep_sync();
     int i;
     const LevelView<T>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1216,6 +1242,7 @@ __global__ void __launch_bounds__(256) k_load_field(Bricks<T> B, int field, cons
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_store_field(Bricks<T> B, int field, double* compact, int unscale) {
+    grid_dep_sync();
     int i;
     const LevelView<T>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1232,6 +1259,7 @@ __global__ void __launch_bounds__(256) k_store_field(Bricks<T> B, int field, dou
 // + k, the level's own frame): b to the array, the array to x (with its
 // periodic images) -- the two ends of a level solver (bmg_set_level_solver).
 __global__ void __launch_bounds__(256) k_b_to_plain32(Bricks<float> B, float* out) {
+    grid_dep_sync();
     int i;
     const LevelView<float>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1241,6 +1269,7 @@ __global__ void __launch_bounds__(256) k_b_to_plain32(Bricks<float> B, float* ou
 }
 
 __global__ void __launch_bounds__(256) k_plain32_to_x(Bricks<float> B, const float* in) {
+    grid_dep_sync();
     int i;
     const LevelView<float>& L = B.v[brick_of(B, blockIdx.z, i)];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1250,6 +1279,7 @@ __global__ void __launch_bounds__(256) k_plain32_to_x(Bricks<float> B, const flo
 }
 
 __global__ void __launch_bounds__(256) k_add_correction(Bricks<double> B, Bricks<float> E) {
+    grid_dep_sync();
     int i;
     const int b = brick_of(B, blockIdx.z, i);
     const LevelView<double>& L = B.v[b];
@@ -1280,9 +1310,9 @@ void launch_colour_pass(const Bricks<T>& B, int colour, cudaStream_t s, bool zer
         const dim3 blk(bx, 256 / bx, 1);
         const dim3 grid((tr + bx - 1) / bx, (L.n1 + blk.y - 1) / blk.y, L.n0);
         if (zero)
-            k_colour_split<T, VAR, true><<<grid, blk, 0, s>>>(L, colour);
+            launch_k(k_colour_split<T, VAR, true>, grid, blk, 0, s, L, colour);
         else
-            k_colour_split<T, VAR, false><<<grid, blk, 0, s>>>(L, colour);
+            launch_k(k_colour_split<T, VAR, false>, grid, blk, 0, s, L, colour);
         return;
     }
     bool quads = true;
@@ -1292,19 +1322,19 @@ void launch_colour_pass(const Bricks<T>& B, int colour, cudaStream_t s, bool zer
         // on the 256^3 level and costs registers in FP64
         const int nq = B.max2 / 4;
         const dim3 blk = nq >= 32 ? dim3(32, 8, 1) : nq >= 8 ? dim3(8, 32, 1) : dim3(2, 128, 1);
-        k_colour_quad<T, VAR><<<grid_for(B, nq, blk), blk, 0, s>>>(B, colour);
+        launch_k(k_colour_quad<T, VAR>, grid_for(B, nq, blk), blk, 0, s, B, colour);
         return;
     }
     const int pairs = (B.max2 + 1) / 2;
     const dim3 blk = pairs >= 32 ? dim3(32, 8, 1) : pairs >= 8 ? dim3(8, 32, 1) : dim3(2, 128, 1);
-    k_colour_pass<T, VAR><<<grid_for(B, pairs, blk), blk, 0, s>>>(B, colour);
+    launch_k(k_colour_pass<T, VAR>, grid_for(B, pairs, blk), blk, 0, s, B, colour);
 }
 
 template <typename T, bool VAR>
 void launch_jacobi(const Bricks<T>& B, T* tmp, cudaStream_t s) {
     const dim3 blk = block_for(B.max2);
-    k_jacobi<T, VAR><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, tmp);
-    k_copy_interior<T><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, tmp);
+    launch_k(k_jacobi<T, VAR>, grid_for(B, B.max2, blk), blk, 0, s, B, tmp);
+    launch_k(k_copy_interior<T>, grid_for(B, B.max2, blk), blk, 0, s, B, tmp);
 }
 
 // factor-2 coarsening along every axis and n2 % 4 == 0 on the fine level
@@ -1328,17 +1358,17 @@ void launch_residual_restrict(const Bricks<T>& F, const Bricks<T>& C, const Tran
         const int groups = F.v[0].kh / 4;
         const dim3 blk = split_block(groups);
         const dim3 grid((groups + blk.x - 1) / blk.x, (C.v[0].n1 + blk.y - 1) / blk.y, C.v[0].n0);
-        k_restrict_split<T, VAR><<<grid, blk, 0, s>>>(F, C, t);
+        launch_k(k_restrict_split<T, VAR>, grid, blk, 0, s, F, C, t);
         return;
     }
     if (quad_transfers(F, t)) {
         const int np = C.max2 / 2;
         const dim3 blk = np >= 32 ? dim3(32, 8, 1) : np >= 8 ? dim3(8, 32, 1) : dim3(2, 128, 1);
-        k_restrict_quad<T, VAR><<<grid_for(C, np, blk), blk, 0, s>>>(F, C, t);
+        launch_k(k_restrict_quad<T, VAR>, grid_for(C, np, blk), blk, 0, s, F, C, t);
         return;
     }
     const dim3 blk = block_for(C.max2);
-    k_residual_restrict<T, VAR><<<grid_for(C, C.max2, blk), blk, 0, s>>>(F, C, t);
+    launch_k(k_residual_restrict<T, VAR>, grid_for(C, C.max2, blk), blk, 0, s, F, C, t);
 }
 
 template <typename T>
@@ -1347,114 +1377,114 @@ void launch_prolong_correct(const Bricks<T>& F, const Bricks<T>& C, const Transf
         const int groups = F.v[0].kh / 4;
         const dim3 blk = split_block(groups);
         const dim3 grid((groups + blk.x - 1) / blk.x, (F.v[0].n1 + blk.y - 1) / blk.y, F.v[0].n0);
-        k_prolong_split<T><<<grid, blk, 0, s>>>(F, C, t);
+        launch_k(k_prolong_split<T>, grid, blk, 0, s, F, C, t);
         return;
     }
     if (quad_transfers(F, t)) {
         const int nq = F.max2 / 4;
         const dim3 blk = nq >= 32 ? dim3(32, 8, 1) : nq >= 8 ? dim3(8, 32, 1) : dim3(2, 128, 1);
-        k_prolong_quad<T><<<grid_for(F, nq, blk), blk, 0, s>>>(F, C, t);
+        launch_k(k_prolong_quad<T>, grid_for(F, nq, blk), blk, 0, s, F, C, t);
         return;
     }
     const dim3 blk = block_for(F.max2);
-    k_prolong_correct<T><<<grid_for(F, F.max2, blk), blk, 0, s>>>(F, C, t);
+    launch_k(k_prolong_correct<T>, grid_for(F, F.max2, blk), blk, 0, s, F, C, t);
 }
 
 template <typename T>
 void launch_coarse_solve(const Bricks<T>& C, const double* ainv, const int* cidx, int n, cudaStream_t s) {
     const int grid = std::min((n + 7) / 8, 1184);  // 8 rows (warps) per CTA
-    k_coarse_solve<T><<<grid, 256, n * sizeof(double), s>>>(C, ainv, cidx, n);
+    launch_k(k_coarse_solve<T>, grid, 256, n * sizeof(double), s, C, ainv, cidx, n);
 }
 
 template <typename T, bool VAR>
 void launch_tail_cycle(const TailPlan<T>& P, cudaStream_t s) {
-    k_tail_cycle<T, VAR><<<1, kTailThreads, P.ncoarse * sizeof(double), s>>>(P);
+    launch_k(k_tail_cycle<T, VAR>, 1, kTailThreads, P.ncoarse * sizeof(double), s, P);
 }
 
 template <typename T>
 void launch_fill_ghosts(T* x, const int* dst, const int* src, long n, cudaStream_t s) {
     const int blocks = (int)std::min<long>((n + 255) / 256, 148L * 8);
-    k_fill_ghosts<T><<<blocks, 256, 0, s>>>(x, dst, src, n);
+    launch_k(k_fill_ghosts<T>, blocks, 256, 0, s, x, dst, src, n);
 }
 
 template <typename T, bool VAR>
 void launch_residual_out(const Bricks<T>& B, double* out, cudaStream_t s) {
     const dim3 blk = block_for(B.max2);
-    k_residual_out<T, VAR><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, out);
+    launch_k(k_residual_out<T, VAR>, grid_for(B, B.max2, blk), blk, 0, s, B, out);
 }
 
 template <bool VAR>
 void launch_residual_norm(const Bricks<double>& B, const Walls& W, int mode, double* partials, float* b32,
                           cudaStream_t s) {
     const dim3 blk = block_for(B.max2);
-    k_residual_norm<VAR><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, W, mode, partials, reduce_blocks(B), b32);
+    launch_k(k_residual_norm<VAR>, grid_for(B, B.max2, blk), blk, 0, s, B, W, mode, partials, reduce_blocks(B), b32);
 }
 
 void launch_finalize(const Bricks<double>& B, const double* partials, SolveState* st, int mode,
                      cudaGraphConditionalHandle cond, int setCondition, cudaStream_t s) {
-    k_finalize<<<1, kFinalThreads, 0, s>>>(partials, reduce_blocks(B), st, mode, cond, setCondition);
+    launch_k(k_finalize, 1, kFinalThreads, 0, s, partials, reduce_blocks(B), st, mode, cond, setCondition);
 }
 
 void launch_finalize_n(const double* partials, long n, SolveState* st, int mode, cudaGraphConditionalHandle cond,
                        int setCondition, cudaStream_t s) {
-    k_finalize<<<1, kFinalThreads, 0, s>>>(partials, n, st, mode, cond, setCondition);
+    launch_k(k_finalize, 1, kFinalThreads, 0, s, partials, n, st, mode, cond, setCondition);
 }
 
 void launch_mean(const Bricks<double>& B, double* partials, SolveState* st, cudaStream_t s) {
     const dim3 blk = block_for(B.max2);
-    k_mean_partials<<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, partials);
-    k_mean_finalize<<<1, kFinalThreads, 0, s>>>(partials, reduce_blocks(B), st);
+    launch_k(k_mean_partials, grid_for(B, B.max2, blk), blk, 0, s, B, partials);
+    launch_k(k_mean_finalize, 1, kFinalThreads, 0, s, partials, reduce_blocks(B), st);
     const long n = B.v[0].cells;
     const int blocks = (int)std::min<long>((n + 255) / 256, 148L * 16);
-    k_sub_mean<<<blocks, 256, 0, s>>>(B.v[0].x, n, st);
+    launch_k(k_sub_mean, blocks, 256, 0, s, B.v[0].x, n, st);
 }
 
 void launch_plain_mean(const Bricks<double>& B, double* partials, SolveState* st, cudaStream_t s) {
     const dim3 blk = block_for(B.max2);
-    k_plain_partials<<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, partials);
-    k_plain_finalize<<<1, kFinalThreads, 0, s>>>(partials, reduce_blocks(B), st);
+    launch_k(k_plain_partials, grid_for(B, B.max2, blk), blk, 0, s, B, partials);
+    launch_k(k_plain_finalize, 1, kFinalThreads, 0, s, partials, reduce_blocks(B), st);
 }
 
 void launch_load_b(const Bricks<double>& B, const Walls& W, const double* compact, cudaStream_t s) {
     const dim3 blk = block_for(B.max2);
-    k_load_b<<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, W, compact);
+    launch_k(k_load_b, grid_for(B, B.max2, blk), blk, 0, s, B, W, compact);
 }
 
 void launch_load_x(const Bricks<double>& B, const double* compact, cudaStream_t s) {
     const dim3 blk = block_for(B.max2);
-    k_load_x<<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, compact);
+    launch_k(k_load_x, grid_for(B, B.max2, blk), blk, 0, s, B, compact);
 }
 
 void launch_store_x(const Bricks<double>& B, double* compact, cudaStream_t s) {
     const dim3 blk = block_for(B.max2);
-    k_store_x<<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, compact);
+    launch_k(k_store_x, grid_for(B, B.max2, blk), blk, 0, s, B, compact);
 }
 
 template <typename T>
 void launch_load_field(const Bricks<T>& B, int field, const double* compact, int unscale, cudaStream_t s) {
     const dim3 blk = block_for(B.max2);
-    k_load_field<T><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, field, compact, unscale);
+    launch_k(k_load_field<T>, grid_for(B, B.max2, blk), blk, 0, s, B, field, compact, unscale);
 }
 
 template <typename T>
 void launch_store_field(const Bricks<T>& B, int field, double* compact, int unscale, cudaStream_t s) {
     const dim3 blk = block_for(B.max2);
-    k_store_field<T><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, field, compact, unscale);
+    launch_k(k_store_field<T>, grid_for(B, B.max2, blk), blk, 0, s, B, field, compact, unscale);
 }
 
 void launch_b_to_plain32(const Bricks<float>& B, float* out, cudaStream_t s) {
     const dim3 blk = block_for(B.max2);
-    k_b_to_plain32<<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, out);
+    launch_k(k_b_to_plain32, grid_for(B, B.max2, blk), blk, 0, s, B, out);
 }
 
 void launch_plain32_to_x(const Bricks<float>& B, const float* in, cudaStream_t s) {
     const dim3 blk = block_for(B.max2);
-    k_plain32_to_x<<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, in);
+    launch_k(k_plain32_to_x, grid_for(B, B.max2, blk), blk, 0, s, B, in);
 }
 
 void launch_add_correction(const Bricks<double>& B, const Bricks<float>& E, cudaStream_t s) {
     const dim3 blk = block_for(B.max2);
-    k_add_correction<<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, E);
+    launch_k(k_add_correction, grid_for(B, B.max2, blk), blk, 0, s, B, E);
 }
 
 // explicit instantiations

@@ -39,6 +39,7 @@ template <bool VAR>
 __global__ void __launch_bounds__(kReduceThreads) k_fcg_residual(Bricks<double> B, Walls W, int mode, double* r_out,
                                                                  float* pre32, double* pre64, double* partials,
                                                                  long nblocks) {
+    grid_dep_sync();
     __shared__ double sh[kReduceThreads / 32];
     int i;
     const int bk = brick_of(B, blockIdx.z, i);
@@ -88,6 +89,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_residual(Bricks<double> 
 template <typename T>
 __global__ void __launch_bounds__(kReduceThreads) k_fcg_dots(Bricks<double> B, const T* z, const double* r,
                                                              const double* q, double* partials, long nblocks) {
+    grid_dep_sync();
     __shared__ double sh[kReduceThreads / 32];
     int i;
     const LevelView<double>& L = B.v[brick_of(B, blockIdx.z, i)];
@@ -111,6 +113,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_dots(Bricks<double> B, c
 
 __global__ void __launch_bounds__(kFinalThreads) k_fcg_beta(const double* partials, long nblocks,
                                                             SolveState* st) {
+    grid_dep_sync();
     __shared__ double sh[kFinalThreads / 32];
     const double a1 = sum_partials<kFinalThreads>(partials, nblocks, sh);
     const double a2 = sum_partials<kFinalThreads>(partials + nblocks, nblocks, sh);
@@ -126,6 +129,7 @@ template <typename T, bool VAR>
 __global__ void __launch_bounds__(kReduceThreads) k_fcg_direction(Bricks<double> B, const T* z, double* p,
                                                                   double* q, double* partials,
                                                                   const SolveState* st) {
+    grid_dep_sync();
     __shared__ double sh[kReduceThreads / 32];
     int i;
     const LevelView<double>& L = B.v[brick_of(B, blockIdx.z, i)];
@@ -155,6 +159,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_direction(Bricks<double>
 
 __global__ void __launch_bounds__(kFinalThreads) k_fcg_alpha(const double* partials, long nblocks,
                                                              SolveState* st) {
+    grid_dep_sync();
     __shared__ double sh[kFinalThreads / 32];
     const double a = sum_partials<kFinalThreads>(partials, nblocks, sh);
     if (threadIdx.x == 0) {
@@ -167,6 +172,7 @@ __global__ void __launch_bounds__(kFinalThreads) k_fcg_alpha(const double* parti
 __global__ void __launch_bounds__(kReduceThreads) k_fcg_update(Bricks<double> B, const double* p, double* r,
                                                                const double* q, float* pre32, double* pre64,
                                                                double* partials, const SolveState* st) {
+    grid_dep_sync();
     __shared__ double sh[kReduceThreads / 32];
     int i;
     const LevelView<double>& L = B.v[brick_of(B, blockIdx.z, i)];
@@ -190,6 +196,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_update(Bricks<double> B,
 
 __global__ void __launch_bounds__(kFinalThreads) k_fcg_true_norm(const double* partials, long nblocks,
                                                                  SolveState* st) {
+    grid_dep_sync();
     __shared__ double sh[kFinalThreads / 32];
     const double a = sum_partials<kFinalThreads>(partials, nblocks, sh);
     if (threadIdx.x == 0) st->l2_true = sqrt(a);
@@ -309,6 +316,7 @@ struct Quad4<float> {
 template <typename T, bool VAR>
 __global__ void __launch_bounds__(kReduceThreads) k_fcg_dots3_4(Bricks<double> B, const T* z, const double* r,
                                                                 const double* q, double* partials, long nblocks) {
+    grid_dep_sync();
     __shared__ double sh[kReduceThreads / 32];
     double a1 = 0.0, a2 = 0.0, a3 = 0.0;
     BMG_QUAD_LOOP(B, {
@@ -338,6 +346,7 @@ template <typename T, bool VAR>
 __global__ void __launch_bounds__(kReduceThreads) k_fcg_step4(Bricks<double> B, const T* z, double* p, double* q,
                                                               double* r, float* pre32, double* pre64,
                                                               double* partials, const SolveState* st) {
+    grid_dep_sync();
     __shared__ double sh[kReduceThreads / 32];
     const double beta = st->beta, alpha = st->alpha;
     double a = 0.0;
@@ -451,6 +460,7 @@ template <typename T, bool VAR>
 __global__ void __launch_bounds__(kReduceThreads, VAR ? 2 : 3) k_fcg_dots3_split(Bricks<double> B, const T* z,
                                                                                   const double* r, const double* q,
                                                                                   double* partials, long nblocks) {
+    grid_dep_sync();
     __shared__ double sh[kReduceThreads / 32];
     double a1 = 0.0, a2 = 0.0, a3 = 0.0;
     BMG_SPLIT_LOOP({
@@ -481,6 +491,7 @@ __global__ void __launch_bounds__(kReduceThreads, VAR ? 2 : 3) k_fcg_step_split(
                                                                                  float* pre32, double* pre64,
                                                                                  double* partials,
                                                                                  const SolveState* st) {
+    grid_dep_sync();
     __shared__ double sh[kReduceThreads / 32];
     const double beta = st->beta, alpha = st->alpha;
     double a = 0.0;
@@ -523,6 +534,7 @@ __global__ void __launch_bounds__(kReduceThreads, VAR ? 2 : 3) k_fcg_step_split(
 
 // beta, (p, V q) and alpha from the one reduction of pass 1
 __global__ void __launch_bounds__(kFinalThreads) k_fcg_coeffs(const double* partials, long nblocks, SolveState* st) {
+    grid_dep_sync();
     __shared__ double sh[kFinalThreads / 32];
     const double zr = sum_partials<kFinalThreads>(partials, nblocks, sh);
     const double zq = sum_partials<kFinalThreads>(partials + nblocks, nblocks, sh);
@@ -563,7 +575,7 @@ template <bool VAR>
 void launch_fcg_residual(const Bricks<double>& B, const Walls& W, int mode, double* r, float* pre32, double* pre64,
                          double* partials, cudaStream_t s) {
     const dim3 blk = block_for(B.max2);
-    k_fcg_residual<VAR><<<grid_for(B, B.max2, blk), blk, 0, s>>>(B, W, mode, r, pre32, pre64, partials,
+    launch_k(k_fcg_residual<VAR>, grid_for(B, B.max2, blk), blk, 0, s, B, W, mode, r, pre32, pre64, partials,
                                                                    reduce_blocks(B));
 }
 
@@ -575,30 +587,30 @@ void launch_fcg_step(const Bricks<double>& B, const T* z, double* p, double* q, 
         // two passes and one reduction (k_fcg_coeffs)
         const dim3 g = quad_grid(B), blk(16, 16, 1);
         if (B.v[0].kh)
-            k_fcg_dots3_split<T, VAR><<<g, blk, 0, s>>>(B, z, r, q, partials, nb);
+            launch_k(k_fcg_dots3_split<T, VAR>, g, blk, 0, s, B, z, r, q, partials, nb);
         else
-            k_fcg_dots3_4<T, VAR><<<g, blk, 0, s>>>(B, z, r, q, partials, nb);
-        k_fcg_coeffs<<<1, kFinalThreads, 0, s>>>(partials, nb, st);
+            launch_k(k_fcg_dots3_4<T, VAR>, g, blk, 0, s, B, z, r, q, partials, nb);
+        launch_k(k_fcg_coeffs, 1, kFinalThreads, 0, s, partials, nb, st);
         if (B.v[0].kh)
-            k_fcg_step_split<T, VAR><<<g, blk, 0, s>>>(B, z, p, q, r, pre32, pre64, partials, st);
+            launch_k(k_fcg_step_split<T, VAR>, g, blk, 0, s, B, z, p, q, r, pre32, pre64, partials, st);
         else
-            k_fcg_step4<T, VAR><<<g, blk, 0, s>>>(B, z, p, q, r, pre32, pre64, partials, st);
+            launch_k(k_fcg_step4<T, VAR>, g, blk, 0, s, B, z, p, q, r, pre32, pre64, partials, st);
         return;
     }
     // rows of n2 % 4 != 0: one cell per thread, three passes
     const dim3 blk = block_for(B.max2);
     const dim3 g = grid_for(B, B.max2, blk);
-    k_fcg_dots<T><<<g, blk, 0, s>>>(B, z, r, q, partials, nb);
-    k_fcg_beta<<<1, kFinalThreads, 0, s>>>(partials, nb, st);
-    k_fcg_direction<T, VAR><<<g, blk, 0, s>>>(B, z, p, q, partials, st);
-    k_fcg_alpha<<<1, kFinalThreads, 0, s>>>(partials, nb, st);
-    k_fcg_update<<<g, blk, 0, s>>>(B, p, r, q, pre32, pre64, partials, st);
+    launch_k(k_fcg_dots<T>, g, blk, 0, s, B, z, r, q, partials, nb);
+    launch_k(k_fcg_beta, 1, kFinalThreads, 0, s, partials, nb, st);
+    launch_k(k_fcg_direction<T, VAR>, g, blk, 0, s, B, z, p, q, partials, st);
+    launch_k(k_fcg_alpha, 1, kFinalThreads, 0, s, partials, nb, st);
+    launch_k(k_fcg_update, g, blk, 0, s, B, p, r, q, pre32, pre64, partials, st);
 }
 
 int fcg_step_launches(const Bricks<double>& B) { return fcg_quads(B) ? 3 : 5; }
 
 void launch_fcg_true_norm(const Bricks<double>& B, const double* partials, SolveState* st, cudaStream_t s) {
-    k_fcg_true_norm<<<1, kFinalThreads, 0, s>>>(partials, reduce_blocks(B), st);
+    launch_k(k_fcg_true_norm, 1, kFinalThreads, 0, s, partials, reduce_blocks(B), st);
 }
 
 template void launch_fcg_residual<false>(const Bricks<double>&, const Walls&, int, double*, float*, double*,

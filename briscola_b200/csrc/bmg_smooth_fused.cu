@@ -158,6 +158,7 @@ __device__ __forceinline__ void cp_quad(T* smem, const T* gmem, bool valid) {
 template <typename T, bool VAR, int S, int KR, int C1>
 __global__ void __launch_bounds__(SweepShape<T, S, KR>::threads, SweepShape<T, S, KR>::min_ctas)
     k_sweep(LevelView<T> L, T* __restrict__ xout, FusedGeom g) {
+    grid_dep_sync();
     using F = SweepShape<T, S, KR>;
     constexpr int EQ = F::EQ, NT = F::NT, RH = F::RH, PH = F::PH, QP = F::QP, U = F::U, KP = F::KP,
                   NX = F::NX, NB = F::NB;
@@ -391,9 +392,9 @@ void launch_one(const LevelView<T>& L, T* xout, const FusedGeom& g, int c1, cuda
     const dim3 grid((g.nk + 4 * kQ - 1) / (4 * kQ), (g.na + KR - 1) / KR, (gg.nm + gg.ti - 1) / gg.ti);
     const dim3 blk(F::EQ, F::EA, 1);
     if (c1)
-        k_sweep<T, VAR, S, KR, 1><<<grid, blk, F::smem, s>>>(L, xout, gg);
+        launch_k(k_sweep<T, VAR, S, KR, 1>, grid, blk, F::smem, s, L, xout, gg);
     else
-        k_sweep<T, VAR, S, KR, 0><<<grid, blk, F::smem, s>>>(L, xout, gg);
+        launch_k(k_sweep<T, VAR, S, KR, 0>, grid, blk, F::smem, s, L, xout, gg);
 }
 
 template <typename T, bool VAR>
