@@ -1558,11 +1558,9 @@ void residualNorm(bmg_ctx* c, int mode, bool setCondition) {
     const Bricks<double> L = bricks<double>(c, 0);
     float* b32 = c->opt.precision == BMG_PRECISION_MIXED ? c->lv[0].b32 : nullptr;
     c->launches += 2;
-    if (c->variable)
-        launch_residual_norm<true>(L, walls(c), mode, c->partials, b32, c->stream);
-    else
-        launch_residual_norm<false>(L, walls(c), mode, c->partials, b32, c->stream);
-    launch_finalize(L, c->partials, c->st, mode, c->cond, setCondition ? 1 : 0, c->stream);
+    const long n = c->variable ? launch_residual_norm<true>(L, walls(c), mode, c->partials, b32, c->stream)
+                               : launch_residual_norm<false>(L, walls(c), mode, c->partials, b32, c->stream);
+    launch_finalize_n(c->partials, n, c->st, mode, c->cond, setCondition ? 1 : 0, c->stream);
 }
 
 SolveState initialState(const bmg_ctx* c) {
@@ -1683,11 +1681,12 @@ void segInitFcg(bmg_ctx* c, const double* bsrc, const double* xsrc, bool zero, b
     }
     float* pre32 = mixed ? c->lv[0].b32 : nullptr;
     double* pre64 = mixed ? nullptr : c->lv[0].b64;
+    long n;
     if (c->variable)
-        launch_fcg_residual<true>(V, walls(c), 0, c->fr, pre32, pre64, c->partials, s);
+        n = launch_fcg_residual<true>(V, walls(c), 0, c->fr, pre32, pre64, c->partials, s);
     else
-        launch_fcg_residual<false>(V, walls(c), 0, c->fr, pre32, pre64, c->partials, s);
-    launch_finalize(V, c->partials, c->st, 0, c->cond, setCondition ? 1 : 0, s);
+        n = launch_fcg_residual<false>(V, walls(c), 0, c->fr, pre32, pre64, c->partials, s);
+    launch_finalize_n(c->partials, n, c->st, 0, c->cond, setCondition ? 1 : 0, s);
     c->launches += 2;
 }
 
@@ -1732,11 +1731,12 @@ void segPostFcg(bmg_ctx* c, double* xdst) {
     cudaStream_t s = c->stream;
     const Bricks<double> V = fcgView(c);
     exchangeField<double>(c, 0, c->fx);
+    long n;
     if (c->variable)
-        launch_fcg_residual<true>(V, walls(c), 2, nullptr, nullptr, nullptr, c->partials, s);
+        n = launch_fcg_residual<true>(V, walls(c), 2, nullptr, nullptr, nullptr, c->partials, s);
     else
-        launch_fcg_residual<false>(V, walls(c), 2, nullptr, nullptr, nullptr, c->partials, s);
-    launch_fcg_true_norm(V, c->partials, c->st, s);
+        n = launch_fcg_residual<false>(V, walls(c), 2, nullptr, nullptr, nullptr, c->partials, s);
+    launch_fcg_true_norm(c->partials, n, c->st, s);
     c->launches += 2;
     if (c->opt.remove_mean && c->singular) {
         launch_mean(V, c->partials, c->st, s);

@@ -250,8 +250,9 @@ void launch_fill_ghosts(T* x, const int* dst, const int* src, long n, cudaStream
 // residual norms of level 0 in FP64.  mode 0: initial (also the norm-factor
 // sum and ||b||^2: three partial arrays), 1: current.  When b32 is given the scaled residual is also written
 // there in FP32 (the right-hand side of the next mixed-precision cycle).
+// Returns the number of per-block partials written (for launch_finalize_n).
 template <bool VAR>
-void launch_residual_norm(const Bricks<double>& B, const Walls& W, int mode, double* partials, float* b32,
+long launch_residual_norm(const Bricks<double>& B, const Walls& W, int mode, double* partials, float* b32,
                           cudaStream_t s);
 void launch_finalize(const Bricks<double>& B, const double* partials, SolveState* st, int mode,
                      cudaGraphConditionalHandle cond, int setCondition, cudaStream_t s);
@@ -267,8 +268,13 @@ void configure_fused_kernels();
 // r = b - A'x into r (and the cycle's right-hand side pre32 or pre64);
 // partials as launch_residual_norm.  mode 2: only ||V r||^2, nothing written.
 template <bool VAR>
-void launch_fcg_residual(const Bricks<double>& B, const Walls& W, int mode, double* r, float* pre32, double* pre64,
+long launch_fcg_residual(const Bricks<double>& B, const Walls& W, int mode, double* r, float* pre32, double* pre64,
                          double* partials, cudaStream_t s);
+// the same residual on a parity-split level 0 (four same-parity cells per
+// thread); returns the number of partials
+template <bool VAR>
+long launch_residual_split(const Bricks<double>& B, const Walls& W, int mode, double* r, float* pre32,
+                           double* pre64, double* partials, cudaStream_t s);
 // one FCG(1) step after the cycle z = M(r): beta, p = z + beta p,
 // q = A'z + beta q, alpha, x += alpha p (B.x, periodic write-through),
 // r -= alpha q, pre = r, and the partials of ||V r||^2 -- two passes and
@@ -284,7 +290,7 @@ long fcg_partials(const Bricks<double>& B);
 void launch_finalize_n(const double* partials, long n, SolveState* st, int mode, cudaGraphConditionalHandle cond,
                        int setCondition, cudaStream_t s);
 // st->l2_true from the partials of a mode-2 residual
-void launch_fcg_true_norm(const Bricks<double>& B, const double* partials, SolveState* st, cudaStream_t s);
+void launch_fcg_true_norm(const double* partials, long n, SolveState* st, cudaStream_t s);
 
 // ---- projection steps either side of the pressure solve (bmg_project.cu) ----
 struct ProjGeom {

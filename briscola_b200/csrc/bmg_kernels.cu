@@ -1051,11 +1051,11 @@ __global__ void __launch_bounds__(kReduceThreads) k_residual_norm(Bricks<double>
     double a1 = 0.0, a2 = 0.0, a3 = 0.0;
     if (j < L.n1 && k < L.n2) {
         const long row = row_at(L, i, j), c = row + kpos(L, k);
-        double w[6], s, d;
+        double w[6];
         const long ckm = row + kpos(L, k - 1), ckp = row + kpos(L, k + 1);
         couplings<double, VAR>(L, i, j, k, c, ckp, w);
-        stencil(L.x, c, ckm, ckp, L.si, L.sj, w, s, d);
-        const double r = L.b[c] + d * L.x[c] - s;
+        const double xn[6] = {L.x[c - L.si], L.x[c + L.si], L.x[c - L.sj], L.x[c + L.sj], L.x[ckm], L.x[ckp]};
+        const double r = res_value(w, xn, L.x[c], L.b[c]);
         const double V = L.tab64[L.to.h[0] + i] * L.tab64[L.to.h[1] + j] * L.tab64[L.to.h[2] + k];
         const double rr = V * r;
         a1 = rr * rr;
@@ -1414,10 +1414,12 @@ void launch_residual_out(const Bricks<T>& B, double* out, cudaStream_t s) {
 }
 
 template <bool VAR>
-void launch_residual_norm(const Bricks<double>& B, const Walls& W, int mode, double* partials, float* b32,
+long launch_residual_norm(const Bricks<double>& B, const Walls& W, int mode, double* partials, float* b32,
                           cudaStream_t s) {
+    if (B.v[0].kh) return launch_residual_split<VAR>(B, W, mode, nullptr, b32, nullptr, partials, s);
     const dim3 blk = block_for(B.max2);
     launch_k(k_residual_norm<VAR>, grid_for(B, B.max2, blk), blk, 0, s, B, W, mode, partials, reduce_blocks(B), b32);
+    return reduce_blocks(B);
 }
 
 void launch_finalize(const Bricks<double>& B, const double* partials, SolveState* st, int mode,
@@ -1511,8 +1513,8 @@ template void launch_tail_cycle<float, false>(const TailPlan<float>&, cudaStream
 template void launch_tail_cycle<float, true>(const TailPlan<float>&, cudaStream_t);
 template void launch_fill_ghosts<double>(double*, const int*, const int*, long, cudaStream_t);
 template void launch_fill_ghosts<float>(float*, const int*, const int*, long, cudaStream_t);
-template void launch_residual_norm<false>(const Bricks<double>&, const Walls&, int, double*, float*, cudaStream_t);
-template void launch_residual_norm<true>(const Bricks<double>&, const Walls&, int, double*, float*, cudaStream_t);
+template long launch_residual_norm<false>(const Bricks<double>&, const Walls&, int, double*, float*, cudaStream_t);
+template long launch_residual_norm<true>(const Bricks<double>&, const Walls&, int, double*, float*, cudaStream_t);
 template void launch_load_field<double>(const Bricks<double>&, int, const double*, int, cudaStream_t);
 template void launch_load_field<float>(const Bricks<float>&, int, const double*, int, cudaStream_t);
 template void launch_store_field<double>(const Bricks<double>&, int, double*, int, cudaStream_t);

@@ -49,11 +49,11 @@ __global__ void __launch_bounds__(kReduceThreads) k_fcg_residual(Bricks<double> 
     double a1 = 0.0, a2 = 0.0, a3 = 0.0;
     if (j < L.n1 && k < L.n2) {
         const long row = row_at(L, i, j), c = row + kpos(L, k);
-        double w[6], s, d;
+        double w[6];
         const long ckm = row + kpos(L, k - 1), ckp = row + kpos(L, k + 1);
         couplings<double, VAR>(L, i, j, k, c, ckp, w);
-        stencil(L.x, c, ckm, ckp, L.si, L.sj, w, s, d);
-        const double r = L.b[c] + d * L.x[c] - s;
+        const double xn[6] = {L.x[c - L.si], L.x[c + L.si], L.x[c - L.sj], L.x[c + L.sj], L.x[ckm], L.x[ckp]};
+        const double r = res_value(w, xn, L.x[c], L.b[c]);
         const double V = cell_volume(L, i, j, k);
         a1 = (V * r) * (V * r);
         if (mode == 0) {
@@ -532,6 +532,114 @@ __global__ void __launch_bounds__(kReduceThreads, VAR ? 2 : 3) k_fcg_step_split(
 #undef BMG_SPLIT_LOOP
 #undef BMG_SPLIT_AZ
 
+// The level-0 FP64 residual of k_residual_norm / k_fcg_residual on a
+// parity-split level (one brick): the thread owns four consecutive positions
+// of one half of a row, the cells k = 2 (m0 + e) + h of one parity (as
+// k_fcg_step_split), so x, its neighbours and b load as whole vectors.  Per
+// cell r = res_value(...), the arithmetic of the natural-order kernels; the
+// partials: ||V r||^2 and, for mode 0, the normFactor sums; r, pre32 and
+// pre64 written where given.
+template <bool VAR>
+__global__ void __launch_bounds__(kReduceThreads, 2) k_residual_split(Bricks<double> B, Walls W, int mode,
+                                                                                 double* r_out, float* pre32,
+                                                                                 double* pre64, double* partials,
+                                                                                 long nblocks) {
+    grid_dep_sync();
+    __shared__ double sh[kReduceThreads / 32];
+    double a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    const LevelView<double>& L = B.v[0];
+    const int qx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int kh = L.kh;
+    if (j < L.n1 && 4 * qx < L.n2) {
+        const double wjl = L.tab64[L.to.wl[1] + j], wjh = L.tab64[L.to.wh[1] + j];
+        const double hj = L.tab64[L.to.h[1] + j];
+        const int h = 4 * qx >= kh ? 1 : 0;
+        const int m0 = 4 * qx - h * kh;
+        double wkl[4], wkh[4], hk[4];
+        Quad4<double>::ld(L.tab64 + L.to.kwl + 4 * qx, 0, wkl);
+        Quad4<double>::ld(L.tab64 + L.to.kwh + 4 * qx, 0, wkh);
+        Quad4<double>::ld(L.tab64 + L.to.ksz + 4 * qx, 0, hk);
+        for (int i = blockIdx.z; i < L.n0; i += gridDim.z) {
+            const long row = row_at(L, i, j), c = row + 4 * qx;
+            const long co = row + (1 - h) * kh + m0;  // the other half, same slots
+            const long ce = h == 0 ? (m0 > 0 ? co - 1 : row - 1) : (m0 + 4 < kh ? co + 4 : row + 2 * kh);
+            double xc[4], xo[4], xim[4], xip[4], xjm[4], xjp[4], bq[4];
+            Quad4<double>::ld(L.x + c, 0, xc);
+            Quad4<double>::ld(L.x + co, 0, xo);
+            Quad4<double>::ld(L.x + c - L.si, 0, xim);
+            Quad4<double>::ld(L.x + c + L.si, 0, xip);
+            Quad4<double>::ld(L.x + c - L.sj, 0, xjm);
+            Quad4<double>::ld(L.x + c + L.sj, 0, xjp);
+            Quad4<double>::ld(L.b + c, 0, bq);
+            const double xe = L.x[ce];
+            const double wil = L.tab64[L.to.wl[0] + i], wih = L.tab64[L.to.wh[0] + i];
+            const double hij = L.tab64[L.to.h[0] + i] * hj;
+            double l0[4], l0p[4], l1[4], l1p[4], l2[4], l2o[4], l2e = 1.0;
+            if (VAR) {
+                Quad4<double>::ld(L.lam0 + c, 0, l0);
+                Quad4<double>::ld(L.lam0 + c + L.si, 0, l0p);
+                Quad4<double>::ld(L.lam1 + c, 0, l1);
+                Quad4<double>::ld(L.lam1 + c + L.sj, 0, l1p);
+                Quad4<double>::ld(L.lam2 + c, 0, l2);
+                Quad4<double>::ld(L.lam2 + co, 0, l2o);  // lower faces of the other half's slots
+                l2e = L.lam2[ce];
+            }
+            double rq[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                double w[6] = {wil, wih, wjl, wjh, wkl[e], wkh[e]};
+                if (VAR) {
+                    w[0] *= l0[e];
+                    w[1] *= l0p[e];
+                    w[2] *= l1[e];
+                    w[3] *= l1p[e];
+                    w[4] *= l2[e];
+                    w[5] *= h == 0 ? l2o[e] : (e < 3 ? l2o[e + 1] : l2e);
+                }
+                const double km = h == 0 ? (e == 0 ? xe : xo[e - 1]) : xo[e];
+                const double kp = h == 0 ? xo[e] : (e == 3 ? xe : xo[e + 1]);
+                const double xn[6] = {xim[e], xip[e], xjm[e], xjp[e], km, kp};
+                const double r = res_value(w, xn, xc[e], bq[e]);
+                rq[e] = r;
+                const double V = hij * hk[e];
+                const double rr = V * r;
+                a1 += rr * rr;
+                if (mode == 0) {
+                    const double bb = V * bq[e];
+                    double ay = 0.0;
+                    if (W.mask[0]) {  // A*mean(x): nonzero only in the rows of Dirichlet faces
+                        const int k = 2 * (m0 + e) + h;
+                        ay = -V * *W.ybar * wall_sum(L, W, 0, i, j, k, c + e, row + kpos(L, k + 1), false);
+                    }
+                    const double t = fabs(rr - bb + ay) + fabs(bb - ay);
+                    a2 += t * t;
+                    a3 += bb * bb;
+                }
+            }
+            if (r_out) Quad4<double>::st(r_out + c, 0, rq);
+            if (pre64) Quad4<double>::st(pre64 + c, 0, rq);
+            if (pre32) {
+                const float f[4] = {(float)rq[0], (float)rq[1], (float)rq[2], (float)rq[3]};
+                Quad4<float>::st(pre32 + c, 0, f);
+            }
+        }
+    }
+    const long bid = block_id();
+    a1 = block_sum<kReduceThreads>(a1, sh);
+    if (mode == 0) {
+        a2 = block_sum<kReduceThreads>(a2, sh);
+        a3 = block_sum<kReduceThreads>(a3, sh);
+    }
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        partials[bid] = a1;
+        if (mode == 0) {
+            partials[nblocks + bid] = a2;
+            partials[2 * nblocks + bid] = a3;
+        }
+    }
+}
+
 // beta, (p, V q) and alpha from the one reduction of pass 1
 __global__ void __launch_bounds__(kFinalThreads) k_fcg_coeffs(const double* partials, long nblocks, SolveState* st) {
     grid_dep_sync();
@@ -572,11 +680,21 @@ long fcg_partials(const Bricks<double>& B) {
 }
 
 template <bool VAR>
-void launch_fcg_residual(const Bricks<double>& B, const Walls& W, int mode, double* r, float* pre32, double* pre64,
+long launch_residual_split(const Bricks<double>& B, const Walls& W, int mode, double* r, float* pre32,
+                           double* pre64, double* partials, cudaStream_t s) {
+    const long nb = fcg_partials(B);
+    launch_k(k_residual_split<VAR>, quad_grid(B), dim3(16, 16, 1), 0, s, B, W, mode, r, pre32, pre64, partials, nb);
+    return nb;
+}
+
+template <bool VAR>
+long launch_fcg_residual(const Bricks<double>& B, const Walls& W, int mode, double* r, float* pre32, double* pre64,
                          double* partials, cudaStream_t s) {
+    if (B.v[0].kh) return launch_residual_split<VAR>(B, W, mode, r, pre32, pre64, partials, s);
     const dim3 blk = block_for(B.max2);
     launch_k(k_fcg_residual<VAR>, grid_for(B, B.max2, blk), blk, 0, s, B, W, mode, r, pre32, pre64, partials,
                                                                    reduce_blocks(B));
+    return reduce_blocks(B);
 }
 
 template <typename T, bool VAR>
@@ -609,14 +727,18 @@ void launch_fcg_step(const Bricks<double>& B, const T* z, double* p, double* q, 
 
 int fcg_step_launches(const Bricks<double>& B) { return fcg_quads(B) ? 3 : 5; }
 
-void launch_fcg_true_norm(const Bricks<double>& B, const double* partials, SolveState* st, cudaStream_t s) {
-    launch_k(k_fcg_true_norm, 1, kFinalThreads, 0, s, partials, reduce_blocks(B), st);
+void launch_fcg_true_norm(const double* partials, long n, SolveState* st, cudaStream_t s) {
+    launch_k(k_fcg_true_norm, 1, kFinalThreads, 0, s, partials, n, st);
 }
 
-template void launch_fcg_residual<false>(const Bricks<double>&, const Walls&, int, double*, float*, double*,
+template long launch_fcg_residual<false>(const Bricks<double>&, const Walls&, int, double*, float*, double*,
                                          double*, cudaStream_t);
-template void launch_fcg_residual<true>(const Bricks<double>&, const Walls&, int, double*, float*, double*,
+template long launch_fcg_residual<true>(const Bricks<double>&, const Walls&, int, double*, float*, double*,
                                         double*, cudaStream_t);
+template long launch_residual_split<false>(const Bricks<double>&, const Walls&, int, double*, float*, double*,
+                                           double*, cudaStream_t);
+template long launch_residual_split<true>(const Bricks<double>&, const Walls&, int, double*, float*, double*,
+                                          double*, cudaStream_t);
 #define BMG_INST(T, V)                                                                                         \
     template void launch_fcg_step<T, V>(const Bricks<double>&, const T*, double*, double*, double*, float*, \
                                         double*, double*, SolveState*, cudaStream_t);

@@ -81,6 +81,21 @@ __device__ __forceinline__ T gs_value(const T w[6], const T xn[6], T b) {
     return gs_div(rn_sub(s, b), d);
 }
 
+// the residual b + d x - s of one cell (s = sum of couplings times
+// neighbour values, d = sum of couplings), rounded step by step in a fixed
+// order, so the level-0 residual kernels give the same bits on natural and
+// parity-split rows
+__device__ __forceinline__ double res_value(const double w[6], const double xn[6], double xc, double b) {
+    double s = rn_mul(w[0], xn[0]);
+    s = rn_fma(w[1], xn[1], s);
+    s = rn_fma(w[2], xn[2], s);
+    s = rn_fma(w[3], xn[3], s);
+    s = rn_fma(w[4], xn[4], s);
+    s = rn_fma(w[5], xn[5], s);
+    const double d = rn_add(rn_add(rn_add(rn_add(rn_add(w[0], w[1]), w[2]), w[3]), w[4]), w[5]);
+    return rn_sub(rn_fma(d, xc, b), s);
+}
+
 // sum of couplings times neighbour values, and the sum of couplings; ckm
 // and ckp are the slab indices of the k neighbours
 template <typename T>
