@@ -1099,7 +1099,7 @@ void build(bmg_ctx* c, HostLevel&& L0) {
         // run (above the single-CTA coarse end's size) whose rows are whole
         // 16-cell blocks
         L.ks = c->opt.row_layout == BMG_ROWS_SPLIT && !c->multi && L.br[0].n[2] % 16 == 0 &&
-               L.ncell > kTailCells;
+               L.ncell > kSplitMinCells;
         buildTables(L);
         L.x64 = dalloc<double>(L.cells);
         L.b64 = dalloc<double>(L.cells);

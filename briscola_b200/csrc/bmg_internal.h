@@ -210,6 +210,7 @@ constexpr int kMaxTail = 6;
 constexpr int kMaxSeq = 16;
 constexpr int kTailThreads = 512;
 constexpr long kTailCells = 4096;  // levels this small run in the fused tail
+constexpr long kSplitMinCells = kTailCells;  // parity-split rows on single-brick levels above this
 
 template <typename T>
 struct TailPlan {
