@@ -72,6 +72,8 @@ struct Tri {
     int ns, cyclic;
     double shift;
     double s0;            // first diagonal entry of a pinned (singular) mode
+    int pin;              // the solve direction is N-N or periodic: the mode whose two
+                          // eigenvalues are zero is singular and pinned (tridiagonalSolver.C)
     const double* A;      // D_k = ((e - A_k) - B_k)
     const double* B;
     const double* DU;
@@ -669,7 +671,7 @@ __global__ void __launch_bounds__(kThreads) k_tridiag(double* __restrict__ w, do
     const long c1 = T.dir1_inner ? ci : co, c2 = T.dir1_inner ? co : ci;
     const double e1 = T.ev1[c1], e2 = T.ev2[c2];
     const double e = e1 + e2;
-    const bool singular = e1 == 0.0 && e2 == 0.0;
+    const bool singular = T.pin && e1 == 0.0 && e2 == 0.0;
     auto diag = [&](int k) {
         const double d = (k == 0 && singular) ? T.s0 : (e - T.A[k]) - T.B[k];
         return d - T.shift;
@@ -777,7 +779,7 @@ __global__ void k_tri_factor(Tri T) {
     const int c1 = T.dir1_inner ? ci : co, c2 = T.dir1_inner ? co : ci;
     const double e1 = T.ev1[c1], e2 = T.ev2[c2];
     const double e = e1 + e2;
-    const bool singular = e1 == 0.0 && e2 == 0.0;
+    const bool singular = T.pin && e1 == 0.0 && e2 == 0.0;
     auto diag = [&](int k) {
         const double d = (k == 0 && singular) ? T.s0 : (e - T.A[k]) - T.B[k];
         return d - T.shift;
@@ -1321,8 +1323,10 @@ void build(bfft_ctx* c, const bfft_desc* d) {
             s0 = -1.0 / (d3e0 * d30) - 2.0 / (d30 * d3w0);
             break;
     }
-    // a pinned mode exists only where both transform directions can have a
-    // zero eigenvalue; elsewhere s0 is never used
+    // a pinned mode exists only where the solve direction has no Dirichlet
+    // face (N-N or periodic) and both transform directions have a zero
+    // eigenvalue; with a Dirichlet face in the solve direction the mode of
+    // zero eigenvalues is an ordinary one
     auto ev = [&](int a) {
         std::vector<double> l = eigen(c->n[a], c->ax[a].pair);
         const double hh = h[a][0] * h[a][0];
@@ -1333,6 +1337,7 @@ void build(bfft_ctx* c, const bfft_desc* d) {
     T.ns = ns;
     T.cyclic = ps == P_CC;
     T.s0 = s0;
+    T.pin = ps == P_NN || ps == P_CC;
     T.A = upload(c, A);
     T.B = upload(c, B);
     T.DU = upload(c, DU);

@@ -45,6 +45,10 @@ def test_known_answer_mixed_faces(stretch):
     ((P, P, P, P, P, P), None),  # triply periodic: cyclic tridiagonal
     ((D, N, P, P, N, D), 0),
     ((N, D, D, N, P, P), None),  # uniform: N-D solve along x, D-N and periodic transforms
+    # zero-eigenvalue modes of the transforms that are not singular (a
+    # Dirichlet face in the solve direction): no pin
+    ((P, P, D, D, P, P), 1),     # channel with Dirichlet walls
+    ((N, N, D, N, N, N), 1),     # closed box with one Dirichlet wall, D-N solve
 ])
 def test_configurations_match_oracle(bc, stretch_axis):
     n = [16, 32, 8]
@@ -74,6 +78,31 @@ def test_thin_and_ragged_shapes(bc, n):
         pts[2] = geometric_points(7, 2.0)
     rng = np.random.default_rng(13)
     f = rng.standard_normal(n)
+    s = fft.FFTPoissonSolver(Brick(pts, bc))
+    x = s.solve(None, f)
+    ref = F.solve(f, pts, bc)
+    assert rel(x, ref) <= 1e-12
+
+
+@pytest.mark.parametrize("bc,n", [
+    ((D, D, N, N, P, P), (2, 16, 4)),  # sine pair of two lines, periodic of four
+    ((N, N, D, D, N, N), (4, 8, 2)),   # cosine transforms of four and two points
+    ((P, P, N, N, D, D), (2, 8, 2)),   # real FFT and sine of two points
+    ((N, N, N, N, D, D), (1, 8, 4)),   # a cosine transform of one point
+    ((D, D, N, N, N, N), (1, 8, 2)),   # a sine transform of one point
+])
+def test_tiny_transform_extents(bc, n):
+    """Transform axes of 1, 2 and 4 cells: the paired real FFTs and
+    Makhoul's cosine and sine transforms at their smallest lengths (no or
+    one Stockham pass), against the restatement; y is stretched, so it is
+    the solve direction."""
+    pts = [uniform_points(m) for m in n]
+    pts[1] = geometric_points(n[1], 2.0)
+    rng = np.random.default_rng(17)
+    f = rng.standard_normal(n)
+    if all(c in (N, P) for c in bc):
+        V = np.diff(pts[0])[:, None, None] * np.diff(pts[1])[None, :, None] * np.diff(pts[2])[None, None, :]
+        f -= (f * V).sum() / V.sum()
     s = fft.FFTPoissonSolver(Brick(pts, bc))
     x = s.solve(None, f)
     ref = F.solve(f, pts, bc)

@@ -59,6 +59,18 @@ def _dirichlet(N):
     return Mesh([br]), rng.standard_normal(N ** 3), None
 
 
+def _thin_rows(N=32):
+    """rows of 16 cells, the narrowest split rows: two threads a half row in
+    FP32, four in FP64; periodic x and z, stretched walls in y"""
+    br = Brick([uniform_points(N), geometric_points(N, 2.0), uniform_points(16)],
+               (PERIODIC, PERIODIC, NEUMANN, NEUMANN, PERIODIC, PERIODIC))
+    rng = np.random.default_rng(12)
+    V = br.cell_volumes()
+    f = rng.standard_normal(br.N)
+    f -= (V * f).sum() / V.sum()
+    return Mesh([br]), np.ascontiguousarray((-V * f).ravel()), None
+
+
 CASES = {
     "channel_fp64": (lambda: workloads.channel(64), dict(relTol=1e-10, precision="fp64")),
     "channel_mixed_fcg": (lambda: workloads.channel(64), dict(relTol=1e-10, precision="mixed", krylov="fcg")),
@@ -79,6 +91,9 @@ CASES = {
                                                          maxIter=12)),
     "no_graph": (lambda: workloads.channel(64), dict(relTol=1e-10, graph="off", precision="mixed",
                                                      krylov="fcg")),
+    "thin_rows_fp64": (_thin_rows, dict(relTol=1e-10, precision="fp64")),
+    "thin_rows_mixed": (_thin_rows, dict(relTol=1e-9, precision="mixed")),
+    "thin_rows_mixed_fcg": (_thin_rows, dict(relTol=1e-10, precision="mixed", krylov="fcg")),
 }
 
 
