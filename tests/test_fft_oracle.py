@@ -100,6 +100,30 @@ def test_homogeneous_faces_with_stretching(bc):
     assert np.abs(r).max() <= 1e-9
 
 
+@pytest.mark.parametrize("bc,n", [
+    ((P, P, D, D, P, P), (8, 16, 8)),   # channel with Dirichlet walls: periodic zero modes
+    ((N, N, D, N, N, N), (8, 16, 4)),   # D-N solve direction, cosine zero modes
+    ((N, N, D, D, N, N), (4, 8, 2)),    # D-D solve direction, tiny cosine transforms
+])
+def test_zero_transform_modes_are_regular_with_a_dirichlet_solve_direction(bc, n):
+    """The mode whose two transform eigenvalues are zero is pinned only when
+    the solve direction is N-N or periodic (tridiagonalSolver.C); with a
+    Dirichlet face there the system is regular and the solution is the
+    finite-volume system's, checked against a sparse direct solve of
+    Laplacian(x) = -f built independently (tests/helpers.py)."""
+    import scipy.sparse.linalg as spl
+
+    from tests.helpers import brick_operator
+
+    pts = [uniform_points(m) for m in n]
+    pts[1] = geometric_points(n[1], 2.0)
+    f = np.random.default_rng(3).standard_normal(n)
+    x = F.solve(f, pts, bc)
+    A, V, _ = brick_operator(pts, bc)
+    xd = spl.spsolve(A.tocsc(), -(V.reshape(n) * f).ravel())
+    assert np.linalg.norm(x.ravel() - xd) <= 1e-12 * np.linalg.norm(xd)
+
+
 def test_known_answer_ddt():
     """Test-FFTPoissonSolverDdt.C: all faces Dirichlet 0, uniform mesh,
     random b and old x; Laplacian(x) - x/dt + b + x_old/dt = 0 per cell."""
